@@ -1,0 +1,768 @@
+// ORACLE — test infrastructure only (see oracle_core.hpp).
+// Integrator::sample (src/pathtrace.rs:1878-2330), the progressive
+// accumulator and its band scheduler (:2526-2591), the resolve
+// (:2593-2734) with ToneMap / sRGB (src/hdr.rs:41-129), and the C entry
+// points the Python test harness calls through ctypes.
+#include <algorithm>
+#include <atomic>
+#include <thread>
+
+#include "oracle_scene.hpp"
+
+namespace oracle {
+
+struct Integrator {
+  const Scene *ts;
+  const EnvironmentMap *env;
+  pt_camera cam;
+  uint32_t width, height;
+  float ambient;
+  pt_path_trace_options pt;
+  float pixel_spread;
+  bool orthographic;
+  mutable uint64_t ext_rays = 0, shadow_rays = 0;
+
+  V3 cv(const float *a) const { return {a[0], a[1], a[2]}; }
+  // Camera::primary_ray, src/camera.rs:489-514.
+  void primary_ray(float px, float py, V3 &o, V3 &d) const {
+    float ndc_x = (px / fmaxr((float)width, 1.0f)) * 2.0f - 1.0f;
+    float ndc_y = 1.0f - (py / fmaxr((float)height, 1.0f)) * 2.0f;
+    V3 off = add(scale(cv(cam.side), ndc_x * cam.half_w), scale(cv(cam.up), ndc_y * cam.half_h));
+    if (cam.projection == PT_PERSPECTIVE) {
+      o = cv(cam.eye);
+      d = normalise(add(off, cv(cam.forward)));
+    } else {
+      o = add(cv(cam.eye), off);
+      d = cv(cam.forward);
+    }
+  }
+  V3 clamp(V3 c) const {
+    float m = max3(c);
+    if (pt.clamp > 0.0f && m > pt.clamp) return scale(c, pt.clamp / m);
+    return c;
+  }
+  float p_env() const {
+    if (env && !ts->emissive.empty()) return 0.5f;
+    if (env) return 1.0f;
+    return 0.0f;
+  }
+  // Integrator::accept, src/pathtrace.rs:1924-1934.
+  bool accept(const Hit &c, const Sampler &s, uint32_t ray, bool primary) const {
+    const pt_material &mat = ts->material_of(c);
+    if (primary && !c.front && !mat.double_sided) return false;
+    switch (mat.alpha_mode) {
+      case PT_ALPHA_MASK:
+        return ts->alpha(c) >= mat.alpha_cutoff;
+      case PT_ALPHA_BLEND:
+        return s.coin(ray, c.global) < ts->alpha(c);
+      default:
+        return true;
+    }
+  }
+  bool visible(V3 o, V3 d, float t_max, const Sampler &s, uint32_t ray, uint32_t skip) const {
+    shadow_rays++;
+    return !ts->occluded_filtered(o, d, 0.0f, t_max,
+                                  [&](const Hit &c) { return c.global != skip && accept(c, s, ray, false); });
+  }
+  // Integrator::emission, src/pathtrace.rs:1951-1966.
+  V3 emission(const Hit &hit) const {
+    const Item &item = ts->item_of(hit);
+    const pt_material &mat = ts->material_of(hit);
+    V3 e = cv(mat.emissive);
+    if (mat.unlit || is_black(e)) return {0, 0, 0};
+    V4 t;
+    if (ts->sample_binding(item, mat.emissive_texture, 3 * (size_t)hit.tri, hit.bary, TexLod{}, true, t))
+      e = mul(e, {t[0], t[1], t[2]});
+    return e;
+  }
+  // Integrator::tri_pdf, src/pathtrace.rs:1972-1991.
+  float tri_pdf(size_t li, uint32_t g, V3 p, V3 q) const {
+    V3 a, b, c;
+    ts->triangle_positions(g, a, b, c);
+    float sel = (1.0f - p_env()) * ts->emissive.pmf[li];
+    float omega = triangle_solid_angle(p, a, b, c);
+    if (omega >= MIN_SPHERICAL_SOLID_ANGLE) return sel / omega;
+    V3 cr = cross(sub(b, a), sub(c, a));
+    float len = std::sqrt(dot(cr, cr));
+    V3 to = sub(q, p);
+    float d2 = dot(to, to);
+    if (len <= 0.0f || d2 <= 0.0f) return 0.0f;
+    float cos = std::fabs(dot(cr, to) / (len * std::sqrt(d2)));
+    if (cos <= 0.0f) return 0.0f;
+    return sel * d2 / (0.5f * len * cos);
+  }
+  float light_pdf(const Hit &hit, V3 p, V3 q) const {
+    if (hit.global >= ts->emissive.lookup.size()) return 0.0f;
+    uint32_t li = ts->emissive.lookup[hit.global];
+    if (li == UINT32_MAX) return 0.0f;
+    return tri_pdf(li, hit.global, p, q);
+  }
+  static float power_heuristic(float a, float b) {
+    float a2 = a * a, b2 = b * b;
+    if (a2 + b2 > 0.0f && std::isfinite(a2 + b2)) return a2 / (a2 + b2);
+    if (std::isinf(a)) return 1.0f;
+    return 0.0f;
+  }
+  static V3 offset_ray_origin(V3 p, V3 n) {
+    const float ORIGIN = 1.0f / 32.0f, FLOAT_SCALE = 1.0f / 65536.0f, INT_SCALE = 256.0f;
+    V3 out;
+    for (int k = 0; k < 3; ++k) {
+      int32_t of_i = f2i32(INT_SCALE * n[k]);
+      int32_t bits;
+      std::memcpy(&bits, &p[k], 4);
+      int32_t moved = p[k] < 0.0f ? (int32_t)((uint32_t)bits - (uint32_t)of_i) : (int32_t)((uint32_t)bits + (uint32_t)of_i);
+      float p_i;
+      std::memcpy(&p_i, &moved, 4);
+      if (std::fabs(p[k]) < ORIGIN)
+        out[k] = p[k] + FLOAT_SCALE * n[k];
+      else if (std::isfinite(p_i))
+        out[k] = p_i;
+      else
+        out[k] = p[k];
+    }
+    return out;
+  }
+
+  // Integrator::sample, src/pathtrace.rs:2004-2329. Returns false when the
+  // sample is uncovered.
+  bool sample(uint32_t x, uint32_t y, uint32_t index, V3 &out) const {
+    Sampler s(pt.seed, x, y, index);
+    float p0[4];
+    s.pattern(0, p0);
+    V3 o, d;
+    primary_ray((float)x + p0[0], (float)y + p0[1], o, d);
+    V3 beta = {1, 1, 1}, radiance = {0, 0, 0};
+    float prev_pdf = 0.0f;
+    V3 prev_pos = {0, 0, 0};
+    bool has_medium = false;
+    V3 sigma = {0, 0, 0};
+    int hero = -1;
+    uint32_t strategy = pt.strategy;
+    uint32_t k = 0;
+    for (;;) {
+      uint32_t ray_id = k << 16;
+      Hit hit;
+      ext_rays++;
+      bool found = ts->closest_hit_filtered(o, d, 0.0f, INF, [&](const Hit &c) { return accept(c, s, ray_id, k == 0); },
+                                            hit);
+      if (has_medium) {
+        if (!found) break;
+        for (int c = 0; c < 3; ++c) beta[c] *= std::exp(-sigma[c] * hit.t);
+      }
+      if (!found) {
+        if (k == 0) return false;
+        V3 le;
+        float w;
+        if (env) {
+          le = env->radiance(d);
+          if (strategy == PT_MIS)
+            w = power_heuristic(prev_pdf, p_env() * env->pdf(d));
+          else if (strategy == PT_LIGHT_ONLY)
+            w = 0.0f;
+          else
+            w = 1.0f;
+        } else {
+          le = {ambient, ambient, ambient};
+          w = 1.0f;
+        }
+        if (w > 0.0f) radiance = add(radiance, clamp(scale(mul(beta, le), w)));
+        break;
+      }
+      Surface surf = ts->surface(hit);
+      const pt_material &pmat = ts->material_of(hit);
+      V3 pem = cv(pmat.emissive);
+      if ((hit.front || pmat.double_sided) && !pmat.unlit && !is_black(pem)) {
+        V3 le = emission(hit);
+        if (!is_black(le)) {
+          if (k == 0) {
+            radiance = add(radiance, mul(beta, le));
+          } else {
+            float pl = light_pdf(hit, prev_pos, surf.position);
+            float w;
+            if (pl <= 0.0f)
+              w = 1.0f;
+            else if (strategy == PT_MIS)
+              w = power_heuristic(prev_pdf, pl);
+            else if (strategy == PT_LIGHT_ONLY)
+              w = 0.0f;
+            else
+              w = 1.0f;
+            if (w > 0.0f) radiance = add(radiance, clamp(scale(mul(beta, le), w)));
+          }
+        }
+      }
+      TexLod lod;
+      if (k == 0) {
+        lod.kind = TexLodKind::Cone;
+        lod.width = orthographic ? pixel_spread : pixel_spread * hit.t;
+        lod.dir = d;
+      }
+      bool flip = !hit.front && pmat.double_sided;
+      MaterialSample mat = ts->material_oriented(hit, surf, lod, flip);
+      if (flip) {
+        mat.normal = neg(mat.normal);
+        mat.clearcoat_normal = neg(mat.clearcoat_normal);
+      }
+      if (mat.unlit) {
+        V3 c = {mat.base_color[0], mat.base_color[1], mat.base_color[2]};
+        V3 contrib = mul(beta, c);
+        radiance = add(radiance, k == 0 ? contrib : clamp(contrib));
+        break;
+      }
+      if (k >= pt.max_bounces) break;
+      if (mat.dispersion > 0.0f && mat.thickness > 0.0f && mat.transmission > 0.0f) {
+        int c;
+        if (hero >= 0) {
+          c = hero;
+        } else {
+          c = (int)std::min<uint64_t>(f2usize(s.coin(ray_id | 0x7fffu, UINT32_MAX) * 3.0f), 2);
+          for (int i = 0; i < 3; ++i) beta[i] = i == c ? beta[i] * 3.0f : 0.0f;
+          hero = c;
+        }
+        float iors[3];
+        dispersion_iors(mat.ior, mat.dispersion, iors);
+        mat.ior = iors[c];
+      }
+      V3 v = neg(d);
+      Bsdf bsdf(mat, v, surf.geometric_normal, hit.front);
+      if (bsdf.is_black()) break;
+      V3 p = surf.position;
+      V3 ng = bsdf.ng;
+      auto spawn = [&](V3 dir) { return dot(dir, ng) >= 0.0f ? offset_ray_origin(p, ng) : offset_ray_origin(p, neg(ng)); };
+
+      // NEE: punctual lights.
+      for (size_t j = 0; j < ts->lights.size(); ++j) {
+        LightSample ls;
+        if (!light_sample(ts->lights[j], p, ls)) continue;
+        V3 f;
+        float pdf_unused;
+        bsdf.eval(ls.l, f, pdf_unused);
+        if (is_black(f)) continue;
+        V3 o2 = spawn(ls.l);
+        float tmax = std::isfinite(ls.distance) ? ls.distance * (1.0f - 1.0e-4f) : INF;
+        if (visible(o2, ls.l, tmax, s, ray_id | 0x8000u | ((uint32_t)j & 0x7fffu), UINT32_MAX))
+          radiance = add(radiance, clamp(mul(mul(beta, f), ls.radiance)));
+      }
+
+      // NEE: area set.
+      float pl_u[4];
+      s.pattern(2 + 2 * k, pl_u);
+      if (strategy != PT_BSDF_ONLY && (env || !ts->emissive.empty())) {
+        float pe = p_env();
+        uint32_t shadow_id = ray_id | 0xffffu;
+        if (pl_u[2] < pe) {
+          V3 l, le;
+          float pdf;
+          if (env && env->sample(pl_u[0], pl_u[1], l, le, pdf)) {
+            float pl = pe * pdf;
+            V3 f;
+            float pb;
+            bsdf.eval(l, f, pb);
+            if (!is_black(f) && !is_black(le) && pl > 0.0f) {
+              float w = strategy == PT_MIS ? power_heuristic(pl, pb) : 1.0f;
+              if (visible(spawn(l), l, INF, s, shadow_id, UINT32_MAX))
+                radiance = add(radiance, clamp(scale(mul(mul(beta, f), le), w / pl)));
+            }
+          }
+        } else if (!ts->emissive.empty()) {
+          float us = pe > 0.0f ? clampr((pl_u[2] - pe) / (1.0f - pe), 0.0f, 0.999999f) : pl_u[2];
+          size_t li = ts->emissive.pick(us);
+          uint32_t g = ts->emissive.tris[li];
+          V3 a, b, c;
+          ts->triangle_positions(g, a, b, c);
+          bool have_target = false;
+          V3 q;
+          if (triangle_solid_angle(p, a, b, c) >= MIN_SPHERICAL_SOLID_ANGLE) {
+            V3 l;
+            if (sample_spherical_triangle(p, a, b, c, pl_u[0], pl_u[1], l)) {
+              V3 n = cross(sub(b, a), sub(c, a));
+              float dn = dot(l, n);
+              if (dn != 0.0f) {
+                float t = dot(sub(a, p), n) / dn;
+                if (t > 0.0f && std::isfinite(t)) {
+                  q = add(p, scale(l, t));
+                  have_target = true;
+                }
+              }
+            }
+          } else {
+            float su = std::sqrt(pl_u[0]);
+            float w[3] = {1.0f - su, su * (1.0f - pl_u[1]), su * pl_u[1]};
+            q = {a.x * w[0] + b.x * w[1] + c.x * w[2], a.y * w[0] + b.y * w[1] + c.y * w[2],
+                 a.z * w[0] + b.z * w[1] + c.z * w[2]};
+            have_target = true;
+          }
+          float bary[3];
+          bool have_bary = false;
+          if (have_target) {
+            // barycentric_of, src/trace.rs:1120-1133.
+            V3 e1 = sub(b, a), e2 = sub(c, a), r = sub(q, a);
+            float d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2);
+            float r1 = dot(r, e1), r2 = dot(r, e2);
+            float det = d11 * d22 - d12 * d12;
+            if (std::isfinite(det) && std::fabs(det) > FLT_MIN) {
+              float u = (d22 * r1 - d12 * r2) / det;
+              float vv = (d11 * r2 - d12 * r1) / det;
+              bary[0] = 1.0f - u - vv;
+              bary[1] = u;
+              bary[2] = vv;
+              have_bary = true;
+            }
+          }
+          if (have_target && have_bary) {
+            for (float &bb : bary) bb = clampr(bb, 0.0f, 1.0f);
+            V3 to = sub(q, p);
+            float dist2 = dot(to, to);
+            Hit lh = ts->make_hit(g, std::sqrt(dist2), bary, true);
+            Surface lsurf = ts->surface(lh);
+            const pt_material &lmat = ts->material_of(lh);
+            if (dist2 > 1.0e-12f) {
+              float dist = std::sqrt(dist2);
+              V3 l = scale(to, 1.0f / dist);
+              float cos_l = -dot(lsurf.geometric_normal, l);
+              float pl = tri_pdf(li, g, p, q);
+              if ((cos_l > 0.0f || (lmat.double_sided && cos_l < 0.0f)) && pl > 0.0f && std::isfinite(pl)) {
+                V3 f;
+                float pb;
+                bsdf.eval(l, f, pb);
+                V3 le = emission(lh);
+                if (!is_black(f) && !is_black(le)) {
+                  float w = strategy == PT_MIS ? power_heuristic(pl, pb) : 1.0f;
+                  V3 o2 = spawn(l);
+                  float tmax = fmaxr(dist * (1.0f - 1.0e-4f), 0.0f);
+                  if (visible(o2, l, tmax, s, shadow_id, g))
+                    radiance = add(radiance, clamp(scale(mul(mul(beta, f), le), w / pl)));
+                }
+              }
+            }
+          }
+        }
+      }
+
+      // BSDF sampling.
+      float pb_u[4];
+      s.pattern(1 + 2 * k, pb_u);
+      V3 l, f;
+      float pdf;
+      if (!bsdf.sample(pb_u, l, f, pdf)) break;
+      beta = mul(beta, scale(f, 1.0f / pdf));
+      if (!finite3(beta)) break;
+      prev_pdf = pdf;
+      prev_pos = p;
+      if (dot(l, ng) < 0.0f && mat.thickness > 0.0f && mat.transmission > 0.0f) {
+        if (hit.front) {
+          float dist = mat.attenuation_distance;
+          if (std::isfinite(dist)) {
+            V3 c = mat.attenuation_color;
+            sigma = {-std::log(fmaxr(c.x, 1.0e-6f)) / dist, -std::log(fmaxr(c.y, 1.0e-6f)) / dist,
+                     -std::log(fmaxr(c.z, 1.0e-6f)) / dist};
+            has_medium = true;
+          } else {
+            has_medium = false;
+          }
+        } else {
+          has_medium = false;
+        }
+      }
+      if (k + 1 >= pt.rr_start) {
+        float q = clampr(max3(beta), 0.05f, 1.0f);
+        if (q < 1.0f) {
+          if (pb_u[3] >= q) break;
+          beta = scale(beta, 1.0f / q);
+        }
+      }
+      o = spawn(l);
+      d = l;
+      k += 1;
+    }
+    out = finite3(radiance) ? radiance : V3{0, 0, 0};
+    return true;
+  }
+};
+
+static Integrator make_integrator(const Scene *sc, const EnvironmentMap *env, const pt_camera &cam,
+                                  const pt_render_options &o) {
+  Integrator it;
+  it.ts = sc;
+  it.env = env;
+  it.cam = cam;
+  it.width = std::max(o.width, 1u);
+  it.height = std::max(o.height, 1u);
+  it.ambient = std::isfinite(o.ambient) ? fmaxr(o.ambient, 0.0f) : 0.0f;
+  it.pt = o.path_trace;
+  it.orthographic = cam.projection == PT_ORTHOGRAPHIC;
+  it.pixel_spread = 2.0f * cam.half_h / (float)it.height;
+  return it;
+}
+
+// ---- resolve (src/hdr.rs:41-129, src/pathtrace.rs:2593-2734) ----------------
+static float srgb_to_linear_f(float c) {
+  if (c <= 0.04045f) return c / 12.92f;
+  return std::pow((c + 0.055f) / 1.055f, 2.4f);
+}
+static float sanitize(float v) { return std::isnan(v) ? 0.0f : v; }
+static float aces(float x) {
+  x = x * 0.6f;
+  float v = (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+  return clampr(v, 0.0f, 1.0f);
+}
+static V3 tone_apply(uint32_t tm, V3 rgb) {
+  rgb = {fmaxr(sanitize(rgb.x), 0.0f), fmaxr(sanitize(rgb.y), 0.0f), fmaxr(sanitize(rgb.z), 0.0f)};
+  if (tm == PT_TONE_REINHARD) {
+    float l = 0.2126f * rgb.x + 0.7152f * rgb.y + 0.0722f * rgb.z;
+    if (l <= 0.0f) return {0, 0, 0};
+    float s = 1.0f / (1.0f + l);
+    return {fminr(rgb.x * s, 1.0f), fminr(rgb.y * s, 1.0f), fminr(rgb.z * s, 1.0f)};
+  }
+  if (tm == PT_TONE_ACES) return {aces(rgb.x), aces(rgb.y), aces(rgb.z)};
+  return {fminr(rgb.x, 1.0f), fminr(rgb.y, 1.0f), fminr(rgb.z, 1.0f)};
+}
+static uint8_t linear_to_srgb_byte(float c) {
+  static float t[255];
+  static bool init = [] {
+    for (int k = 0; k < 255; ++k) t[k] = srgb_to_linear_f(((float)k + 0.5f) / 255.0f);
+    return true;
+  }();
+  (void)init;
+  if (std::isnan(c)) return 0;
+  return (uint8_t)(std::upper_bound(t, t + 255, c) - t);
+}
+static void bg_linear(const pt_render_options &o, float bg[4]) {
+  for (int k = 0; k < 3; ++k) bg[k] = srgb_to_linear_f((float)o.background[k] / 255.0f);
+  bg[3] = (float)o.background[3] / 255.0f;
+}
+static void mix(const float m[3], float f, const float bg[4], float out[4]) {
+  float a_sum = f + (1.0f - f) * bg[3];
+  if (a_sum > 0.0f) {
+    for (int k = 0; k < 3; ++k) out[k] = (f * m[k] + (1.0f - f) * bg[k] * bg[3]) / a_sum;
+    out[3] = a_sum;
+  } else {
+    for (int k = 0; k < 3; ++k) out[k] = f * m[k] + (1.0f - f) * bg[k];
+    out[3] = 0.0f;
+  }
+}
+static bool resolve_pixel(const double *a, uint32_t samples, const float bg[4], bool tone, const pt_render_options &o,
+                          float out[4]) {
+  if (a[3] <= 0.0 || samples == 0) return false;
+  float m[3] = {(float)(a[0] / a[3]), (float)(a[1] / a[3]), (float)(a[2] / a[3])};
+  float f = (float)clampd(a[3] / (double)samples, 0.0, 1.0);
+  V3 c = {m[0], m[1], m[2]};
+  if (tone) c = tone_apply(o.tone_map, scale(c, o.exposure));
+  float cm[3] = {c.x, c.y, c.z};
+  if (f >= 1.0f) {
+    out[0] = c.x;
+    out[1] = c.y;
+    out[2] = c.z;
+    out[3] = 1.0f;
+  } else {
+    mix(cm, f, bg, out);
+  }
+  return true;
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+
+extern "C" {
+
+void *oracle_scene_create(const pt_scene_desc *desc) {
+  try {
+    return new Scene(*desc);
+  } catch (...) {
+    return nullptr;
+  }
+}
+void oracle_scene_destroy(void *s) { delete (Scene *)s; }
+uint64_t oracle_scene_triangles(const void *s) { return ((const Scene *)s)->triangle_count(); }
+void *oracle_env_create(const pt_environment *env) { return new EnvironmentMap(*env); }
+void oracle_env_destroy(void *e) { delete (EnvironmentMap *)e; }
+
+// PathTracer::refine over a caller-owned f64 accumulator (width*height*4):
+// threads pull 4-row bands, each pixel runs samples first..first+n in order.
+int oracle_refine(const void *scene, const void *env, const pt_camera *cam, const pt_render_options *opts,
+                  uint32_t first, uint32_t samples, int threads, double *accum, uint64_t *ray_counts) {
+  const Scene *sc = (const Scene *)scene;
+  Integrator base = make_integrator(sc, (const EnvironmentMap *)env, *cam, *opts);
+  uint32_t w = base.width, h = base.height;
+  const uint32_t BAND_ROWS = 4;
+  uint32_t bands = (h + BAND_ROWS - 1) / BAND_ROWS;
+  std::atomic<uint32_t> next{0};
+  std::atomic<uint64_t> ext{0}, sh{0};
+  int nthreads = std::max(1, std::min<int>(threads > 0 ? threads : (int)std::thread::hardware_concurrency(),
+                                           (int)(h / BAND_ROWS + 1)));
+  auto work = [&]() {
+    Integrator it = base;
+    for (;;) {
+      uint32_t band = next.fetch_add(1);
+      if (band >= bands) break;
+      for (uint32_t y = band * BAND_ROWS; y < std::min(h, (band + 1) * BAND_ROWS); ++y)
+        for (uint32_t x = 0; x < w; ++x) {
+          double *px = accum + ((size_t)y * w + x) * 4;
+          for (uint32_t si = 0; si < samples; ++si) {
+            V3 c;
+            if (it.sample(x, y, first + si, c)) {
+              px[0] += (double)c.x;
+              px[1] += (double)c.y;
+              px[2] += (double)c.z;
+              px[3] += 1.0;
+            }
+          }
+        }
+    }
+    ext += it.ext_rays;
+    sh += it.shadow_rays;
+  };
+  if (nthreads <= 1) {
+    work();
+  } else {
+    std::vector<std::thread> pool;
+    for (int i = 0; i < nthreads; ++i) pool.emplace_back(work);
+    for (auto &t : pool) t.join();
+  }
+  if (ray_counts) {
+    ray_counts[0] = ext.load();
+    ray_counts[1] = sh.load();
+  }
+  return 0;
+}
+
+// One sample of one pixel (radiance, covered flag); for per-sample checks.
+int oracle_sample(const void *scene, const void *env, const pt_camera *cam, const pt_render_options *opts, uint32_t x,
+                  uint32_t y, uint32_t index, float out_rgb[3]) {
+  Integrator it = make_integrator((const Scene *)scene, (const EnvironmentMap *)env, *cam, *opts);
+  V3 c;
+  bool cov = it.sample(x, y, index, c);
+  out_rgb[0] = c.x;
+  out_rgb[1] = c.y;
+  out_rgb[2] = c.z;
+  return cov ? 1 : 0;
+}
+
+void oracle_resolve_hdr(const double *accum, uint32_t samples, const pt_render_options *o, float *out) {
+  float bg[4];
+  bg_linear(*o, bg);
+  size_t n = (size_t)std::max(o->width, 1u) * std::max(o->height, 1u);
+  for (size_t i = 0; i < n; ++i) {
+    float px[4];
+    if (!resolve_pixel(accum + 4 * i, samples, bg, false, *o, px)) std::memcpy(px, bg, sizeof px);
+    std::memcpy(out + 4 * i, px, sizeof px);
+  }
+}
+
+void oracle_resolve_image(const double *accum, uint32_t samples, const pt_render_options *o, uint8_t *out) {
+  float bg[4];
+  bg_linear(*o, bg);
+  size_t n = (size_t)std::max(o->width, 1u) * std::max(o->height, 1u);
+  for (size_t i = 0; i < n; ++i) {
+    float c[4];
+    if (!resolve_pixel(accum + 4 * i, samples, bg, true, *o, c)) {
+      std::memcpy(out + 4 * i, o->background, 4);
+      continue;
+    }
+    for (int k = 0; k < 3; ++k) out[4 * i + k] = linear_to_srgb_byte(c[k]);
+    out[4 * i + 3] = (uint8_t)f2usize(std::round(clampr(c[3], 0.0f, 1.0f) * 255.0f));
+  }
+}
+
+// Primary (k = 0) closest hit of sample `index` for every pixel, with the
+// camera-ray acceptance filter. global = UINT32_MAX on a miss.
+void oracle_primary_hits(const void *scene, const pt_camera *cam, const pt_render_options *opts, uint32_t index,
+                         uint32_t *out_global, float *out_t, float *out_bary) {
+  Integrator it = make_integrator((const Scene *)scene, nullptr, *cam, *opts);
+  for (uint32_t y = 0; y < it.height; ++y)
+    for (uint32_t x = 0; x < it.width; ++x) {
+      Sampler s(it.pt.seed, x, y, index);
+      float p0[4];
+      s.pattern(0, p0);
+      V3 o, d;
+      it.primary_ray((float)x + p0[0], (float)y + p0[1], o, d);
+      Hit h;
+      size_t i = (size_t)y * it.width + x;
+      if (it.ts->closest_hit_filtered(o, d, 0.0f, INF, [&](const Hit &c) { return it.accept(c, s, 0, true); }, h)) {
+        out_global[i] = h.global;
+        out_t[i] = h.t;
+        if (out_bary)
+          for (int k = 0; k < 3; ++k) out_bary[3 * i + k] = h.bary[k];
+      } else {
+        out_global[i] = UINT32_MAX;
+        out_t[i] = INF;
+      }
+    }
+}
+
+// Unfiltered closest hit / occlusion (TraceScene::closest_hit, ::occluded).
+int oracle_closest_hit(const void *scene, const float o[3], const float d[3], float t_min, float t_max,
+                       uint32_t *global, float *t, float bary[3], int *front) {
+  const Scene *sc = (const Scene *)scene;
+  Hit h;
+  if (!sc->closest_hit_filtered({o[0], o[1], o[2]}, {d[0], d[1], d[2]}, t_min, t_max, [](const Hit &) { return true; },
+                                h))
+    return 0;
+  *global = h.global;
+  *t = h.t;
+  for (int k = 0; k < 3; ++k) bary[k] = h.bary[k];
+  *front = h.front ? 1 : 0;
+  return 1;
+}
+int oracle_occluded(const void *scene, const float o[3], const float d[3], float t_min, float t_max) {
+  const Scene *sc = (const Scene *)scene;
+  return sc->occluded_filtered({o[0], o[1], o[2]}, {d[0], d[1], d[2]}, t_min, t_max, [](const Hit &) { return true; })
+             ? 1
+             : 0;
+}
+void oracle_surface(const void *scene, uint32_t global, const float bary[3], float out_pos[3], float out_ng[3],
+                    float out_sn[3]) {
+  const Scene *sc = (const Scene *)scene;
+  float b[3] = {bary[0], bary[1], bary[2]};
+  Hit h = sc->make_hit(global, 0.0f, b, true);
+  Surface s = sc->surface(h);
+  for (int k = 0; k < 3; ++k) {
+    out_pos[k] = s.position[k];
+    out_ng[k] = s.geometric_normal[k];
+    out_sn[k] = s.shading_normal[k];
+  }
+}
+// Material base colour / metallic / roughness at a hit (TexLod::Base).
+void oracle_material_base(const void *scene, uint32_t global, const float bary[3], float out[6]) {
+  const Scene *sc = (const Scene *)scene;
+  float b[3] = {bary[0], bary[1], bary[2]};
+  Hit h = sc->make_hit(global, 0.0f, b, true);
+  Surface s = sc->surface(h);
+  MaterialSample m = sc->material_oriented(h, s, TexLod{}, false);
+  for (int k = 0; k < 4; ++k) out[k] = m.base_color[k];
+  out[4] = m.metallic;
+  out[5] = m.roughness;
+}
+void oracle_emissive_table(const void *scene, uint32_t *count, const uint32_t **tris, const float **pmf,
+                           const float **cdf) {
+  const Scene *sc = (const Scene *)scene;
+  *count = (uint32_t)sc->emissive.tris.size();
+  *tris = sc->emissive.tris.data();
+  *pmf = sc->emissive.pmf.data();
+  *cdf = sc->emissive.cdf.data();
+}
+
+void oracle_sobol_owen_4d(uint32_t index, uint32_t seed, float out[4]) { sobol_owen_4d(index, seed, out); }
+uint32_t oracle_sobol(uint32_t index, uint32_t dim) { return sobol(index, (int)dim); }
+void oracle_sampler_pattern(uint32_t seed, uint32_t x, uint32_t y, uint32_t index, uint32_t pattern, float out[4]) {
+  Sampler s(seed, x, y, index);
+  s.pattern(pattern, out);
+}
+float oracle_sampler_coin(uint32_t seed, uint32_t x, uint32_t y, uint32_t index, uint32_t ray, uint32_t tri) {
+  return Sampler(seed, x, y, index).coin(ray, tri);
+}
+uint32_t oracle_pcg_hash(uint32_t x) { return pcg_hash(x); }
+
+float oracle_triangle_solid_angle(const float p[3], const float a[3], const float b[3], const float c[3]) {
+  return triangle_solid_angle({p[0], p[1], p[2]}, {a[0], a[1], a[2]}, {b[0], b[1], b[2]}, {c[0], c[1], c[2]});
+}
+int oracle_sample_spherical_triangle(const float p[3], const float a[3], const float b[3], const float c[3], float u0,
+                                     float u1, float out[3]) {
+  V3 o;
+  if (!sample_spherical_triangle({p[0], p[1], p[2]}, {a[0], a[1], a[2]}, {b[0], b[1], b[2]}, {c[0], c[1], c[2]}, u0,
+                                 u1, o))
+    return 0;
+  out[0] = o.x;
+  out[1] = o.y;
+  out[2] = o.z;
+  return 1;
+}
+void oracle_iridescent_fresnel(float outside, float film, const float f0[3], float thick, float cos1, float out[3]) {
+  V3 r = iridescent_fresnel(outside, film, {f0[0], f0[1], f0[2]}, thick, cos1);
+  out[0] = r.x;
+  out[1] = r.y;
+  out[2] = r.z;
+}
+void oracle_dispersion_iors(float ior, float dispersion, float out[3]) { dispersion_iors(ior, dispersion, out); }
+const float *oracle_sheen_lut(void) { return sheen_lut().data(); }
+
+float oracle_env_pdf(const void *env, const float d[3]) { return ((const EnvironmentMap *)env)->pdf({d[0], d[1], d[2]}); }
+int oracle_env_sample(const void *env, float u0, float u1, float d[3], float le[3], float *pdf) {
+  V3 dd, l;
+  if (!((const EnvironmentMap *)env)->sample(u0, u1, dd, l, *pdf)) return 0;
+  d[0] = dd.x;
+  d[1] = dd.y;
+  d[2] = dd.z;
+  le[0] = l.x;
+  le[1] = l.y;
+  le[2] = l.z;
+  return 1;
+}
+
+// MaterialSample as a flat float array for the BSDF tests (layout below).
+// [0..4) base_color, 4 metallic, 5 roughness, [6..9) normal, 9 specular,
+// [10..13) specular_color, 13 transmission, 14 thickness, 15 ior,
+// 16 clearcoat, 17 clearcoat_roughness, [18..21) clearcoat_normal,
+// [21..24) sheen_color, 24 sheen_roughness, 25 anisotropy,
+// [26..29) anisotropy_direction, 29 iridescence, 30 iridescence_ior,
+// 31 iridescence_thickness, 32 diffuse_transmission, [33..36) dt_color.
+static MaterialSample ms_from(const float *a) {
+  MaterialSample m;
+  for (int k = 0; k < 4; ++k) m.base_color[k] = a[k];
+  m.metallic = a[4];
+  m.roughness = a[5];
+  m.normal = {a[6], a[7], a[8]};
+  m.specular = a[9];
+  m.specular_color = {a[10], a[11], a[12]};
+  m.transmission = a[13];
+  m.thickness = a[14];
+  m.ior = a[15];
+  m.clearcoat = a[16];
+  m.clearcoat_roughness = a[17];
+  m.clearcoat_normal = {a[18], a[19], a[20]};
+  m.sheen_color = {a[21], a[22], a[23]};
+  m.sheen_roughness = a[24];
+  m.anisotropy = a[25];
+  m.anisotropy_direction = {a[26], a[27], a[28]};
+  m.iridescence = a[29];
+  m.iridescence_ior = a[30];
+  m.iridescence_thickness = a[31];
+  m.diffuse_transmission = a[32];
+  m.diffuse_transmission_color = {a[33], a[34], a[35]};
+  return m;
+}
+void oracle_bsdf_eval(const float *ms, const float v[3], const float ng[3], int front, const float l[3], float f[3],
+                      float *pdf, float probs[6]) {
+  Bsdf b(ms_from(ms), {v[0], v[1], v[2]}, {ng[0], ng[1], ng[2]}, front != 0);
+  V3 ff;
+  b.eval({l[0], l[1], l[2]}, ff, *pdf);
+  f[0] = ff.x;
+  f[1] = ff.y;
+  f[2] = ff.z;
+  if (probs)
+    for (int i = 0; i < 6; ++i) probs[i] = b.probs[i];
+}
+// Batched eval over n directions (quadrature in the tests).
+void oracle_bsdf_eval_many(const float *ms, const float v[3], const float ng[3], int front, uint32_t n, const float *l,
+                           float *f, float *pdf) {
+  Bsdf b(ms_from(ms), {v[0], v[1], v[2]}, {ng[0], ng[1], ng[2]}, front != 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    V3 ff;
+    b.eval({l[3 * i], l[3 * i + 1], l[3 * i + 2]}, ff, pdf[i]);
+    f[3 * i] = ff.x;
+    f[3 * i + 1] = ff.y;
+    f[3 * i + 2] = ff.z;
+  }
+}
+// Batched sample over n lobe/direction triples u[3*i..].
+void oracle_bsdf_sample_many(const float *ms, const float v[3], const float ng[3], int front, uint32_t n,
+                             const float *u, float *l, float *f, float *pdf, uint8_t *ok) {
+  Bsdf b(ms_from(ms), {v[0], v[1], v[2]}, {ng[0], ng[1], ng[2]}, front != 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    V3 ll, ff;
+    float p = 0.0f;
+    bool good = b.sample(u + 3 * i, ll, ff, p);
+    ok[i] = good ? 1 : 0;
+    if (!good) continue;
+    l[3 * i] = ll.x;
+    l[3 * i + 1] = ll.y;
+    l[3 * i + 2] = ll.z;
+    f[3 * i] = ff.x;
+    f[3 * i + 1] = ff.y;
+    f[3 * i + 2] = ff.z;
+    pdf[i] = p;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,223 @@
+"""ctypes mirrors of the C ABI structs declared in include/pt_b200.h.
+
+Field order, widths and names follow the header one for one; the CPU test
+suite compiles the header with gcc and checks every size and offset against
+these classes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+PT_MAX_UV_SETS = 4
+
+PT_OK = 0
+STATUS_NAMES = {
+    0: "PT_OK",
+    1: "PT_ERR_INVALID_ARG",
+    2: "PT_ERR_OOM",
+    3: "PT_ERR_DEVICE",
+    4: "PT_ERR_TIMEOUT",
+    5: "PT_ERR_EVICTED",
+    6: "PT_ERR_CANCELLED",
+    7: "PT_ERR_NOT_FOUND",
+    8: "PT_ERR_NOT_READY",
+}
+
+PT_ALPHA_OPAQUE, PT_ALPHA_MASK, PT_ALPHA_BLEND = 0, 1, 2
+
+PT_EXT_SPECULAR = 1 << 0
+PT_EXT_TRANSMISSION = 1 << 1
+PT_EXT_VOLUME = 1 << 2
+PT_EXT_CLEARCOAT = 1 << 3
+PT_EXT_SHEEN = 1 << 4
+PT_EXT_ANISOTROPY = 1 << 5
+PT_EXT_IRIDESCENCE = 1 << 6
+PT_EXT_DIFFUSE_TRANSMISSION = 1 << 7
+PT_EXT_DISPERSION = 1 << 8
+
+PT_FILTER_NEAREST, PT_FILTER_LINEAR = 0, 1
+(PT_MIN_NEAREST, PT_MIN_LINEAR, PT_MIN_NEAREST_MIP_NEAREST, PT_MIN_LINEAR_MIP_NEAREST,
+ PT_MIN_NEAREST_MIP_LINEAR, PT_MIN_LINEAR_MIP_LINEAR) = range(6)
+PT_WRAP_REPEAT, PT_WRAP_CLAMP, PT_WRAP_MIRROR = 0, 1, 2
+PT_PIXELS_RGBA8, PT_PIXELS_RGBA_F32 = 0, 1
+PT_LIGHT_DIRECTIONAL, PT_LIGHT_POINT, PT_LIGHT_SPOT = 0, 1, 2
+PT_PERSPECTIVE, PT_ORTHOGRAPHIC = 0, 1
+PT_MIS, PT_LIGHT_ONLY, PT_BSDF_ONLY = 0, 1, 2
+PT_TONE_CLAMP, PT_TONE_REINHARD, PT_TONE_ACES = 0, 1, 2
+
+f3 = C.c_float * 3
+f4 = C.c_float * 4
+
+
+class pt_texture_binding(C.Structure):
+    _fields_ = [
+        ("texture", C.c_int32),
+        ("uv_set", C.c_uint32),
+        ("has_transform", C.c_uint32),
+        ("transform", C.c_float * 6),
+    ]
+
+
+def no_binding() -> pt_texture_binding:
+    b = pt_texture_binding()
+    b.texture = -1
+    return b
+
+
+class pt_material(C.Structure):
+    _fields_ = [
+        ("base_color", f4),
+        ("base_color_texture", pt_texture_binding),
+        ("metallic", C.c_float),
+        ("roughness", C.c_float),
+        ("metallic_roughness_texture", pt_texture_binding),
+        ("normal_texture", pt_texture_binding),
+        ("normal_scale", C.c_float),
+        ("occlusion_texture", pt_texture_binding),
+        ("occlusion_strength", C.c_float),
+        ("emissive", f3),
+        ("emissive_texture", pt_texture_binding),
+        ("alpha_mode", C.c_uint32),
+        ("alpha_cutoff", C.c_float),
+        ("double_sided", C.c_uint32),
+        ("unlit", C.c_uint32),
+        ("ior", C.c_float),
+        ("ext_flags", C.c_uint32),
+        ("specular_factor", C.c_float),
+        ("specular_texture", pt_texture_binding),
+        ("specular_color_factor", f3),
+        ("specular_color_texture", pt_texture_binding),
+        ("transmission_factor", C.c_float),
+        ("transmission_texture", pt_texture_binding),
+        ("thickness_factor", C.c_float),
+        ("thickness_texture", pt_texture_binding),
+        ("attenuation_distance", C.c_float),
+        ("attenuation_color", f3),
+        ("clearcoat_factor", C.c_float),
+        ("clearcoat_texture", pt_texture_binding),
+        ("clearcoat_roughness_factor", C.c_float),
+        ("clearcoat_roughness_texture", pt_texture_binding),
+        ("clearcoat_normal_texture", pt_texture_binding),
+        ("clearcoat_normal_scale", C.c_float),
+        ("sheen_color_factor", f3),
+        ("sheen_color_texture", pt_texture_binding),
+        ("sheen_roughness_factor", C.c_float),
+        ("sheen_roughness_texture", pt_texture_binding),
+        ("anisotropy_strength", C.c_float),
+        ("anisotropy_rotation", C.c_float),
+        ("anisotropy_texture", pt_texture_binding),
+        ("iridescence_factor", C.c_float),
+        ("iridescence_texture", pt_texture_binding),
+        ("iridescence_ior", C.c_float),
+        ("iridescence_thickness_min", C.c_float),
+        ("iridescence_thickness_max", C.c_float),
+        ("iridescence_thickness_texture", pt_texture_binding),
+        ("diffuse_transmission_factor", C.c_float),
+        ("diffuse_transmission_texture", pt_texture_binding),
+        ("diffuse_transmission_color_factor", f3),
+        ("diffuse_transmission_color_texture", pt_texture_binding),
+        ("dispersion", C.c_float),
+    ]
+
+
+class pt_texture(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("format", C.c_uint32),
+        ("pixels", C.c_void_p),
+        ("mag_filter", C.c_uint32),
+        ("min_filter", C.c_uint32),
+        ("wrap_s", C.c_uint32),
+        ("wrap_t", C.c_uint32),
+    ]
+
+
+class pt_draw_item(C.Structure):
+    _fields_ = [
+        ("triangle_count", C.c_uint32),
+        ("positions", C.POINTER(C.c_float)),
+        ("normals", C.POINTER(C.c_float)),
+        ("has_vertex_normals", C.c_uint32),
+        ("tangents", C.POINTER(C.c_float)),
+        ("uvs", C.POINTER(C.c_float) * PT_MAX_UV_SETS),
+        ("colors", C.POINTER(C.c_float)),
+        ("material", C.c_uint32),
+    ]
+
+
+class pt_light(C.Structure):
+    _fields_ = [
+        ("kind", C.c_uint32),
+        ("color", f3),
+        ("intensity", C.c_float),
+        ("position", f3),
+        ("direction", f3),
+        ("has_range", C.c_uint32),
+        ("range", C.c_float),
+        ("inner_cone_angle", C.c_float),
+        ("outer_cone_angle", C.c_float),
+    ]
+
+
+class pt_scene_desc(C.Structure):
+    _fields_ = [
+        ("item_count", C.c_uint32),
+        ("items", C.POINTER(pt_draw_item)),
+        ("material_count", C.c_uint32),
+        ("materials", C.POINTER(pt_material)),
+        ("texture_count", C.c_uint32),
+        ("textures", C.POINTER(pt_texture)),
+        ("light_count", C.c_uint32),
+        ("lights", C.POINTER(pt_light)),
+    ]
+
+
+class pt_environment(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("pixels", C.POINTER(C.c_float)),
+        ("intensity", C.c_float),
+    ]
+
+
+class pt_camera(C.Structure):
+    _fields_ = [
+        ("eye", f3),
+        ("forward", f3),
+        ("side", f3),
+        ("up", f3),
+        ("half_w", C.c_float),
+        ("half_h", C.c_float),
+        ("projection", C.c_uint32),
+    ]
+
+
+class pt_path_trace_options(C.Structure):
+    _fields_ = [
+        ("samples_per_pixel", C.c_uint32),
+        ("max_bounces", C.c_uint32),
+        ("rr_start", C.c_uint32),
+        ("clamp", C.c_float),
+        ("seed", C.c_uint32),
+        ("strategy", C.c_uint32),
+    ]
+
+
+class pt_render_options(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("background", C.c_uint8 * 4),
+        ("tone_map", C.c_uint32),
+        ("exposure", C.c_float),
+        ("ambient", C.c_float),
+        ("path_trace", pt_path_trace_options),
+    ]
+
+
+ABI_STRUCTS = [
+    pt_texture_binding, pt_material, pt_texture, pt_draw_item, pt_light,
+    pt_scene_desc, pt_environment, pt_camera, pt_path_trace_options, pt_render_options,
+]
