@@ -36,6 +36,12 @@ extern "C" {
 
 #define PT_ABI_VERSION 1u
 
+#if defined(__GNUC__)
+#define PT_API __attribute__((visibility("default")))
+#else
+#define PT_API
+#endif
+
 /* ------------------------------------------------------------------ status */
 
 /* Maps to oxideav_render::Error (src/error.rs:16-43): INVALID_ARG ->
@@ -281,21 +287,21 @@ typedef struct pt_render_options {
 typedef struct pt_context pt_context;
 
 /* Create a context on CUDA device `device` (one per GPU). */
-pt_status pt_create(pt_context **out, int device);
-void pt_destroy(pt_context *ctx);
+PT_API pt_status pt_create(pt_context **out, int device);
+PT_API void pt_destroy(pt_context *ctx);
 /* Message of the last failing call on ctx (or of pt_create when ctx is NULL). */
-const char *pt_last_error(const pt_context *ctx);
-uint32_t pt_abi_version(void);
+PT_API const char *pt_last_error(const pt_context *ctx);
+PT_API uint32_t pt_abi_version(void);
 
 /* Upload a prepared scene: builds the BVH on the host (binned SAH), the
  * emissive-triangle table (EmissiveLights::build, src/pathtrace.rs:1479-1543)
  * and the texture mip chains, and copies everything to device memory, where it
  * stays until pt_scene_release (or until the serving cache evicts it). */
-pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *scene_id);
-pt_status pt_scene_release(pt_context *ctx, uint32_t scene_id);
+PT_API pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *scene_id);
+PT_API pt_status pt_scene_release(pt_context *ctx, uint32_t scene_id);
 /* Device bytes held by a resident scene. */
-pt_status pt_scene_device_bytes(pt_context *ctx, uint32_t scene_id, uint64_t *bytes);
-pt_status pt_scene_triangle_count(pt_context *ctx, uint32_t scene_id, uint64_t *count);
+PT_API pt_status pt_scene_device_bytes(pt_context *ctx, uint32_t scene_id, uint64_t *bytes);
+PT_API pt_status pt_scene_triangle_count(pt_context *ctx, uint32_t scene_id, uint64_t *count);
 
 /* ------------------------------------------------------------------ progressive tracer */
 
@@ -303,41 +309,41 @@ pt_status pt_scene_triangle_count(pt_context *ctx, uint32_t scene_id, uint64_t *
  * (per pixel: sum r, sum g, sum b over covered samples, covered count, f64). */
 typedef struct pt_tracer pt_tracer;
 
-pt_status pt_tracer_create(pt_context *ctx, pt_tracer **out);
-void pt_tracer_destroy(pt_tracer *tr);
+PT_API pt_status pt_tracer_create(pt_context *ctx, pt_tracer **out);
+PT_API void pt_tracer_destroy(pt_tracer *tr);
 /* PathTracer::sync: bind scene + camera + options. Resets the accumulator
  * exactly when the scene changed (other id, or invalidate_scene was called)
  * or the radiance key changed (radiance_key, src/pathtrace.rs:2402-2418:
  * everything except background, tone map, exposure and spp). *reset receives
  * 1 when it reset. */
-pt_status pt_tracer_sync(pt_tracer *tr, uint32_t scene_id, const pt_camera *camera,
+PT_API pt_status pt_tracer_sync(pt_tracer *tr, uint32_t scene_id, const pt_camera *camera,
                          const pt_render_options *opts, int *reset);
 /* PathTracer::refine: add `samples` samples to every pixel; sample indices
  * continue from pt_tracer_samples, so refine(a); refine(b) == refine(a + b)
  * bit for bit. Blocks until the device work is done. */
-pt_status pt_tracer_refine(pt_tracer *tr, uint32_t samples);
-pt_status pt_tracer_samples(const pt_tracer *tr, uint32_t *samples);
-pt_status pt_tracer_is_converged(const pt_tracer *tr, int *converged);
-pt_status pt_tracer_reset(pt_tracer *tr);
-pt_status pt_tracer_invalidate_scene(pt_tracer *tr);
+PT_API pt_status pt_tracer_refine(pt_tracer *tr, uint32_t samples);
+PT_API pt_status pt_tracer_samples(const pt_tracer *tr, uint32_t *samples);
+PT_API pt_status pt_tracer_is_converged(const pt_tracer *tr, int *converged);
+PT_API pt_status pt_tracer_reset(pt_tracer *tr);
+PT_API pt_status pt_tracer_invalidate_scene(pt_tracer *tr);
 /* PathTracer::set_environment: env == NULL removes it. Resets accumulation. */
-pt_status pt_tracer_set_environment(pt_tracer *tr, const pt_environment *env);
+PT_API pt_status pt_tracer_set_environment(pt_tracer *tr, const pt_environment *env);
 /* PathTracer::hdr (src/pathtrace.rs:2717-2734): width*height*4 floats. */
-pt_status pt_tracer_read_hdr(pt_tracer *tr, float *out_rgba, size_t out_floats);
+PT_API pt_status pt_tracer_read_hdr(pt_tracer *tr, float *out_rgba, size_t out_floats);
 /* PathTracer::image (src/pathtrace.rs:2687-2713): width*height*4 bytes. */
-pt_status pt_tracer_read_image(pt_tracer *tr, uint8_t *out_rgba, size_t out_bytes);
+PT_API pt_status pt_tracer_read_image(pt_tracer *tr, uint8_t *out_rgba, size_t out_bytes);
 /* Raw accumulator: width*height*4 doubles (sum r, g, b, covered count). */
-pt_status pt_tracer_read_accum(pt_tracer *tr, double *out, size_t out_doubles);
+PT_API pt_status pt_tracer_read_accum(pt_tracer *tr, double *out, size_t out_doubles);
 /* Rays traced by the last refine: closest-hit (extension) and any-hit (shadow). */
-pt_status pt_tracer_ray_counts(const pt_tracer *tr, uint64_t *extension_rays, uint64_t *shadow_rays);
+PT_API pt_status pt_tracer_ray_counts(const pt_tracer *tr, uint64_t *extension_rays, uint64_t *shadow_rays);
 
 /* PathTraceRenderer::render / render_hdr (src/pathtrace.rs:2761-2777):
  * invalidate -> sync -> refine(max(spp, 1)) -> image / hdr, on a temporary
  * tracer. env may be NULL. */
-pt_status pt_render_hdr(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+PT_API pt_status pt_render_hdr(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                         const pt_render_options *opts, const pt_environment *env,
                         float *out_rgba, size_t out_floats);
-pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+PT_API pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                           const pt_render_options *opts, const pt_environment *env,
                           uint8_t *out_rgba, size_t out_bytes);
 

@@ -1,0 +1,51 @@
+/*
+ * pt_b200_debug.h — test and measurement hooks of the B200 path tracer.
+ *
+ * These have no counterpart in the reference's Renderer / PathTracer API;
+ * they expose intermediate values of the hot path (sampler values, primary
+ * hits, BSDF evaluations, traversal counters) so parity tests can compare
+ * them one by one with a CPU restatement of the reference, and select the
+ * schedule the tracer uses.
+ */
+#ifndef PT_B200_DEBUG_H
+#define PT_B200_DEBUG_H
+
+#include "pt_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* sobol_owen_4d(i, seed) for i in 0..n (src/pathtrace.rs:388-398): 4n floats. */
+PT_API pt_status pt_debug_sobol(pt_context *ctx, uint32_t n, uint32_t seed, float *out);
+/* Sampler::pattern(pattern) of sample `index` for every pixel of the synced
+ * tracer: width*height*4 floats. */
+PT_API pt_status pt_debug_pattern(pt_tracer *tr, uint32_t index, uint32_t pattern, float *out);
+/* Camera-ray closest hit (k = 0 acceptance filter) of sample `index` for every
+ * pixel: global triangle id (0xffffffff on a miss) and (t, b0, b1, b2). */
+PT_API pt_status pt_debug_primary_hits(pt_tracer *tr, uint32_t index, uint32_t *out_global, float *out_tbary);
+/* Bsdf::new(ms, v, ng, front) then eval(dirs[i]) and sample(us[i]) for i < n.
+ * params: 36 MaterialSample floats (layout of the oracle's test hook) then
+ * v[3], ng[3], front. out: 12 floats per i = f[3], pdf, ok, l[3], f_s[3], pdf_s. */
+PT_API pt_status pt_debug_bsdf(pt_context *ctx, const float *params, const float *dirs, const float *us, uint32_t n,
+                        float *out);
+/* Traversal work of the last refine: BVH nodes visited, triangles tested. */
+PT_API pt_status pt_tracer_traversal_counts(const pt_tracer *tr, uint64_t *nodes, uint64_t *tris);
+/* BVH statistics of a resident scene. */
+PT_API pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes, uint32_t *leaves,
+                             uint32_t *max_depth, double *sah_cost, double *build_seconds);
+
+/* Schedule of the hot loop: 0 = one path per thread (megakernel). */
+typedef enum pt_schedule { PT_SCHEDULE_MEGAKERNEL = 0 } pt_schedule;
+PT_API pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule);
+/* Maximum path slots per wave (device sample buffer 16 B per slot). */
+PT_API pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots);
+/* Device time in ms of the last refine's path-tracing kernels (CUDA events
+ * on the context stream). */
+PT_API pt_status pt_tracer_last_kernel_ms(const pt_tracer *tr, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PT_B200_DEBUG_H */

@@ -49,6 +49,8 @@ def lib():
                 "oracle_occluded": (i32, [vp, fp, fp, f32, f32]),
                 "oracle_surface": (None, [vp, u32, fp, fp, fp, fp]),
                 "oracle_material_base": (None, [vp, u32, fp, fp]),
+                "oracle_texture_sample": (None, [vp, f32, f32, f32, i32, fp, u32p, fp]),
+                "oracle_emissive_table": (None, [vp, u32p, C.POINTER(u32p), C.POINTER(fp), C.POINTER(fp)]),
                 "oracle_sobol_owen_4d": (None, [u32, u32, fp]),
                 "oracle_sobol": (u32, [u32, u32]),
                 "oracle_sampler_pattern": (None, [u32, u32, u32, u32, u32, fp]),
@@ -253,6 +255,23 @@ class Bsdf:
                                       pdf.ctypes.data_as(C.POINTER(C.c_float)),
                                       ok.ctypes.data_as(C.POINTER(C.c_uint8)))
         return l, f, pdf, ok.astype(bool)
+
+
+def texture_sample(pixels: np.ndarray, sampler, u: float, v: float, lod: float, srgb: bool):
+    """(rgba, mip level count, last level's texel) of PreparedTexture::sample_lod."""
+    a = _abi()
+    px = np.ascontiguousarray(pixels)
+    fmt = a.PT_PIXELS_RGBA8 if px.dtype == np.uint8 else a.PT_PIXELS_RGBA_F32
+    if fmt == a.PT_PIXELS_RGBA_F32:
+        px = np.ascontiguousarray(px, dtype=np.float32)
+    t = a.pt_texture(px.shape[1], px.shape[0], fmt, px.ctypes.data, sampler.mag_filter, sampler.min_filter,
+                     sampler.wrap_s, sampler.wrap_t)
+    out = np.zeros(4, np.float32)
+    top = np.zeros(4, np.float32)
+    levels = C.c_uint32()
+    lib().oracle_texture_sample(C.addressof(t), u, v, lod, 1 if srgb else 0, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                C.byref(levels), top.ctypes.data_as(C.POINTER(C.c_float)))
+    return out, levels.value, top
 
 
 def sobol_owen_4d(index: int, seed: int) -> np.ndarray:

@@ -643,6 +643,27 @@ void oracle_emissive_table(const void *scene, uint32_t *count, const uint32_t **
   *cdf = sc->emissive.cdf.data();
 }
 
+// PreparedTexture::sample_lod on a one-texture scene; also reports the
+// number of mip levels and the last level's first texel.
+void oracle_texture_sample(const pt_texture *t, float u, float v, float lod, int srgb, float out[4],
+                           uint32_t *levels, float top[4]) {
+  pt_material m{};
+  m.base_color_texture.texture = -1;
+  pt_scene_desc d{};
+  d.material_count = 1;
+  d.materials = &m;
+  d.texture_count = 1;
+  d.textures = t;
+  Scene sc(d);
+  const Texture *tex = sc.textures[0].get();
+  V4 r = tex->sample_lod(u, v, lod, srgb != 0);
+  for (int k = 0; k < 4; ++k) out[k] = r[k];
+  const std::vector<MipLevel> &mips = tex->mips(srgb != 0);
+  if (levels) *levels = (uint32_t)mips.size();
+  if (top)
+    for (int k = 0; k < 4; ++k) top[k] = mips.back().texels[0][k];
+}
+
 void oracle_sobol_owen_4d(uint32_t index, uint32_t seed, float out[4]) { sobol_owen_4d(index, seed, out); }
 uint32_t oracle_sobol(uint32_t index, uint32_t dim) { return sobol(index, (int)dim); }
 void oracle_sampler_pattern(uint32_t seed, uint32_t x, uint32_t y, uint32_t index, uint32_t pattern, float out[4]) {

@@ -11,6 +11,8 @@ import ctypes as C
 PT_MAX_UV_SETS = 4
 
 PT_OK = 0
+(PT_ERR_INVALID_ARG, PT_ERR_OOM, PT_ERR_DEVICE, PT_ERR_TIMEOUT, PT_ERR_EVICTED, PT_ERR_CANCELLED, PT_ERR_NOT_FOUND,
+ PT_ERR_NOT_READY) = range(1, 9)
 STATUS_NAMES = {
     0: "PT_OK",
     1: "PT_ERR_INVALID_ARG",

@@ -1,0 +1,300 @@
+"""The reference's path-tracer interface over the CUDA library.
+
+* `PathTracer` mirrors oxideav_render::pathtrace::PathTracer
+  (src/pathtrace.rs:2369-2735): `sync` / `refine` / `samples` /
+  `is_converged` / `image` / `hdr` / `set_environment` /
+  `invalidate_scene` / `reset`, with the same reset rule and the same
+  sample-index continuation, the accumulator living on the GPU.
+* `PathTraceCudaRenderer` mirrors `PathTraceRenderer` (:2745-2782):
+  `render` / `render_hdr` re-prepare the scene and take `samples_per_pixel`
+  samples.
+* `make_renderer(RenderBackend.PathTraceCuda)` is the one new match arm of
+  `make_renderer` (src/lib.rs:174-180).
+
+Scenes are `PreparedScene`s (the reference's `PreparedScene::build` output);
+the camera is `Camera.resolve` of the options, exactly as the reference's
+`sync` does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import abi, native
+from .native import RenderError, check
+from .options import RenderBackend, RenderOptions, radiance_key
+from .scene import Camera, PreparedScene, SceneDesc
+
+
+class Context:
+    """One CUDA device (pt_context)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = native.load()
+        p = C.c_void_p()
+        st = self.lib.pt_create(C.byref(p), device)
+        if st != abi.PT_OK:
+            raise RenderError(st, (self.lib.pt_last_error(None) or b"").decode())
+        self.ptr = p
+        self.device = device
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.lib.pt_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, st: int):
+        check(st, self.ptr)
+
+    def upload(self, desc: SceneDesc) -> int:
+        sid = C.c_uint32()
+        self.check(self.lib.pt_scene_upload(self.ptr, C.byref(desc.desc), C.byref(sid)))
+        return sid.value
+
+    def release(self, scene_id: int) -> None:
+        self.check(self.lib.pt_scene_release(self.ptr, scene_id))
+
+    def scene_bytes(self, scene_id: int) -> int:
+        b = C.c_uint64()
+        self.check(self.lib.pt_scene_device_bytes(self.ptr, scene_id, C.byref(b)))
+        return b.value
+
+    def bvh_stats(self, scene_id: int) -> dict:
+        n, l, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        sah, sec = C.c_double(), C.c_double()
+        self.check(self.lib.pt_scene_bvh_stats(self.ptr, scene_id, C.byref(n), C.byref(l), C.byref(d),
+                                               C.byref(sah), C.byref(sec)))
+        return {"nodes": n.value, "leaves": l.value, "max_depth": d.value, "sah_cost": sah.value,
+                "build_seconds": sec.value}
+
+    def set_schedule(self, schedule: int) -> None:
+        self.check(self.lib.pt_set_schedule(self.ptr, schedule))
+
+    def set_wave_slots(self, slots: int) -> None:
+        self.check(self.lib.pt_set_wave_slots(self.ptr, slots))
+
+    def debug_sobol(self, n: int, seed: int) -> np.ndarray:
+        out = np.zeros((n, 4), np.float32)
+        self.check(self.lib.pt_debug_sobol(self.ptr, n, seed & 0xFFFFFFFF, out.ctypes.data_as(native.fp)))
+        return out
+
+    def debug_bsdf(self, ms: np.ndarray, v, ng, front: bool, dirs: np.ndarray, us: np.ndarray) -> np.ndarray:
+        params = np.zeros(43, np.float32)
+        params[:36] = ms
+        params[36:39] = v
+        params[39:42] = ng
+        params[42] = 1.0 if front else 0.0
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        us = np.ascontiguousarray(us, np.float32)
+        n = dirs.shape[0]
+        out = np.zeros((n, 12), np.float32)
+        self.check(self.lib.pt_debug_bsdf(self.ptr, params.ctypes.data_as(native.fp), dirs.ctypes.data_as(native.fp),
+                                          us.ctypes.data_as(native.fp), n, out.ctypes.data_as(native.fp)))
+        return out
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class EnvironmentMap:
+    """Equirectangular HDR environment (src/pathtrace.rs:1557-1741):
+    scene-linear RGBA f32 pixels (h, w, 4), row 0 = +Y, times `intensity`."""
+
+    def __init__(self, pixels: np.ndarray, intensity: float = 1.0):
+        self.pixels = np.ascontiguousarray(pixels, dtype=np.float32)
+        self.intensity = float(intensity)
+
+    def to_c(self) -> abi.pt_environment:
+        return abi.pt_environment(self.pixels.shape[1], self.pixels.shape[0],
+                                  self.pixels.ctypes.data_as(C.POINTER(C.c_float)), self.intensity)
+
+
+class PathTracer:
+    """Progressive path tracer with a device-resident accumulator."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.lib = self.ctx.lib
+        p = C.c_void_p()
+        self.ctx.check(self.lib.pt_tracer_create(self.ctx.ptr, C.byref(p)))
+        self.ptr = p
+        self.opts = RenderOptions()
+        self._scene = None
+        self._scene_key = None
+        self._scene_id = None
+        self._desc = None
+        self._dirty = True
+        self._env = None
+        self.camera: Optional[Camera] = None
+
+    def close(self):
+        if getattr(self, "ptr", None):
+            self.lib.pt_tracer_destroy(self.ptr)
+            self.ptr = None
+        if self._scene_id is not None and self.ctx.ptr:
+            self.ctx.release(self._scene_id)
+            self._scene_id = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _prep_key(o: RenderOptions):
+        # PrepareOptions::from_render_options (src/prepare.rs:137-146).
+        return (o.time, o.animation, o.material_variant, o.use_scene_lights, o.light)
+
+    def sync(self, scene: PreparedScene, opts: RenderOptions) -> bool:
+        """PathTracer::sync: re-uploads the scene when invalidated or when a
+        preparation input changed; resets exactly when radiance inputs change."""
+        key = (id(scene), self._prep_key(opts))
+        need_prepare = self._dirty or self._scene is not scene or self._scene_key != key
+        if need_prepare:
+            desc = scene.to_desc(opts)
+            sid = self.ctx.upload(desc)
+            if self._scene_id is not None:
+                self.ctx.release(self._scene_id)
+            self._scene_id, self._desc, self._scene, self._scene_key = sid, desc, scene, key
+            self._dirty = False
+            self.lib.pt_tracer_invalidate_scene(self.ptr)
+        w, h = max(opts.width, 1), max(opts.height, 1)
+        self.camera = Camera.resolve(scene, opts, w, h)
+        cam = self.camera.to_c()
+        o = opts.to_c()
+        reset = C.c_int()
+        self.ctx.check(self.lib.pt_tracer_sync(self.ptr, self._scene_id, C.byref(cam), C.byref(o), C.byref(reset)))
+        self.opts = opts
+        return bool(reset.value)
+
+    def refine(self, samples: int) -> None:
+        self.ctx.check(self.lib.pt_tracer_refine(self.ptr, int(samples)))
+
+    def samples(self) -> int:
+        s = C.c_uint32()
+        self.ctx.check(self.lib.pt_tracer_samples(self.ptr, C.byref(s)))
+        return s.value
+
+    def is_converged(self) -> bool:
+        c = C.c_int()
+        self.ctx.check(self.lib.pt_tracer_is_converged(self.ptr, C.byref(c)))
+        return bool(c.value)
+
+    def reset(self) -> None:
+        self.ctx.check(self.lib.pt_tracer_reset(self.ptr))
+
+    def invalidate_scene(self) -> None:
+        self._dirty = True
+        self.ctx.check(self.lib.pt_tracer_invalidate_scene(self.ptr))
+
+    def set_environment(self, env: Optional[EnvironmentMap]) -> None:
+        self._env = env
+        if env is None:
+            self.ctx.check(self.lib.pt_tracer_set_environment(self.ptr, None))
+        else:
+            e = env.to_c()
+            self.ctx.check(self.lib.pt_tracer_set_environment(self.ptr, C.byref(e)))
+
+    def _dims(self):
+        return max(self.opts.width, 1), max(self.opts.height, 1)
+
+    def hdr(self) -> np.ndarray:
+        w, h = self._dims()
+        out = np.zeros((h, w, 4), np.float32)
+        self.ctx.check(self.lib.pt_tracer_read_hdr(self.ptr, out.ctypes.data_as(native.fp), out.size))
+        return out
+
+    def image(self) -> np.ndarray:
+        w, h = self._dims()
+        out = np.zeros((h, w, 4), np.uint8)
+        self.ctx.check(self.lib.pt_tracer_read_image(self.ptr, out.ctypes.data_as(native.u8p), out.size))
+        return out
+
+    def accum(self) -> np.ndarray:
+        w, h = self._dims()
+        out = np.zeros((h, w, 4), np.float64)
+        self.ctx.check(self.lib.pt_tracer_read_accum(self.ptr, out.ctypes.data_as(native.dp), out.size))
+        return out
+
+    def ray_counts(self):
+        e, s = C.c_uint64(), C.c_uint64()
+        self.ctx.check(self.lib.pt_tracer_ray_counts(self.ptr, C.byref(e), C.byref(s)))
+        return e.value, s.value
+
+    def traversal_counts(self):
+        n, t = C.c_uint64(), C.c_uint64()
+        self.ctx.check(self.lib.pt_tracer_traversal_counts(self.ptr, C.byref(n), C.byref(t)))
+        return n.value, t.value
+
+    def last_kernel_ms(self) -> float:
+        m = C.c_float()
+        self.ctx.check(self.lib.pt_tracer_last_kernel_ms(self.ptr, C.byref(m)))
+        return m.value
+
+    @property
+    def scene_id(self):
+        return self._scene_id
+
+    def debug_pattern(self, index: int, pattern: int) -> np.ndarray:
+        w, h = self._dims()
+        out = np.zeros((h, w, 4), np.float32)
+        self.ctx.check(self.lib.pt_debug_pattern(self.ptr, index, pattern, out.ctypes.data_as(native.fp)))
+        return out
+
+    def debug_primary_hits(self, index: int = 0):
+        w, h = self._dims()
+        g = np.zeros((h, w), np.uint32)
+        tb = np.zeros((h, w, 4), np.float32)
+        self.ctx.check(self.lib.pt_debug_primary_hits(self.ptr, index, g.ctypes.data_as(native.u32p),
+                                                      tb.ctypes.data_as(native.fp)))
+        return g, tb
+
+
+class PathTraceCudaRenderer:
+    """Renderer for RenderBackend::PathTraceCuda (PathTraceRenderer semantics)."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.tracer = PathTracer(ctx)
+
+    def tracer_mut(self) -> PathTracer:
+        return self.tracer
+
+    def _run(self, scene: PreparedScene, opts: RenderOptions) -> None:
+        self.tracer.invalidate_scene()
+        self.tracer.sync(scene, opts)
+        self.tracer.refine(max(opts.path_trace.samples_per_pixel, 1))
+
+    def render(self, scene: PreparedScene, opts: RenderOptions) -> np.ndarray:
+        self._run(scene, opts)
+        return self.tracer.image()
+
+    def render_hdr(self, scene: PreparedScene, opts: RenderOptions) -> np.ndarray:
+        self._run(scene, opts)
+        return self.tracer.hdr()
+
+
+def make_renderer(backend: RenderBackend, ctx: Optional[Context] = None):
+    """make_renderer (src/lib.rs:174-180) for the backend this library provides."""
+    if backend == RenderBackend.PathTraceCuda:
+        return PathTraceCudaRenderer(ctx)
+    raise NotImplementedError(f"{backend} is served by the reference crate, not by this library")
+
+
+__all__ = ["Context", "EnvironmentMap", "PathTracer", "PathTraceCudaRenderer", "make_renderer", "RenderError",
+           "radiance_key"]

@@ -1,0 +1,656 @@
+// extern "C" entry points (include/pt_b200.h, include/pt_b200_debug.h).
+//
+// pt_tracer mirrors PathTracer (src/pathtrace.rs:2369-2735): the same reset
+// rule (radiance_key, :2402-2418), sample indices continuing across refine
+// calls (:2526-2591) and the same resolve (:2593-2734), with the f64
+// accumulator resident on the device. No exception crosses the ABI: every
+// entry point catches and maps failures to a pt_status plus a message.
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pt_b200.h"
+#include "../../include/pt_b200_debug.h"
+#include "host_scene.h"
+#include "kernels.h"
+
+using namespace ptd;
+
+struct pt_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::map<uint32_t, std::unique_ptr<SceneHost>> scenes;
+  uint32_t next_id = 1;
+  uint32_t schedule = PT_SCHEDULE_MEGAKERNEL;
+  uint32_t wave_slots = 1u << 22;
+  float4 *d_out = nullptr;
+  size_t out_cap = 0;
+  WaveSegment *d_segs = nullptr;
+  size_t seg_cap = 0;
+  DevCounters *d_ctr = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct pt_tracer {
+  pt_context *ctx = nullptr;
+  bool have_state = false, dirty = true;
+  uint32_t scene_id = 0;
+  pt_camera cam{};
+  pt_render_options opts{};
+  std::unique_ptr<EnvHost> env;
+  double *d_accum = nullptr;
+  size_t accum_cap = 0;
+  DevRequest *d_req = nullptr;
+  void *d_resolve = nullptr;
+  size_t resolve_cap = 0;
+  uint32_t w = 1, h = 1, samples = 0;
+  uint64_t ext = 0, sh = 0, nodes = 0, tris = 0;
+  float last_ms = 0.0f;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+pt_status fail(pt_context *ctx, pt_status st, const std::string &msg) {
+  if (ctx)
+    ctx->err = msg;
+  else
+    g_create_error = msg;
+  return st;
+}
+
+#define CK(ctx, call)                                                                            \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return fail((ctx), e_ == cudaErrorMemoryAllocation ? PT_ERR_OOM : PT_ERR_DEVICE,           \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+  } while (0)
+
+template <class F>
+pt_status guard(pt_context *ctx, F &&f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc &) {
+    return fail(ctx, PT_ERR_OOM, "host allocation failed");
+  } catch (const std::exception &e) {
+    return fail(ctx, PT_ERR_DEVICE, e.what());
+  } catch (...) {
+    return fail(ctx, PT_ERR_DEVICE, "unknown failure");
+  }
+}
+
+template <class T>
+pt_status ensure(pt_context *ctx, T *&p, size_t &cap, size_t need) {
+  if (need <= cap && p) return PT_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  CK(ctx, cudaMalloc(&p, std::max<size_t>(need, 1) * sizeof(T)));
+  cap = need;
+  return PT_OK;
+}
+
+bool same_radiance_key(const pt_tracer &t, const pt_camera &cam, const pt_render_options &o) {
+  const pt_render_options &a = t.opts;
+  pt_path_trace_options pa = a.path_trace, pb = o.path_trace;
+  pa.samples_per_pixel = pb.samples_per_pixel = 0;
+  return std::memcmp(&t.cam, &cam, sizeof cam) == 0 && a.width == o.width && a.height == o.height &&
+         std::memcmp(&a.ambient, &o.ambient, sizeof(float)) == 0 && std::memcmp(&pa, &pb, sizeof pa) == 0;
+}
+
+pt_status validate_opts(pt_context *ctx, const pt_camera *cam, const pt_render_options *o) {
+  if (!cam || !o) return fail(ctx, PT_ERR_INVALID_ARG, "camera / options pointer is NULL");
+  if (o->path_trace.max_bounces > 1024)
+    return fail(ctx, PT_ERR_INVALID_ARG, "path_trace.max_bounces must be <= 1024");
+  if (o->path_trace.strategy > PT_BSDF_ONLY) return fail(ctx, PT_ERR_INVALID_ARG, "unknown light strategy");
+  if (o->tone_map > PT_TONE_ACES) return fail(ctx, PT_ERR_INVALID_ARG, "unknown tone map");
+  if (cam->projection > PT_ORTHOGRAPHIC) return fail(ctx, PT_ERR_INVALID_ARG, "unknown projection");
+  uint64_t px = (uint64_t)std::max(o->width, 1u) * std::max(o->height, 1u);
+  if (px > (1ull << 28)) return fail(ctx, PT_ERR_INVALID_ARG, "image larger than 268435456 pixels");
+  return PT_OK;
+}
+
+DevRequest make_request(const pt_tracer &t, const SceneHost &sc) {
+  DevRequest rq;
+  std::memset(&rq, 0, sizeof rq);
+  rq.scene = sc.d_desc;
+  rq.env = t.env ? t.env->d_desc : nullptr;
+  rq.cam = t.cam;
+  rq.width = t.w;
+  rq.height = t.h;
+  rq.ambient = std::isfinite(t.opts.ambient) ? std::fmax(t.opts.ambient, 0.0f) : 0.0f;
+  rq.pixel_spread = 2.0f * t.cam.half_h / (float)t.h;
+  rq.orthographic = t.cam.projection == PT_ORTHOGRAPHIC ? 1u : 0u;
+  rq.max_bounces = t.opts.path_trace.max_bounces;
+  rq.rr_start = t.opts.path_trace.rr_start;
+  rq.seed = t.opts.path_trace.seed;
+  rq.strategy = t.opts.path_trace.strategy;
+  rq.clamp = t.opts.path_trace.clamp;
+  rq.p_env = t.env ? (sc.dev.em_count > 0 ? 0.5f : 1.0f) : 0.0f;
+  rq.accum = t.d_accum;
+  return rq;
+}
+
+float4 bg_linear(const pt_render_options &o) {
+  return make_float4(host_srgb_to_linear((float)o.background[0] / 255.0f),
+                     host_srgb_to_linear((float)o.background[1] / 255.0f),
+                     host_srgb_to_linear((float)o.background[2] / 255.0f), (float)o.background[3] / 255.0f);
+}
+
+SceneHost *find_scene(pt_context *ctx, uint32_t id) {
+  auto it = ctx->scenes.find(id);
+  return it == ctx->scenes.end() ? nullptr : it->second.get();
+}
+
+pt_status refine_impl(pt_tracer *t, uint32_t n) {
+  pt_context *ctx = t->ctx;
+  if (!t->have_state || n == 0) return PT_OK;
+  n = std::min(n, 0xffffffffu - t->samples);
+  if (n == 0) return PT_OK;
+  SceneHost *sc = find_scene(ctx, t->scene_id);
+  if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
+  CK(ctx, cudaSetDevice(ctx->device));
+  DevRequest rq = make_request(*t, *sc);
+  CK(ctx, cudaMemcpyAsync(t->d_req, &rq, sizeof rq, cudaMemcpyHostToDevice, ctx->stream));
+  const uint64_t npix = (uint64_t)t->w * t->h;
+  const uint64_t cap = std::max<uint32_t>(ctx->wave_slots, 1024);
+  std::vector<WaveSegment> waves;
+  uint32_t done = 0;
+  while (done < n) {
+    if (npix <= cap) {
+      uint32_t c = (uint32_t)std::min<uint64_t>(n - done, std::max<uint64_t>(cap / npix, 1));
+      waves.push_back(WaveSegment{0, 0, 0, (uint32_t)npix, t->samples + done, c, 0, 0});
+      done += c;
+    } else {
+      for (uint64_t p0 = 0; p0 < npix; p0 += cap)
+        waves.push_back(
+            WaveSegment{0, 0, (uint32_t)p0, (uint32_t)std::min<uint64_t>(cap, npix - p0), t->samples + done, 1, 0, 0});
+      done += 1;
+    }
+  }
+  size_t max_slots = 0;
+  uint32_t max_pix = 0;
+  for (const WaveSegment &w : waves) {
+    max_slots = std::max<size_t>(max_slots, (size_t)w.pixel_count * w.spp);
+    max_pix = std::max(max_pix, w.pixel_count);
+  }
+  pt_status st = ensure(ctx, ctx->d_out, ctx->out_cap, max_slots);
+  if (st != PT_OK) return st;
+  st = ensure(ctx, ctx->d_segs, ctx->seg_cap, waves.size());
+  if (st != PT_OK) return st;
+  CK(ctx, cudaMemcpyAsync(ctx->d_segs, waves.data(), waves.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  CK(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
+  CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  for (size_t i = 0; i < waves.size(); ++i) {
+    uint32_t total = waves[i].pixel_count * waves[i].spp;
+    CK(ctx, launch_megakernel(t->d_req, ctx->d_segs + i, 1, total, ctx->d_out, ctx->d_ctr, ctx->stream));
+    CK(ctx, launch_accumulate(t->d_req, ctx->d_segs + i, 1, waves[i].pixel_count, ctx->d_out, ctx->stream));
+  }
+  CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+  DevCounters c;
+  CK(ctx, cudaMemcpyAsync(&c, ctx->d_ctr, sizeof c, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  CK(ctx, cudaEventElapsedTime(&t->last_ms, ctx->ev0, ctx->ev1));
+  t->ext = c.ext_rays;
+  t->sh = c.shadow_rays;
+  t->nodes = c.nodes;
+  t->tris = c.tris;
+  if (c.error_flags & ERR_STACK_OVERFLOW) return fail(ctx, PT_ERR_DEVICE, "BVH traversal stack overflow");
+  t->samples += n;
+  return PT_OK;
+}
+
+pt_status sync_impl(pt_tracer *t, uint32_t scene_id, const pt_camera *cam, const pt_render_options *opts, int *reset) {
+  pt_context *ctx = t->ctx;
+  pt_status st = validate_opts(ctx, cam, opts);
+  if (st != PT_OK) return st;
+  if (!find_scene(ctx, scene_id)) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene " + std::to_string(scene_id));
+  bool need_prepare = t->dirty || !t->have_state || t->scene_id != scene_id;
+  bool changed = need_prepare || !same_radiance_key(*t, *cam, *opts);
+  t->opts = *opts;
+  t->cam = *cam;
+  if (reset) *reset = changed ? 1 : 0;
+  if (!changed) return PT_OK;
+  CK(ctx, cudaSetDevice(ctx->device));
+  t->scene_id = scene_id;
+  t->w = std::max(opts->width, 1u);
+  t->h = std::max(opts->height, 1u);
+  size_t n = (size_t)t->w * t->h * 4;
+  st = ensure(ctx, t->d_accum, t->accum_cap, n);
+  if (st != PT_OK) return st;
+  CK(ctx, cudaMemsetAsync(t->d_accum, 0, n * sizeof(double), ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  t->samples = 0;
+  t->have_state = true;
+  t->dirty = false;
+  return PT_OK;
+}
+
+pt_status read_impl(pt_tracer *t, void *out, size_t count, bool image) {
+  pt_context *ctx = t->ctx;
+  if (!out) return fail(ctx, PT_ERR_INVALID_ARG, "output pointer is NULL");
+  uint32_t w = t->have_state ? t->w : std::max(t->opts.width, 1u);
+  uint32_t h = t->have_state ? t->h : std::max(t->opts.height, 1u);
+  size_t n = (size_t)w * h;
+  if (count < n * 4) return fail(ctx, PT_ERR_INVALID_ARG, "output buffer too small");
+  float4 bg = bg_linear(t->opts);
+  if (!t->have_state) {
+    for (size_t i = 0; i < n; ++i) {
+      if (image)
+        std::memcpy((uint8_t *)out + 4 * i, t->opts.background, 4);
+      else
+        std::memcpy((float *)out + 4 * i, &bg, sizeof bg);
+    }
+    return PT_OK;
+  }
+  CK(ctx, cudaSetDevice(ctx->device));
+  size_t elem = image ? 4 : 16;
+  if (t->resolve_cap < n * elem) {
+    if (t->d_resolve) cudaFree(t->d_resolve);
+    t->d_resolve = nullptr;
+    t->resolve_cap = 0;
+    CK(ctx, cudaMalloc(&t->d_resolve, n * elem));
+    t->resolve_cap = n * elem;
+  }
+  if (image) {
+    uchar4 bb = make_uchar4(t->opts.background[0], t->opts.background[1], t->opts.background[2],
+                            t->opts.background[3]);
+    CK(ctx, launch_resolve_image(t->d_accum, (uint32_t)n, t->samples, bg, bb, t->opts.tone_map, t->opts.exposure,
+                                 (uchar4 *)t->d_resolve, ctx->stream));
+  } else {
+    CK(ctx, launch_resolve_hdr(t->d_accum, (uint32_t)n, t->samples, bg, (float4 *)t->d_resolve, ctx->stream));
+  }
+  CK(ctx, cudaMemcpyAsync(out, t->d_resolve, n * elem, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return PT_OK;
+}
+
+pt_status set_env_impl(pt_tracer *t, const pt_environment *env) {
+  pt_context *ctx = t->ctx;
+  CK(ctx, cudaSetDevice(ctx->device));
+  if (t->env) {
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    release_env(*t->env);
+    t->env.reset();
+  }
+  if (env) {
+    auto e = std::make_unique<EnvHost>();
+    bool oom = false;
+    std::string err = upload_env(*env, *e, oom);
+    if (!err.empty()) return fail(ctx, oom ? PT_ERR_OOM : PT_ERR_DEVICE, err);
+    t->env = std::move(e);
+  }
+  // PathTracer::set_environment resets the accumulation.
+  t->samples = 0;
+  if (t->have_state && t->d_accum) {
+    CK(ctx, cudaMemsetAsync(t->d_accum, 0, (size_t)t->w * t->h * 4 * sizeof(double), ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return PT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t pt_abi_version(void) { return PT_ABI_VERSION; }
+
+pt_status pt_create(pt_context **out, int device) {
+  if (!out) return fail(nullptr, PT_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  return guard(nullptr, [&]() -> pt_status {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+      return fail(nullptr, PT_ERR_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= count) return fail(nullptr, PT_ERR_INVALID_ARG, "device index out of range");
+    auto ctx = std::make_unique<pt_context>();
+    ctx->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    float sheen[512], thr[255];
+    host_sheen_lut(sheen);
+    host_srgb_thresholds(thr);
+    if (e == cudaSuccess) e = set_tables(sheen, thr);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_ctr, sizeof(DevCounters));
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e != cudaSuccess) {
+      pt_destroy(ctx.release());
+      return fail(nullptr, PT_ERR_DEVICE, std::string("context setup failed: ") + cudaGetErrorString(e));
+    }
+    *out = ctx.release();
+    return PT_OK;
+  });
+}
+
+void pt_destroy(pt_context *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &kv : ctx->scenes) release_scene(*kv.second);
+  ctx->scenes.clear();
+  if (ctx->d_out) cudaFree(ctx->d_out);
+  if (ctx->d_segs) cudaFree(ctx->d_segs);
+  if (ctx->d_ctr) cudaFree(ctx->d_ctr);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char *pt_last_error(const pt_context *ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *scene_id) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (!desc || !scene_id) return fail(ctx, PT_ERR_INVALID_ARG, "desc / scene_id is NULL");
+  return guard(ctx, [&]() -> pt_status {
+    CK(ctx, cudaSetDevice(ctx->device));
+    auto sc = std::make_unique<SceneHost>();
+    bool oom = false;
+    std::string err = upload_scene(*desc, *sc, oom);
+    if (!err.empty()) return fail(ctx, oom ? PT_ERR_OOM : PT_ERR_INVALID_ARG, err);
+    uint32_t id = ctx->next_id++;
+    ctx->scenes[id] = std::move(sc);
+    *scene_id = id;
+    return PT_OK;
+  });
+}
+
+pt_status pt_scene_release(pt_context *ctx, uint32_t scene_id) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  return guard(ctx, [&]() -> pt_status {
+    auto it = ctx->scenes.find(scene_id);
+    if (it == ctx->scenes.end()) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+    CK(ctx, cudaSetDevice(ctx->device));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    release_scene(*it->second);
+    ctx->scenes.erase(it);
+    return PT_OK;
+  });
+}
+
+pt_status pt_scene_device_bytes(pt_context *ctx, uint32_t scene_id, uint64_t *bytes) {
+  if (!ctx || !bytes) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  SceneHost *s = find_scene(ctx, scene_id);
+  if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+  *bytes = s->arena.bytes;
+  return PT_OK;
+}
+
+pt_status pt_scene_triangle_count(pt_context *ctx, uint32_t scene_id, uint64_t *count) {
+  if (!ctx || !count) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  SceneHost *s = find_scene(ctx, scene_id);
+  if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+  *count = s->tri_count;
+  return PT_OK;
+}
+
+pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes, uint32_t *leaves,
+                             uint32_t *max_depth, double *sah_cost, double *build_seconds) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  SceneHost *s = find_scene(ctx, scene_id);
+  if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+  if (nodes) *nodes = s->bvh.nodes;
+  if (leaves) *leaves = s->bvh.leaves;
+  if (max_depth) *max_depth = s->bvh.max_depth;
+  if (sah_cost) *sah_cost = s->bvh.sah_cost;
+  if (build_seconds) *build_seconds = s->bvh.seconds;
+  return PT_OK;
+}
+
+pt_status pt_tracer_create(pt_context *ctx, pt_tracer **out) {
+  if (!ctx || !out) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(ctx, [&]() -> pt_status {
+    auto t = std::make_unique<pt_tracer>();
+    t->ctx = ctx;
+    CK(ctx, cudaSetDevice(ctx->device));
+    CK(ctx, cudaMalloc(&t->d_req, sizeof(DevRequest)));
+    *out = t.release();
+    return PT_OK;
+  });
+}
+
+void pt_tracer_destroy(pt_tracer *t) {
+  if (!t) return;
+  cudaSetDevice(t->ctx->device);
+  cudaStreamSynchronize(t->ctx->stream);
+  if (t->env) release_env(*t->env);
+  if (t->d_accum) cudaFree(t->d_accum);
+  if (t->d_req) cudaFree(t->d_req);
+  if (t->d_resolve) cudaFree(t->d_resolve);
+  delete t;
+}
+
+pt_status pt_tracer_sync(pt_tracer *t, uint32_t scene_id, const pt_camera *camera, const pt_render_options *opts,
+                         int *reset) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  return guard(t->ctx, [&] { return sync_impl(t, scene_id, camera, opts, reset); });
+}
+
+pt_status pt_tracer_refine(pt_tracer *t, uint32_t samples) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  return guard(t->ctx, [&] { return refine_impl(t, samples); });
+}
+
+pt_status pt_tracer_samples(const pt_tracer *t, uint32_t *samples) {
+  if (!t || !samples) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  *samples = t->samples;
+  return PT_OK;
+}
+
+pt_status pt_tracer_is_converged(const pt_tracer *t, int *converged) {
+  if (!t || !converged) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  *converged = t->samples >= t->opts.path_trace.samples_per_pixel ? 1 : 0;
+  return PT_OK;
+}
+
+pt_status pt_tracer_reset(pt_tracer *t) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  return guard(t->ctx, [&]() -> pt_status {
+    pt_context *ctx = t->ctx;
+    t->samples = 0;
+    if (t->have_state && t->d_accum) {
+      CK(ctx, cudaSetDevice(ctx->device));
+      CK(ctx, cudaMemsetAsync(t->d_accum, 0, (size_t)t->w * t->h * 4 * sizeof(double), ctx->stream));
+      CK(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return PT_OK;
+  });
+}
+
+pt_status pt_tracer_invalidate_scene(pt_tracer *t) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  t->dirty = true;
+  return PT_OK;
+}
+
+pt_status pt_tracer_set_environment(pt_tracer *t, const pt_environment *env) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  return guard(t->ctx, [&] { return set_env_impl(t, env); });
+}
+
+pt_status pt_tracer_read_hdr(pt_tracer *t, float *out, size_t n) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  return guard(t->ctx, [&] { return read_impl(t, out, n, false); });
+}
+
+pt_status pt_tracer_read_image(pt_tracer *t, uint8_t *out, size_t n) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  return guard(t->ctx, [&] { return read_impl(t, out, n, true); });
+}
+
+pt_status pt_tracer_read_accum(pt_tracer *t, double *out, size_t n) {
+  if (!t || !out) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(t->ctx, [&]() -> pt_status {
+    pt_context *ctx = t->ctx;
+    size_t need = (size_t)t->w * t->h * 4;
+    if (n < need) return fail(ctx, PT_ERR_INVALID_ARG, "output buffer too small");
+    if (!t->have_state) {
+      std::memset(out, 0, need * sizeof(double));
+      return PT_OK;
+    }
+    CK(ctx, cudaSetDevice(ctx->device));
+    CK(ctx, cudaMemcpyAsync(out, t->d_accum, need * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return PT_OK;
+  });
+}
+
+pt_status pt_tracer_ray_counts(const pt_tracer *t, uint64_t *ext, uint64_t *shadow) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  if (ext) *ext = t->ext;
+  if (shadow) *shadow = t->sh;
+  return PT_OK;
+}
+
+pt_status pt_tracer_traversal_counts(const pt_tracer *t, uint64_t *nodes, uint64_t *tris) {
+  if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
+  if (nodes) *nodes = t->nodes;
+  if (tris) *tris = t->tris;
+  return PT_OK;
+}
+
+pt_status pt_tracer_last_kernel_ms(const pt_tracer *t, float *ms) {
+  if (!t || !ms) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  *ms = t->last_ms;
+  return PT_OK;
+}
+
+static pt_status render_impl(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+                             const pt_render_options *opts, const pt_environment *env, void *out, size_t n,
+                             bool image) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  pt_tracer *t = nullptr;
+  pt_status st = pt_tracer_create(ctx, &t);
+  if (st != PT_OK) return st;
+  std::unique_ptr<pt_tracer, void (*)(pt_tracer *)> hold(t, pt_tracer_destroy);
+  if (env && (st = pt_tracer_set_environment(t, env)) != PT_OK) return st;
+  t->dirty = true;
+  if ((st = pt_tracer_sync(t, scene_id, camera, opts, nullptr)) != PT_OK) return st;
+  if ((st = pt_tracer_refine(t, std::max(opts->path_trace.samples_per_pixel, 1u))) != PT_OK) return st;
+  return image ? pt_tracer_read_image(t, (uint8_t *)out, n) : pt_tracer_read_hdr(t, (float *)out, n);
+}
+
+pt_status pt_render_hdr(pt_context *ctx, uint32_t scene_id, const pt_camera *camera, const pt_render_options *opts,
+                        const pt_environment *env, float *out, size_t n) {
+  return guard(ctx, [&] { return render_impl(ctx, scene_id, camera, opts, env, out, n, false); });
+}
+
+pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *camera, const pt_render_options *opts,
+                          const pt_environment *env, uint8_t *out, size_t n) {
+  return guard(ctx, [&] { return render_impl(ctx, scene_id, camera, opts, env, out, n, true); });
+}
+
+// ---------------------------------------------------------------- debug hooks
+pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (schedule != PT_SCHEDULE_MEGAKERNEL) return fail(ctx, PT_ERR_INVALID_ARG, "unknown schedule");
+  ctx->schedule = schedule;
+  return PT_OK;
+}
+
+pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots) {
+  if (!ctx || slots == 0) return fail(ctx, PT_ERR_INVALID_ARG, "bad argument");
+  ctx->wave_slots = slots;
+  return PT_OK;
+}
+
+pt_status pt_debug_sobol(pt_context *ctx, uint32_t n, uint32_t seed, float *out) {
+  if (!ctx || !out) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(ctx, [&]() -> pt_status {
+    if (n == 0) return PT_OK;
+    CK(ctx, cudaSetDevice(ctx->device));
+    float4 *d = nullptr;
+    CK(ctx, cudaMalloc(&d, (size_t)n * sizeof(float4)));
+    cudaError_t e = launch_debug_sobol(n, seed, d, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, (size_t)n * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    CK(ctx, e);
+    return PT_OK;
+  });
+}
+
+pt_status pt_debug_pattern(pt_tracer *t, uint32_t index, uint32_t pattern, float *out) {
+  if (!t || !out) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(t->ctx, [&]() -> pt_status {
+    pt_context *ctx = t->ctx;
+    if (!t->have_state) return fail(ctx, PT_ERR_INVALID_ARG, "tracer not synced");
+    SceneHost *sc = find_scene(ctx, t->scene_id);
+    if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene not resident");
+    CK(ctx, cudaSetDevice(ctx->device));
+    DevRequest rq = make_request(*t, *sc);
+    CK(ctx, cudaMemcpyAsync(t->d_req, &rq, sizeof rq, cudaMemcpyHostToDevice, ctx->stream));
+    uint32_t npix = t->w * t->h;
+    float4 *d = nullptr;
+    CK(ctx, cudaMalloc(&d, (size_t)npix * sizeof(float4)));
+    cudaError_t e = launch_debug_pattern(t->d_req, npix, index, pattern, d, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out, d, (size_t)npix * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    CK(ctx, e);
+    return PT_OK;
+  });
+}
+
+pt_status pt_debug_primary_hits(pt_tracer *t, uint32_t index, uint32_t *out_g, float *out_tb) {
+  if (!t || !out_g || !out_tb) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(t->ctx, [&]() -> pt_status {
+    pt_context *ctx = t->ctx;
+    if (!t->have_state) return fail(ctx, PT_ERR_INVALID_ARG, "tracer not synced");
+    SceneHost *sc = find_scene(ctx, t->scene_id);
+    if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene not resident");
+    CK(ctx, cudaSetDevice(ctx->device));
+    DevRequest rq = make_request(*t, *sc);
+    CK(ctx, cudaMemcpyAsync(t->d_req, &rq, sizeof rq, cudaMemcpyHostToDevice, ctx->stream));
+    uint32_t npix = t->w * t->h;
+    uint32_t *dg = nullptr;
+    float4 *dt = nullptr;
+    CK(ctx, cudaMalloc(&dg, (size_t)npix * 4));
+    cudaError_t e = cudaMalloc(&dt, (size_t)npix * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream);
+    if (e == cudaSuccess) e = launch_debug_primary(t->d_req, npix, index, dg, dt, ctx->d_ctr, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_g, dg, (size_t)npix * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out_tb, dt, (size_t)npix * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(dg);
+    if (dt) cudaFree(dt);
+    CK(ctx, e);
+    return PT_OK;
+  });
+}
+
+pt_status pt_debug_bsdf(pt_context *ctx, const float *params, const float *dirs, const float *us, uint32_t n,
+                        float *out) {
+  if (!ctx || !params || !dirs || !us || !out) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(ctx, [&]() -> pt_status {
+    if (n == 0) return PT_OK;
+    CK(ctx, cudaSetDevice(ctx->device));
+    float *d = nullptr;
+    size_t fl = 43 + 3 * (size_t)n + 3 * (size_t)n + 12 * (size_t)n;
+    CK(ctx, cudaMalloc(&d, fl * 4));
+    float *dp = d, *dd = d + 43, *du = dd + 3 * (size_t)n, *dout = du + 3 * (size_t)n;
+    cudaError_t e = cudaMemcpyAsync(dp, params, 43 * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dd, dirs, 12 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(du, us, 12 * (size_t)n, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_debug_bsdf(dp, dd, du, n, dout, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, 48 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    CK(ctx, e);
+    return PT_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// Device-resident scene / request layout shared by host and device code.
+//
+// HBM layout of one resident scene (all arrays 256-byte aligned):
+//   nodes     BvhNode[node_count]        64 B  two child boxes + child refs
+//   tris      float4[3 * tri_count]      48 B  leaf-ordered triangle records:
+//                                              (v0.xyz, global id), v1, v2
+//   tri_info  uint2[tri_count]            8 B  (material, attribute flags) by global id
+//   pos       float[9 * tri_count]       36 B  corner positions by global id
+//   nrm/tan/uv[s]/col                          optional corner streams by global id
+//   materials, textures (+ one float4 texel pool for every mip level of
+//   every texture, sRGB and linear chains), lights, emissive table.
+// Per request: the camera, options, an f64 accumulator (32 B / pixel).
+#pragma once
+
+#include <cstdint>
+
+#include <vector_types.h>
+
+#include "../../include/pt_b200.h"
+
+namespace ptd {
+
+// Two-child node, 64 bytes, fetched as four float4:
+//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   d = (child0, child1, count0, count1) as int: child >= 0 is an interior
+//       node index, child < 0 is a leaf whose first triangle record is ~child.
+struct alignas(16) BvhNode {
+  float4 a, b, c;
+  int4 d;
+};
+
+enum TriFlags : uint32_t {
+  TRI_HAS_VN = 1u << 0,       // has_vertex_normals and a normal stream
+  TRI_HAS_TANGENTS = 1u << 1,
+  TRI_HAS_COLORS = 1u << 2,
+  TRI_UV0 = 1u << 3,          // TRI_UV0 << s: UV set s present
+};
+
+// Triangle record flags (second record's w): what the any-hit filter needs
+// without touching the material table.
+enum RecordFlags : uint32_t { REC_OPAQUE = 1u, REC_DOUBLE_SIDED = 2u };
+
+constexpr int kMaxMipLevels = 16;
+
+struct DevTexture {
+  uint32_t img_w, img_h, levels;
+  uint32_t mag, min, wrap_s, wrap_t, pad;
+  uint32_t lw[kMaxMipLevels], lh[kMaxMipLevels];
+  uint64_t srgb_off[kMaxMipLevels], lin_off[kMaxMipLevels];  // texel offsets into the pool
+};
+
+// pt_material plus values the host precomputes so the device never
+// evaluates a transcendental of a scene constant.
+struct DevMaterial {
+  pt_material m;
+  float aniso_sin, aniso_cos;  // sin / cos of fin(anisotropy_rotation, 0)
+  uint32_t emissive_nonblack;  // !is_black(emissive)
+  uint32_t pad;
+};
+
+struct DevLight {
+  pt_light l;
+  float cos_outer, cos_inner;  // spot cone cosines
+};
+
+struct DevScene {
+  const BvhNode *nodes;
+  const float4 *tris;
+  const uint2 *tri_info;
+  const float *pos, *nrm, *tan, *uv[PT_MAX_UV_SETS], *col;
+  const DevMaterial *materials;
+  const DevTexture *textures;
+  const float4 *texels;
+  const DevLight *lights;
+  const uint32_t *em_tris;
+  const float *em_pmf, *em_cdf;
+  const uint32_t *em_lookup;
+  uint32_t node_count, tri_count, material_count, texture_count, light_count, em_count;
+  uint32_t max_depth, pad;
+};
+
+struct DevEnv {
+  uint32_t w, h, uniform, pad;
+  float intensity, pad1, pad2, pad3;
+  const float4 *pixels;       // w * h texels (scene-linear RGBA)
+  const float *marginal;      // h + 1
+  const float *conditional;   // h * (w + 1)
+  const float *mass;          // w * h
+};
+
+// Everything one accumulation needs (the reference's Integrator,
+// src/pathtrace.rs:1878-1890): scene, environment, camera, options.
+struct DevRequest {
+  const DevScene *scene;
+  const DevEnv *env;  // nullptr: constant sky `ambient`
+  pt_camera cam;
+  uint32_t width, height;
+  float ambient, pixel_spread;
+  uint32_t orthographic, max_bounces, rr_start, seed, strategy;
+  float clamp;
+  float p_env;  // probability the area-light sampler picks the environment
+  uint32_t pad;
+  double *accum;  // width * height * 4 (sum r, g, b, covered count)
+};
+
+// A contiguous run of path slots of one request within a wave: slot
+// `slot_begin + s * pixel_count + i` traces sample `sample_begin + s` of
+// pixel `pixel_begin + i` (i < pixel_count, s < spp).
+struct WaveSegment {
+  uint32_t request;
+  uint32_t slot_begin;
+  uint32_t pixel_begin, pixel_count;
+  uint32_t sample_begin, spp;
+  uint32_t pad0, pad1;
+};
+
+// Per-launch device counters (rays traced, traversal work, errors).
+struct DevCounters {
+  unsigned long long ext_rays, shadow_rays, nodes, tris;
+  unsigned int error_flags, pad;
+};
+enum ErrorFlags : uint32_t { ERR_STACK_OVERFLOW = 1u };
+
+}  // namespace ptd

@@ -1,0 +1,853 @@
+// Host-side scene preparation and upload (see host_scene.h).
+//
+// Reference behaviour restated here (host side, computed once per scene):
+//   - TraceScene soup + TriRef order (src/trace.rs:328-351): global triangle
+//     ids follow item order, then triangle order within an item;
+//   - build_mips (src/texture.rs:324-383) for the sRGB and linear chains;
+//   - EmissiveLights::build (src/pathtrace.rs:1479-1543), f64 CDF;
+//   - EnvironmentMap::new (src/pathtrace.rs:1575-1638), f64 CDFs;
+//   - sheen_lut (src/pathtrace.rs:645-674) and the sRGB byte thresholds
+//     (src/hdr.rs:116-129).
+// The BVH is this library's own: binned SAH (Wald, "On fast Construction of
+// SAH-based Bounding Volume Hierarchies", 2007), built in parallel over
+// subtrees, emitted depth-first as two-child nodes.
+#include "host_scene.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <thread>
+
+#include <cuda_runtime.h>
+
+namespace ptd {
+
+// ============================================================ tables
+float host_srgb_to_linear(float c) {
+  if (c <= 0.04045f) return c / 12.92f;
+  return std::pow((c + 0.055f) / 1.055f, 2.4f);
+}
+void host_srgb_thresholds(float out[255]) {
+  for (int k = 0; k < 255; ++k) out[k] = host_srgb_to_linear(((float)k + 0.5f) / 255.0f);
+}
+
+static float h_d_charlie(float n_dot_h, float a) {
+  float inv = 1.0f / std::fmax(a, 1.0e-3f);
+  float sin2 = std::fmax(1.0f - n_dot_h * n_dot_h, 0.0f);
+  return (2.0f + inv) * std::pow(sin2, inv * 0.5f) / (2.0f * 3.14159265358979323846f);
+}
+static float h_v_neubelt(float nl, float nv) { return 1.0f / std::fmax(4.0f * (nl + nv - nl * nv), 1.0e-6f); }
+void host_sheen_lut(float out[512]) {
+  const float PI = 3.14159265358979323846f, HALF_PI = 1.57079632679489661923f;
+  const int nt = 48, np = 24, NC = 32, NR = 16;
+  for (int ri = 0; ri < NR; ++ri) {
+    float r = (float)ri / (float)(NR - 1);
+    float a = std::fmax(r * r, 1.0e-3f);
+    for (int ci = 0; ci < NC; ++ci) {
+      float cv = std::fmax(((float)ci + 0.5f) / (float)NC, 1.0e-3f);
+      float v[3] = {std::sqrt(1.0f - cv * cv), 0.0f, cv};
+      float sum = 0.0f;
+      for (int i = 0; i < nt; ++i) {
+        float th = ((float)i + 0.5f) / (float)nt * HALF_PI;
+        float st = std::sin(th), ct = std::cos(th);
+        for (int j = 0; j < np; ++j) {
+          float ph = ((float)j + 0.5f) / (float)np * PI;
+          float l[3] = {st * std::cos(ph), st * std::sin(ph), ct};
+          float h[3] = {v[0] + l[0], v[1] + l[1], v[2] + l[2]};
+          float len = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+          float hz = len < 1.1920929e-07f ? 0.0f : h[2] / len;
+          float f = h_d_charlie(hz, a) * h_v_neubelt(ct, cv);
+          sum += f * ct * st;
+        }
+      }
+      float dw = (HALF_PI / (float)nt) * (PI / (float)np) * 2.0f;
+      float x = sum * dw;
+      out[ri * NC + ci] = x < 0.0f ? 0.0f : (x > 1.0f ? 1.0f : x);
+    }
+  }
+}
+
+// ============================================================ BVH build
+namespace {
+
+struct BNode {
+  float lo[3], hi[3];
+  uint32_t left;         // interior: children left, left + 1
+  uint32_t first, count;  // leaf when count > 0
+};
+
+struct Builder {
+  const float *pos;
+  uint32_t n;
+  std::vector<float> cen;    // 3 per tri
+  std::vector<float> blo, bhi;
+  std::vector<uint32_t> idx;
+  std::vector<BNode> nodes;
+  std::atomic<uint32_t> node_count{1};
+  std::atomic<uint32_t> max_depth{0};
+
+  struct Task {
+    uint32_t node, begin, end, depth;
+  };
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Task> stack;
+  int active = 0;
+  bool done = false;
+
+  static constexpr int kBins = 16;
+  static constexpr uint32_t kMaxLeaf = 8;
+  static constexpr uint32_t kLocalThreshold = 32768;
+
+  static float area(const float lo[3], const float hi[3]) {
+    float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    if (!(dx >= 0.0f) || !(dy >= 0.0f) || !(dz >= 0.0f)) return 0.0f;
+    return dx * dy + dy * dz + dz * dx;
+  }
+
+  void make_leaf(BNode &nd, uint32_t b, uint32_t e) {
+    nd.first = b;
+    nd.count = e - b;
+    nd.left = 0;
+  }
+
+  // Processes one node; returns the child tasks (0 or 2).
+  int split(const Task &t, Task out[2]) {
+    BNode &nd = nodes[t.node];
+    uint32_t cnt = t.end - t.begin;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = t.begin; i < t.end; ++i) {
+      uint32_t g = idx[i];
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], blo[3 * g + k]);
+        hi[k] = std::max(hi[k], bhi[3 * g + k]);
+        clo[k] = std::min(clo[k], cen[3 * g + k]);
+        chi[k] = std::max(chi[k], cen[3 * g + k]);
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      nd.lo[k] = lo[k];
+      nd.hi[k] = hi[k];
+    }
+    uint32_t d = max_depth.load(std::memory_order_relaxed);
+    while (t.depth > d && !max_depth.compare_exchange_weak(d, t.depth)) {
+    }
+    if (cnt <= 1) {
+      make_leaf(nd, t.begin, t.end);
+      return 0;
+    }
+    // Keep the tree shallow enough for a 64-entry traversal stack: near
+    // the limit, split at the object median (halves the count per level).
+    uint32_t need = 0;
+    for (uint32_t c = cnt; c > kMaxLeaf; c = (c + 1) / 2) ++need;
+    bool median = t.depth + need >= 56;
+    int axis = -1;
+    uint32_t mid = 0;
+    int best_bin = 0;
+    float best_cost = INFINITY;
+    if (!median) {
+      float parent = area(lo, hi);
+      for (int k = 0; k < 3; ++k) {
+        float span = chi[k] - clo[k];
+        if (!(span > 0.0f)) continue;
+        float scale = (float)kBins / span;
+        uint32_t bc[kBins] = {0};
+        float bl[kBins][3], bh[kBins][3];
+        for (int b = 0; b < kBins; ++b)
+          for (int a = 0; a < 3; ++a) {
+            bl[b][a] = INFINITY;
+            bh[b][a] = -INFINITY;
+          }
+        for (uint32_t i = t.begin; i < t.end; ++i) {
+          uint32_t g = idx[i];
+          int b = std::min(kBins - 1, (int)((cen[3 * g + k] - clo[k]) * scale));
+          bc[b]++;
+          for (int a = 0; a < 3; ++a) {
+            bl[b][a] = std::min(bl[b][a], blo[3 * g + a]);
+            bh[b][a] = std::max(bh[b][a], bhi[3 * g + a]);
+          }
+        }
+        float rl[kBins][3], rh[kBins][3];
+        uint32_t rc[kBins];
+        float accl[3] = {INFINITY, INFINITY, INFINITY}, acch[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t acc = 0;
+        for (int b = kBins - 1; b >= 1; --b) {
+          acc += bc[b];
+          for (int a = 0; a < 3; ++a) {
+            accl[a] = std::min(accl[a], bl[b][a]);
+            acch[a] = std::max(acch[a], bh[b][a]);
+          }
+          rc[b] = acc;
+          for (int a = 0; a < 3; ++a) {
+            rl[b][a] = accl[a];
+            rh[b][a] = acch[a];
+          }
+        }
+        float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t lc = 0;
+        for (int s = 1; s < kBins; ++s) {
+          lc += bc[s - 1];
+          for (int a = 0; a < 3; ++a) {
+            ll[a] = std::min(ll[a], bl[s - 1][a]);
+            lh[a] = std::max(lh[a], bh[s - 1][a]);
+          }
+          if (lc == 0 || rc[s] == 0) continue;
+          float cost = 1.0f + (area(ll, lh) * (float)lc + area(rl[s], rh[s]) * (float)rc[s]) / std::max(parent, 1e-30f);
+          if (cost < best_cost) {
+            best_cost = cost;
+            axis = k;
+            best_bin = s;
+          }
+        }
+      }
+      if (cnt <= kMaxLeaf && (axis < 0 || (float)cnt <= best_cost)) {
+        make_leaf(nd, t.begin, t.end);
+        return 0;
+      }
+    }
+    if (axis >= 0) {
+      float span = chi[axis] - clo[axis];
+      float scale = (float)kBins / span;
+      auto it = std::partition(idx.begin() + t.begin, idx.begin() + t.end, [&](uint32_t g) {
+        return std::min(kBins - 1, (int)((cen[3 * g + axis] - clo[axis]) * scale)) < best_bin;
+      });
+      mid = (uint32_t)(it - idx.begin());
+    }
+    if (axis < 0 || mid == t.begin || mid == t.end) {
+      // Object median along the widest centroid axis (or index halves when
+      // every centroid coincides).
+      int ax = 0;
+      float w = chi[0] - clo[0];
+      for (int k = 1; k < 3; ++k)
+        if (chi[k] - clo[k] > w) {
+          w = chi[k] - clo[k];
+          ax = k;
+        }
+      mid = t.begin + cnt / 2;
+      if (w > 0.0f)
+        std::nth_element(idx.begin() + t.begin, idx.begin() + mid, idx.begin() + t.end,
+                         [&](uint32_t a, uint32_t b) { return cen[3 * a + ax] < cen[3 * b + ax]; });
+    }
+    uint32_t c = node_count.fetch_add(2);
+    nd.left = c;
+    nd.count = 0;
+    out[0] = {c, t.begin, mid, t.depth + 1};
+    out[1] = {c + 1, mid, t.end, t.depth + 1};
+    return 2;
+  }
+
+  void local_build(Task t) {
+    std::vector<Task> st{t};
+    while (!st.empty()) {
+      Task cur = st.back();
+      st.pop_back();
+      Task ch[2];
+      if (split(cur, ch) == 2) {
+        st.push_back(ch[1]);
+        st.push_back(ch[0]);
+      }
+    }
+  }
+
+  void worker() {
+    for (;;) {
+      Task t;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return done || !stack.empty(); });
+        if (stack.empty()) return;
+        t = stack.back();
+        stack.pop_back();
+        ++active;
+      }
+      if (t.end - t.begin <= kLocalThreshold) {
+        local_build(t);
+      } else {
+        Task ch[2];
+        if (split(t, ch) == 2) {
+          std::lock_guard<std::mutex> lk(mu);
+          stack.push_back(ch[0]);
+          stack.push_back(ch[1]);
+          cv.notify_all();
+        }
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        --active;
+        if (active == 0 && stack.empty()) {
+          done = true;
+          cv.notify_all();
+        }
+      }
+    }
+  }
+
+  void run(int threads) {
+    nodes.resize(std::max<size_t>(2 * (size_t)n, 1));
+    if (threads <= 1 || n <= kLocalThreshold) {
+      local_build({0, 0, n, 0});
+    } else {
+      stack.push_back({0, 0, n, 0});
+      std::vector<std::thread> pool;
+      for (int i = 0; i < threads; ++i) pool.emplace_back([this] { worker(); });
+      for (auto &th : pool) th.join();
+    }
+    nodes.resize(node_count.load());
+  }
+};
+
+void pad_box(const float lo[3], const float hi[3], float plo[3], float phi[3]) {
+  float ext = 0.0f;
+  for (int k = 0; k < 3; ++k)
+    ext = std::max({ext, hi[k] - lo[k], std::fabs(lo[k]), std::fabs(hi[k])});
+  float pad = ext * 1.0e-5f + 1.0e-30f;
+  for (int k = 0; k < 3; ++k) {
+    plo[k] = lo[k] - pad;
+    phi[k] = hi[k] + pad;
+  }
+}
+
+}  // namespace
+
+void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
+               std::vector<float4> &records, BvhBuildStats &stats, int threads) {
+  auto t0 = std::chrono::steady_clock::now();
+  out_nodes.clear();
+  records.clear();
+  stats = BvhBuildStats{};
+  if (tri_count == 0) return;
+  Builder b;
+  b.pos = pos;
+  b.n = tri_count;
+  b.cen.resize(3 * (size_t)tri_count);
+  b.blo.resize(3 * (size_t)tri_count);
+  b.bhi.resize(3 * (size_t)tri_count);
+  b.idx.resize(tri_count);
+  std::iota(b.idx.begin(), b.idx.end(), 0u);
+  for (size_t g = 0; g < tri_count; ++g) {
+    const float *p = pos + 9 * g;
+    for (int k = 0; k < 3; ++k) {
+      float lo = std::min({p[k], p[3 + k], p[6 + k]}), hi = std::max({p[k], p[3 + k], p[6 + k]});
+      b.blo[3 * g + k] = lo;
+      b.bhi[3 * g + k] = hi;
+      b.cen[3 * g + k] = (lo + hi) * 0.5f;
+    }
+  }
+  b.run(std::max(1, threads));
+
+  // Depth-first two-child layout.
+  auto leaf_ref = [](uint32_t first, uint32_t count) { return (int)~(first | (count << 27)); };
+  std::vector<uint32_t> gstack;
+  const BNode &root = b.nodes[0];
+  auto child_box = [&](const BNode &c, float lo[3], float hi[3]) { pad_box(c.lo, c.hi, lo, hi); };
+  auto fill = [&](BvhNode &gn, const BNode &c0, const BNode &c1, int r0, int r1) {
+    float l0[3], h0[3], l1[3], h1[3];
+    child_box(c0, l0, h0);
+    child_box(c1, l1, h1);
+    gn.a = make_float4(l0[0], h0[0], l0[1], h0[1]);
+    gn.b = make_float4(l1[0], h1[0], l1[1], h1[1]);
+    gn.c = make_float4(l0[2], h0[2], l1[2], h1[2]);
+    gn.d = make_int4(r0, r1, (int)c0.count, (int)c1.count);
+  };
+  if (root.count > 0) {
+    BvhNode gn;
+    BNode empty = root;
+    empty.count = 0;
+    fill(gn, root, root, leaf_ref(root.first, root.count), leaf_ref(root.first, 0));
+    out_nodes.push_back(gn);
+    stats.leaves = 1;
+  } else {
+    // Iterative DFS: each interior binary node becomes one GPU node.
+    struct Item {
+      uint32_t bin, gpu;
+    };
+    std::vector<Item> st;
+    out_nodes.push_back(BvhNode{});
+    st.push_back({0, 0});
+    while (!st.empty()) {
+      Item it = st.back();
+      st.pop_back();
+      const BNode &nd = b.nodes[it.bin];
+      const BNode &c0 = b.nodes[nd.left];
+      const BNode &c1 = b.nodes[nd.left + 1];
+      int r[2];
+      const BNode *cs[2] = {&c0, &c1};
+      for (int k = 0; k < 2; ++k) {
+        if (cs[k]->count > 0) {
+          r[k] = leaf_ref(cs[k]->first, cs[k]->count);
+          stats.leaves++;
+        } else {
+          r[k] = (int)out_nodes.size();
+          out_nodes.push_back(BvhNode{});
+        }
+      }
+      fill(out_nodes[it.gpu], c0, c1, r[0], r[1]);
+      // Right first on the stack so the left subtree is laid out first.
+      if (cs[1]->count == 0) st.push_back({nd.left + 1, (uint32_t)r[1]});
+      if (cs[0]->count == 0) st.push_back({nd.left, (uint32_t)r[0]});
+    }
+  }
+  records.resize(3 * (size_t)tri_count);
+  for (size_t i = 0; i < tri_count; ++i) {
+    uint32_t g = b.idx[i];
+    const float *p = pos + 9 * (size_t)g;
+    float gid, fl;
+    std::memcpy(&gid, &g, 4);
+    uint32_t f = rec_flags ? rec_flags[g] : 0u;
+    std::memcpy(&fl, &f, 4);
+    records[3 * i] = make_float4(p[0], p[1], p[2], gid);
+    records[3 * i + 1] = make_float4(p[3], p[4], p[5], fl);
+    records[3 * i + 2] = make_float4(p[6], p[7], p[8], 0.0f);
+  }
+  stats.nodes = (uint32_t)out_nodes.size();
+  stats.max_depth = b.max_depth.load();
+  // SAH cost of the tree (traversal 1, intersection 1, relative to the root box).
+  double root_area = Builder::area(b.nodes[0].lo, b.nodes[0].hi);
+  double cost = 0.0;
+  for (const BNode &nd : b.nodes) {
+    double a = Builder::area(nd.lo, nd.hi) / std::max(root_area, 1e-30);
+    cost += nd.count > 0 ? a * nd.count : a;
+  }
+  stats.sah_cost = cost;
+  stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ============================================================ arena
+void DeviceArena::release() {
+  if (base) cudaFree(base);
+  base = nullptr;
+  bytes = 0;
+}
+
+namespace {
+
+struct ArenaPlan {
+  std::vector<std::pair<const void *, size_t>> parts;  // host source, bytes
+  std::vector<size_t> offsets;
+  size_t total = 0;
+  size_t add(const void *src, size_t bytes) {
+    size_t off = (total + 255) & ~(size_t)255;
+    parts.push_back({src, bytes});
+    offsets.push_back(off);
+    total = off + bytes;
+    return parts.size() - 1;
+  }
+};
+
+std::string commit(ArenaPlan &plan, DeviceArena &arena, bool &oom) {
+  if (plan.total == 0) plan.total = 256;
+  cudaError_t e = cudaMalloc(&arena.base, plan.total);
+  if (e != cudaSuccess) {
+    oom = e == cudaErrorMemoryAllocation;
+    arena.base = nullptr;
+    return std::string("cudaMalloc of ") + std::to_string(plan.total) + " bytes failed: " + cudaGetErrorString(e);
+  }
+  arena.bytes = plan.total;
+  std::vector<uint8_t> staging(plan.total, 0);
+  for (size_t i = 0; i < plan.parts.size(); ++i)
+    if (plan.parts[i].second) std::memcpy(staging.data() + plan.offsets[i], plan.parts[i].first, plan.parts[i].second);
+  e = cudaMemcpy(arena.base, staging.data(), plan.total, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return std::string("scene upload failed: ") + cudaGetErrorString(e);
+  return "";
+}
+
+template <class T>
+const T *dptr(const DeviceArena &a, const ArenaPlan &p, size_t part) {
+  return reinterpret_cast<const T *>(static_cast<uint8_t *>(a.base) + p.offsets[part]);
+}
+
+struct MipChain {
+  std::vector<uint32_t> w, h;
+  std::vector<std::vector<float4>> levels;
+};
+
+void build_mips(const pt_texture &img, bool srgb, MipChain &out) {
+  static float lut[256];
+  static bool init = [] {
+    for (int i = 0; i < 256; ++i) lut[i] = host_srgb_to_linear((float)i / 255.0f);
+    return true;
+  }();
+  (void)init;
+  size_t n = (size_t)img.width * img.height;
+  std::vector<float4> l0(n);
+  if (img.format == PT_PIXELS_RGBA8) {
+    const uint8_t *p = (const uint8_t *)img.pixels;
+    for (size_t i = 0; i < n; ++i) {
+      auto c = [&](uint8_t v) { return srgb ? lut[v] : (float)v / 255.0f; };
+      l0[i] = make_float4(c(p[4 * i]), c(p[4 * i + 1]), c(p[4 * i + 2]), (float)p[4 * i + 3] / 255.0f);
+    }
+  } else {
+    const float *p = (const float *)img.pixels;
+    for (size_t i = 0; i < n; ++i) l0[i] = make_float4(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
+  }
+  out.w.push_back(img.width);
+  out.h.push_back(img.height);
+  out.levels.push_back(std::move(l0));
+  for (;;) {
+    uint32_t pw = out.w.back(), ph = out.h.back();
+    if (pw == 1 && ph == 1) break;
+    uint32_t w = std::max(pw / 2, 1u), h = std::max(ph / 2, 1u);
+    const std::vector<float4> &prev = out.levels.back();
+    std::vector<float4> nx((size_t)w * h);
+    for (uint32_t y = 0; y < h; ++y)
+      for (uint32_t x = 0; x < w; ++x) {
+        size_t x0 = std::min(2 * x, pw - 1), x1 = std::min(2 * x + 1, pw - 1);
+        size_t y0 = std::min(2 * y, ph - 1), y1 = std::min(2 * y + 1, ph - 1);
+        const float4 *q[4] = {&prev[y0 * pw + x0], &prev[y0 * pw + x1], &prev[y1 * pw + x0], &prev[y1 * pw + x1]};
+        float acc[4] = {0, 0, 0, 0};
+        for (const float4 *t : q) {
+          acc[0] += t->x;
+          acc[1] += t->y;
+          acc[2] += t->z;
+          acc[3] += t->w;
+        }
+        nx[(size_t)y * w + x] = make_float4(acc[0] * 0.25f, acc[1] * 0.25f, acc[2] * 0.25f, acc[3] * 0.25f);
+      }
+    out.w.push_back(w);
+    out.h.push_back(h);
+    out.levels.push_back(std::move(nx));
+  }
+}
+
+}  // namespace
+
+// ============================================================ scene upload
+std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
+  oom = false;
+  if (desc.item_count && !desc.items) return "pt_scene_desc.items is NULL";
+  if (desc.material_count == 0 || !desc.materials) return "pt_scene_desc needs at least one material";
+  if (desc.texture_count && !desc.textures) return "pt_scene_desc.textures is NULL";
+  if (desc.light_count && !desc.lights) return "pt_scene_desc.lights is NULL";
+  uint64_t T = 0;
+  for (uint32_t i = 0; i < desc.item_count; ++i) {
+    const pt_draw_item &it = desc.items[i];
+    if (it.triangle_count && !it.positions) return "item " + std::to_string(i) + " has no positions";
+    if (it.material >= desc.material_count) return "item " + std::to_string(i) + " material index out of range";
+    T += it.triangle_count;
+  }
+  if (T >= (1ull << 27)) return "scene has " + std::to_string(T) + " triangles; the limit is 134217727";
+  const uint32_t tc = (uint32_t)T;
+
+  // Textures: mip chains in one texel pool.
+  std::vector<DevTexture> texs(desc.texture_count);
+  std::vector<float4> pool;
+  std::vector<bool> tex_ok(desc.texture_count, false);
+  for (uint32_t i = 0; i < desc.texture_count; ++i) {
+    const pt_texture &t = desc.textures[i];
+    DevTexture &d = texs[i];
+    std::memset(&d, 0, sizeof d);
+    if (!t.pixels || t.width == 0 || t.height == 0) continue;
+    if (t.format > PT_PIXELS_RGBA_F32) return "texture " + std::to_string(i) + " has an unknown pixel format";
+    MipChain s, l;
+    build_mips(t, true, s);
+    build_mips(t, false, l);
+    if (s.levels.size() > (size_t)kMaxMipLevels) return "texture " + std::to_string(i) + " is too large";
+    d.img_w = t.width;
+    d.img_h = t.height;
+    d.levels = (uint32_t)s.levels.size();
+    d.mag = t.mag_filter;
+    d.min = t.min_filter;
+    d.wrap_s = t.wrap_s;
+    d.wrap_t = t.wrap_t;
+    for (uint32_t k = 0; k < d.levels; ++k) {
+      d.lw[k] = s.w[k];
+      d.lh[k] = s.h[k];
+      d.srgb_off[k] = pool.size();
+      pool.insert(pool.end(), s.levels[k].begin(), s.levels[k].end());
+      d.lin_off[k] = pool.size();
+      pool.insert(pool.end(), l.levels[k].begin(), l.levels[k].end());
+    }
+    tex_ok[i] = true;
+  }
+  auto fix_binding = [&](pt_texture_binding &b) {
+    if (b.texture >= 0 && ((uint32_t)b.texture >= desc.texture_count || !tex_ok[b.texture])) b.texture = -1;
+  };
+
+  // Materials.
+  std::vector<DevMaterial> mats(desc.material_count);
+  for (uint32_t m = 0; m < desc.material_count; ++m) {
+    DevMaterial &dm = mats[m];
+    std::memset(&dm, 0, sizeof dm);
+    dm.m = desc.materials[m];
+    pt_texture_binding *bs[] = {&dm.m.base_color_texture, &dm.m.metallic_roughness_texture, &dm.m.normal_texture,
+                                &dm.m.occlusion_texture, &dm.m.emissive_texture, &dm.m.specular_texture,
+                                &dm.m.specular_color_texture, &dm.m.transmission_texture, &dm.m.thickness_texture,
+                                &dm.m.clearcoat_texture, &dm.m.clearcoat_roughness_texture,
+                                &dm.m.clearcoat_normal_texture, &dm.m.sheen_color_texture,
+                                &dm.m.sheen_roughness_texture, &dm.m.anisotropy_texture, &dm.m.iridescence_texture,
+                                &dm.m.iridescence_thickness_texture, &dm.m.diffuse_transmission_texture,
+                                &dm.m.diffuse_transmission_color_texture};
+    for (pt_texture_binding *b : bs) fix_binding(*b);
+    float rot = std::isfinite(dm.m.anisotropy_rotation) ? dm.m.anisotropy_rotation : 0.0f;
+    dm.aniso_sin = std::sin(rot);
+    dm.aniso_cos = std::cos(rot);
+    dm.emissive_nonblack = (dm.m.emissive[0] > 0.0f || dm.m.emissive[1] > 0.0f || dm.m.emissive[2] > 0.0f) ? 1u : 0u;
+  }
+
+  // Attribute streams by global triangle id.
+  bool any_vn = false, any_tan = false, any_col = false, any_uv[PT_MAX_UV_SETS] = {false, false, false, false};
+  for (uint32_t i = 0; i < desc.item_count; ++i) {
+    const pt_draw_item &it = desc.items[i];
+    any_vn |= it.normals && it.has_vertex_normals;
+    any_tan |= it.tangents != nullptr;
+    any_col |= it.colors != nullptr;
+    for (int s = 0; s < PT_MAX_UV_SETS; ++s) any_uv[s] |= it.uvs[s] != nullptr;
+  }
+  std::vector<float> pos(9 * (size_t)tc), nrm(any_vn ? 9 * (size_t)tc : 0), tan(any_tan ? 12 * (size_t)tc : 0),
+      col(any_col ? 12 * (size_t)tc : 0);
+  std::vector<float> uv[PT_MAX_UV_SETS];
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s)
+    if (any_uv[s]) uv[s].assign(6 * (size_t)tc, 0.0f);
+  std::vector<uint2> info(tc);
+  std::vector<uint32_t> rec_flags(tc);
+  size_t g0 = 0;
+  for (uint32_t i = 0; i < desc.item_count; ++i) {
+    const pt_draw_item &it = desc.items[i];
+    size_t n = it.triangle_count;
+    std::memcpy(pos.data() + 9 * g0, it.positions, 36 * n);
+    uint32_t flags = 0;
+    if (it.normals && it.has_vertex_normals) {
+      std::memcpy(nrm.data() + 9 * g0, it.normals, 36 * n);
+      flags |= TRI_HAS_VN;
+    }
+    if (it.tangents) {
+      std::memcpy(tan.data() + 12 * g0, it.tangents, 48 * n);
+      flags |= TRI_HAS_TANGENTS;
+    }
+    if (it.colors) {
+      std::memcpy(col.data() + 12 * g0, it.colors, 48 * n);
+      flags |= TRI_HAS_COLORS;
+    }
+    for (int s = 0; s < PT_MAX_UV_SETS; ++s)
+      if (it.uvs[s]) {
+        std::memcpy(uv[s].data() + 6 * g0, it.uvs[s], 24 * n);
+        flags |= TRI_UV0 << s;
+      }
+    const pt_material &mm = desc.materials[it.material];
+    uint32_t rf = (mm.alpha_mode == PT_ALPHA_OPAQUE ? REC_OPAQUE : 0u) | (mm.double_sided ? REC_DOUBLE_SIDED : 0u);
+    for (size_t t = 0; t < n; ++t) {
+      info[g0 + t] = make_uint2(it.material, flags);
+      rec_flags[g0 + t] = rf;
+    }
+    g0 += n;
+  }
+
+  // BVH.
+  std::vector<BvhNode> nodes;
+  std::vector<float4> records;
+  int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  build_bvh(pos.data(), tc, rec_flags.data(), nodes, records, out.bvh, threads);
+
+  // Lights.
+  std::vector<DevLight> lights(desc.light_count);
+  for (uint32_t j = 0; j < desc.light_count; ++j) {
+    lights[j].l = desc.lights[j];
+    lights[j].cos_outer = std::cos(desc.lights[j].outer_cone_angle);
+    lights[j].cos_inner = std::cos(desc.lights[j].inner_cone_angle);
+  }
+
+  // EmissiveLights::build.
+  std::vector<float> mean_e(3 * (size_t)desc.material_count);
+  for (uint32_t m = 0; m < desc.material_count; ++m) {
+    const pt_material &mt = mats[m].m;
+    float e[3] = {0.0f, 0.0f, 0.0f};
+    if (!mt.unlit) {
+      e[0] = mt.emissive[0];
+      e[1] = mt.emissive[1];
+      e[2] = mt.emissive[2];
+      int ti = mt.emissive_texture.texture;
+      if (ti >= 0) {
+        const DevTexture &d = texs[ti];
+        const float4 &c = pool[d.srgb_off[d.levels - 1]];
+        e[0] = e[0] * c.x;
+        e[1] = e[1] * c.y;
+        e[2] = e[2] * c.z;
+      }
+    }
+    std::memcpy(&mean_e[3 * m], e, sizeof e);
+  }
+  std::vector<uint32_t> em_tris, em_lookup(tc, 0xffffffffu);
+  std::vector<float> power;
+  for (uint32_t g = 0; g < tc; ++g) {
+    const float *e = &mean_e[3 * (size_t)info[g].x];
+    float lum = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2];
+    if (std::isnan(lum) || lum <= 0.0f) continue;
+    const float *p = pos.data() + 9 * (size_t)g;
+    float e1[3] = {p[3] - p[0], p[4] - p[1], p[5] - p[2]}, e2[3] = {p[6] - p[0], p[7] - p[1], p[8] - p[2]};
+    float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    float ar = 0.5f * std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    if (std::isnan(ar) || ar <= 0.0f || !std::isfinite(ar)) continue;
+    float sides = mats[info[g].x].m.double_sided ? 2.0f : 1.0f;
+    em_lookup[g] = (uint32_t)em_tris.size();
+    em_tris.push_back(g);
+    power.push_back(ar * lum * sides);
+  }
+  double total = 0.0;
+  for (float p : power) total += (double)p;
+  std::vector<float> pmf, cdf;
+  double acc = 0.0;
+  for (float pw : power) {
+    pmf.push_back((float)((double)pw / total));
+    acc += (double)pw / total;
+    cdf.push_back((float)acc);
+  }
+  if (!cdf.empty()) cdf.back() = 1.0f;
+
+  // One arena.
+  ArenaPlan plan;
+  size_t p_nodes = plan.add(nodes.data(), nodes.size() * sizeof(BvhNode));
+  size_t p_rec = plan.add(records.data(), records.size() * sizeof(float4));
+  size_t p_info = plan.add(info.data(), info.size() * sizeof(uint2));
+  size_t p_pos = plan.add(pos.data(), pos.size() * 4);
+  size_t p_nrm = plan.add(nrm.data(), nrm.size() * 4);
+  size_t p_tan = plan.add(tan.data(), tan.size() * 4);
+  size_t p_col = plan.add(col.data(), col.size() * 4);
+  size_t p_uv[PT_MAX_UV_SETS];
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s) p_uv[s] = plan.add(uv[s].data(), uv[s].size() * 4);
+  size_t p_mat = plan.add(mats.data(), mats.size() * sizeof(DevMaterial));
+  size_t p_tex = plan.add(texs.data(), texs.size() * sizeof(DevTexture));
+  size_t p_pool = plan.add(pool.data(), pool.size() * sizeof(float4));
+  size_t p_lights = plan.add(lights.data(), lights.size() * sizeof(DevLight));
+  size_t p_emt = plan.add(em_tris.data(), em_tris.size() * 4);
+  size_t p_pmf = plan.add(pmf.data(), pmf.size() * 4);
+  size_t p_cdf = plan.add(cdf.data(), cdf.size() * 4);
+  size_t p_lookup = plan.add(em_lookup.data(), em_lookup.size() * 4);
+  DevScene tmp{};
+  size_t p_desc = plan.add(&tmp, sizeof(DevScene));
+  std::string err = commit(plan, out.arena, oom);
+  if (!err.empty()) {
+    out.arena.release();
+    return err;
+  }
+  DevScene &d = out.dev;
+  auto opt = [&](size_t part, size_t bytes) -> const float * {
+    return bytes ? dptr<float>(out.arena, plan, part) : nullptr;
+  };
+  d.nodes = dptr<BvhNode>(out.arena, plan, p_nodes);
+  d.tris = dptr<float4>(out.arena, plan, p_rec);
+  d.tri_info = dptr<uint2>(out.arena, plan, p_info);
+  d.pos = dptr<float>(out.arena, plan, p_pos);
+  d.nrm = opt(p_nrm, nrm.size());
+  d.tan = opt(p_tan, tan.size());
+  d.col = opt(p_col, col.size());
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s) d.uv[s] = opt(p_uv[s], uv[s].size());
+  d.materials = dptr<DevMaterial>(out.arena, plan, p_mat);
+  d.textures = dptr<DevTexture>(out.arena, plan, p_tex);
+  d.texels = dptr<float4>(out.arena, plan, p_pool);
+  d.lights = dptr<DevLight>(out.arena, plan, p_lights);
+  d.em_tris = dptr<uint32_t>(out.arena, plan, p_emt);
+  d.em_pmf = dptr<float>(out.arena, plan, p_pmf);
+  d.em_cdf = dptr<float>(out.arena, plan, p_cdf);
+  d.em_lookup = dptr<uint32_t>(out.arena, plan, p_lookup);
+  d.node_count = (uint32_t)nodes.size();
+  d.tri_count = tc;
+  d.material_count = desc.material_count;
+  d.texture_count = desc.texture_count;
+  d.light_count = desc.light_count;
+  d.em_count = (uint32_t)em_tris.size();
+  d.max_depth = out.bvh.max_depth;
+  out.d_desc = const_cast<DevScene *>(dptr<DevScene>(out.arena, plan, p_desc));
+  cudaError_t e = cudaMemcpy(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    out.arena.release();
+    return std::string("scene descriptor upload failed: ") + cudaGetErrorString(e);
+  }
+  out.tri_count = tc;
+  out.light_count = desc.light_count;
+  return "";
+}
+
+void release_scene(SceneHost &s) {
+  s.arena.release();
+  s.d_desc = nullptr;
+}
+
+// ============================================================ environment
+std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom) {
+  oom = false;
+  const float PI = 3.14159265358979323846f;
+  uint32_t w = std::max(env.width, 1u), h = std::max(env.height, 1u);
+  bool valid = env.pixels != nullptr && env.width > 0 && env.height > 0;
+  std::vector<float4> px;
+  if (valid) {
+    px.resize((size_t)w * h);
+    std::memcpy(px.data(), env.pixels, px.size() * sizeof(float4));
+  }
+  std::vector<double> weights((size_t)w * h, 0.0);
+  if (valid)
+    for (uint32_t y = 0; y < h; ++y) {
+      double st = (double)std::sin(PI * ((float)y + 0.5f) / (float)h);
+      for (uint32_t x = 0; x < w; ++x) {
+        const float4 &c = px[(size_t)y * w + x];
+        float l = 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z;
+        weights[(size_t)y * w + x] = (std::isfinite(l) && l > 0.0f) ? (double)l * st : 0.0;
+      }
+    }
+  double total = 0.0;
+  for (double x : weights) total += x;
+  bool uniform = !(total > 0.0 && std::isfinite(total));
+  if (uniform)
+    for (size_t i = 0; i < weights.size(); ++i)
+      weights[i] = (double)std::sin(PI * ((float)(i / w) + 0.5f) / (float)h);
+  total = 0.0;
+  for (double x : weights) total += x;
+  std::vector<float> marginal, conditional, mass(weights.size());
+  double acc = 0.0;
+  marginal.push_back(0.0f);
+  for (uint32_t y = 0; y < h; ++y) {
+    double row = 0.0;
+    for (uint32_t x = 0; x < w; ++x) row += weights[(size_t)y * w + x];
+    double racc = 0.0;
+    conditional.push_back(0.0f);
+    for (uint32_t x = 0; x < w; ++x) {
+      racc += weights[(size_t)y * w + x];
+      conditional.push_back(row > 0.0 ? (float)(racc / row) : (float)(x + 1) / (float)w);
+    }
+    acc += row;
+    marginal.push_back((float)(acc / total));
+  }
+  marginal.back() = 1.0f;
+  for (size_t i = 0; i < weights.size(); ++i) mass[i] = (float)(weights[i] / total);
+
+  ArenaPlan plan;
+  size_t p_px = plan.add(px.data(), px.size() * sizeof(float4));
+  size_t p_m = plan.add(marginal.data(), marginal.size() * 4);
+  size_t p_c = plan.add(conditional.data(), conditional.size() * 4);
+  size_t p_mass = plan.add(mass.data(), mass.size() * 4);
+  DevEnv tmp{};
+  size_t p_desc = plan.add(&tmp, sizeof(DevEnv));
+  std::string err = commit(plan, out.arena, oom);
+  if (!err.empty()) {
+    out.arena.release();
+    return err;
+  }
+  DevEnv &d = out.dev;
+  d.w = w;
+  d.h = h;
+  d.uniform = uniform ? 1u : 0u;
+  d.intensity = std::isfinite(env.intensity) ? std::fmax(env.intensity, 0.0f) : 0.0f;
+  d.pixels = valid ? dptr<float4>(out.arena, plan, p_px) : nullptr;
+  d.marginal = dptr<float>(out.arena, plan, p_m);
+  d.conditional = dptr<float>(out.arena, plan, p_c);
+  d.mass = dptr<float>(out.arena, plan, p_mass);
+  out.d_desc = const_cast<DevEnv *>(dptr<DevEnv>(out.arena, plan, p_desc));
+  cudaError_t e = cudaMemcpy(out.d_desc, &d, sizeof(DevEnv), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    out.arena.release();
+    return std::string("environment upload failed: ") + cudaGetErrorString(e);
+  }
+  return "";
+}
+
+void release_env(EnvHost &e) {
+  e.arena.release();
+  e.d_desc = nullptr;
+}
+
+}  // namespace ptd

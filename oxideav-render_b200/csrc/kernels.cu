@@ -1,0 +1,355 @@
+// Kernels of the plain (one path per thread) schedule, the in-order f64
+// accumulator, the resolve kernels and the test hooks.
+#include <cstdio>
+
+#include "dev_integrator.cuh"
+#include "kernels.h"
+
+namespace ptd {
+
+__device__ float g_srgb_thresh[255];  // srgb_to_linear((k + 0.5) / 255)
+
+PT_DEV const WaveSegment &find_segment(const WaveSegment *segs, uint32_t nseg, uint32_t slot) {
+  uint32_t lo = 0, hi = nseg;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (segs[mid].slot_begin <= slot)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return segs[lo];
+}
+
+PT_DEV void flush_stats(DevCounters *ctr, const ThreadStats &ts) {
+  unsigned long long e = ts.ext_rays, s = ts.shadow_rays, n = ts.nodes, t = ts.tris;
+  unsigned int err = ts.err;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    e += __shfl_down_sync(0xffffffffu, e, off);
+    s += __shfl_down_sync(0xffffffffu, s, off);
+    n += __shfl_down_sync(0xffffffffu, n, off);
+    t += __shfl_down_sync(0xffffffffu, t, off);
+    err |= __shfl_down_sync(0xffffffffu, err, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&ctr->ext_rays, e);
+    atomicAdd(&ctr->shadow_rays, s);
+    atomicAdd(&ctr->nodes, n);
+    atomicAdd(&ctr->tris, t);
+    if (err) atomicOr(&ctr->error_flags, err);
+  }
+}
+
+PT_DEV void slot_pixel(const DevRequest &rq, const WaveSegment &seg, uint32_t slot, uint32_t &x, uint32_t &y,
+                       uint32_t &index) {
+  uint32_t local = slot - seg.slot_begin;
+  uint32_t s = local / seg.pixel_count, i = local - s * seg.pixel_count;
+  uint32_t p = seg.pixel_begin + i;
+  y = p / rq.width;
+  x = p - y * rq.width;
+  index = seg.sample_begin + s;
+}
+
+struct ImmediateSink {
+  const DevRequest *rq;
+  PathState *ps;
+  ThreadStats *ts;
+  PT_DEV void emit(const ShadowRay &sr) {
+    if (trace_shadow(*rq, *ps, sr, *ts)) ps->radiance = vadd(ps->radiance, sr.contrib);
+  }
+};
+
+// One thread traces one (pixel, sample) path to the end.
+__global__ void __launch_bounds__(128) k_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg,
+                                                    uint32_t total, float4 *out, DevCounters *ctr) {
+  uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+  ThreadStats ts{0, 0, 0, 0, 0};
+  if (slot < total) {
+    const WaveSegment &seg = find_segment(segs, nseg, slot);
+    const DevRequest &rq = reqs[seg.request];
+    uint32_t x, y, index;
+    slot_pixel(rq, seg, slot, x, y, index);
+    PathState ps;
+    init_path(rq, x, y, index, ps);
+    ImmediateSink sink{&rq, &ps, &ts};
+    for (;;) {
+      Hit h;
+      bool found = trace_extension(rq, ps, h, ts);
+      if (!shade(rq, ps, found, h, sink)) break;
+    }
+    out[slot] = path_result(ps);
+  }
+  flush_stats(ctr, ts);
+}
+
+// accum[p] += covered samples of pixel p in sample order (f64, as the
+// reference's refine loop adds them, src/pathtrace.rs:2569-2578).
+__global__ void k_accumulate(const DevRequest *reqs, const WaveSegment *segs, const float4 *out) {
+  const WaveSegment &seg = segs[blockIdx.y];
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= seg.pixel_count) return;
+  const DevRequest &rq = reqs[seg.request];
+  double4 *acc = reinterpret_cast<double4 *>(rq.accum) + seg.pixel_begin + i;
+  double4 a = *acc;
+  const float4 *src = out + seg.slot_begin + i;
+  for (uint32_t s = 0; s < seg.spp; ++s) {
+    float4 v = src[(size_t)s * seg.pixel_count];
+    if (v.w > 0.0f) {
+      a.x += (double)v.x;
+      a.y += (double)v.y;
+      a.z += (double)v.z;
+      a.w += 1.0;
+    }
+  }
+  *acc = a;
+}
+
+// ---------------------------------------------------------------- resolve
+PT_DEV bool resolve_pixel(const double *a, uint32_t samples, float4 bg, float m_out[3], float &f) {
+  if (a[3] <= 0.0 || samples == 0) return false;
+  m_out[0] = (float)(a[0] / a[3]);
+  m_out[1] = (float)(a[1] / a[3]);
+  m_out[2] = (float)(a[2] / a[3]);
+  f = (float)clampd(a[3] / (double)samples, 0.0, 1.0);
+  return true;
+}
+PT_DEV float4 mix_bg(const float c[3], float f, float4 bg) {
+  float a_sum = f + (1.0f - f) * bg.w;
+  if (a_sum > 0.0f)
+    return make_float4((f * c[0] + (1.0f - f) * bg.x * bg.w) / a_sum, (f * c[1] + (1.0f - f) * bg.y * bg.w) / a_sum,
+                       (f * c[2] + (1.0f - f) * bg.z * bg.w) / a_sum, a_sum);
+  return make_float4(f * c[0] + (1.0f - f) * bg.x, f * c[1] + (1.0f - f) * bg.y, f * c[2] + (1.0f - f) * bg.z, 0.0f);
+}
+PT_DEV float sanitize(float v) { return isnan(v) ? 0.0f : v; }
+PT_DEV float aces(float x) {
+  x = x * 0.6f;
+  float v = (x * (2.51f * x + 0.03f)) / (x * (2.43f * x + 0.59f) + 0.14f);
+  return clampr(v, 0.0f, 1.0f);
+}
+// ToneMap::apply, src/hdr.rs:44-67.
+PT_DEV void tone_apply(uint32_t tm, float c[3]) {
+  float r = fmaxf(sanitize(c[0]), 0.0f), g = fmaxf(sanitize(c[1]), 0.0f), b = fmaxf(sanitize(c[2]), 0.0f);
+  if (tm == PT_TONE_REINHARD) {
+    float l = 0.2126f * r + 0.7152f * g + 0.0722f * b;
+    if (l <= 0.0f) {
+      c[0] = c[1] = c[2] = 0.0f;
+      return;
+    }
+    float s = 1.0f / (1.0f + l);
+    c[0] = fminf(r * s, 1.0f);
+    c[1] = fminf(g * s, 1.0f);
+    c[2] = fminf(b * s, 1.0f);
+  } else if (tm == PT_TONE_ACES) {
+    c[0] = aces(r);
+    c[1] = aces(g);
+    c[2] = aces(b);
+  } else {
+    c[0] = fminf(r, 1.0f);
+    c[1] = fminf(g, 1.0f);
+    c[2] = fminf(b, 1.0f);
+  }
+}
+// linear_to_srgb_byte, src/hdr.rs:116-129 (partition point over the thresholds).
+PT_DEV uint8_t srgb_byte(float c) {
+  if (isnan(c)) return 0;
+  uint32_t lo = 0, hi = 255;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (g_srgb_thresh[mid] <= c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (uint8_t)lo;
+}
+
+// PathTracer::hdr, src/pathtrace.rs:2717-2734.
+__global__ void k_resolve_hdr(const double *accum, uint32_t n, uint32_t samples, float4 bg, float4 *out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 a4 = reinterpret_cast<const double4 *>(accum)[i];
+  double a[4] = {a4.x, a4.y, a4.z, a4.w};
+  float m[3], f;
+  if (!resolve_pixel(a, samples, bg, m, f)) {
+    out[i] = bg;
+    return;
+  }
+  out[i] = f >= 1.0f ? make_float4(m[0], m[1], m[2], 1.0f) : mix_bg(m, f, bg);
+}
+
+// PathTracer::image, src/pathtrace.rs:2687-2713.
+__global__ void k_resolve_image(const double *accum, uint32_t n, uint32_t samples, float4 bg, uchar4 bg_bytes,
+                                uint32_t tone_map, float exposure, uchar4 *out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 a4 = reinterpret_cast<const double4 *>(accum)[i];
+  double a[4] = {a4.x, a4.y, a4.z, a4.w};
+  float m[3], f;
+  if (!resolve_pixel(a, samples, bg, m, f)) {
+    out[i] = bg_bytes;
+    return;
+  }
+  float c[3] = {m[0] * exposure, m[1] * exposure, m[2] * exposure};
+  tone_apply(tone_map, c);
+  float4 r = f >= 1.0f ? make_float4(c[0], c[1], c[2], 1.0f) : mix_bg(c, f, bg);
+  out[i] = make_uchar4(srgb_byte(r.x), srgb_byte(r.y), srgb_byte(r.z),
+                       (uint8_t)f2u32(roundf(clampr(r.w, 0.0f, 1.0f) * 255.0f)));
+}
+
+// ---------------------------------------------------------------- test hooks
+__global__ void k_debug_sobol(uint32_t n, uint32_t seed, float4 *out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float v[4];
+  sobol_owen_4d(i, seed, v);
+  out[i] = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// Pattern `pattern` of sample `index` for every pixel of the request.
+__global__ void k_debug_pattern(const DevRequest *rq, uint32_t index, uint32_t pattern, float4 *out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= rq->width * rq->height) return;
+  Sampler smp;
+  smp.init(rq->seed, i % rq->width, i / rq->width, index);
+  float v[4];
+  smp.pattern(pattern, v);
+  out[i] = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// Primary hit (k = 0 acceptance) of sample `index` for every pixel.
+__global__ void k_debug_primary(const DevRequest *rq, uint32_t index, uint32_t *out_g, float4 *out_tb,
+                                DevCounters *ctr) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  ThreadStats ts{0, 0, 0, 0, 0};
+  if (i < rq->width * rq->height) {
+    PathState ps;
+    init_path(*rq, i % rq->width, i / rq->width, index, ps);
+    Hit h;
+    if (trace_extension(*rq, ps, h, ts)) {
+      out_g[i] = h.g;
+      out_tb[i] = make_float4(h.t, h.b0, h.b1, h.b2);
+    } else {
+      out_g[i] = 0xffffffffu;
+      out_tb[i] = make_float4(inf(), 0.0f, 0.0f, 0.0f);
+    }
+  }
+  flush_stats(ctr, ts);
+}
+
+PT_DEV MaterialSample ms_from(const float *a) {
+  MaterialSample m;
+  for (int k = 0; k < 4; ++k) m.base_color[k] = a[k];
+  m.metallic = a[4];
+  m.roughness = a[5];
+  m.normal = {a[6], a[7], a[8]};
+  m.specular = a[9];
+  m.specular_color = {a[10], a[11], a[12]};
+  m.transmission = a[13];
+  m.thickness = a[14];
+  m.ior = a[15];
+  m.clearcoat = a[16];
+  m.clearcoat_roughness = a[17];
+  m.clearcoat_normal = {a[18], a[19], a[20]};
+  m.sheen_color = {a[21], a[22], a[23]};
+  m.sheen_roughness = a[24];
+  m.anisotropy = a[25];
+  m.anisotropy_direction = {a[26], a[27], a[28]};
+  m.iridescence = a[29];
+  m.iridescence_ior = a[30];
+  m.iridescence_thickness = a[31];
+  m.diffuse_transmission = a[32];
+  m.diffuse_transmission_color = {a[33], a[34], a[35]};
+  m.emissive = vzero();
+  m.unlit = 0;
+  m.double_sided = 0;
+  m.attenuation_color = {1.0f, 1.0f, 1.0f};
+  m.attenuation_distance = inf();
+  m.dispersion = 0.0f;
+  return m;
+}
+
+// BSDF eval of n directions and BSDF sampling of n lobe triples
+// (params: 36 MaterialSample floats, v, ng, front).
+__global__ void k_debug_bsdf(const float *params, const float *dirs, const float *us, uint32_t n, float *out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  MaterialSample m = ms_from(params);
+  Bsdf b;
+  b.init(m, {params[36], params[37], params[38]}, {params[39], params[40], params[41]}, params[42] != 0.0f);
+  V3 f;
+  float pdf;
+  b.eval({dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]}, f, pdf);
+  float *o = out + 12 * i;
+  o[0] = f.x;
+  o[1] = f.y;
+  o[2] = f.z;
+  o[3] = pdf;
+  V3 l, fs;
+  float ps;
+  bool ok = b.sample(us + 3 * i, l, fs, ps);
+  o[4] = ok ? 1.0f : 0.0f;
+  o[5] = ok ? l.x : 0.0f;
+  o[6] = ok ? l.y : 0.0f;
+  o[7] = ok ? l.z : 0.0f;
+  o[8] = ok ? fs.x : 0.0f;
+  o[9] = ok ? fs.y : 0.0f;
+  o[10] = ok ? fs.z : 0.0f;
+  o[11] = ok ? ps : 0.0f;
+}
+
+// ---------------------------------------------------------------- launchers
+#define LAUNCH_CHECK() cudaGetLastError()
+
+cudaError_t set_tables(const float *sheen_lut, const float *srgb_thresh) {
+  cudaError_t e = cudaMemcpyToSymbol(g_sheen_lut, sheen_lut, sizeof(float) * SHEEN_LUT_COS * SHEEN_LUT_ROUGH);
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(g_srgb_thresh, srgb_thresh, sizeof(float) * 255);
+}
+
+cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
+                              float4 *out, DevCounters *ctr, cudaStream_t st) {
+  if (total == 0) return cudaSuccess;
+  k_megakernel<<<(total + 127) / 128, 128, 0, st>>>(reqs, segs, nseg, total, out, ctr);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_accumulate(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t max_pixels,
+                              const float4 *out, cudaStream_t st) {
+  if (nseg == 0 || max_pixels == 0) return cudaSuccess;
+  dim3 grid((max_pixels + 255) / 256, nseg);
+  k_accumulate<<<grid, 256, 0, st>>>(reqs, segs, out);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_resolve_hdr(const double *accum, uint32_t n, uint32_t samples, float4 bg, float4 *out,
+                               cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_resolve_hdr<<<(n + 255) / 256, 256, 0, st>>>(accum, n, samples, bg, out);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_resolve_image(const double *accum, uint32_t n, uint32_t samples, float4 bg, uchar4 bg_bytes,
+                                 uint32_t tone_map, float exposure, uchar4 *out, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_resolve_image<<<(n + 255) / 256, 256, 0, st>>>(accum, n, samples, bg, bg_bytes, tone_map, exposure, out);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_debug_sobol(uint32_t n, uint32_t seed, float4 *out, cudaStream_t st) {
+  k_debug_sobol<<<(n + 255) / 256, 256, 0, st>>>(n, seed, out);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_debug_pattern(const DevRequest *rq, uint32_t npix, uint32_t index, uint32_t pattern, float4 *out,
+                                 cudaStream_t st) {
+  k_debug_pattern<<<(npix + 255) / 256, 256, 0, st>>>(rq, index, pattern, out);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_debug_primary(const DevRequest *rq, uint32_t npix, uint32_t index, uint32_t *out_g, float4 *out_tb,
+                                 DevCounters *ctr, cudaStream_t st) {
+  k_debug_primary<<<(npix + 127) / 128, 128, 0, st>>>(rq, index, out_g, out_tb, ctr);
+  return LAUNCH_CHECK();
+}
+cudaError_t launch_debug_bsdf(const float *params, const float *dirs, const float *us, uint32_t n, float *out,
+                              cudaStream_t st) {
+  k_debug_bsdf<<<(n + 127) / 128, 128, 0, st>>>(params, dirs, us, n, out);
+  return LAUNCH_CHECK();
+}
+
+}  // namespace ptd

@@ -1,0 +1,27 @@
+// Host-side declarations of the kernel launchers (kernels.cu, wavefront.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dev_types.h"
+
+namespace ptd {
+
+cudaError_t set_tables(const float *sheen_lut, const float *srgb_thresh);
+cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
+                              float4 *out, DevCounters *ctr, cudaStream_t st);
+cudaError_t launch_accumulate(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t max_pixels,
+                              const float4 *out, cudaStream_t st);
+cudaError_t launch_resolve_hdr(const double *accum, uint32_t n, uint32_t samples, float4 bg, float4 *out,
+                               cudaStream_t st);
+cudaError_t launch_resolve_image(const double *accum, uint32_t n, uint32_t samples, float4 bg, uchar4 bg_bytes,
+                                 uint32_t tone_map, float exposure, uchar4 *out, cudaStream_t st);
+cudaError_t launch_debug_sobol(uint32_t n, uint32_t seed, float4 *out, cudaStream_t st);
+cudaError_t launch_debug_pattern(const DevRequest *rq, uint32_t npix, uint32_t index, uint32_t pattern, float4 *out,
+                                 cudaStream_t st);
+cudaError_t launch_debug_primary(const DevRequest *rq, uint32_t npix, uint32_t index, uint32_t *out_g, float4 *out_tb,
+                                 DevCounters *ctr, cudaStream_t st);
+cudaError_t launch_debug_bsdf(const float *params, const float *dirs, const float *us, uint32_t n, float *out,
+                              cudaStream_t st);
+
+}  // namespace ptd

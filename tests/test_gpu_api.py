@@ -1,0 +1,122 @@
+"""PathTracer / PathTraceCudaRenderer semantics on the GPU (ports of
+src/pathtrace.rs:3566-3626 and the robustness tests of src/lib.rs:385-655)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oxideav_render_b200 import abi, api, testscenes as ts
+from oxideav_render_b200.options import (BackgroundColor, CameraSpec, PathTraceOptions, Projection, RenderBackend,
+                                         ToneMap)
+from oxideav_render_b200.scene import PreparedScene, Primitive
+
+pytestmark = pytest.mark.gpu
+
+
+def test_renders_are_deterministic_and_refinement_is_additive(ctx):
+    scene = ts.area_light_scene(0.5, 0.0)
+    o = ts.pt_opts(9, 8, 4)
+    r = api.PathTraceCudaRenderer(ctx)
+    a = r.render_hdr(scene, o)
+    b = api.PathTraceCudaRenderer(ctx).render_hdr(scene, o)
+    assert np.array_equal(a, b)
+    t = api.PathTracer(ctx)
+    t.sync(scene, o)
+    t.refine(3)
+    t.refine(5)
+    assert t.samples() == 8
+    assert np.array_equal(t.hdr(), a), "refine(3)+refine(5) must equal refine(8)"
+    assert not np.array_equal(api.PathTraceCudaRenderer(ctx).render_hdr(scene, ts.pt_opts(9, 8, 4, seed=1)), a)
+
+
+def test_refinement_is_additive_across_waves(ctx):
+    # Small waves split one refine into many launches; results are unchanged.
+    scene, opts = ts.cornell_c0()
+    o = opts.replace(width=40, height=30, path_trace=PathTraceOptions(samples_per_pixel=12, max_bounces=4))
+    t1 = api.PathTracer(ctx)
+    t1.sync(scene, o)
+    t1.refine(12)
+    ref = t1.accum()
+    ctx.set_wave_slots(1024)
+    try:
+        t2 = api.PathTracer(ctx)
+        t2.sync(scene, o)
+        t2.refine(5)
+        t2.refine(7)
+        assert np.array_equal(t2.accum(), ref)
+    finally:
+        ctx.set_wave_slots(1 << 22)
+
+
+def test_sync_resets_only_on_radiance_changes(ctx):
+    scene = ts.area_light_scene(0.5, 0.0)
+    o = ts.pt_opts(6, 8, 2)
+    t = api.PathTracer(ctx)
+    assert t.sync(scene, o)
+    t.refine(2)
+    display = o.replace(exposure=2.0, tone_map=ToneMap.AcesFitted,
+                        path_trace=PathTraceOptions(samples_per_pixel=1000, max_bounces=2))
+    assert not t.sync(scene, display)
+    assert t.samples() == 2
+    assert not t.is_converged()
+    moved = display.replace(scene_camera=None, projection=Projection.Orthographic)
+    assert t.sync(scene, moved)
+    assert t.samples() == 0
+    t.invalidate_scene()
+    t.refine(1)
+    assert t.sync(scene, moved)
+
+
+def test_primary_misses_keep_background_bytes(ctx):
+    scene = ts.area_light_scene(0.5, 0.0)
+    o = ts.pt_opts(16, 4, 1, background=BackgroundColor((200, 10, 77, 128)), scene_camera=None,
+                   camera=CameraSpec(0.0, 0.0, 3.0))
+    img = api.PathTraceCudaRenderer(ctx).render(scene, o)
+    assert tuple(img[0, 0]) == (200, 10, 77, 128)
+    empty = api.PathTraceCudaRenderer(ctx).render(PreparedScene(), o)
+    assert np.all(empty == np.array([200, 10, 77, 128], np.uint8))
+
+
+def test_hostile_inputs_render_well_formed_images(ctx):
+    # 1x1 renders, a degenerate triangle, huge coordinates, a scene of one
+    # triangle; every render terminates with finite bytes.
+    s = PreparedScene()
+    m = s.add_material(ts.diffuse_material((0.5, 0.5, 0.5), 1.0))
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    s.add_primitive(Primitive(tri, np.array([0, 1, 2], np.uint32), material=m))
+    s.add_primitive(Primitive(np.zeros((3, 3), np.float32), np.array([0, 1, 2], np.uint32), material=m))
+    s.add_primitive(Primitive(tri * 1e30, np.array([0, 1, 2], np.uint32), material=m))
+    for w, h in [(1, 1), (7, 3)]:
+        o = ts.pt_opts(w, 4, 3, h=h, scene_camera=None)
+        img = api.PathTraceCudaRenderer(ctx).render(s, o)
+        assert img.shape == (h, w, 4)
+        hdr = api.PathTraceCudaRenderer(ctx).render_hdr(s, o)
+        assert np.all(np.isfinite(hdr))
+
+
+def test_invalid_options_are_rejected(ctx):
+    scene = ts.lambert_plane(0.5)
+    t = api.PathTracer(ctx)
+    with pytest.raises(api.RenderError) as e:
+        t.sync(scene, ts.pt_opts(4, 1, 2000))
+    assert e.value.status == abi.PT_ERR_INVALID_ARG
+
+
+def test_make_renderer_arm(ctx):
+    r = api.make_renderer(RenderBackend.PathTraceCuda, ctx)
+    img = r.render(ts.lambert_plane(0.5), ts.pt_opts(8, 2, 1, ambient=1.0))
+    assert img.shape == (8, 8, 4)
+    with pytest.raises(NotImplementedError):
+        api.make_renderer(RenderBackend.Scanline, ctx)
+
+
+def test_scene_release_and_counts(ctx):
+    scene, opts = ts.cornell_c0()
+    desc = scene.to_desc(opts)
+    sid = ctx.upload(desc)
+    assert ctx.scene_bytes(sid) > 0
+    st = ctx.bvh_stats(sid)
+    assert st["max_depth"] < 64 and st["nodes"] >= 1
+    ctx.release(sid)
+    with pytest.raises(api.RenderError):
+        ctx.release(sid)
