@@ -1,0 +1,354 @@
+"""Benchmark: samples/s of the path-tracing hot path on one B200 (or N, weak scaling).
+
+Workload (default): the metallic x roughness sphere grid — 7x7 UV spheres of
+64x32 segments (200,706 triangles with the floor), a 512^2 sRGB checker floor
+texture with trilinear mips, one directional and one point light, sky 0.3;
+512x512 pixels, 256 samples per pixel, 8 bounces. One step = one frame:
+`PathTracer.refine(256)` on the resident scene (67,108,864 camera paths).
+
+Reported (one JSON line from rank 0):
+  value      samples/s over all ranks, device time (CUDA events on the
+             library's stream around the path-tracing kernels), max over ranks;
+  e2e        the same metric through `PathTraceCudaRenderer.render` (scene
+             upload with the host BVH build, refine, image readback), wall time;
+  roofline   the path kernel's algorithmic bytes (per-ray / per-vertex byte
+             model of the design notes, from device counters) / kernel time,
+             against the measured HBM copy bandwidth;
+  cpu_baseline  the CPU restatement of the reference (oracle) on this host's
+             cores on a bounded sample of the same frame.
+`--impl reference` times that CPU restatement alone (the Rust reference has no
+toolchain here) on the same workload and prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+import __graft_entry__ as entry  # noqa: E402
+
+METRIC = "samples/s & Mrays/s vs plain GPU path; p50/p99 request latency at PSNR≥45dB"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(name: str):
+    ts = entry.load_package().testscenes
+    if name == "c1":
+        scene, opts = ts.sphere_grid_c1(512, 256)
+        return scene, opts, None, "sphere_grid_7x7_64x32 512x512 256spp 8 bounces (200,706 tris)"
+    if name == "c0":
+        scene, opts = ts.cornell_c0()
+        return scene, opts, None, "cornell_unit_box 256x256 64spp 8 bounces (36 tris)"
+    if name == "c2":
+        scene, opts, env = ts.stress_c2()
+        return scene, opts, env, "stress_heightfield_spheres 1920x1080 64spp 8 bounces (~4.1M tris, env 512x256)"
+    raise SystemExit(f"unknown config {name}")
+
+
+def algorithmic_bytes(ext_rays, shadow_rays, nodes, tris, samples):
+    """Byte model per unit of work: per traced ray 32 B ray + 16 B hit, 64 B
+    per BVH node visited, 48 B per triangle record tested; per shaded vertex
+    16 B hit + 128 B path state read/write + 32 B per spawned ray; 32 B per
+    accumulated sample (16 B read + 16 B write)."""
+    rays = ext_rays + shadow_rays
+    return (48 * rays + 64 * nodes + 48 * tris + ext_rays * (16 + 128) + 32 * (ext_rays + shadow_rays)
+            + 32 * samples)
+
+
+def cpu_baseline(scene, opts, env, budget_s: float):
+    """Oracle on this host's cores over a bounded band of rows of the frame."""
+    orc = entry.load_oracle()
+    from oxideav_render_b200.scene import Camera
+    desc = scene.to_desc(opts)
+    sc = orc.OracleScene(desc)
+    cam = Camera.resolve(scene, opts, opts.width, opts.height)
+    oenv = orc.OracleEnv(env) if env is not None else None
+    cores = os.cpu_count() or 1
+    # Rows spread evenly over the frame; calibrate at 1 spp, then size the
+    # sample so it takes about `budget_s`.
+    rows = min(64, opts.height)
+    stride = max(opts.height // rows, 1)
+    t0 = time.perf_counter()
+    orc.refine_rows(sc, cam, opts, oenv, stride // 2, stride, rows, 0, 1, cores)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    spp = max(1, min(opts.path_trace.samples_per_pixel, int(budget_s / dt)))
+    t0 = time.perf_counter()
+    _, rc = orc.refine_rows(sc, cam, opts, oenv, stride // 2, stride, rows, 0, spp, cores)
+    dt = time.perf_counter() - t0
+    n = opts.width * rows * spp
+    return {"value": n / dt, "unit": "samples/s", "cores": cores, "kind": "port",
+            "sample": f"every {stride}th row ({rows} of {opts.height}) x {spp} spp of the frame "
+                      f"({n} camera paths, {dt:.1f} s)",
+            "mrays_per_s": (rc[0] + rc[1]) / dt / 1e6}
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        torch.cuda.synchronize()
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    pkg = entry.load_package()
+    scene, opts, env, wname = workload(args.config)
+    orc = entry.load_oracle()
+    from oxideav_render_b200.scene import Camera
+    desc = scene.to_desc(opts)
+    sc = orc.OracleScene(desc)
+    cam = Camera.resolve(scene, opts, opts.width, opts.height)
+    oenv = orc.OracleEnv(env) if env is not None else None
+    cores = os.cpu_count() or 1
+    rows, spp = min(args.ref_rows, opts.height), args.ref_spp
+    stride = max(opts.height // rows, 1)
+    times, rays = [], 0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _, rc = orc.refine_rows(sc, cam, opts, oenv, stride // 2, stride, rows, i * spp, spp, cores)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+            rays += rc[0] + rc[1]
+    n = opts.width * rows * spp
+    value = n * len(times) / sum(times)
+    sample = f"every {stride}th row ({rows} of {opts.height}) x {spp} spp per step ({n} camera paths)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": wname, "parallelism": "host threads"},
+        "mrays_per_s": rays / sum(times) / 1e6,
+        "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def run_b200(args):
+    import torch
+    ws, rank, local = dist_setup()
+    pkg = entry.load_package()
+    from oxideav_render_b200 import api
+    scene, opts, env, wname = workload(args.config)
+    if args.spp:
+        opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__,
+                                                                   "samples_per_pixel": args.spp}))
+        wname += f" (override: {args.spp} spp)"
+    spp = opts.path_trace.samples_per_pixel
+    samples_per_step = opts.width * opts.height * spp
+    ctx = api.Context(local if ws > 1 else torch.cuda.current_device())
+    if args.seed_per_rank and ws > 1:
+        opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__, "seed": rank}))
+    tracer = api.PathTracer(ctx)
+    if env is not None:
+        tracer.set_environment(api.EnvironmentMap(env))
+    tracer.sync(scene, opts)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    for _ in range(args.warmup):
+        tracer.refine(spp)
+    barrier(ws)
+    kernel_ms, wall_ms = [], []
+    ext = shadow = nodes = tris = 0
+    with ClockSampler(local if ws > 1 else torch.cuda.current_device()) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tracer.refine(spp)
+            wall_ms.append(1000 * (time.perf_counter() - t0))
+            kernel_ms.append(tracer.last_kernel_ms())
+            e, s = tracer.ray_counts()
+            n, t = tracer.traversal_counts()
+            ext, shadow, nodes, tris = ext + e, shadow + s, nodes + n, tris + t
+    barrier(ws)
+    dev_s = max_over_ranks(sum(kernel_ms) / 1000.0, ws)
+    value = samples_per_step * args.steps * ws / dev_s
+    ms_per_step = 1000 * dev_s / args.steps
+    rays = ext + shadow
+    mrays = max(rays / (sum(kernel_ms) / 1000.0) / 1e6, 0.0)
+    # Roofline of the path kernel (bytes per launch / launch time).
+    peak, peak_kind = load_peaks()
+    alg = algorithmic_bytes(ext, shadow, nodes, tris, samples_per_step * args.steps)
+    achieved = alg / (sum(kernel_ms) / 1000.0) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", f"traffic_{args.config}.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch")
+
+    # End to end: the reference-facing one-shot call (re-prepare + render + image).
+    renderer = api.PathTraceCudaRenderer(ctx)
+    if env is not None:
+        renderer.tracer_mut().set_environment(api.EnvironmentMap(env))
+    e2e_s = []
+    h2d = d2h = 0
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img = renderer.render(scene, opts)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_s.append(dt)
+        h2d = ctx.scene_bytes(renderer.tracer.scene_id)
+        d2h = img.nbytes
+    e2e = None
+    if e2e_s:
+        e2e_t = max_over_ranks(sum(e2e_s) / len(e2e_s), ws)
+        e2e = {"value": samples_per_step * ws / e2e_t, "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_t,
+               "call": "PathTraceCudaRenderer.render (scene upload incl. host BVH build, refine, "
+                       "sRGB image readback)"}
+    waves = math.ceil(samples_per_step / (1 << 22))
+    launches = args.steps * 2 * max(waves, 1)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(scene, opts, env, args.cpu_seconds)
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wname, "samples_per_step": samples_per_step, "global_batch": samples_per_step * ws,
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "flushed (256 MB write) before every timed step", "schedule": "megakernel"},
+            "mrays_per_s": mrays, "rays_per_step": rays / args.steps, "wall_ms_per_step": statistics.mean(wall_ms),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "k_megakernel (+ k_accumulate)",
+                         "bytes_per_launch": alg / max(launches // 2, 1)},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(out))
+    tracer.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed-per-rank", action="store_true")
+    ap.add_argument("--ref-rows", type=int, default=32)
+    ap.add_argument("--ref-spp", type=int, default=8)
+    ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling cases)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

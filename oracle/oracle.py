@@ -42,6 +42,7 @@ def lib():
                 "oracle_env_destroy": (None, [vp]),
                 "oracle_refine": (i32, [vp, vp, vp, vp, u32, u32, i32, dp, u64p]),
                 "oracle_sample": (i32, [vp, vp, vp, vp, u32, u32, u32, fp]),
+                "oracle_refine_rows": (i32, [vp, vp, vp, vp, u32, u32, u32, u32, u32, i32, dp, u64p]),
                 "oracle_resolve_hdr": (None, [dp, u32, vp, fp]),
                 "oracle_resolve_image": (None, [dp, u32, vp, u8p]),
                 "oracle_primary_hits": (None, [vp, vp, vp, u32, u32p, fp, fp]),
@@ -181,6 +182,20 @@ class OracleTracer:
                                   g.ctypes.data_as(C.POINTER(C.c_uint32)), t.ctypes.data_as(C.POINTER(C.c_float)),
                                   b.ctypes.data_as(C.POINTER(C.c_float)))
         return g, t, b
+
+
+def refine_rows(scene: OracleScene, camera, opts, env, row0: int, stride: int, count: int, first: int, samples: int,
+                threads: int = 0):
+    """refine() over rows row0 + i*stride (i < count) of the full frame.
+    Returns (accum[count, width, 4] f64, (extension rays, shadow rays))."""
+    cam = camera.to_c() if hasattr(camera, "to_c") else camera
+    o = opts.to_c() if hasattr(opts, "to_c") else opts
+    acc = np.zeros((count, o.width, 4), np.float64)
+    rc = np.zeros(2, np.uint64)
+    lib().oracle_refine_rows(scene.ptr, env.ptr if env else None, C.byref(cam), C.byref(o), row0, stride, count,
+                             first, samples, threads, acc.ctypes.data_as(C.POINTER(C.c_double)),
+                             rc.ctypes.data_as(C.POINTER(C.c_uint64)))
+    return acc, (int(rc[0]), int(rc[1]))
 
 
 def render_hdr(desc, camera, opts, env=None, threads=0):

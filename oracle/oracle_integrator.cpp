@@ -527,6 +527,51 @@ int oracle_refine(const void *scene, const void *env, const pt_camera *cam, cons
   return 0;
 }
 
+// refine over a strided subset of rows (row0 + i * stride, i < count) of the
+// full frame: the bounded CPU baseline sample. accum holds width*count*4.
+int oracle_refine_rows(const void *scene, const void *env, const pt_camera *cam, const pt_render_options *opts,
+                       uint32_t row0, uint32_t stride, uint32_t count, uint32_t first, uint32_t samples, int threads,
+                       double *accum, uint64_t *ray_counts) {
+  const Scene *sc = (const Scene *)scene;
+  Integrator base = make_integrator(sc, (const EnvironmentMap *)env, *cam, *opts);
+  uint32_t w = base.width;
+  std::atomic<uint32_t> next{0};
+  std::atomic<uint64_t> ext{0}, sh{0};
+  int nthreads = std::max(1, std::min<int>(threads > 0 ? threads : (int)std::thread::hardware_concurrency(),
+                                           (int)count));
+  auto work = [&]() {
+    Integrator it = base;
+    for (;;) {
+      uint32_t r = next.fetch_add(1);
+      if (r >= count) break;
+      uint32_t y = row0 + r * stride;
+      if (y >= base.height) continue;
+      for (uint32_t x = 0; x < w; ++x) {
+        double *px = accum + ((size_t)r * w + x) * 4;
+        for (uint32_t si = 0; si < samples; ++si) {
+          V3 c;
+          if (it.sample(x, y, first + si, c)) {
+            px[0] += (double)c.x;
+            px[1] += (double)c.y;
+            px[2] += (double)c.z;
+            px[3] += 1.0;
+          }
+        }
+      }
+    }
+    ext += it.ext_rays;
+    sh += it.shadow_rays;
+  };
+  std::vector<std::thread> pool;
+  for (int i = 0; i < nthreads; ++i) pool.emplace_back(work);
+  for (auto &t : pool) t.join();
+  if (ray_counts) {
+    ray_counts[0] = ext.load();
+    ray_counts[1] = sh.load();
+  }
+  return 0;
+}
+
 // One sample of one pixel (radiance, covered flag); for per-sample checks.
 int oracle_sample(const void *scene, const void *env, const pt_camera *cam, const pt_render_options *opts, uint32_t x,
                   uint32_t y, uint32_t index, float out_rgb[3]) {
