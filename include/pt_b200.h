@@ -343,6 +343,26 @@ PT_API pt_status pt_tracer_ray_counts(const pt_tracer *tr, uint64_t *extension_r
 PT_API pt_status pt_render_hdr(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                         const pt_render_options *opts, const pt_environment *env,
                         float *out_rgba, size_t out_floats);
+/* Refine without allocating. This entry point has no counterpart in the
+ * reference. It is for callers that cannot allocate device memory inside a
+ * call — a render loop whose frame budget forbids cudaMalloc / cudaFree
+ * (they can synchronise the device), or a host whose memory all comes from
+ * its own pool. The caller owns the output: `d_accum` is a device buffer of
+ * width*height*4 doubles (sum r, g, b, covered count per pixel) that this
+ * call adds `samples` samples to, starting at sample index `first_sample`
+ * (so consecutive calls continue the sequence exactly like
+ * pt_tracer_refine). The per-wave path samples live in a fixed scratch array
+ * compiled into the library (1,048,576 path slots, 16 MiB, held by every GPU
+ * that loads the library until the process exits); images above 1,048,576
+ * pixels are rejected with PT_ERR_INVALID_ARG. No environment map (the sky is
+ * `ambient`). The first call on a device looks up the scratch address for
+ * that device; make that first call before any stream capture. Every call
+ * reuses the same scratch, so calls that overlap on the GPU race: serialise
+ * them. */
+PT_API pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+                                   const pt_render_options *opts, uint32_t first_sample, uint32_t samples,
+                                   double *d_accum);
+
 PT_API pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                           const pt_render_options *opts, const pt_environment *env,
                           uint8_t *out_rgba, size_t out_bytes);

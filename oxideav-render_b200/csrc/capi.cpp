@@ -15,26 +15,11 @@
 
 #include "../../include/pt_b200.h"
 #include "../../include/pt_b200_debug.h"
+#include "context.h"
 #include "host_scene.h"
 #include "kernels.h"
 
 using namespace ptd;
-
-struct pt_context {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  std::map<uint32_t, std::unique_ptr<SceneHost>> scenes;
-  uint32_t next_id = 1;
-  uint32_t schedule = PT_SCHEDULE_MEGAKERNEL;
-  uint32_t wave_slots = 1u << 22;
-  float4 *d_out = nullptr;
-  size_t out_cap = 0;
-  WaveSegment *d_segs = nullptr;
-  size_t seg_cap = 0;
-  DevCounters *d_ctr = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-};
 
 struct pt_tracer {
   pt_context *ctx = nullptr;
@@ -298,6 +283,11 @@ pt_status set_env_impl(pt_tracer *t, const pt_environment *env) {
 }
 
 }  // namespace
+
+namespace ptd {
+pt_status ctx_fail(pt_context *ctx, pt_status st, const std::string &msg) { return fail(ctx, st, msg); }
+SceneHost *ctx_find_scene(pt_context *ctx, uint32_t id) { return find_scene(ctx, id); }
+}  // namespace ptd
 
 extern "C" {
 

@@ -1,0 +1,36 @@
+// The context object behind the opaque pt_context handle, shared by the C
+// entry points (capi.cpp, noalloc.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+
+#include "../../include/pt_b200.h"
+#include "../../include/pt_b200_debug.h"
+#include "host_scene.h"
+
+struct pt_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::map<uint32_t, std::unique_ptr<ptd::SceneHost>> scenes;
+  uint32_t next_id = 1;
+  uint32_t schedule = PT_SCHEDULE_MEGAKERNEL;
+  uint32_t wave_slots = 1u << 22;
+  float4 *d_out = nullptr;
+  size_t out_cap = 0;
+  ptd::WaveSegment *d_segs = nullptr;
+  size_t seg_cap = 0;
+  ptd::DevCounters *d_ctr = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace ptd {
+// Records `msg` as the context's last error and returns `st`.
+pt_status ctx_fail(pt_context *ctx, pt_status st, const std::string &msg);
+// The resident scene `id`, or nullptr.
+SceneHost *ctx_find_scene(pt_context *ctx, uint32_t id);
+}  // namespace ptd

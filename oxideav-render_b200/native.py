@@ -59,6 +59,8 @@ SIGNATURES = {
                             C.POINTER(abi.pt_environment), fp, C.c_size_t]),
     "pt_render_image": (i32, [vp, u32, C.POINTER(abi.pt_camera), C.POINTER(abi.pt_render_options),
                               C.POINTER(abi.pt_environment), u8p, C.c_size_t]),
+    "pt_refine_noalloc": (i32, [vp, u32, C.POINTER(abi.pt_camera), C.POINTER(abi.pt_render_options), u32, u32,
+                                C.c_void_p]),
     # include/pt_b200_debug.h
     "pt_debug_sobol": (i32, [vp, u32, u32, fp]),
     "pt_debug_pattern": (i32, [vp, u32, u32, fp]),
