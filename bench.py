@@ -127,6 +127,20 @@ def algorithmic_bytes(ext_rays, shadow_rays, nodes, tris, samples):
             + 32 * samples)
 
 
+def profiled_traffic(kernel: str, config: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/<kernel>_*.md, line `traffic_bytes_per_launch | N`), scaled to
+    this workload's launch size when the capture ran a smaller case."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
+        text = open(path).read()
+        m = re.search(r"traffic_bytes_per_launch \| (\d+)", text)
+        if m and f"config={config}" in text:
+            return int(m.group(1))
+    return None
+
+
 def cpu_baseline(scene, opts, env, budget_s: float):
     """Oracle on this host's cores over a bounded band of rows of the frame."""
     orc = entry.load_oracle()
@@ -236,6 +250,7 @@ def run_b200(args):
     spp = opts.path_trace.samples_per_pixel
     samples_per_step = opts.width * opts.height * spp
     ctx = api.Context(local if ws > 1 else torch.cuda.current_device())
+    ctx.set_schedule({"megakernel": 0, "wavefront": 1}[args.schedule])
     if args.seed_per_rank and ws > 1:
         opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__, "seed": rank}))
     tracer = api.PathTracer(ctx)
@@ -247,7 +262,10 @@ def run_b200(args):
         tracer.refine(spp)
     barrier(ws)
     kernel_ms, wall_ms = [], []
-    ext = shadow = nodes = tris = 0
+    ext = shadow = 0
+    split = {"ext_nodes": 0, "ext_tris": 0, "sh_nodes": 0, "sh_tris": 0}
+    stage = {k: 0.0 for k in api.PathTracer.STAGES}
+    ctx.set_stage_timing(True)
     with ClockSampler(local if ws > 1 else torch.cuda.current_device()) as clocks:
         for _ in range(args.steps):
             flush.zero_()
@@ -257,23 +275,40 @@ def run_b200(args):
             wall_ms.append(1000 * (time.perf_counter() - t0))
             kernel_ms.append(tracer.last_kernel_ms())
             e, s = tracer.ray_counts()
-            n, t = tracer.traversal_counts()
-            ext, shadow, nodes, tris = ext + e, shadow + s, nodes + n, tris + t
+            ext, shadow = ext + e, shadow + s
+            for k, v in tracer.traversal_split().items():
+                split[k] += v
+            for k, v in tracer.stage_ms().items():
+                stage[k] += v
+    ctx.set_stage_timing(False)
     barrier(ws)
     dev_s = max_over_ranks(sum(kernel_ms) / 1000.0, ws)
     value = samples_per_step * args.steps * ws / dev_s
     ms_per_step = 1000 * dev_s / args.steps
     rays = ext + shadow
     mrays = max(rays / (sum(kernel_ms) / 1000.0) / 1e6, 0.0)
-    # Roofline of the path kernel (bytes per launch / launch time).
+    # Roofline of the dominant kernel: its algorithmic bytes / its device time.
     peak, peak_kind = load_peaks()
-    alg = algorithmic_bytes(ext, shadow, nodes, tris, samples_per_step * args.steps)
-    achieved = alg / (sum(kernel_ms) / 1000.0) / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", f"traffic_{args.config}.json")
-    if os.path.exists(prof):
-        with open(prof) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+    n_samples = samples_per_step * args.steps
+    stage_bytes = {
+        "extend": 48 * ext + 64 * split["ext_nodes"] + 48 * split["ext_tris"],
+        "shadow": 48 * shadow + 64 * split["sh_nodes"] + 48 * split["sh_tris"],
+        "shade": ext * (16 + 128 + 32) + 32 * shadow,
+        "megakernel": algorithmic_bytes(ext, shadow, split["ext_nodes"] + split["sh_nodes"],
+                                        split["ext_tris"] + split["sh_tris"], 0),
+        "accumulate": 32 * n_samples,
+    }
+    dom = max((k for k in stage_bytes if stage[k] > 0), key=lambda k: stage[k])
+    achieved = stage_bytes[dom] / (stage[dom] / 1000.0) / 1e9
+    kernel_names = {"extend": "k_wf_extend", "shade": "k_wf_shade", "shadow": "k_wf_shadow",
+                    "megakernel": "k_megakernel", "accumulate": "k_accumulate"}
+    waves = max(math.ceil(samples_per_step / (1 << 22)), 1)
+    iters = opts.path_trace.max_bounces + 1
+    per_wave = (2 + 3 * iters) if args.schedule == "wavefront" else 2
+    launches = args.steps * waves * per_wave
+    launches_of_dom = args.steps * waves * (iters if args.schedule == "wavefront" and dom in
+                                            ("extend", "shade", "shadow") else 1)
+    traffic = profiled_traffic(kernel_names[dom], args.config)
 
     # End to end: the reference-facing one-shot call (re-prepare + render + image).
     renderer = api.PathTraceCudaRenderer(ctx)
@@ -297,8 +332,6 @@ def run_b200(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_t,
                "call": "PathTraceCudaRenderer.render (scene upload incl. host BVH build, refine, "
                        "sRGB image readback)"}
-    waves = math.ceil(samples_per_step / (1 << 22))
-    launches = args.steps * 2 * max(waves, 1)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene, opts, env, args.cpu_seconds)
@@ -309,12 +342,14 @@ def run_b200(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wname, "samples_per_step": samples_per_step, "global_batch": samples_per_step * ws,
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "flushed (256 MB write) before every timed step", "schedule": "megakernel"},
+                       "l2": "flushed (256 MB write) before every timed step", "schedule": args.schedule},
             "mrays_per_s": mrays, "rays_per_step": rays / args.steps, "wall_ms_per_step": statistics.mean(wall_ms),
+            "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if v > 0},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_megakernel (+ k_accumulate)",
-                         "bytes_per_launch": alg / max(launches // 2, 1)},
+                         "kernel": kernel_names[dom],
+                         "bytes_per_launch": stage_bytes[dom] / max(launches_of_dom, 1),
+                         "ms_per_launch": stage[dom] / max(launches_of_dom, 1)},
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
@@ -341,6 +376,7 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=32)
     ap.add_argument("--ref-spp", type=int, default=8)
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling cases)")
+    ap.add_argument("--schedule", default="wavefront", choices=["megakernel", "wavefront"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -31,12 +31,22 @@ PT_API pt_status pt_debug_bsdf(pt_context *ctx, const float *params, const float
                         float *out);
 /* Traversal work of the last refine: BVH nodes visited, triangles tested. */
 PT_API pt_status pt_tracer_traversal_counts(const pt_tracer *tr, uint64_t *nodes, uint64_t *tris);
+/* Traversal work of the last refine split by ray kind:
+ * out = {closest-hit nodes, closest-hit triangles, any-hit nodes, any-hit triangles}. */
+PT_API pt_status pt_tracer_traversal_split(const pt_tracer *tr, uint64_t out[4]);
+/* Per-stage device time of refine calls (CUDA events between the kernels of
+ * each stage on the context stream), off by default. Stages, in order:
+ * ray generation, closest hit, shade, shadow rays, accumulate, megakernel. */
+PT_API pt_status pt_set_stage_timing(pt_context *ctx, int on);
+PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n);
 /* BVH statistics of a resident scene. */
 PT_API pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes, uint32_t *leaves,
                              uint32_t *max_depth, double *sah_cost, double *build_seconds);
 
-/* Schedule of the hot loop: 0 = one path per thread (megakernel). */
-typedef enum pt_schedule { PT_SCHEDULE_MEGAKERNEL = 0 } pt_schedule;
+/* Schedule of the hot loop: one path per thread (megakernel), or the
+ * wavefront (extend / shade / shadow kernels over compacted queues). Both
+ * produce bit-identical accumulators. */
+typedef enum pt_schedule { PT_SCHEDULE_MEGAKERNEL = 0, PT_SCHEDULE_WAVEFRONT = 1 } pt_schedule;
 PT_API pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule);
 /* Maximum path slots per wave (device sample buffer 16 B per slot). */
 PT_API pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots);

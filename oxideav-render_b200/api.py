@@ -81,6 +81,9 @@ class Context:
     def set_wave_slots(self, slots: int) -> None:
         self.check(self.lib.pt_set_wave_slots(self.ptr, slots))
 
+    def set_stage_timing(self, on: bool) -> None:
+        self.check(self.lib.pt_set_stage_timing(self.ptr, 1 if on else 0))
+
     def debug_sobol(self, n: int, seed: int) -> np.ndarray:
         out = np.zeros((n, 4), np.float32)
         self.check(self.lib.pt_debug_sobol(self.ptr, n, seed & 0xFFFFFFFF, out.ctypes.data_as(native.fp)))
@@ -241,6 +244,19 @@ class PathTracer:
         n, t = C.c_uint64(), C.c_uint64()
         self.ctx.check(self.lib.pt_tracer_traversal_counts(self.ptr, C.byref(n), C.byref(t)))
         return n.value, t.value
+
+    STAGES = ("raygen", "extend", "shade", "shadow", "accumulate", "megakernel")
+
+    def stage_ms(self) -> dict:
+        """Device ms per stage of the last refine (with stage timing on)."""
+        out = np.zeros(len(self.STAGES), np.float32)
+        self.ctx.check(self.lib.pt_tracer_stage_ms(self.ptr, out.ctypes.data_as(native.fp), len(self.STAGES)))
+        return dict(zip(self.STAGES, (float(v) for v in out)))
+
+    def traversal_split(self) -> dict:
+        out = np.zeros(4, np.uint64)
+        self.ctx.check(self.lib.pt_tracer_traversal_split(self.ptr, out.ctypes.data_as(native.u64p)))
+        return {"ext_nodes": int(out[0]), "ext_tris": int(out[1]), "sh_nodes": int(out[2]), "sh_tris": int(out[3])}
 
     def last_kernel_ms(self) -> float:
         m = C.c_float()

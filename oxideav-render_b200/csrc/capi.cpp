@@ -34,8 +34,9 @@ struct pt_tracer {
   void *d_resolve = nullptr;
   size_t resolve_cap = 0;
   uint32_t w = 1, h = 1, samples = 0;
-  uint64_t ext = 0, sh = 0, nodes = 0, tris = 0;
+  uint64_t ext = 0, sh = 0, ext_nodes = 0, ext_tris = 0, sh_nodes = 0, sh_tris = 0;
   float last_ms = 0.0f;
+  float stage_ms[STAGE_COUNT] = {};
 };
 
 namespace {
@@ -134,6 +135,61 @@ SceneHost *find_scene(pt_context *ctx, uint32_t id) {
   return it == ctx->scenes.end() ? nullptr : it->second.get();
 }
 
+// (Re)allocates the wavefront arena for `capacity` slots with `shadow_slots`
+// queued shadow rays each and `iterations` bounce rounds.
+pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_slots, uint32_t iterations) {
+  WaveBuffers &w = ctx->wf;
+  if (ctx->wf_arena && w.capacity >= capacity && w.shadow_slots >= shadow_slots) {
+    if (w.iterations >= iterations) return PT_OK;
+  }
+  if (ctx->wf_arena) {
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->wf_arena);
+    ctx->wf_arena = nullptr;
+    ctx->wf_bytes = 0;
+  }
+  capacity = std::max(capacity, w.capacity);
+  shadow_slots = std::max(shadow_slots, w.shadow_slots);
+  iterations = std::max(iterations, w.iterations);
+  size_t P = capacity, S = shadow_slots;
+  size_t sizes[] = {16 * P, 16 * P, 16 * P, 16 * P, 16 * P, 16 * P, 16 * P,  // o d beta rad prev sigma seed
+                    16 * P, 4 * P,                                           // hit_tb hit_g
+                    16 * P * S, 16 * P * S, 16 * P * S, 4 * P,               // sh_o sh_d sh_c sh_n
+                    4 * P, 4 * P, 4 * P,                                     // q0 q1 q_shadow
+                    4 * (size_t)kWfCounterStride * (iterations + 1)};
+  size_t off[sizeof(sizes) / sizeof(sizes[0])], total = 0;
+  for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); ++i) {
+    total = (total + 255) & ~(size_t)255;
+    off[i] = total;
+    total += sizes[i];
+  }
+  CK(ctx, cudaMalloc(&ctx->wf_arena, total));
+  ctx->wf_bytes = total;
+  char *b = static_cast<char *>(ctx->wf_arena);
+  int k = 0;
+  w.o = (float4 *)(b + off[k++]);
+  w.d = (float4 *)(b + off[k++]);
+  w.beta = (float4 *)(b + off[k++]);
+  w.rad = (float4 *)(b + off[k++]);
+  w.prev = (float4 *)(b + off[k++]);
+  w.sigma = (float4 *)(b + off[k++]);
+  w.seed = (uint4 *)(b + off[k++]);
+  w.hit_tb = (float4 *)(b + off[k++]);
+  w.hit_g = (uint32_t *)(b + off[k++]);
+  w.sh_o = (float4 *)(b + off[k++]);
+  w.sh_d = (float4 *)(b + off[k++]);
+  w.sh_c = (float4 *)(b + off[k++]);
+  w.sh_n = (uint32_t *)(b + off[k++]);
+  w.q[0] = (uint32_t *)(b + off[k++]);
+  w.q[1] = (uint32_t *)(b + off[k++]);
+  w.q_shadow = (uint32_t *)(b + off[k++]);
+  w.counters = (uint32_t *)(b + off[k++]);
+  w.capacity = capacity;
+  w.shadow_slots = shadow_slots;
+  w.iterations = iterations;
+  return PT_OK;
+}
+
 pt_status refine_impl(pt_tracer *t, uint32_t n) {
   pt_context *ctx = t->ctx;
   if (!t->have_state || n == 0) return PT_OK;
@@ -166,19 +222,45 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
     max_slots = std::max<size_t>(max_slots, (size_t)w.pixel_count * w.spp);
     max_pix = std::max(max_pix, w.pixel_count);
   }
-  pt_status st = ensure(ctx, ctx->d_out, ctx->out_cap, max_slots);
+  const bool wavefront = ctx->schedule == PT_SCHEDULE_WAVEFRONT;
+  pt_status st = wavefront ? ensure_wavefront(ctx, (uint32_t)max_slots, sc->light_count + 1,
+                                              t->opts.path_trace.max_bounces + 1)
+                           : ensure(ctx, ctx->d_out, ctx->out_cap, max_slots);
   if (st != PT_OK) return st;
   st = ensure(ctx, ctx->d_segs, ctx->seg_cap, waves.size());
   if (st != PT_OK) return st;
   CK(ctx, cudaMemcpyAsync(ctx->d_segs, waves.data(), waves.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice,
                           ctx->stream));
   CK(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
+  StageTimer timer;
+  if (ctx->stage_timing) {
+    size_t need = waves.size() * (3 * (size_t)(t->opts.path_trace.max_bounces + 1) + 3) + 1;
+    while (ctx->stage_events.size() < need) {
+      cudaEvent_t ev;
+      CK(ctx, cudaEventCreate(&ev));
+      ctx->stage_events.push_back(ev);
+    }
+    timer.events = ctx->stage_events.data();
+    timer.capacity = ctx->stage_events.size();
+  }
   CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   for (size_t i = 0; i < waves.size(); ++i) {
     uint32_t total = waves[i].pixel_count * waves[i].spp;
-    CK(ctx, launch_megakernel(t->d_req, ctx->d_segs + i, 1, total, ctx->d_out, ctx->d_ctr, ctx->stream));
-    CK(ctx, launch_accumulate(t->d_req, ctx->d_segs + i, 1, waves[i].pixel_count, ctx->d_out, ctx->stream));
+    if (wavefront) {
+      WaveBuffers w = ctx->wf;
+      w.iterations = t->opts.path_trace.max_bounces + 1;
+      CK(ctx, launch_wavefront(t->d_req, ctx->d_segs + i, 1, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream,
+                               &timer));
+      timer.mark(STAGE_ACCUMULATE, ctx->stream);
+      CK(ctx, launch_accumulate(t->d_req, ctx->d_segs + i, 1, waves[i].pixel_count, w.rad, ctx->stream));
+    } else {
+      timer.mark(STAGE_MEGAKERNEL, ctx->stream);
+      CK(ctx, launch_megakernel(t->d_req, ctx->d_segs + i, 1, total, ctx->d_out, ctx->d_ctr, ctx->stream));
+      timer.mark(STAGE_ACCUMULATE, ctx->stream);
+      CK(ctx, launch_accumulate(t->d_req, ctx->d_segs + i, 1, waves[i].pixel_count, ctx->d_out, ctx->stream));
+    }
   }
+  timer.mark(STAGE_END, ctx->stream);
   CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
   DevCounters c;
   CK(ctx, cudaMemcpyAsync(&c, ctx->d_ctr, sizeof c, cudaMemcpyDeviceToHost, ctx->stream));
@@ -186,8 +268,16 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
   CK(ctx, cudaEventElapsedTime(&t->last_ms, ctx->ev0, ctx->ev1));
   t->ext = c.ext_rays;
   t->sh = c.shadow_rays;
-  t->nodes = c.nodes;
-  t->tris = c.tris;
+  t->ext_nodes = c.ext_nodes;
+  t->ext_tris = c.ext_tris;
+  t->sh_nodes = c.sh_nodes;
+  t->sh_tris = c.sh_tris;
+  for (int k = 0; k < STAGE_COUNT; ++k) t->stage_ms[k] = 0.0f;
+  for (size_t i = 0; i + 1 < timer.count(); ++i) {
+    float ms = 0.0f;
+    CK(ctx, cudaEventElapsedTime(&ms, ctx->stage_events[i], ctx->stage_events[i + 1]));
+    t->stage_ms[timer.kinds[i]] += ms;
+  }
   if (c.error_flags & ERR_STACK_OVERFLOW) return fail(ctx, PT_ERR_DEVICE, "BVH traversal stack overflow");
   t->samples += n;
   return PT_OK;
@@ -313,6 +403,7 @@ pt_status pt_create(pt_context **out, int device) {
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_ctr, sizeof(DevCounters));
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
       pt_destroy(ctx.release());
       return fail(nullptr, PT_ERR_DEVICE, std::string("context setup failed: ") + cudaGetErrorString(e));
@@ -329,8 +420,10 @@ void pt_destroy(pt_context *ctx) {
   for (auto &kv : ctx->scenes) release_scene(*kv.second);
   ctx->scenes.clear();
   if (ctx->d_out) cudaFree(ctx->d_out);
+  if (ctx->wf_arena) cudaFree(ctx->wf_arena);
   if (ctx->d_segs) cudaFree(ctx->d_segs);
   if (ctx->d_ctr) cudaFree(ctx->d_ctr);
+  for (cudaEvent_t ev : ctx->stage_events) cudaEventDestroy(ev);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -504,8 +597,29 @@ pt_status pt_tracer_ray_counts(const pt_tracer *t, uint64_t *ext, uint64_t *shad
 
 pt_status pt_tracer_traversal_counts(const pt_tracer *t, uint64_t *nodes, uint64_t *tris) {
   if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
-  if (nodes) *nodes = t->nodes;
-  if (tris) *tris = t->tris;
+  if (nodes) *nodes = t->ext_nodes + t->sh_nodes;
+  if (tris) *tris = t->ext_tris + t->sh_tris;
+  return PT_OK;
+}
+
+pt_status pt_tracer_traversal_split(const pt_tracer *t, uint64_t out[4]) {
+  if (!t || !out) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  out[0] = t->ext_nodes;
+  out[1] = t->ext_tris;
+  out[2] = t->sh_nodes;
+  out[3] = t->sh_tris;
+  return PT_OK;
+}
+
+pt_status pt_set_stage_timing(pt_context *ctx, int on) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  ctx->stage_timing = on != 0;
+  return PT_OK;
+}
+
+pt_status pt_tracer_stage_ms(const pt_tracer *t, float *out, uint32_t n) {
+  if (!t || !out) return fail(t ? t->ctx : nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  for (uint32_t k = 0; k < n && k < (uint32_t)STAGE_COUNT; ++k) out[k] = t->stage_ms[k];
   return PT_OK;
 }
 
@@ -543,7 +657,8 @@ pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *c
 // ---------------------------------------------------------------- debug hooks
 pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule) {
   if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
-  if (schedule != PT_SCHEDULE_MEGAKERNEL) return fail(ctx, PT_ERR_INVALID_ARG, "unknown schedule");
+  if (schedule != PT_SCHEDULE_MEGAKERNEL && schedule != PT_SCHEDULE_WAVEFRONT)
+    return fail(ctx, PT_ERR_INVALID_ARG, "unknown schedule");
   ctx->schedule = schedule;
   return PT_OK;
 }

@@ -7,6 +7,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/pt_b200.h"
 #include "../../include/pt_b200_debug.h"
@@ -26,6 +27,13 @@ struct pt_context {
   size_t seg_cap = 0;
   ptd::DevCounters *d_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int num_sms = 148;
+  bool stage_timing = false;
+  std::vector<cudaEvent_t> stage_events;
+  // Wavefront schedule: one arena holding the SoA path state and queues.
+  ptd::WaveBuffers wf{};
+  void *wf_arena = nullptr;
+  size_t wf_bytes = 0;
 };
 
 namespace ptd {

@@ -35,8 +35,28 @@ struct ShadowRay {
 };
 
 struct ThreadStats {
-  uint32_t ext_rays, shadow_rays, nodes, tris, err;
+  uint32_t ext_rays, shadow_rays, ext_nodes, ext_tris, sh_nodes, sh_tris, err;
 };
+
+// Warp-reduces the per-thread counters into the launch's DevCounters.
+PT_DEV void flush_stats(DevCounters *ctr, const ThreadStats &ts) {
+  unsigned long long v[6] = {ts.ext_rays, ts.shadow_rays, ts.ext_nodes, ts.ext_tris, ts.sh_nodes, ts.sh_tris};
+  unsigned int err = ts.err;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    err |= __shfl_down_sync(0xffffffffu, err, off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    unsigned long long *dst[6] = {&ctr->ext_rays, &ctr->shadow_rays, &ctr->ext_nodes,
+                                  &ctr->ext_tris, &ctr->sh_nodes, &ctr->sh_tris};
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      if (v[k]) atomicAdd(dst[k], v[k]);
+    if (err) atomicOr(&ctr->error_flags, err);
+  }
+}
 
 PT_DEV V3 clamp_contrib(const DevRequest &rq, V3 c) {
   float m = max3(c);
@@ -127,8 +147,8 @@ PT_DEV bool trace_extension(const DevRequest &rq, const PathState &ps, Hit &hit,
   TraversalStats st{0, 0};
   ts.ext_rays++;
   bool found = closest_hit(s, ps.o, ps.d, 0.0f, inf(), acc, hit, st, ts.err);
-  ts.nodes += st.nodes;
-  ts.tris += st.tris;
+  ts.ext_nodes += st.nodes;
+  ts.ext_tris += st.tris;
   return found;
 }
 
@@ -138,8 +158,8 @@ PT_DEV bool trace_shadow(const DevRequest &rq, const PathState &ps, const Shadow
   TraversalStats st{0, 0};
   ts.shadow_rays++;
   bool occ = occluded(s, sr.o, sr.d, 0.0f, sr.tmax, acc, st, ts.err);
-  ts.nodes += st.nodes;
-  ts.tris += st.tris;
+  ts.sh_nodes += st.nodes;
+  ts.sh_tris += st.tris;
   return !occ;
 }
 

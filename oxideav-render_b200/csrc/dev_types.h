@@ -116,11 +116,35 @@ struct WaveSegment {
   uint32_t pad0, pad1;
 };
 
+// Structure-of-arrays path state of one wave of the wavefront schedule
+// (wavefront.cuh), `capacity` slots, `shadow_slots` queued shadow rays per
+// slot.
+constexpr uint32_t kWfCounterStride = 4;  // per iteration: active count, shadow count, spare, spare
+
+struct WaveBuffers {
+  float4 *o, *d, *beta, *rad, *prev, *sigma;
+  uint4 *seed;                 // pixel_seed, sample index, path_seed, request
+  float4 *hit_tb;              // t, b0, b1, b2
+  uint32_t *hit_g;             // global id | front << 31 | found << 30
+  float4 *sh_o, *sh_d, *sh_c;  // [shadow_slots][capacity]: (o, tmax), (d, ray id), (contrib, skip)
+  uint32_t *sh_n;              // shadow rays queued per slot
+  uint32_t *q[2];              // active queues (ping-pong by iteration)
+  uint32_t *q_shadow;
+  uint32_t *counters;          // [iterations][kWfCounterStride]
+  uint32_t capacity, shadow_slots, iterations, pad;
+};
+
 // Per-launch device counters (rays traced, traversal work, errors).
 struct DevCounters {
-  unsigned long long ext_rays, shadow_rays, nodes, tris;
+  unsigned long long ext_rays, shadow_rays;
+  unsigned long long ext_nodes, ext_tris;  // traversal work of closest-hit rays
+  unsigned long long sh_nodes, sh_tris;    // traversal work of any-hit (shadow) rays
   unsigned int error_flags, pad;
 };
+
+// Stages timed by the optional per-stage CUDA events.
+enum Stage : int { STAGE_RAYGEN = 0, STAGE_EXTEND, STAGE_SHADE, STAGE_SHADOW, STAGE_ACCUMULATE, STAGE_MEGAKERNEL,
+                   STAGE_END, STAGE_COUNT = STAGE_END };
 enum ErrorFlags : uint32_t { ERR_STACK_OVERFLOW = 1u };
 
 }  // namespace ptd

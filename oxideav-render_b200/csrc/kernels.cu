@@ -4,6 +4,7 @@
 
 #include "dev_integrator.cuh"
 #include "kernels.h"
+#include "wavefront.cuh"
 
 namespace ptd {
 
@@ -19,26 +20,6 @@ PT_DEV const WaveSegment &find_segment(const WaveSegment *segs, uint32_t nseg, u
       hi = mid;
   }
   return segs[lo];
-}
-
-PT_DEV void flush_stats(DevCounters *ctr, const ThreadStats &ts) {
-  unsigned long long e = ts.ext_rays, s = ts.shadow_rays, n = ts.nodes, t = ts.tris;
-  unsigned int err = ts.err;
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    e += __shfl_down_sync(0xffffffffu, e, off);
-    s += __shfl_down_sync(0xffffffffu, s, off);
-    n += __shfl_down_sync(0xffffffffu, n, off);
-    t += __shfl_down_sync(0xffffffffu, t, off);
-    err |= __shfl_down_sync(0xffffffffu, err, off);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&ctr->ext_rays, e);
-    atomicAdd(&ctr->shadow_rays, s);
-    atomicAdd(&ctr->nodes, n);
-    atomicAdd(&ctr->tris, t);
-    if (err) atomicOr(&ctr->error_flags, err);
-  }
 }
 
 PT_DEV void slot_pixel(const DevRequest &rq, const WaveSegment &seg, uint32_t slot, uint32_t &x, uint32_t &y,
@@ -64,7 +45,7 @@ struct ImmediateSink {
 __global__ void __launch_bounds__(128) k_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg,
                                                     uint32_t total, float4 *out, DevCounters *ctr) {
   uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-  ThreadStats ts{0, 0, 0, 0, 0};
+  ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
   if (slot < total) {
     const WaveSegment &seg = find_segment(segs, nseg, slot);
     const DevRequest &rq = reqs[seg.request];
@@ -96,6 +77,8 @@ __global__ void k_accumulate(const DevRequest *reqs, const WaveSegment *segs, co
   for (uint32_t s = 0; s < seg.spp; ++s) {
     float4 v = src[(size_t)s * seg.pixel_count];
     if (v.w > 0.0f) {
+      // Non-finite radiance counts as a covered black sample (src/pathtrace.rs:2324-2328).
+      if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) v = make_float4(0.0f, 0.0f, 0.0f, v.w);
       a.x += (double)v.x;
       a.y += (double)v.y;
       a.z += (double)v.z;
@@ -221,7 +204,7 @@ __global__ void k_debug_pattern(const DevRequest *rq, uint32_t index, uint32_t p
 __global__ void k_debug_primary(const DevRequest *rq, uint32_t index, uint32_t *out_g, float4 *out_tb,
                                 DevCounters *ctr) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  ThreadStats ts{0, 0, 0, 0, 0};
+  ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
   if (i < rq->width * rq->height) {
     PathState ps;
     init_path(*rq, i % rq->width, i / rq->width, index, ps);
@@ -313,6 +296,30 @@ cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, u
   k_megakernel<<<(total + 127) / 128, 128, 0, st>>>(reqs, segs, nseg, total, out, ctr);
   return LAUNCH_CHECK();
 }
+// One wave of the wavefront schedule: raygen, then `w.iterations` rounds of
+// extend / shade / shadow over device-side queue counters (no host sync).
+cudaError_t launch_wavefront(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
+                             const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
+                             StageTimer *timer) {
+  if (total == 0) return cudaSuccess;
+  StageTimer none;
+  StageTimer &tm = timer ? *timer : none;
+  cudaError_t e = cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * kWfCounterStride * (w.iterations + 1), st);
+  if (e != cudaSuccess) return e;
+  tm.mark(STAGE_RAYGEN, st);
+  k_wf_raygen<<<(total + 255) / 256, 256, 0, st>>>(reqs, segs, nseg, total, w);
+  const uint32_t g_ext = (uint32_t)num_sms * 8, g_shade = (uint32_t)num_sms * 6, g_sh = (uint32_t)num_sms * 8;
+  for (uint32_t it = 0; it < w.iterations; ++it) {
+    tm.mark(STAGE_EXTEND, st);
+    k_wf_extend<<<g_ext, 256, 0, st>>>(reqs, w, it, ctr);
+    tm.mark(STAGE_SHADE, st);
+    k_wf_shade<<<g_shade, 128, 0, st>>>(reqs, w, it);
+    tm.mark(STAGE_SHADOW, st);
+    k_wf_shadow<<<g_sh, 256, 0, st>>>(reqs, w, it, ctr);
+  }
+  return LAUNCH_CHECK();
+}
+
 cudaError_t launch_accumulate(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t max_pixels,
                               const float4 *out, cudaStream_t st) {
   if (nseg == 0 || max_pixels == 0) return cudaSuccess;

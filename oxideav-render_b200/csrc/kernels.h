@@ -3,13 +3,32 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "dev_types.h"
 
 namespace ptd {
 
+// Optional per-stage CUDA events: mark(kind) records the next event of a
+// caller-owned pool on the stream; consecutive events bracket one stage.
+struct StageTimer {
+  cudaEvent_t *events = nullptr;
+  size_t capacity = 0;
+  std::vector<int> kinds;
+  size_t count() const { return kinds.size(); }
+  void mark(int kind, cudaStream_t st) {
+    if (!events || kinds.size() >= capacity) return;
+    cudaEventRecord(events[kinds.size()], st);
+    kinds.push_back(kind);
+  }
+};
+
 cudaError_t set_tables(const float *sheen_lut, const float *srgb_thresh);
 cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
                               float4 *out, DevCounters *ctr, cudaStream_t st);
+cudaError_t launch_wavefront(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
+                             const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
+                             StageTimer *timer = nullptr);
 cudaError_t launch_accumulate(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t max_pixels,
                               const float4 *out, cudaStream_t st);
 cudaError_t launch_resolve_hdr(const double *accum, uint32_t n, uint32_t samples, float4 bg, float4 *out,

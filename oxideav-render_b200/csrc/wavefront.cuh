@@ -1,0 +1,206 @@
+// Wavefront schedule of the path loop: the per-vertex steps of
+// dev_integrator.cuh run as separate kernels over compacted queues of path
+// slots, with the path state held in structure-of-arrays form.
+//
+//   k_wf_raygen   camera rays for every slot of the wave (active queue 0);
+//   k_wf_extend   closest hit of each queued path (traversal only: small
+//                 register footprint, high occupancy);
+//   k_wf_shade    emission, material, BSDF, NEE shadow-ray generation,
+//                 BSDF sampling, roulette; survivors are appended to the next
+//                 active queue and paths with shadow rays to the shadow queue
+//                 (warp-aggregated atomics);
+//   k_wf_shadow   each queued path's shadow rays, in generation order; a
+//                 visible ray adds its contribution to the path radiance.
+// The contributions of a vertex therefore reach the radiance sum in the
+// reference's order (emission, punctual lights, area sample, next vertex):
+// the per-sample radiance is bit-identical to the megakernel's.
+// Queue lengths live in device memory (one counter block per bounce), so a
+// wave runs max_bounces + 1 iterations without a host round trip; kernels
+// of an exhausted iteration exit at once.
+#pragma once
+
+#include "dev_integrator.cuh"
+
+namespace ptd {
+
+enum : uint32_t { HIT_FRONT = 1u << 31, HIT_FOUND = 1u << 30, HIT_G_MASK = (1u << 30) - 1u };
+enum : uint32_t { PF_MEDIUM = 1u, PF_COVERED = 2u, PF_HERO_SHIFT = 2u };
+
+PT_DEV void wf_store(const WaveBuffers &w, uint32_t slot, const PathState &ps, uint32_t request) {
+  w.o[slot] = make_float4(ps.o.x, ps.o.y, ps.o.z, __uint_as_float(ps.k));
+  w.d[slot] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.prev_pdf);
+  uint32_t flags = (ps.has_medium ? PF_MEDIUM : 0u) | (ps.covered ? PF_COVERED : 0u) |
+                   ((uint32_t)(ps.hero + 1) << PF_HERO_SHIFT);
+  w.beta[slot] = make_float4(ps.beta.x, ps.beta.y, ps.beta.z, __uint_as_float(flags));
+  w.rad[slot] = make_float4(ps.radiance.x, ps.radiance.y, ps.radiance.z, ps.covered ? 1.0f : 0.0f);
+  w.prev[slot] = make_float4(ps.prev_pos.x, ps.prev_pos.y, ps.prev_pos.z, 0.0f);
+  w.sigma[slot] = make_float4(ps.sigma.x, ps.sigma.y, ps.sigma.z, 0.0f);
+  w.seed[slot] = make_uint4(ps.smp.pixel_seed, ps.smp.index, ps.smp.path_seed, request);
+}
+
+PT_DEV uint32_t wf_load(const WaveBuffers &w, uint32_t slot, PathState &ps) {
+  float4 o = w.o[slot], d = w.d[slot], b = w.beta[slot], r = w.rad[slot], p = w.prev[slot], s = w.sigma[slot];
+  uint4 sd = w.seed[slot];
+  ps.o = {o.x, o.y, o.z};
+  ps.k = __float_as_uint(o.w);
+  ps.d = {d.x, d.y, d.z};
+  ps.prev_pdf = d.w;
+  uint32_t flags = __float_as_uint(b.w);
+  ps.beta = {b.x, b.y, b.z};
+  ps.has_medium = (flags & PF_MEDIUM) ? 1u : 0u;
+  ps.covered = (flags & PF_COVERED) ? 1u : 0u;
+  ps.hero = (int32_t)(flags >> PF_HERO_SHIFT) - 1;
+  ps.radiance = {r.x, r.y, r.z};
+  ps.prev_pos = {p.x, p.y, p.z};
+  ps.sigma = {s.x, s.y, s.z};
+  ps.smp.pixel_seed = sd.x;
+  ps.smp.index = sd.y;
+  ps.smp.path_seed = sd.z;
+  return sd.w;
+}
+
+// Warp-aggregated append: one atomic per warp for the lanes with `pred`.
+PT_DEV void wf_append(uint32_t *queue, uint32_t *count, bool pred, uint32_t value) {
+  uint32_t active = __activemask();
+  uint32_t mask = __ballot_sync(active, pred);
+  if (mask == 0) return;
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(mask));
+  base = __shfl_sync(active, base, leader);
+  if (pred) queue[base + __popc(mask & ((1u << lane) - 1u))] = value;
+}
+
+struct DeferredSink {
+  const WaveBuffers *w;
+  uint32_t slot, count;
+  PT_DEV void emit(const ShadowRay &sr) {
+    if (count >= w->shadow_slots) return;  // host sizes shadow_slots >= lights + 1
+    size_t i = (size_t)count * w->capacity + slot;
+    w->sh_o[i] = make_float4(sr.o.x, sr.o.y, sr.o.z, sr.tmax);
+    w->sh_d[i] = make_float4(sr.d.x, sr.d.y, sr.d.z, __uint_as_float(sr.ray_id));
+    w->sh_c[i] = make_float4(sr.contrib.x, sr.contrib.y, sr.contrib.z, __uint_as_float(sr.skip));
+    ++count;
+  }
+};
+
+__global__ void __launch_bounds__(256) k_wf_raygen(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg,
+                                                   uint32_t total, WaveBuffers w) {
+  uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot == 0) w.counters[0] = total;
+  if (slot >= total) return;
+  uint32_t lo = 0, hi = nseg;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (segs[mid].slot_begin <= slot)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const WaveSegment &seg = segs[lo];
+  const DevRequest &rq = reqs[seg.request];
+  uint32_t local = slot - seg.slot_begin;
+  uint32_t s = local / seg.pixel_count, i = local - s * seg.pixel_count;
+  uint32_t p = seg.pixel_begin + i;
+  uint32_t y = p / rq.width, x = p - y * rq.width;
+  PathState ps;
+  init_path(rq, x, y, seg.sample_begin + s, ps);
+  wf_store(w, slot, ps, seg.request);
+  w.q[0][slot] = slot;
+}
+
+__global__ void __launch_bounds__(256) k_wf_extend(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+                                                   DevCounters *ctr) {
+  const uint32_t n = w.counters[iter * kWfCounterStride + 0];
+  const uint32_t *q = w.q[iter & 1u];
+  ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t slot = q[i];
+    float4 o = w.o[slot], d = w.d[slot];
+    uint4 sd = w.seed[slot];
+    const DevRequest &rq = reqs[sd.w];
+    PathState ps;
+    ps.o = {o.x, o.y, o.z};
+    ps.d = {d.x, d.y, d.z};
+    ps.k = __float_as_uint(o.w);
+    ps.smp.pixel_seed = sd.x;
+    ps.smp.index = sd.y;
+    ps.smp.path_seed = sd.z;
+    Hit h;
+    bool found = trace_extension(rq, ps, h, ts);
+    if (found) {
+      w.hit_tb[slot] = make_float4(h.t, h.b0, h.b1, h.b2);
+      w.hit_g[slot] = (h.g & HIT_G_MASK) | HIT_FOUND | (h.front ? HIT_FRONT : 0u);
+    } else {
+      w.hit_g[slot] = 0u;
+    }
+  }
+  flush_stats(ctr, ts);
+}
+
+__global__ void __launch_bounds__(128) k_wf_shade(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+  const uint32_t n = w.counters[iter * kWfCounterStride + 0];
+  const uint32_t *q = w.q[iter & 1u];
+  uint32_t *q_next = w.q[(iter + 1) & 1u];
+  uint32_t *n_next = w.counters + (iter + 1) * kWfCounterStride + 0;
+  uint32_t *n_shadow = w.counters + iter * kWfCounterStride + 1;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t slot = q[i];
+    PathState ps;
+    uint32_t request = wf_load(w, slot, ps);
+    const DevRequest &rq = reqs[request];
+    uint32_t hg = w.hit_g[slot];
+    bool found = (hg & HIT_FOUND) != 0;
+    Hit h;
+    if (found) {
+      float4 tb = w.hit_tb[slot];
+      h.t = tb.x;
+      h.b0 = tb.y;
+      h.b1 = tb.z;
+      h.b2 = tb.w;
+      h.g = hg & HIT_G_MASK;
+      h.front = (hg & HIT_FRONT) != 0;
+    }
+    DeferredSink sink{&w, slot, 0};
+    bool alive = shade(rq, ps, found, h, sink);
+    wf_store(w, slot, ps, request);
+    w.sh_n[slot] = sink.count;
+    wf_append(q_next, n_next, alive, slot);
+    wf_append(w.q_shadow, n_shadow, sink.count > 0, slot);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_wf_shadow(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+                                                   DevCounters *ctr) {
+  const uint32_t n = w.counters[iter * kWfCounterStride + 1];
+  ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t slot = w.q_shadow[i];
+    uint4 sd = w.seed[slot];
+    const DevRequest &rq = reqs[sd.w];
+    PathState ps;
+    ps.smp.pixel_seed = sd.x;
+    ps.smp.index = sd.y;
+    ps.smp.path_seed = sd.z;
+    float4 r = w.rad[slot];
+    V3 rad = {r.x, r.y, r.z};
+    uint32_t cnt = w.sh_n[slot];
+    for (uint32_t j = 0; j < cnt; ++j) {
+      size_t k = (size_t)j * w.capacity + slot;
+      float4 so = w.sh_o[k], sdd = w.sh_d[k], sc = w.sh_c[k];
+      ShadowRay sr;
+      sr.o = {so.x, so.y, so.z};
+      sr.tmax = so.w;
+      sr.d = {sdd.x, sdd.y, sdd.z};
+      sr.ray_id = __float_as_uint(sdd.w);
+      sr.contrib = {sc.x, sc.y, sc.z};
+      sr.skip = __float_as_uint(sc.w);
+      if (trace_shadow(rq, ps, sr, ts)) rad = vadd(rad, sr.contrib);
+    }
+    w.rad[slot] = make_float4(rad.x, rad.y, rad.z, r.w);
+  }
+  flush_stats(ctr, ts);
+}
+
+}  // namespace ptd

@@ -67,6 +67,9 @@ SIGNATURES = {
     "pt_debug_primary_hits": (i32, [vp, u32, u32p, fp]),
     "pt_debug_bsdf": (i32, [vp, fp, fp, fp, u32, fp]),
     "pt_tracer_traversal_counts": (i32, [vp, u64p, u64p]),
+    "pt_tracer_traversal_split": (i32, [vp, u64p]),
+    "pt_set_stage_timing": (i32, [vp, i32]),
+    "pt_tracer_stage_ms": (i32, [vp, fp, u32]),
     "pt_scene_bvh_stats": (i32, [vp, u32, u32p, u32p, u32p, dp, dp]),
     "pt_set_schedule": (i32, [vp, u32]),
     "pt_set_wave_slots": (i32, [vp, u32]),

@@ -48,6 +48,44 @@ def test_refinement_is_additive_across_waves(ctx):
         ctx.set_wave_slots(1 << 22)
 
 
+def _accum_with(ctx, schedule, scene, opts, env=None):
+    ctx.set_schedule(schedule)
+    try:
+        t = api.PathTracer(ctx)
+        if env is not None:
+            t.set_environment(api.EnvironmentMap(env))
+        t.sync(scene, opts)
+        t.refine(opts.path_trace.samples_per_pixel)
+        out = t.accum(), t.ray_counts(), t.traversal_counts()
+        t.close()
+        return out
+    finally:
+        ctx.set_schedule(0)
+
+
+@pytest.mark.parametrize("case", ["cornell", "spheres", "materials", "env", "alpha", "dispersion"])
+def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
+    env = None
+    if case == "cornell":
+        scene, opts = ts.cornell_c0()
+        opts = opts.replace(width=96, height=80, path_trace=PathTraceOptions(samples_per_pixel=8, max_bounces=8))
+    elif case == "spheres":
+        scene, opts = ts.sphere_grid_c1(96, 4)
+    elif case == "materials":
+        scene, opts = ts.material_extensions(), ts.pt_opts(80, 4, 6)
+    elif case == "env":
+        scene, opts = ts.area_light_scene(0.35, 0.5), ts.pt_opts(48, 8, 4)
+        env = ts.env_noise(64, 32, np.random.default_rng(4))
+    elif case == "alpha":
+        scene, opts = ts.alpha_planes(), ts.pt_opts(48, 8, 4)
+    else:
+        scene, opts = ts.dispersive_sphere(1.0), ts.pt_opts(48, 8, 8)
+    a, ra, ta = _accum_with(ctx, 0, scene, opts, env)
+    b, rb, tb = _accum_with(ctx, 1, scene, opts, env)
+    assert np.array_equal(a, b)
+    assert ra == rb and ta == tb
+
+
 def test_sync_resets_only_on_radiance_changes(ctx):
     scene = ts.area_light_scene(0.5, 0.0)
     o = ts.pt_opts(6, 8, 2)
