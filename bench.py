@@ -117,6 +117,91 @@ def workload(name: str):
     raise SystemExit(f"unknown config {name}")
 
 
+def mixed_requests(n: int, seed: int, stress_grid: int = 1024, stress_spheres: int = 500):
+    """The batched workload: `n` requests, each drawing its scene uniformly
+    from {Cornell box, sphere grid, stress scene, 8 random soups of
+    10k-500k triangles}, its resolution from {128^2, 256^2, 512^2, 1024x768},
+    its spp from {1, 4, 16, 64} and its bounce limit from {2, 4, 8}."""
+    ts = entry.load_package().testscenes
+    from oxideav_render_b200.options import PathTraceOptions
+    rng = np.random.default_rng(seed)
+    scenes = {}
+
+    def scene(k):
+        if k not in scenes:
+            if k == 0:
+                s, o = ts.cornell_c0()
+                scenes[k] = (s, o, None)
+            elif k == 1:
+                s, o = ts.sphere_grid_c1(512, 256)
+                scenes[k] = (s, o, None)
+            elif k == 2:
+                s, o, env = ts.stress_c2(grid=stress_grid, spheres=stress_spheres)
+                scenes[k] = (s, o, env)
+            else:
+                tris = int(np.random.default_rng(100 + k).integers(10_000, 500_001))
+                s = ts.random_soup(tris, seed=100 + k)
+                scenes[k] = (s, ts.pt_opts(64, 1, 8, scene_camera=0, ambient=0.1), None)
+        return scenes[k]
+
+    res = [(128, 128), (256, 256), (512, 512), (1024, 768)]
+    out = []
+    for i in range(n):
+        k = int(rng.integers(0, 11))
+        w, h = res[int(rng.integers(0, 4))]
+        spp = [1, 4, 16, 64][int(rng.integers(0, 4))]
+        b = [2, 4, 8][int(rng.integers(0, 3))]
+        s, o, env = scene(k)
+        opts = o.replace(width=w, height=h, path_trace=PathTraceOptions(samples_per_pixel=spp, max_bounces=b,
+                                                                        seed=i))
+        out.append((k, s, opts, env))
+    return out, scenes
+
+
+def run_mixed(ctx, api, torch, n_requests: int, seed: int, check: int = 8):
+    """Plain per-request GPU path (each request synced, refined and read back
+    alone, one after another) against the batched path (all requests in one
+    pt_tracer_refine_many call, then read back). Returns the comparison."""
+    reqs, scenes = mixed_requests(n_requests, seed)
+    tracers = []
+    for k, s, o, env in reqs:
+        t = api.PathTracer(ctx)
+        if env is not None:
+            t.set_environment(api.EnvironmentMap(env))
+        t.sync(s, o)
+        tracers.append(t)
+    total = sum(o.width * o.height * o.path_trace.samples_per_pixel for _, _, o, _ in reqs)
+    # Warm-up (loads modules, allocates wave buffers).
+    api.refine_many(ctx, tracers[:4], [1] * 4)
+    for t in tracers[:4]:
+        t.reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for t, (_, _, o, _) in zip(tracers, reqs):
+        t.refine(o.path_trace.samples_per_pixel)
+        t.hdr()
+    plain_s = time.perf_counter() - t0
+    plain_acc = [tracers[i].accum() for i in range(min(check, len(tracers)))]
+    for t in tracers:
+        t.reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    api.refine_many(ctx, tracers, [o.path_trace.samples_per_pixel for _, _, o, _ in reqs])
+    for t in tracers:
+        t.hdr()
+    batched_s = time.perf_counter() - t0
+    st = api.batch_stats(ctx)
+    identical = all(np.array_equal(tracers[i].accum(), plain_acc[i]) for i in range(len(plain_acc)))
+    for t in tracers:
+        t.close()
+    return {"requests": n_requests, "samples": int(total), "plain_s": plain_s, "batched_s": batched_s,
+            "plain_samples_per_s": total / plain_s, "batched_samples_per_s": total / batched_s,
+            "speedup": plain_s / batched_s, "batched_waves": st["waves"],
+            "batched_mrays_per_s": st["rays"] / (st["ms"] / 1000.0) / 1e6 if st["ms"] > 0 else None,
+            "bit_identical_checked": len(plain_acc), "bit_identical": identical,
+            "timing": "wall clock, host submit to HDR readback of every request"}
+
+
 def algorithmic_bytes(ext_rays, shadow_rays, nodes, tris, samples):
     """Byte model per unit of work: per traced ray 32 B ray + 16 B hit, 64 B
     per BVH node visited, 48 B per triangle record tested; per shaded vertex
@@ -332,6 +417,9 @@ def run_b200(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_t,
                "call": "PathTraceCudaRenderer.render (scene upload incl. host BVH build, refine, "
                        "sRGB image readback)"}
+    mixed = None
+    if args.mixed > 0:
+        mixed = run_mixed(ctx, api, torch, args.mixed, 2026 + rank)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene, opts, env, args.cpu_seconds)
@@ -351,6 +439,7 @@ def run_b200(args):
                          "bytes_per_launch": stage_bytes[dom] / max(launches_of_dom, 1),
                          "ms_per_launch": stage[dom] / max(launches_of_dom, 1)},
             "e2e": e2e,
+            "batched_mixed": mixed,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,
@@ -377,6 +466,7 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=8)
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling cases)")
     ap.add_argument("--schedule", default="wavefront", choices=["megakernel", "wavefront"])
+    ap.add_argument("--mixed", type=int, default=64, help="requests in the batched-vs-plain comparison (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -323,6 +323,16 @@ PT_API pt_status pt_tracer_sync(pt_tracer *tr, uint32_t scene_id, const pt_camer
  * bit for bit. Blocks until the device work is done. */
 PT_API pt_status pt_tracer_refine(pt_tracer *tr, uint32_t samples);
 PT_API pt_status pt_tracer_samples(const pt_tracer *tr, uint32_t *samples);
+/* Batched refine (no counterpart in the reference, which refines one
+ * tracer at a time): adds samples[i] samples to tracers[i] for every i, all
+ * in shared waves of path slots on the context's device, each path reading
+ * its own tracer's scene, camera, options and accumulator. Every tracer ends
+ * bit-identical to pt_tracer_refine(tracers[i], samples[i]) run alone. All
+ * tracers must belong to ctx and appear once. */
+PT_API pt_status pt_tracer_refine_many(pt_context *ctx, pt_tracer *const *tracers, const uint32_t *samples,
+                                       uint32_t count);
+/* Device time, wave count and rays traced of the last refine / batch. */
+PT_API pt_status pt_batch_stats(const pt_context *ctx, float *ms, uint32_t *waves, uint64_t *rays);
 PT_API pt_status pt_tracer_is_converged(const pt_tracer *tr, int *converged);
 PT_API pt_status pt_tracer_reset(pt_tracer *tr);
 PT_API pt_status pt_tracer_invalidate_scene(pt_tracer *tr);

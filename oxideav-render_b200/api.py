@@ -282,6 +282,21 @@ class PathTracer:
         return g, tb
 
 
+def refine_many(ctx: Context, tracers, samples) -> None:
+    """Batched refine: tracers[i] gains samples[i] samples, all in shared
+    waves (bit-identical to refining each alone)."""
+    n = len(tracers)
+    arr = (C.c_void_p * max(n, 1))(*[t.ptr for t in tracers])
+    sp = (C.c_uint32 * max(n, 1))(*[int(s) for s in samples])
+    ctx.check(ctx.lib.pt_tracer_refine_many(ctx.ptr, arr, sp, n))
+
+
+def batch_stats(ctx: Context) -> dict:
+    ms, waves, rays = C.c_float(), C.c_uint32(), C.c_uint64()
+    ctx.check(ctx.lib.pt_batch_stats(ctx.ptr, C.byref(ms), C.byref(waves), C.byref(rays)))
+    return {"ms": ms.value, "waves": waves.value, "rays": rays.value}
+
+
 class PathTraceCudaRenderer:
     """Renderer for RenderBackend::PathTraceCuda (PathTraceRenderer semantics)."""
 

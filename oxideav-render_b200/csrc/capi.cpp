@@ -190,51 +190,105 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   return PT_OK;
 }
 
-pt_status refine_impl(pt_tracer *t, uint32_t n) {
-  pt_context *ctx = t->ctx;
-  if (!t->have_state || n == 0) return PT_OK;
-  n = std::min(n, 0xffffffffu - t->samples);
-  if (n == 0) return PT_OK;
-  SceneHost *sc = find_scene(ctx, t->scene_id);
-  if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
-  CK(ctx, cudaSetDevice(ctx->device));
-  DevRequest rq = make_request(*t, *sc);
-  CK(ctx, cudaMemcpyAsync(t->d_req, &rq, sizeof rq, cudaMemcpyHostToDevice, ctx->stream));
-  const uint64_t npix = (uint64_t)t->w * t->h;
-  const uint64_t cap = std::max<uint32_t>(ctx->wave_slots, 1024);
-  std::vector<WaveSegment> waves;
-  uint32_t done = 0;
-  while (done < n) {
-    if (npix <= cap) {
-      uint32_t c = (uint32_t)std::min<uint64_t>(n - done, std::max<uint64_t>(cap / npix, 1));
-      waves.push_back(WaveSegment{0, 0, 0, (uint32_t)npix, t->samples + done, c, 0, 0});
-      done += c;
-    } else {
-      for (uint64_t p0 = 0; p0 < npix; p0 += cap)
-        waves.push_back(
-            WaveSegment{0, 0, (uint32_t)p0, (uint32_t)std::min<uint64_t>(cap, npix - p0), t->samples + done, 1, 0, 0});
-      done += 1;
+// One refine job of a batch: `target` samples added to tracer `t`.
+struct Job {
+  pt_tracer *t;
+  uint32_t target;
+  uint32_t first;         // sample index of the job's first sample
+  uint32_t npix;
+  uint32_t done = 0;      // whole samples finished
+  uint32_t pix_done = 0;  // pixels of sample `done` finished (partial-pixel waves)
+  uint32_t iterations = 1;
+  uint32_t shadow_slots = 1;
+};
+
+// Packs the jobs' (pixel, sample) work into waves of at most `cap` path
+// slots. A job contributes at most one segment per wave, so the segments of
+// one wave never touch the same pixel twice and the accumulate kernel can
+// process them in parallel; within a job, waves run its samples in order.
+// One job packs exactly as a single-tracer refine: full-image segments of
+// floor(cap / pixels) samples, or one pixel range of one sample when the
+// image is larger than a wave.
+std::vector<std::vector<WaveSegment>> pack_waves(std::vector<Job> &jobs, uint64_t cap) {
+  std::vector<std::vector<WaveSegment>> waves;
+  for (;;) {
+    std::vector<WaveSegment> segs;
+    uint64_t slot = 0;
+    for (uint32_t j = 0; j < jobs.size() && slot < cap; ++j) {
+      Job &jb = jobs[j];
+      if (jb.done >= jb.target) continue;
+      uint64_t left = cap - slot;
+      if (jb.pix_done > 0 || jb.npix > left) {
+        uint32_t m = (uint32_t)std::min<uint64_t>(jb.npix - jb.pix_done, left);
+        if (m == 0) continue;
+        segs.push_back(WaveSegment{j, (uint32_t)slot, jb.pix_done, m, jb.first + jb.done, 1, 0, 0});
+        slot += m;
+        jb.pix_done += m;
+        if (jb.pix_done == jb.npix) {
+          jb.pix_done = 0;
+          jb.done += 1;
+        }
+      } else {
+        uint32_t c = (uint32_t)std::min<uint64_t>(jb.target - jb.done, left / jb.npix);
+        segs.push_back(WaveSegment{j, (uint32_t)slot, 0, jb.npix, jb.first + jb.done, c, 0, 0});
+        slot += (uint64_t)jb.npix * c;
+        jb.done += c;
+      }
     }
+    if (segs.empty()) break;
+    waves.push_back(std::move(segs));
   }
+  return waves;
+}
+
+// Runs a batch of refine jobs in merged waves: every wave carries path
+// slots of several tracers, each path reading its own request (scene,
+// camera, options, accumulator). Per-sample radiance is a pure function of
+// (request, pixel, sample), and each pixel's samples are accumulated in
+// sample order, so every tracer ends bit-identical to refining it alone.
+pt_status run_jobs(pt_context *ctx, std::vector<Job> &jobs, pt_tracer *stats_to) {
+  if (jobs.empty()) return PT_OK;
+  CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<DevRequest> reqs(jobs.size());
+  uint32_t max_iter = 1, max_shadow = 1;
+  for (size_t j = 0; j < jobs.size(); ++j) {
+    pt_tracer *t = jobs[j].t;
+    SceneHost *sc = find_scene(ctx, t->scene_id);
+    if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
+    reqs[j] = make_request(*t, *sc);
+    jobs[j].iterations = t->opts.path_trace.max_bounces + 1;
+    jobs[j].shadow_slots = sc->light_count + 1;
+    max_iter = std::max(max_iter, jobs[j].iterations);
+    max_shadow = std::max(max_shadow, jobs[j].shadow_slots);
+  }
+  const uint64_t cap = std::max<uint32_t>(ctx->wave_slots, 1024);
+  std::vector<std::vector<WaveSegment>> waves = pack_waves(jobs, cap);
+  std::vector<WaveSegment> flat;
+  std::vector<size_t> first_seg;
   size_t max_slots = 0;
-  uint32_t max_pix = 0;
-  for (const WaveSegment &w : waves) {
-    max_slots = std::max<size_t>(max_slots, (size_t)w.pixel_count * w.spp);
-    max_pix = std::max(max_pix, w.pixel_count);
+  for (auto &w : waves) {
+    first_seg.push_back(flat.size());
+    size_t slots = 0;
+    for (WaveSegment &s : w) {
+      slots += (size_t)s.pixel_count * s.spp;
+      flat.push_back(s);
+    }
+    max_slots = std::max(max_slots, slots);
   }
   const bool wavefront = ctx->schedule == PT_SCHEDULE_WAVEFRONT;
-  pt_status st = wavefront ? ensure_wavefront(ctx, (uint32_t)max_slots, sc->light_count + 1,
-                                              t->opts.path_trace.max_bounces + 1)
+  pt_status st = wavefront ? ensure_wavefront(ctx, (uint32_t)max_slots, max_shadow, max_iter)
                            : ensure(ctx, ctx->d_out, ctx->out_cap, max_slots);
   if (st != PT_OK) return st;
-  st = ensure(ctx, ctx->d_segs, ctx->seg_cap, waves.size());
-  if (st != PT_OK) return st;
-  CK(ctx, cudaMemcpyAsync(ctx->d_segs, waves.data(), waves.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice,
+  if ((st = ensure(ctx, ctx->d_segs, ctx->seg_cap, flat.size())) != PT_OK) return st;
+  if ((st = ensure(ctx, ctx->d_reqs, ctx->req_cap, reqs.size())) != PT_OK) return st;
+  CK(ctx, cudaMemcpyAsync(ctx->d_reqs, reqs.data(), reqs.size() * sizeof(DevRequest), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  CK(ctx, cudaMemcpyAsync(ctx->d_segs, flat.data(), flat.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice,
                           ctx->stream));
   CK(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
   StageTimer timer;
   if (ctx->stage_timing) {
-    size_t need = waves.size() * (3 * (size_t)(t->opts.path_trace.max_bounces + 1) + 3) + 1;
+    size_t need = waves.size() * (3 * (size_t)max_iter + 3) + 1;
     while (ctx->stage_events.size() < need) {
       cudaEvent_t ev;
       CK(ctx, cudaEventCreate(&ev));
@@ -245,19 +299,24 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
   }
   CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   for (size_t i = 0; i < waves.size(); ++i) {
-    uint32_t total = waves[i].pixel_count * waves[i].spp;
+    const WaveSegment *segs = ctx->d_segs + first_seg[i];
+    uint32_t nseg = (uint32_t)waves[i].size(), total = 0, max_pix = 0, iters = 1;
+    for (const WaveSegment &s : waves[i]) {
+      total += s.pixel_count * s.spp;
+      max_pix = std::max(max_pix, s.pixel_count);
+      iters = std::max(iters, jobs[s.request].iterations);
+    }
     if (wavefront) {
       WaveBuffers w = ctx->wf;
-      w.iterations = t->opts.path_trace.max_bounces + 1;
-      CK(ctx, launch_wavefront(t->d_req, ctx->d_segs + i, 1, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream,
-                               &timer));
+      w.iterations = iters;
+      CK(ctx, launch_wavefront(ctx->d_reqs, segs, nseg, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream, &timer));
       timer.mark(STAGE_ACCUMULATE, ctx->stream);
-      CK(ctx, launch_accumulate(t->d_req, ctx->d_segs + i, 1, waves[i].pixel_count, w.rad, ctx->stream));
+      CK(ctx, launch_accumulate(ctx->d_reqs, segs, nseg, max_pix, w.rad, ctx->stream));
     } else {
       timer.mark(STAGE_MEGAKERNEL, ctx->stream);
-      CK(ctx, launch_megakernel(t->d_req, ctx->d_segs + i, 1, total, ctx->d_out, ctx->d_ctr, ctx->stream));
+      CK(ctx, launch_megakernel(ctx->d_reqs, segs, nseg, total, ctx->d_out, ctx->d_ctr, ctx->stream));
       timer.mark(STAGE_ACCUMULATE, ctx->stream);
-      CK(ctx, launch_accumulate(t->d_req, ctx->d_segs + i, 1, waves[i].pixel_count, ctx->d_out, ctx->stream));
+      CK(ctx, launch_accumulate(ctx->d_reqs, segs, nseg, max_pix, ctx->d_out, ctx->stream));
     }
   }
   timer.mark(STAGE_END, ctx->stream);
@@ -265,22 +324,52 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
   DevCounters c;
   CK(ctx, cudaMemcpyAsync(&c, ctx->d_ctr, sizeof c, cudaMemcpyDeviceToHost, ctx->stream));
   CK(ctx, cudaStreamSynchronize(ctx->stream));
-  CK(ctx, cudaEventElapsedTime(&t->last_ms, ctx->ev0, ctx->ev1));
-  t->ext = c.ext_rays;
-  t->sh = c.shadow_rays;
-  t->ext_nodes = c.ext_nodes;
-  t->ext_tris = c.ext_tris;
-  t->sh_nodes = c.sh_nodes;
-  t->sh_tris = c.sh_tris;
-  for (int k = 0; k < STAGE_COUNT; ++k) t->stage_ms[k] = 0.0f;
-  for (size_t i = 0; i + 1 < timer.count(); ++i) {
-    float ms = 0.0f;
-    CK(ctx, cudaEventElapsedTime(&ms, ctx->stage_events[i], ctx->stage_events[i + 1]));
-    t->stage_ms[timer.kinds[i]] += ms;
+  float ms = 0.0f;
+  CK(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  ctx->last_batch_ms = ms;
+  ctx->last_batch_waves = (uint32_t)waves.size();
+  if (stats_to) {
+    pt_tracer *t = stats_to;
+    t->last_ms = ms;
+    t->ext = c.ext_rays;
+    t->sh = c.shadow_rays;
+    t->ext_nodes = c.ext_nodes;
+    t->ext_tris = c.ext_tris;
+    t->sh_nodes = c.sh_nodes;
+    t->sh_tris = c.sh_tris;
+    for (int k = 0; k < STAGE_COUNT; ++k) t->stage_ms[k] = 0.0f;
+    for (size_t i = 0; i + 1 < timer.count(); ++i) {
+      float sm = 0.0f;
+      CK(ctx, cudaEventElapsedTime(&sm, ctx->stage_events[i], ctx->stage_events[i + 1]));
+      t->stage_ms[timer.kinds[i]] += sm;
+    }
   }
+  ctx->last_batch_rays = c.ext_rays + c.shadow_rays;
   if (c.error_flags & ERR_STACK_OVERFLOW) return fail(ctx, PT_ERR_DEVICE, "BVH traversal stack overflow");
-  t->samples += n;
+  for (Job &jb : jobs) jb.t->samples += jb.target;
   return PT_OK;
+}
+
+pt_status refine_impl(pt_tracer *t, uint32_t n) {
+  if (!t->have_state || n == 0) return PT_OK;
+  n = std::min(n, 0xffffffffu - t->samples);
+  if (n == 0) return PT_OK;
+  std::vector<Job> jobs{Job{t, n, t->samples, t->w * t->h}};
+  return run_jobs(t->ctx, jobs, t);
+}
+
+pt_status refine_many_impl(pt_context *ctx, pt_tracer *const *tracers, const uint32_t *samples, uint32_t count) {
+  std::vector<Job> jobs;
+  for (uint32_t i = 0; i < count; ++i) {
+    pt_tracer *t = tracers[i];
+    if (!t || t->ctx != ctx) return fail(ctx, PT_ERR_INVALID_ARG, "tracer " + std::to_string(i) + " is not of ctx");
+    for (uint32_t j = 0; j < i; ++j)
+      if (tracers[j] == t) return fail(ctx, PT_ERR_INVALID_ARG, "a tracer appears twice in one batch");
+    if (!t->have_state || samples[i] == 0) continue;
+    uint32_t n = std::min(samples[i], 0xffffffffu - t->samples);
+    if (n) jobs.push_back(Job{t, n, t->samples, t->w * t->h});
+  }
+  return run_jobs(ctx, jobs, jobs.size() == 1 ? jobs[0].t : nullptr);
 }
 
 pt_status sync_impl(pt_tracer *t, uint32_t scene_id, const pt_camera *cam, const pt_render_options *opts, int *reset) {
@@ -422,6 +511,7 @@ void pt_destroy(pt_context *ctx) {
   if (ctx->d_out) cudaFree(ctx->d_out);
   if (ctx->wf_arena) cudaFree(ctx->wf_arena);
   if (ctx->d_segs) cudaFree(ctx->d_segs);
+  if (ctx->d_reqs) cudaFree(ctx->d_reqs);
   if (ctx->d_ctr) cudaFree(ctx->d_ctr);
   for (cudaEvent_t ev : ctx->stage_events) cudaEventDestroy(ev);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -522,6 +612,21 @@ pt_status pt_tracer_sync(pt_tracer *t, uint32_t scene_id, const pt_camera *camer
 pt_status pt_tracer_refine(pt_tracer *t, uint32_t samples) {
   if (!t) return fail(nullptr, PT_ERR_INVALID_ARG, "tracer is NULL");
   return guard(t->ctx, [&] { return refine_impl(t, samples); });
+}
+
+pt_status pt_tracer_refine_many(pt_context *ctx, pt_tracer *const *tracers, const uint32_t *samples,
+                                uint32_t count) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (count && (!tracers || !samples)) return fail(ctx, PT_ERR_INVALID_ARG, "tracers / samples is NULL");
+  return guard(ctx, [&] { return refine_many_impl(ctx, tracers, samples, count); });
+}
+
+pt_status pt_batch_stats(const pt_context *ctx, float *ms, uint32_t *waves, uint64_t *rays) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (ms) *ms = ctx->last_batch_ms;
+  if (waves) *waves = ctx->last_batch_waves;
+  if (rays) *rays = ctx->last_batch_rays;
+  return PT_OK;
 }
 
 pt_status pt_tracer_samples(const pt_tracer *t, uint32_t *samples) {

@@ -25,6 +25,11 @@ struct pt_context {
   size_t out_cap = 0;
   ptd::WaveSegment *d_segs = nullptr;
   size_t seg_cap = 0;
+  ptd::DevRequest *d_reqs = nullptr;  // requests of the running batch
+  size_t req_cap = 0;
+  float last_batch_ms = 0.0f;
+  uint32_t last_batch_waves = 0;
+  uint64_t last_batch_rays = 0;
   ptd::DevCounters *d_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 148;

@@ -46,6 +46,8 @@ SIGNATURES = {
     "pt_tracer_sync": (i32, [vp, u32, C.POINTER(abi.pt_camera), C.POINTER(abi.pt_render_options),
                              C.POINTER(C.c_int)]),
     "pt_tracer_refine": (i32, [vp, u32]),
+    "pt_tracer_refine_many": (i32, [vp, C.POINTER(vp), u32p, u32]),
+    "pt_batch_stats": (i32, [vp, fp, u32p, u64p]),
     "pt_tracer_samples": (i32, [vp, u32p]),
     "pt_tracer_is_converged": (i32, [vp, C.POINTER(C.c_int)]),
     "pt_tracer_reset": (i32, [vp]),
