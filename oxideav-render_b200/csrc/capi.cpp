@@ -5,6 +5,7 @@
 // calls (:2526-2591) and the same resolve (:2593-2734), with the f64
 // accumulator resident on the device. No exception crosses the ABI: every
 // entry point catches and maps failures to a pt_status plus a message.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -20,24 +21,6 @@
 #include "kernels.h"
 
 using namespace ptd;
-
-struct pt_tracer {
-  pt_context *ctx = nullptr;
-  bool have_state = false, dirty = true;
-  uint32_t scene_id = 0;
-  pt_camera cam{};
-  pt_render_options opts{};
-  std::unique_ptr<EnvHost> env;
-  double *d_accum = nullptr;
-  size_t accum_cap = 0;
-  DevRequest *d_req = nullptr;
-  void *d_resolve = nullptr;
-  size_t resolve_cap = 0;
-  uint32_t w = 1, h = 1, samples = 0;
-  uint64_t ext = 0, sh = 0, ext_nodes = 0, ext_tris = 0, sh_nodes = 0, sh_tris = 0;
-  float last_ms = 0.0f;
-  float stage_ms[STAGE_COUNT] = {};
-};
 
 namespace {
 
@@ -103,11 +86,15 @@ pt_status validate_opts(pt_context *ctx, const pt_camera *cam, const pt_render_o
   return PT_OK;
 }
 
-DevRequest make_request(const pt_tracer &t, const SceneHost &sc) {
+}  // namespace
+
+namespace ptd {
+
+DevRequest make_request(const pt_tracer &t, const SceneHost &sc, const EnvHost *env) {
   DevRequest rq;
   std::memset(&rq, 0, sizeof rq);
   rq.scene = sc.d_desc;
-  rq.env = t.env ? t.env->d_desc : nullptr;
+  rq.env = env ? env->d_desc : nullptr;
   rq.cam = t.cam;
   rq.width = t.w;
   rq.height = t.h;
@@ -119,10 +106,56 @@ DevRequest make_request(const pt_tracer &t, const SceneHost &sc) {
   rq.seed = t.opts.path_trace.seed;
   rq.strategy = t.opts.path_trace.strategy;
   rq.clamp = t.opts.path_trace.clamp;
-  rq.p_env = t.env ? (sc.dev.em_count > 0 ? 0.5f : 1.0f) : 0.0f;
+  rq.p_env = env ? (sc.dev.em_count > 0 ? 0.5f : 1.0f) : 0.0f;
   rq.accum = t.d_accum;
   return rq;
 }
+
+Job make_job(const pt_tracer &t, const SceneHost &sc, const EnvHost *env, uint32_t n) {
+  Job j{};
+  j.req = make_request(t, sc, env);
+  j.target = n;
+  j.first = t.samples;
+  j.npix = t.w * t.h;
+  j.iterations = t.opts.path_trace.max_bounces + 1;
+  j.shadow_slots = sc.light_count + 1;
+  j.scene_key = t.scene_id;
+  return j;
+}
+
+std::vector<WaveSegment> pack_wave(std::vector<Job> &jobs, const std::vector<uint32_t> &order, uint64_t cap) {
+  std::vector<WaveSegment> segs;
+  uint64_t slot = 0;
+  for (uint32_t oj = 0; oj < order.size() && slot < cap; ++oj) {
+    const uint32_t j = order[oj];
+    Job &jb = jobs[j];
+    if (jb.finished()) continue;
+    uint64_t left = cap - slot;
+    if (jb.pix_done > 0 || jb.npix > left) {
+      // One pixel range of one sample (the image is larger than what is
+      // left of the wave, or a previous wave ended inside this sample).
+      uint32_t m = (uint32_t)std::min<uint64_t>(jb.npix - jb.pix_done, left);
+      if (m == 0) continue;
+      segs.push_back(WaveSegment{j, (uint32_t)slot, jb.pix_done, m, jb.first + jb.done, 1, 0, 0});
+      slot += m;
+      jb.pix_done += m;
+      if (jb.pix_done == jb.npix) {
+        jb.pix_done = 0;
+        jb.done += 1;
+      }
+    } else {
+      uint32_t c = (uint32_t)std::min<uint64_t>(jb.target - jb.done, left / jb.npix);
+      segs.push_back(WaveSegment{j, (uint32_t)slot, 0, jb.npix, jb.first + jb.done, c, 0, 0});
+      slot += (uint64_t)jb.npix * c;
+      jb.done += c;
+    }
+  }
+  return segs;
+}
+
+}  // namespace ptd
+
+namespace {
 
 float4 bg_linear(const pt_render_options &o) {
   return make_float4(host_srgb_to_linear((float)o.background[0] / 255.0f),
@@ -190,79 +223,33 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   return PT_OK;
 }
 
-// One refine job of a batch: `target` samples added to tracer `t`.
-struct Job {
-  pt_tracer *t;
-  uint32_t target;
-  uint32_t first;         // sample index of the job's first sample
-  uint32_t npix;
-  uint32_t done = 0;      // whole samples finished
-  uint32_t pix_done = 0;  // pixels of sample `done` finished (partial-pixel waves)
-  uint32_t iterations = 1;
-  uint32_t shadow_slots = 1;
-};
-
-// Packs the jobs' (pixel, sample) work into waves of at most `cap` path
-// slots. A job contributes at most one segment per wave, so the segments of
-// one wave never touch the same pixel twice and the accumulate kernel can
-// process them in parallel; within a job, waves run its samples in order.
-// One job packs exactly as a single-tracer refine: full-image segments of
-// floor(cap / pixels) samples, or one pixel range of one sample when the
-// image is larger than a wave.
-std::vector<std::vector<WaveSegment>> pack_waves(std::vector<Job> &jobs, uint64_t cap) {
-  std::vector<std::vector<WaveSegment>> waves;
-  for (;;) {
-    std::vector<WaveSegment> segs;
-    uint64_t slot = 0;
-    for (uint32_t j = 0; j < jobs.size() && slot < cap; ++j) {
-      Job &jb = jobs[j];
-      if (jb.done >= jb.target) continue;
-      uint64_t left = cap - slot;
-      if (jb.pix_done > 0 || jb.npix > left) {
-        uint32_t m = (uint32_t)std::min<uint64_t>(jb.npix - jb.pix_done, left);
-        if (m == 0) continue;
-        segs.push_back(WaveSegment{j, (uint32_t)slot, jb.pix_done, m, jb.first + jb.done, 1, 0, 0});
-        slot += m;
-        jb.pix_done += m;
-        if (jb.pix_done == jb.npix) {
-          jb.pix_done = 0;
-          jb.done += 1;
-        }
-      } else {
-        uint32_t c = (uint32_t)std::min<uint64_t>(jb.target - jb.done, left / jb.npix);
-        segs.push_back(WaveSegment{j, (uint32_t)slot, 0, jb.npix, jb.first + jb.done, c, 0, 0});
-        slot += (uint64_t)jb.npix * c;
-        jb.done += c;
-      }
-    }
-    if (segs.empty()) break;
-    waves.push_back(std::move(segs));
-  }
-  return waves;
-}
-
 // Runs a batch of refine jobs in merged waves: every wave carries path
 // slots of several tracers, each path reading its own request (scene,
 // camera, options, accumulator). Per-sample radiance is a pure function of
 // (request, pixel, sample), and each pixel's samples are accumulated in
 // sample order, so every tracer ends bit-identical to refining it alone.
-pt_status run_jobs(pt_context *ctx, std::vector<Job> &jobs, pt_tracer *stats_to) {
+pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vector<Job> &jobs,
+                   pt_tracer *stats_to) {
   if (jobs.empty()) return PT_OK;
   CK(ctx, cudaSetDevice(ctx->device));
-  std::vector<DevRequest> reqs(jobs.size());
   uint32_t max_iter = 1, max_shadow = 1;
-  for (size_t j = 0; j < jobs.size(); ++j) {
-    pt_tracer *t = jobs[j].t;
-    SceneHost *sc = find_scene(ctx, t->scene_id);
-    if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
-    reqs[j] = make_request(*t, *sc);
-    jobs[j].iterations = t->opts.path_trace.max_bounces + 1;
-    jobs[j].shadow_slots = sc->light_count + 1;
-    max_iter = std::max(max_iter, jobs[j].iterations);
-    max_shadow = std::max(max_shadow, jobs[j].shadow_slots);
+  for (const Job &jb : jobs) {
+    max_iter = std::max(max_iter, jb.iterations);
+    max_shadow = std::max(max_shadow, jb.shadow_slots);
   }
+  // Visit jobs grouped by scene (stable within a scene) so a wave mostly
+  // traverses one BVH: cache locality only, results do not depend on it.
+  std::vector<uint32_t> order(jobs.size());
+  for (uint32_t j = 0; j < jobs.size(); ++j) order[j] = j;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return jobs[a].scene_key < jobs[b].scene_key; });
   const uint64_t cap = std::max<uint32_t>(ctx->wave_slots, 1024);
-  std::vector<std::vector<WaveSegment>> waves = pack_waves(jobs, cap);
+  std::vector<std::vector<WaveSegment>> waves;
+  for (;;) {
+    std::vector<WaveSegment> w = pack_wave(jobs, order, cap);
+    if (w.empty()) break;
+    waves.push_back(std::move(w));
+  }
   std::vector<WaveSegment> flat;
   std::vector<size_t> first_seg;
   size_t max_slots = 0;
@@ -275,12 +262,12 @@ pt_status run_jobs(pt_context *ctx, std::vector<Job> &jobs, pt_tracer *stats_to)
     }
     max_slots = std::max(max_slots, slots);
   }
-  const bool wavefront = ctx->schedule == PT_SCHEDULE_WAVEFRONT;
-  pt_status st = wavefront ? ensure_wavefront(ctx, (uint32_t)max_slots, max_shadow, max_iter)
-                           : ensure(ctx, ctx->d_out, ctx->out_cap, max_slots);
+  pt_status st = engine_reserve(ctx, max_slots, max_shadow, max_iter);
   if (st != PT_OK) return st;
   if ((st = ensure(ctx, ctx->d_segs, ctx->seg_cap, flat.size())) != PT_OK) return st;
-  if ((st = ensure(ctx, ctx->d_reqs, ctx->req_cap, reqs.size())) != PT_OK) return st;
+  if ((st = ensure(ctx, ctx->d_reqs, ctx->req_cap, jobs.size())) != PT_OK) return st;
+  std::vector<DevRequest> reqs(jobs.size());
+  for (size_t j = 0; j < jobs.size(); ++j) reqs[j] = jobs[j].req;
   CK(ctx, cudaMemcpyAsync(ctx->d_reqs, reqs.data(), reqs.size() * sizeof(DevRequest), cudaMemcpyHostToDevice,
                           ctx->stream));
   CK(ctx, cudaMemcpyAsync(ctx->d_segs, flat.data(), flat.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice,
@@ -299,25 +286,10 @@ pt_status run_jobs(pt_context *ctx, std::vector<Job> &jobs, pt_tracer *stats_to)
   }
   CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   for (size_t i = 0; i < waves.size(); ++i) {
-    const WaveSegment *segs = ctx->d_segs + first_seg[i];
-    uint32_t nseg = (uint32_t)waves[i].size(), total = 0, max_pix = 0, iters = 1;
-    for (const WaveSegment &s : waves[i]) {
-      total += s.pixel_count * s.spp;
-      max_pix = std::max(max_pix, s.pixel_count);
-      iters = std::max(iters, jobs[s.request].iterations);
-    }
-    if (wavefront) {
-      WaveBuffers w = ctx->wf;
-      w.iterations = iters;
-      CK(ctx, launch_wavefront(ctx->d_reqs, segs, nseg, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream, &timer));
-      timer.mark(STAGE_ACCUMULATE, ctx->stream);
-      CK(ctx, launch_accumulate(ctx->d_reqs, segs, nseg, max_pix, w.rad, ctx->stream));
-    } else {
-      timer.mark(STAGE_MEGAKERNEL, ctx->stream);
-      CK(ctx, launch_megakernel(ctx->d_reqs, segs, nseg, total, ctx->d_out, ctx->d_ctr, ctx->stream));
-      timer.mark(STAGE_ACCUMULATE, ctx->stream);
-      CK(ctx, launch_accumulate(ctx->d_reqs, segs, nseg, max_pix, ctx->d_out, ctx->stream));
-    }
+    uint32_t iters = 1;
+    for (const WaveSegment &s : waves[i]) iters = std::max(iters, jobs[s.request].iterations);
+    st = launch_wave(ctx, ctx->d_reqs, ctx->d_segs + first_seg[i], waves[i], iters, &timer);
+    if (st != PT_OK) return st;
   }
   timer.mark(STAGE_END, ctx->stream);
   CK(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
@@ -346,7 +318,17 @@ pt_status run_jobs(pt_context *ctx, std::vector<Job> &jobs, pt_tracer *stats_to)
   }
   ctx->last_batch_rays = c.ext_rays + c.shadow_rays;
   if (c.error_flags & ERR_STACK_OVERFLOW) return fail(ctx, PT_ERR_DEVICE, "BVH traversal stack overflow");
-  for (Job &jb : jobs) jb.t->samples += jb.target;
+  for (size_t j = 0; j < jobs.size(); ++j) tracers[j]->samples += jobs[j].target;
+  return PT_OK;
+}
+
+// Appends the job of tracer `t` (n more samples) to a batch.
+pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_tracer *> &tracers,
+                  std::vector<Job> &jobs) {
+  SceneHost *sc = find_scene(ctx, t->scene_id);
+  if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
+  tracers.push_back(t);
+  jobs.push_back(make_job(*t, *sc, t->env.get(), n));
   return PT_OK;
 }
 
@@ -354,22 +336,31 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
   if (!t->have_state || n == 0) return PT_OK;
   n = std::min(n, 0xffffffffu - t->samples);
   if (n == 0) return PT_OK;
-  std::vector<Job> jobs{Job{t, n, t->samples, t->w * t->h}};
-  return run_jobs(t->ctx, jobs, t);
+  std::vector<pt_tracer *> tracers;
+  std::vector<Job> jobs;
+  pt_status st = add_job(t->ctx, t, n, tracers, jobs);
+  if (st != PT_OK) return st;
+  return run_jobs(t->ctx, tracers, jobs, t);
 }
 
 pt_status refine_many_impl(pt_context *ctx, pt_tracer *const *tracers, const uint32_t *samples, uint32_t count) {
+  std::vector<pt_tracer *> ts;
   std::vector<Job> jobs;
   for (uint32_t i = 0; i < count; ++i) {
     pt_tracer *t = tracers[i];
     if (!t || t->ctx != ctx) return fail(ctx, PT_ERR_INVALID_ARG, "tracer " + std::to_string(i) + " is not of ctx");
     for (uint32_t j = 0; j < i; ++j)
       if (tracers[j] == t) return fail(ctx, PT_ERR_INVALID_ARG, "a tracer appears twice in one batch");
+  }
+  for (uint32_t i = 0; i < count; ++i) {
+    pt_tracer *t = tracers[i];
     if (!t->have_state || samples[i] == 0) continue;
     uint32_t n = std::min(samples[i], 0xffffffffu - t->samples);
-    if (n) jobs.push_back(Job{t, n, t->samples, t->w * t->h});
+    if (!n) continue;
+    pt_status st = add_job(ctx, t, n, ts, jobs);
+    if (st != PT_OK) return st;
   }
-  return run_jobs(ctx, jobs, jobs.size() == 1 ? jobs[0].t : nullptr);
+  return run_jobs(ctx, ts, jobs, jobs.size() == 1 ? ts[0] : nullptr);
 }
 
 pt_status sync_impl(pt_tracer *t, uint32_t scene_id, const pt_camera *cam, const pt_render_options *opts, int *reset) {
@@ -466,6 +457,60 @@ pt_status set_env_impl(pt_tracer *t, const pt_environment *env) {
 namespace ptd {
 pt_status ctx_fail(pt_context *ctx, pt_status st, const std::string &msg) { return fail(ctx, st, msg); }
 SceneHost *ctx_find_scene(pt_context *ctx, uint32_t id) { return find_scene(ctx, id); }
+
+pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations) {
+  if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) return ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations);
+  return ensure(ctx, ctx->d_out, ctx->out_cap, slots);
+}
+
+pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
+                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer) {
+  uint32_t nseg = (uint32_t)segs.size(), total = 0, max_pix = 0;
+  for (const WaveSegment &s : segs) {
+    total += s.pixel_count * s.spp;
+    max_pix = std::max(max_pix, s.pixel_count);
+  }
+  if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
+    WaveBuffers w = ctx->wf;
+    w.iterations = iters;
+    CK(ctx, launch_wavefront(d_reqs, d_segs, nseg, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream, timer));
+    if (timer) timer->mark(STAGE_ACCUMULATE, ctx->stream);
+    CK(ctx, launch_accumulate(d_reqs, d_segs, nseg, max_pix, w.rad, ctx->stream));
+  } else {
+    if (timer) timer->mark(STAGE_MEGAKERNEL, ctx->stream);
+    CK(ctx, launch_megakernel(d_reqs, d_segs, nseg, total, ctx->d_out, ctx->d_ctr, ctx->stream));
+    if (timer) timer->mark(STAGE_ACCUMULATE, ctx->stream);
+    CK(ctx, launch_accumulate(d_reqs, d_segs, nseg, max_pix, ctx->d_out, ctx->stream));
+  }
+  return PT_OK;
+}
+
+pt_status engine_create(int device, pt_context **out) {
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(nullptr, PT_ERR_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= count) return fail(nullptr, PT_ERR_INVALID_ARG, "device index out of range");
+  auto ctx = std::make_unique<pt_context>();
+  ctx->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  float sheen[512], thr[255];
+  host_sheen_lut(sheen);
+  host_srgb_thresholds(thr);
+  if (e == cudaSuccess) e = set_tables(sheen, thr);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_ctr, sizeof(DevCounters));
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    pt_destroy(ctx.release());
+    return fail(nullptr, PT_ERR_DEVICE, std::string("context setup failed: ") + cudaGetErrorString(e));
+  }
+  *out = ctx.release();
+  return PT_OK;
+}
 }  // namespace ptd
 
 extern "C" {
@@ -475,31 +520,7 @@ uint32_t pt_abi_version(void) { return PT_ABI_VERSION; }
 pt_status pt_create(pt_context **out, int device) {
   if (!out) return fail(nullptr, PT_ERR_INVALID_ARG, "out is NULL");
   *out = nullptr;
-  return guard(nullptr, [&]() -> pt_status {
-    int count = 0;
-    cudaError_t e = cudaGetDeviceCount(&count);
-    if (e != cudaSuccess || count == 0)
-      return fail(nullptr, PT_ERR_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
-    if (device < 0 || device >= count) return fail(nullptr, PT_ERR_INVALID_ARG, "device index out of range");
-    auto ctx = std::make_unique<pt_context>();
-    ctx->device = device;
-    e = cudaSetDevice(device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-    float sheen[512], thr[255];
-    host_sheen_lut(sheen);
-    host_srgb_thresholds(thr);
-    if (e == cudaSuccess) e = set_tables(sheen, thr);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_ctr, sizeof(DevCounters));
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
-    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) {
-      pt_destroy(ctx.release());
-      return fail(nullptr, PT_ERR_DEVICE, std::string("context setup failed: ") + cudaGetErrorString(e));
-    }
-    *out = ctx.release();
-    return PT_OK;
-  });
+  return guard(nullptr, [&]() -> pt_status { return engine_create(device, out); });
 }
 
 void pt_destroy(pt_context *ctx) {
@@ -798,7 +819,7 @@ pt_status pt_debug_pattern(pt_tracer *t, uint32_t index, uint32_t pattern, float
     SceneHost *sc = find_scene(ctx, t->scene_id);
     if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene not resident");
     CK(ctx, cudaSetDevice(ctx->device));
-    DevRequest rq = make_request(*t, *sc);
+    DevRequest rq = make_request(*t, *sc, t->env.get());
     CK(ctx, cudaMemcpyAsync(t->d_req, &rq, sizeof rq, cudaMemcpyHostToDevice, ctx->stream));
     uint32_t npix = t->w * t->h;
     float4 *d = nullptr;
@@ -821,7 +842,7 @@ pt_status pt_debug_primary_hits(pt_tracer *t, uint32_t index, uint32_t *out_g, f
     SceneHost *sc = find_scene(ctx, t->scene_id);
     if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene not resident");
     CK(ctx, cudaSetDevice(ctx->device));
-    DevRequest rq = make_request(*t, *sc);
+    DevRequest rq = make_request(*t, *sc, t->env.get());
     CK(ctx, cudaMemcpyAsync(t->d_req, &rq, sizeof rq, cudaMemcpyHostToDevice, ctx->stream));
     uint32_t npix = t->w * t->h;
     uint32_t *dg = nullptr;

@@ -12,6 +12,7 @@
 #include "../../include/pt_b200.h"
 #include "../../include/pt_b200_debug.h"
 #include "host_scene.h"
+#include "kernels.h"
 
 struct pt_context {
   int device = 0;
@@ -41,9 +42,69 @@ struct pt_context {
   size_t wf_bytes = 0;
 };
 
+// The object behind pt_tracer: one progressive accumulation (the
+// reference's PathTracer state, src/pathtrace.rs:2369-2400).
+struct pt_tracer {
+  pt_context *ctx = nullptr;
+  bool have_state = false, dirty = true;
+  uint32_t scene_id = 0;
+  pt_camera cam{};
+  pt_render_options opts{};
+  std::unique_ptr<ptd::EnvHost> env;
+  double *d_accum = nullptr;
+  size_t accum_cap = 0;
+  ptd::DevRequest *d_req = nullptr;
+  void *d_resolve = nullptr;
+  size_t resolve_cap = 0;
+  uint32_t w = 1, h = 1, samples = 0;
+  uint64_t ext = 0, sh = 0, ext_nodes = 0, ext_tris = 0, sh_nodes = 0, sh_tris = 0;
+  float last_ms = 0.0f;
+  float stage_ms[ptd::STAGE_COUNT] = {};
+};
+
 namespace ptd {
 // Records `msg` as the context's last error and returns `st`.
 pt_status ctx_fail(pt_context *ctx, pt_status st, const std::string &msg);
 // The resident scene `id`, or nullptr.
 SceneHost *ctx_find_scene(pt_context *ctx, uint32_t id);
+
+// ---- the wave engine shared by refine, refine_many and the server ----
+
+// One refine job: `target` samples added to an accumulation whose device
+// request is `req` (scene, environment, camera, options, accumulator).
+struct Job {
+  DevRequest req;
+  uint32_t target;
+  uint32_t first;         // sample index of the job's first sample
+  uint32_t npix;
+  uint32_t done = 0;      // whole samples finished
+  uint32_t pix_done = 0;  // pixels of sample `done` finished (partial-pixel waves)
+  uint32_t iterations = 1;
+  uint32_t shadow_slots = 1;
+  uint32_t scene_key = 0;  // only orders the packing (locality)
+  bool finished() const { return done >= target; }
+};
+
+// The device request of tracer `t` drawing on resident scene `sc` and
+// environment `env` (nullptr: constant sky).
+DevRequest make_request(const pt_tracer &t, const SceneHost &sc, const EnvHost *env);
+// A job adding `n` samples to `t` (whose samples so far are `t.samples`).
+Job make_job(const pt_tracer &t, const SceneHost &sc, const EnvHost *env, uint32_t n);
+
+// Packs the next wave of at most `cap` path slots from `jobs`, visiting
+// them in `order`, and advances the jobs' progress. WaveSegment.request is
+// the index into `jobs`. A job contributes at most one segment per wave;
+// within a job, samples (and pixel ranges of one sample) go in order.
+std::vector<WaveSegment> pack_wave(std::vector<Job> &jobs, const std::vector<uint32_t> &order, uint64_t cap);
+
+// Sizes the context's wave buffers for waves of `slots` paths with up to
+// `shadow_slots` shadow rays per path and `iterations` bounce rounds.
+pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations);
+// Enqueues one wave on ctx->stream: path kernels + ordered accumulate.
+// `d_reqs` / `d_segs` are device copies of the wave's request table and
+// `segs`; `iters` is the largest bounce-round count among the wave's jobs.
+pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
+                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer);
+// A new context's engine state on `device` (stream, tables, counters).
+pt_status engine_create(int device, pt_context **out);
 }  // namespace ptd

@@ -420,9 +420,15 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
 
 // ============================================================ arena
 void DeviceArena::release() {
-  if (base) cudaFree(base);
+  if (base) {
+    if (stream)
+      cudaFreeAsync(base, stream);
+    else
+      cudaFree(base);
+  }
   base = nullptr;
   bytes = 0;
+  stream = nullptr;
 }
 
 namespace {
@@ -518,8 +524,7 @@ void build_mips(const pt_texture &img, bool srgb, MipChain &out) {
 }  // namespace
 
 // ============================================================ scene upload
-std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
-  oom = false;
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   if (desc.item_count && !desc.items) return "pt_scene_desc.items is NULL";
   if (desc.material_count == 0 || !desc.materials) return "pt_scene_desc needs at least one material";
   if (desc.texture_count && !desc.textures) return "pt_scene_desc.textures is NULL";
@@ -642,7 +647,7 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
   std::vector<BvhNode> nodes;
   std::vector<float4> records;
   int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  build_bvh(pos.data(), tc, rec_flags.data(), nodes, records, out.bvh, threads);
+  build_bvh(pos.data(), tc, rec_flags.data(), nodes, records, img.bvh, threads);
 
   // Lights.
   std::vector<DevLight> lights(desc.light_count);
@@ -720,47 +725,106 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
   size_t p_lookup = plan.add(em_lookup.data(), em_lookup.size() * 4);
   DevScene tmp{};
   size_t p_desc = plan.add(&tmp, sizeof(DevScene));
-  std::string err = commit(plan, out.arena, oom);
-  if (!err.empty()) {
-    out.arena.release();
-    return err;
-  }
-  DevScene &d = out.dev;
-  auto opt = [&](size_t part, size_t bytes) -> const float * {
-    return bytes ? dptr<float>(out.arena, plan, part) : nullptr;
-  };
-  d.nodes = dptr<BvhNode>(out.arena, plan, p_nodes);
-  d.tris = dptr<float4>(out.arena, plan, p_rec);
-  d.tri_info = dptr<uint2>(out.arena, plan, p_info);
-  d.pos = dptr<float>(out.arena, plan, p_pos);
-  d.nrm = opt(p_nrm, nrm.size());
-  d.tan = opt(p_tan, tan.size());
-  d.col = opt(p_col, col.size());
-  for (int s = 0; s < PT_MAX_UV_SETS; ++s) d.uv[s] = opt(p_uv[s], uv[s].size());
-  d.materials = dptr<DevMaterial>(out.arena, plan, p_mat);
-  d.textures = dptr<DevTexture>(out.arena, plan, p_tex);
-  d.texels = dptr<float4>(out.arena, plan, p_pool);
-  d.lights = dptr<DevLight>(out.arena, plan, p_lights);
-  d.em_tris = dptr<uint32_t>(out.arena, plan, p_emt);
-  d.em_pmf = dptr<float>(out.arena, plan, p_pmf);
-  d.em_cdf = dptr<float>(out.arena, plan, p_cdf);
-  d.em_lookup = dptr<uint32_t>(out.arena, plan, p_lookup);
+  img.blob.assign(std::max<size_t>(plan.total, 256), 0);
+  for (size_t i = 0; i < plan.parts.size(); ++i)
+    if (plan.parts[i].second) std::memcpy(img.blob.data() + plan.offsets[i], plan.parts[i].first, plan.parts[i].second);
+  // Pointer fields hold offset + 1 until commit_scene rebases them.
+  auto rel = [&](size_t part, size_t bytes) -> uintptr_t { return bytes ? (uintptr_t)plan.offsets[part] + 1 : 0; };
+  DevScene &d = img.rel;
+  std::memset(&d, 0, sizeof d);
+  d.nodes = (const BvhNode *)rel(p_nodes, 1);
+  d.tris = (const float4 *)rel(p_rec, 1);
+  d.tri_info = (const uint2 *)rel(p_info, 1);
+  d.pos = (const float *)rel(p_pos, 1);
+  d.nrm = (const float *)rel(p_nrm, nrm.size());
+  d.tan = (const float *)rel(p_tan, tan.size());
+  d.col = (const float *)rel(p_col, col.size());
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s) d.uv[s] = (const float *)rel(p_uv[s], uv[s].size());
+  d.materials = (const DevMaterial *)rel(p_mat, 1);
+  d.textures = (const DevTexture *)rel(p_tex, 1);
+  d.texels = (const float4 *)rel(p_pool, 1);
+  d.lights = (const DevLight *)rel(p_lights, 1);
+  d.em_tris = (const uint32_t *)rel(p_emt, 1);
+  d.em_pmf = (const float *)rel(p_pmf, 1);
+  d.em_cdf = (const float *)rel(p_cdf, 1);
+  d.em_lookup = (const uint32_t *)rel(p_lookup, 1);
   d.node_count = (uint32_t)nodes.size();
   d.tri_count = tc;
   d.material_count = desc.material_count;
   d.texture_count = desc.texture_count;
   d.light_count = desc.light_count;
   d.em_count = (uint32_t)em_tris.size();
-  d.max_depth = out.bvh.max_depth;
-  out.d_desc = const_cast<DevScene *>(dptr<DevScene>(out.arena, plan, p_desc));
-  cudaError_t e = cudaMemcpy(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice);
+  d.max_depth = img.bvh.max_depth;
+  img.desc_off = plan.offsets[p_desc];
+  img.tri_count = tc;
+  img.light_count = desc.light_count;
+  return "";
+}
+
+namespace {
+template <class T>
+void rebase(const T *&p, uint8_t *base) {
+  p = p ? reinterpret_cast<const T *>(base + (reinterpret_cast<uintptr_t>(p) - 1)) : nullptr;
+}
+}  // namespace
+
+std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaStream_t stream) {
+  oom = false;
+  const size_t total = img.blob.size();
+  cudaError_t e = stream ? cudaMallocAsync(&out.arena.base, total, stream) : cudaMalloc(&out.arena.base, total);
+  if (e != cudaSuccess) {
+    oom = e == cudaErrorMemoryAllocation;
+    out.arena.base = nullptr;
+    cudaGetLastError();
+    return std::string("device allocation of ") + std::to_string(total) + " bytes failed: " + cudaGetErrorString(e);
+  }
+  out.arena.bytes = total;
+  out.arena.stream = stream;
+  uint8_t *base = static_cast<uint8_t *>(out.arena.base);
+  DevScene d = img.rel;
+  rebase(d.nodes, base);
+  rebase(d.tris, base);
+  rebase(d.tri_info, base);
+  rebase(d.pos, base);
+  rebase(d.nrm, base);
+  rebase(d.tan, base);
+  rebase(d.col, base);
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s) rebase(d.uv[s], base);
+  rebase(d.materials, base);
+  rebase(d.textures, base);
+  rebase(d.texels, base);
+  rebase(d.lights, base);
+  rebase(d.em_tris, base);
+  rebase(d.em_pmf, base);
+  rebase(d.em_cdf, base);
+  rebase(d.em_lookup, base);
+  out.dev = d;
+  out.d_desc = reinterpret_cast<DevScene *>(base + img.desc_off);
+  if (stream) {
+    // Pageable sources: both calls return once the bytes are staged.
+    e = cudaMemcpyAsync(base, img.blob.data(), total, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  } else {
+    e = cudaMemcpy(base, img.blob.data(), total, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     out.arena.release();
-    return std::string("scene descriptor upload failed: ") + cudaGetErrorString(e);
+    return std::string("scene upload failed: ") + cudaGetErrorString(e);
   }
-  out.tri_count = tc;
-  out.light_count = desc.light_count;
+  out.tri_count = img.tri_count;
+  out.bvh = img.bvh;
+  out.light_count = img.light_count;
   return "";
+}
+
+std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
+  oom = false;
+  SceneImage img;
+  std::string err = build_scene_image(desc, img);
+  if (!err.empty()) return err;
+  return commit_scene(img, out, oom);
 }
 
 void release_scene(SceneHost &s) {

@@ -3,6 +3,8 @@
 // single device arena each resident scene lives in.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -23,11 +25,27 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
                std::vector<float4> &records, BvhBuildStats &stats, int threads);
 
 // One device allocation holding a scene (or an environment) plus the
-// device copy of its descriptor.
+// device copy of its descriptor. `stream` non-null: the allocation is
+// stream-ordered (cudaMallocAsync) and is freed in that stream's order.
 struct DeviceArena {
   void *base = nullptr;
   uint64_t bytes = 0;
+  cudaStream_t stream = nullptr;
   void release();
+};
+
+// A scene fully prepared on the host: the exact bytes of its device arena
+// (BVH nodes, triangle records, attribute streams, materials, texel pool,
+// lights, emissive tables) plus a descriptor whose pointer fields hold
+// arena offsets + 1 (0 = absent). Uploading it is one allocation and one
+// copy, so an evicted scene comes back without another BVH build.
+struct SceneImage {
+  std::vector<uint8_t> blob;
+  DevScene rel{};
+  uint64_t desc_off = 0;
+  uint64_t tri_count = 0;
+  BvhBuildStats bvh;
+  uint32_t light_count = 0;
 };
 
 struct SceneHost {
@@ -39,9 +57,13 @@ struct SceneHost {
   uint32_t light_count = 0;
 };
 
-// Validates `desc`, builds everything on the host and uploads it.
-// Returns an empty string on success, else an error message
-// (`oom` set when the failure was a device allocation).
+// Validates `desc` and builds its device image on the host. Returns an
+// empty string on success, else an error message.
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img);
+// Allocates the arena and copies `img` into it (stream-ordered when `stream`
+// is non-null). `oom` is set when the failure was a device allocation.
+std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaStream_t stream = nullptr);
+// build_scene_image + commit_scene.
 std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom);
 void release_scene(SceneHost &s);
 
