@@ -117,33 +117,38 @@ def workload(name: str):
     raise SystemExit(f"unknown config {name}")
 
 
-def mixed_requests(n: int, seed: int, stress_grid: int = 1024, stress_spheres: int = 500):
+_MIXED_SCENES = {}
+
+
+def mixed_scene(k: int, stress_grid: int = 1024, stress_spheres: int = 500):
+    """Scene k of the mixed workload (built once): 0 Cornell box, 1 sphere
+    grid, 2 stress scene, 3-10 random soups of 10k-500k triangles."""
+    if k in _MIXED_SCENES:
+        return _MIXED_SCENES[k]
+    ts = entry.load_package().testscenes
+    if k == 0:
+        s, o = ts.cornell_c0()
+        v = (s, o, None)
+    elif k == 1:
+        s, o = ts.sphere_grid_c1(512, 256)
+        v = (s, o, None)
+    elif k == 2:
+        v = ts.stress_c2(grid=stress_grid, spheres=stress_spheres)
+    else:
+        tris = int(np.random.default_rng(100 + k).integers(10_000, 500_001))
+        s = ts.random_soup(tris, seed=100 + k)
+        v = (s, ts.pt_opts(64, 1, 8, scene_camera=0, ambient=0.1), None)
+    _MIXED_SCENES[k] = v
+    return v
+
+
+def mixed_requests(n: int, seed: int):
     """The batched workload: `n` requests, each drawing its scene uniformly
     from {Cornell box, sphere grid, stress scene, 8 random soups of
     10k-500k triangles}, its resolution from {128^2, 256^2, 512^2, 1024x768},
     its spp from {1, 4, 16, 64} and its bounce limit from {2, 4, 8}."""
-    ts = entry.load_package().testscenes
     from oxideav_render_b200.options import PathTraceOptions
     rng = np.random.default_rng(seed)
-    scenes = {}
-
-    def scene(k):
-        if k not in scenes:
-            if k == 0:
-                s, o = ts.cornell_c0()
-                scenes[k] = (s, o, None)
-            elif k == 1:
-                s, o = ts.sphere_grid_c1(512, 256)
-                scenes[k] = (s, o, None)
-            elif k == 2:
-                s, o, env = ts.stress_c2(grid=stress_grid, spheres=stress_spheres)
-                scenes[k] = (s, o, env)
-            else:
-                tris = int(np.random.default_rng(100 + k).integers(10_000, 500_001))
-                s = ts.random_soup(tris, seed=100 + k)
-                scenes[k] = (s, ts.pt_opts(64, 1, 8, scene_camera=0, ambient=0.1), None)
-        return scenes[k]
-
     res = [(128, 128), (256, 256), (512, 512), (1024, 768)]
     out = []
     for i in range(n):
@@ -151,18 +156,18 @@ def mixed_requests(n: int, seed: int, stress_grid: int = 1024, stress_spheres: i
         w, h = res[int(rng.integers(0, 4))]
         spp = [1, 4, 16, 64][int(rng.integers(0, 4))]
         b = [2, 4, 8][int(rng.integers(0, 3))]
-        s, o, env = scene(k)
+        s, o, env = mixed_scene(k)
         opts = o.replace(width=w, height=h, path_trace=PathTraceOptions(samples_per_pixel=spp, max_bounces=b,
                                                                         seed=i))
         out.append((k, s, opts, env))
-    return out, scenes
+    return out
 
 
 def run_mixed(ctx, api, torch, n_requests: int, seed: int, check: int = 8):
     """Plain per-request GPU path (each request synced, refined and read back
     alone, one after another) against the batched path (all requests in one
     pt_tracer_refine_many call, then read back). Returns the comparison."""
-    reqs, scenes = mixed_requests(n_requests, seed)
+    reqs = mixed_requests(n_requests, seed)
     tracers = []
     for k, s, o, env in reqs:
         t = api.PathTracer(ctx)
@@ -200,6 +205,157 @@ def run_mixed(ctx, api, torch, n_requests: int, seed: int, check: int = 8):
             "batched_mrays_per_s": st["rays"] / (st["ms"] / 1000.0) / 1e6 if st["ms"] > 0 else None,
             "bit_identical_checked": len(plain_acc), "bit_identical": identical,
             "timing": "wall clock, host submit to HDR readback of every request"}
+
+
+def serving_scenes(n: int, seed: int):
+    """The served workload's resident scenes: the mixed workload's eleven
+    (Cornell box, sphere grid, ~4.1M-triangle stress scene, eight soups)
+    plus random soups of 10k-1M triangles (log-uniform) up to `n`."""
+    ts = entry.load_package().testscenes
+    out = [mixed_scene(k) for k in range(11)]
+    rng = np.random.default_rng(seed + 1)
+    for k in range(11, n):
+        tris = int(np.exp(rng.uniform(np.log(10_000), np.log(1_000_000))))
+        s = ts.random_soup(tris, seed=1000 + k)
+        out.append((s, ts.pt_opts(64, 1, 8, scene_camera=0, ambient=0.1), None))
+    return out
+
+
+def run_served(ctx, api, torch, args):
+    """Poisson arrivals of mixed requests against the render server, per
+    arrival rate: p50/p99 latency (submit -> HDR in host memory) and the
+    delivered samples/s; beside it the plain per-request path on a bounded
+    sample of the same requests, timed back to back."""
+    from oxideav_render_b200.options import PathTraceOptions
+    from oxideav_render_b200.serve import RenderServer
+    t0 = time.perf_counter()
+    scenes = serving_scenes(args.serve_scenes, 2026)
+    gen_s = time.perf_counter() - t0
+    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)))
+    t0 = time.perf_counter()
+    keys = [srv.register(s, o, api.EnvironmentMap(e) if e is not None else None) for s, o, e in scenes]
+    register_s = time.perf_counter() - t0
+    # Make every scene resident (one tiny request each), as a warm server is.
+    t0 = time.perf_counter()
+    warm = [srv.submit(k, o.replace(width=16, height=16, path_trace=PathTraceOptions(samples_per_pixel=1)))
+            for k, (_, o, _) in zip(keys, scenes)]
+    for t in warm:
+        srv.wait(t)
+        srv.release(t)
+    admit_s = time.perf_counter() - t0
+    res = [(128, 128), (256, 256), (512, 512), (1024, 768)]
+    runs = []
+    sample_reqs = None
+    for rate in args.serve_rates:
+        rng = np.random.default_rng(int(rate * 1000) + 17)
+        n = max(8, min(int(rate * args.serve_seconds), args.serve_max))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        spec = []
+        for i in range(n):
+            if i > 0 and rng.random() < 0.2:
+                spec.append(("cont", int(rng.integers(0, i)), 16))
+            else:
+                k = int(rng.integers(0, len(scenes)))
+                w, h = res[int(rng.integers(0, 4))]
+                spp = [1, 4, 16, 64][int(rng.integers(0, 4))]
+                b = [2, 4, 8][int(rng.integers(0, 3))]
+                o = scenes[k][1].replace(width=w, height=h,
+                                         path_trace=PathTraceOptions(samples_per_pixel=spp, max_bounces=b, seed=i))
+                spec.append(("new", k, o))
+        tickets, submit_t, samples = [None] * n, [0.0] * n, [0] * n
+        start = time.perf_counter()
+        for i, sp in enumerate(spec):
+            delay = start + arrivals[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            submit_t[i] = time.perf_counter()
+            if sp[0] == "new":
+                tickets[i] = srv.submit(keys[sp[1]], sp[2])
+                samples[i] = sp[2].width * sp[2].height * sp[2].path_trace.samples_per_pixel
+            else:
+                base = sp[1]
+                while spec[base][0] == "cont":
+                    base = spec[base][1]
+                o = spec[base][2]
+                tickets[i] = srv.submit_continuation(tickets[sp[1]], sp[2])
+                samples[i] = o.width * o.height * sp[2]
+        lat, done_t, images = [], [], {}
+        for i, t in enumerate(tickets):
+            img, st = srv.wait(t)
+            lat.append(st["latency_ms"])
+            done_t.append(submit_t[i] + st["latency_ms"] / 1000.0)
+            if spec[i][0] == "new" and len(images) < args.serve_check:
+                images[i] = img
+        makespan = max(done_t) - submit_t[0]
+        stats = srv.stats()
+        for t in tickets:
+            srv.release(t)
+        runs.append({"rate_per_s": rate, "requests": n, "continuations": sum(1 for s in spec if s[0] == "cont"),
+                     "samples": int(sum(samples)), "makespan_s": makespan,
+                     "samples_per_s": sum(samples) / makespan,
+                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                     "max_ms": float(max(lat))})
+        sample_reqs = (spec, arrivals, images)
+    st = srv.stats()
+    srv.close()
+
+    # Plain per-request path on the saturated run's requests (new ones, in
+    # arrival order) within a time budget: one-shot render (scene prepared
+    # and uploaded per request, PathTraceRenderer::render_hdr semantics) and,
+    # separately, refine + hdr on a tracer whose scene is already uploaded.
+    spec, arrivals, images = sample_reqs
+    renderer = api.PathTraceCudaRenderer(ctx)
+    plain_t, plain_n, resident_t, identical, arr = [], [], [], [], []
+    budget_end = time.perf_counter() + args.plain_seconds
+    for i, sp in enumerate(spec):
+        if sp[0] != "new":
+            continue
+        if time.perf_counter() > budget_end:
+            break
+        s, _, e = scenes[sp[1]]
+        o = sp[2]
+        renderer.tracer_mut().set_environment(api.EnvironmentMap(e) if e is not None else None)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img = renderer.render_hdr(s, o)
+        plain_t.append(time.perf_counter() - t0)
+        plain_n.append(o.width * o.height * o.path_trace.samples_per_pixel)
+        arr.append(arrivals[i])
+        if i in images:
+            identical.append(bool(np.array_equal(img, images[i])))
+        tr = renderer.tracer
+        tr.reset()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tr.refine(o.path_trace.samples_per_pixel)
+        tr.hdr()
+        resident_t.append(time.perf_counter() - t0)
+    renderer.tracer.close()
+    # Latency of the plain path under the same arrivals: one request at a
+    # time, first come first served (Lindley recursion on measured times).
+    free_at, plain_lat = 0.0, []
+    for a, s_ in zip(arr, plain_t):
+        begin = max(a, free_at)
+        free_at = begin + s_
+        plain_lat.append(1000.0 * (free_at - a))
+    sat = max(runs, key=lambda r: r["rate_per_s"])
+    plain_sps = sum(plain_n) / sum(plain_t)
+    resident_sps = sum(plain_n) / sum(resident_t)
+    return {
+        "scenes": len(scenes), "budget_gb": args.serve_budget_gb, "scene_gen_s": gen_s, "register_s": register_s,
+        "first_admission_s": admit_s, "scene_uploads": st["scene_uploads"], "scene_evictions": st["scene_evictions"],
+        "peak_resident_gb": st["peak_resident_bytes"] / (1 << 30), "waves": st["waves"],
+        "gpu_mrays_per_s": st["rays"] / (st["gpu_ms"] / 1000.0) / 1e6 if st["gpu_ms"] > 0 else None,
+        "runs": runs,
+        "plain_render": {"requests": len(plain_t), "samples_per_s": plain_sps,
+                         "p50_ms": float(np.percentile(plain_lat, 50)), "p99_ms": float(np.percentile(plain_lat, 99)),
+                         "call": "PathTraceCudaRenderer.render_hdr per request (scene prepared + uploaded per call)"},
+        "plain_resident": {"requests": len(resident_t), "samples_per_s": resident_sps,
+                           "call": "PathTracer.refine + hdr per request, scene already on the device"},
+        "speedup_vs_plain_render": sat["samples_per_s"] / plain_sps,
+        "speedup_vs_plain_resident": sat["samples_per_s"] / resident_sps,
+        "bit_identical_checked": len(identical), "bit_identical": all(identical) if identical else None,
+    }
 
 
 def algorithmic_bytes(ext_rays, shadow_rays, nodes, tris, samples):
@@ -420,6 +576,9 @@ def run_b200(args):
     mixed = None
     if args.mixed > 0:
         mixed = run_mixed(ctx, api, torch, args.mixed, 2026 + rank)
+    served = None
+    if args.serve_rates:
+        served = run_served(ctx, api, torch, args)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(scene, opts, env, args.cpu_seconds)
@@ -440,6 +599,7 @@ def run_b200(args):
                          "ms_per_launch": stage[dom] / max(launches_of_dom, 1)},
             "e2e": e2e,
             "batched_mixed": mixed,
+            "served": served,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,
@@ -467,7 +627,16 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling cases)")
     ap.add_argument("--schedule", default="wavefront", choices=["megakernel", "wavefront"])
     ap.add_argument("--mixed", type=int, default=64, help="requests in the batched-vs-plain comparison (0: skip)")
+    ap.add_argument("--serve-rates", default="5,20,200",
+                    help="Poisson arrival rates (requests/s) of the served runs, comma-separated ('' : skip)")
+    ap.add_argument("--serve-seconds", type=float, default=8.0, help="arrival window per served run")
+    ap.add_argument("--serve-max", type=int, default=96, help="requests per served run at most")
+    ap.add_argument("--serve-scenes", type=int, default=32, help="resident scenes of the served runs")
+    ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
+    ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
+    ap.add_argument("--plain-seconds", type=float, default=15.0, help="time budget of the plain-path sample")
     args = ap.parse_args()
+    args.serve_rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -1,0 +1,122 @@
+/*
+ * pt_b200_serve.h — serving layer of the B200 path tracer: continuous
+ * batching of render requests over scenes kept resident in HBM.
+ *
+ * The reference renders one request per call (Renderer::render ->
+ * PathTracer::{sync, refine, hdr}, src/pathtrace.rs:2745-2782 and
+ * 2474-2734) and re-prepares the scene every time; it has no serving layer.
+ * This one keeps that per-request contract and changes only where the work
+ * runs:
+ *
+ *   - Scenes are registered once. The server keeps each scene's prepared
+ *     host image (BVH, triangle records, attributes, materials, texel pool,
+ *     light tables) and makes it resident on the device on demand, within an
+ *     HBM budget, evicting the least recently used scene that no running
+ *     request needs. A re-admitted scene is one host-to-device copy (no
+ *     second BVH build).
+ *   - Every request owns a progressive accumulator on the device (the
+ *     PathTracer's f64 accumulator). A continuation request adds samples to
+ *     the accumulator of an earlier request (PathTracer::refine on a live
+ *     tracer) and returns the refined image.
+ *   - A worker thread admits requests as accumulator slots and scene memory
+ *     allow and runs waves of path slots drawn from every admitted request
+ *     (shortest remaining work first), so requests that arrive while others
+ *     are on the GPU share the next waves.
+ *
+ * Determinism: every sample is a pure function of (request seed, pixel,
+ * sample index) and each pixel's samples are accumulated in index order, so
+ * the HDR image of a request is bit-identical to rendering it alone with
+ * pt_tracer_sync / pt_tracer_refine / pt_tracer_read_hdr and the same scene,
+ * camera, options and sample count, however the requests were mixed.
+ *
+ * Threading: all pt_server_* calls are thread-safe; GPU work runs on the
+ * server's own stream and buffers, independent of any pt_context's.
+ */
+#ifndef PT_B200_SERVE_H
+#define PT_B200_SERVE_H
+
+#include "pt_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pt_server pt_server;
+
+typedef struct pt_server_config {
+  uint64_t hbm_budget_bytes; /* device bytes for resident scenes and their environments; 0 = no limit */
+  uint32_t wave_slots;       /* path slots per wave; 0 = 4194304 */
+  uint32_t max_active;       /* requests admitted to the GPU at once; 0 = 256 */
+  uint32_t megakernel;       /* nonzero: one-kernel-per-path schedule instead of the wavefront */
+  uint32_t pipeline_depth;   /* waves in flight on the stream; 0 = 2 */
+  uint32_t reserved[2];
+} pt_server_config;
+
+typedef struct pt_server_request {
+  uint32_t scene;             /* key from pt_server_scene_register (ignored for continuations) */
+  uint32_t samples;           /* samples per pixel to add (>= 1) */
+  uint64_t continues;         /* 0: a new accumulation; else the ticket whose accumulator gains `samples` */
+  pt_camera camera;           /* Camera::resolve output (ignored for continuations) */
+  pt_render_options options;  /* as for pt_tracer_sync (ignored for continuations) */
+} pt_server_request;
+
+typedef struct pt_request_stats {
+  double queue_ms;   /* submit -> admitted to the GPU */
+  double latency_ms; /* submit -> HDR image in host memory */
+  uint32_t width, height;
+  uint32_t samples;  /* samples per pixel in the accumulation after this request */
+  uint32_t waves;    /* waves that carried this request's paths */
+} pt_request_stats;
+
+typedef struct pt_server_stats {
+  uint64_t submitted, completed, failed;
+  uint64_t samples;         /* camera paths traced */
+  uint64_t waves;
+  uint64_t rays;            /* extension + shadow rays traced */
+  double gpu_ms;            /* device time of all completed waves */
+  uint64_t scene_uploads;   /* device commits of scene images (first admissions and re-admissions) */
+  uint64_t scene_evictions;
+  uint64_t resident_bytes, peak_resident_bytes;
+  uint32_t resident_scenes, active, pending, accumulators;
+} pt_server_stats;
+
+/* A server on `ctx`'s device. `cfg` may be NULL (defaults). The server does
+ * not use ctx's stream or buffers; ctx must outlive the server. */
+PT_API pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_server **out);
+/* Cancels pending requests (PT_ERR_CANCELLED), lets waves in flight finish,
+ * frees everything. */
+PT_API void pt_server_destroy(pt_server *server);
+/* Message of the last failed pt_server_* call on the calling thread. */
+PT_API const char *pt_server_last_error(const pt_server *server);
+
+/* Prepares `desc` on the host (validation, BVH build, tables) and keeps the
+ * image; the device copy is made when a request first needs it. `env` may
+ * be NULL (constant sky `ambient`); it is the scene's environment map for
+ * every request on it (PathTracer::set_environment). */
+PT_API pt_status pt_server_scene_register(pt_server *server, const pt_scene_desc *desc, const pt_environment *env,
+                                          uint32_t *scene_key);
+/* Forgets a scene. PT_ERR_INVALID_ARG while a pending or running request
+ * uses it; continuations of finished requests on it then fail. */
+PT_API pt_status pt_server_scene_unregister(pt_server *server, uint32_t scene_key);
+PT_API pt_status pt_server_scene_info(pt_server *server, uint32_t scene_key, uint64_t *device_bytes,
+                                      int *resident);
+
+/* Queues a request and returns its ticket at once. */
+PT_API pt_status pt_server_submit(pt_server *server, const pt_server_request *request, uint64_t *ticket);
+/* Waits up to `timeout_ms` (< 0: no limit) for `ticket`. PT_OK: the request
+ * finished; its HDR image (width * height * 4 floats, row-major RGBA) is
+ * copied to `hdr` when non-NULL (`hdr_floats` is its capacity) and `stats`
+ * is filled when non-NULL. PT_ERR_NOT_READY: still running at the timeout.
+ * Any other status is the request's own failure. */
+PT_API pt_status pt_server_wait(pt_server *server, uint64_t ticket, int32_t timeout_ms, float *hdr,
+                                size_t hdr_floats, pt_request_stats *stats);
+/* Drops a finished request's image; the accumulator goes once no ticket on
+ * it is left. A released ticket cannot be continued. */
+PT_API pt_status pt_server_release(pt_server *server, uint64_t ticket);
+PT_API pt_status pt_server_stats_get(pt_server *server, pt_server_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PT_B200_SERVE_H */

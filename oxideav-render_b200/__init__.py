@@ -21,7 +21,7 @@ __all__ = [
 def __getattr__(name):
     # The native bindings load lazily so the package imports on hosts
     # without a GPU (or before the library is built).
-    if name in ("api", "native"):
+    if name in ("api", "native", "serve"):
         import importlib
         return importlib.import_module(f"{__name__}.{name}")
     raise AttributeError(name)

@@ -219,7 +219,61 @@ class pt_render_options(C.Structure):
     ]
 
 
+# include/pt_b200_serve.h
+class pt_server_config(C.Structure):
+    _fields_ = [
+        ("hbm_budget_bytes", C.c_uint64),
+        ("wave_slots", C.c_uint32),
+        ("max_active", C.c_uint32),
+        ("megakernel", C.c_uint32),
+        ("pipeline_depth", C.c_uint32),
+        ("reserved", C.c_uint32 * 2),
+    ]
+
+
+class pt_server_request(C.Structure):
+    _fields_ = [
+        ("scene", C.c_uint32),
+        ("samples", C.c_uint32),
+        ("continues", C.c_uint64),
+        ("camera", pt_camera),
+        ("options", pt_render_options),
+    ]
+
+
+class pt_request_stats(C.Structure):
+    _fields_ = [
+        ("queue_ms", C.c_double),
+        ("latency_ms", C.c_double),
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("samples", C.c_uint32),
+        ("waves", C.c_uint32),
+    ]
+
+
+class pt_server_stats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("failed", C.c_uint64),
+        ("samples", C.c_uint64),
+        ("waves", C.c_uint64),
+        ("rays", C.c_uint64),
+        ("gpu_ms", C.c_double),
+        ("scene_uploads", C.c_uint64),
+        ("scene_evictions", C.c_uint64),
+        ("resident_bytes", C.c_uint64),
+        ("peak_resident_bytes", C.c_uint64),
+        ("resident_scenes", C.c_uint32),
+        ("active", C.c_uint32),
+        ("pending", C.c_uint32),
+        ("accumulators", C.c_uint32),
+    ]
+
+
 ABI_STRUCTS = [
     pt_texture_binding, pt_material, pt_texture, pt_draw_item, pt_light,
     pt_scene_desc, pt_environment, pt_camera, pt_path_trace_options, pt_render_options,
+    pt_server_config, pt_server_request, pt_request_stats, pt_server_stats,
 ]

@@ -153,15 +153,19 @@ std::vector<WaveSegment> pack_wave(std::vector<Job> &jobs, const std::vector<uin
   return segs;
 }
 
-}  // namespace ptd
-
-namespace {
+pt_status check_options(pt_context *ctx, const pt_camera *cam, const pt_render_options *o) {
+  return validate_opts(ctx, cam, o);
+}
 
 float4 bg_linear(const pt_render_options &o) {
   return make_float4(host_srgb_to_linear((float)o.background[0] / 255.0f),
                      host_srgb_to_linear((float)o.background[1] / 255.0f),
                      host_srgb_to_linear((float)o.background[2] / 255.0f), (float)o.background[3] / 255.0f);
 }
+
+}  // namespace ptd
+
+namespace {
 
 SceneHost *find_scene(pt_context *ctx, uint32_t id) {
   auto it = ctx->scenes.find(id);

@@ -107,4 +107,9 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
                       const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer);
 // A new context's engine state on `device` (stream, tables, counters).
 pt_status engine_create(int device, pt_context **out);
+// The background colour in linear light (PathTracer::bg_linear,
+// src/pathtrace.rs:2593-2602).
+float4 bg_linear(const pt_render_options &o);
+// PathTracer::sync's option checks (camera / enum / size limits).
+pt_status check_options(pt_context *ctx, const pt_camera *cam, const pt_render_options *o);
 }  // namespace ptd

@@ -446,20 +446,25 @@ struct ArenaPlan {
   }
 };
 
-std::string commit(ArenaPlan &plan, DeviceArena &arena, bool &oom) {
+std::string commit(ArenaPlan &plan, DeviceArena &arena, bool &oom, cudaStream_t stream) {
   if (plan.total == 0) plan.total = 256;
-  cudaError_t e = cudaMalloc(&arena.base, plan.total);
+  cudaError_t e = stream ? cudaMallocAsync(&arena.base, plan.total, stream) : cudaMalloc(&arena.base, plan.total);
   if (e != cudaSuccess) {
     oom = e == cudaErrorMemoryAllocation;
     arena.base = nullptr;
-    return std::string("cudaMalloc of ") + std::to_string(plan.total) + " bytes failed: " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return std::string("device allocation of ") + std::to_string(plan.total) + " bytes failed: " +
+           cudaGetErrorString(e);
   }
   arena.bytes = plan.total;
+  arena.stream = stream;
   std::vector<uint8_t> staging(plan.total, 0);
   for (size_t i = 0; i < plan.parts.size(); ++i)
     if (plan.parts[i].second) std::memcpy(staging.data() + plan.offsets[i], plan.parts[i].first, plan.parts[i].second);
-  e = cudaMemcpy(arena.base, staging.data(), plan.total, cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return std::string("scene upload failed: ") + cudaGetErrorString(e);
+  // A pageable-source async copy returns once the bytes are staged.
+  e = stream ? cudaMemcpyAsync(arena.base, staging.data(), plan.total, cudaMemcpyHostToDevice, stream)
+             : cudaMemcpy(arena.base, staging.data(), plan.total, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return std::string("upload failed: ") + cudaGetErrorString(e);
   return "";
 }
 
@@ -801,10 +806,10 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
   out.dev = d;
   out.d_desc = reinterpret_cast<DevScene *>(base + img.desc_off);
   if (stream) {
-    // Pageable sources: both calls return once the bytes are staged.
+    // Pageable sources: both calls return once the bytes are staged, and
+    // the copies run in the stream's order (before any later wave).
     e = cudaMemcpyAsync(base, img.blob.data(), total, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   } else {
     e = cudaMemcpy(base, img.blob.data(), total, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice);
@@ -833,7 +838,7 @@ void release_scene(SceneHost &s) {
 }
 
 // ============================================================ environment
-std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom) {
+std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom, cudaStream_t stream) {
   oom = false;
   const float PI = 3.14159265358979323846f;
   uint32_t w = std::max(env.width, 1u), h = std::max(env.height, 1u);
@@ -886,7 +891,7 @@ std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom) {
   size_t p_mass = plan.add(mass.data(), mass.size() * 4);
   DevEnv tmp{};
   size_t p_desc = plan.add(&tmp, sizeof(DevEnv));
-  std::string err = commit(plan, out.arena, oom);
+  std::string err = commit(plan, out.arena, oom, stream);
   if (!err.empty()) {
     out.arena.release();
     return err;
@@ -901,7 +906,8 @@ std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom) {
   d.conditional = dptr<float>(out.arena, plan, p_c);
   d.mass = dptr<float>(out.arena, plan, p_mass);
   out.d_desc = const_cast<DevEnv *>(dptr<DevEnv>(out.arena, plan, p_desc));
-  cudaError_t e = cudaMemcpy(out.d_desc, &d, sizeof(DevEnv), cudaMemcpyHostToDevice);
+  cudaError_t e = stream ? cudaMemcpyAsync(out.d_desc, &d, sizeof(DevEnv), cudaMemcpyHostToDevice, stream)
+                         : cudaMemcpy(out.d_desc, &d, sizeof(DevEnv), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     out.arena.release();
     return std::string("environment upload failed: ") + cudaGetErrorString(e);

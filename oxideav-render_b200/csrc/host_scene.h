@@ -72,7 +72,9 @@ struct EnvHost {
   DevEnv *d_desc = nullptr;
   DeviceArena arena;
 };
-std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom);
+// Builds the environment's CDFs and uploads them (stream-ordered when
+// `stream` is non-null).
+std::string upload_env(const pt_environment &env, EnvHost &out, bool &oom, cudaStream_t stream = nullptr);
 void release_env(EnvHost &e);
 
 // Host-built tables the kernels read (sheen albedo, sRGB thresholds).

@@ -63,6 +63,17 @@ SIGNATURES = {
                               C.POINTER(abi.pt_environment), u8p, C.c_size_t]),
     "pt_refine_noalloc": (i32, [vp, u32, C.POINTER(abi.pt_camera), C.POINTER(abi.pt_render_options), u32, u32,
                                 C.c_void_p]),
+    # include/pt_b200_serve.h
+    "pt_server_create": (i32, [vp, C.POINTER(abi.pt_server_config), C.POINTER(vp)]),
+    "pt_server_destroy": (None, [vp]),
+    "pt_server_last_error": (C.c_char_p, [vp]),
+    "pt_server_scene_register": (i32, [vp, C.POINTER(abi.pt_scene_desc), C.POINTER(abi.pt_environment), u32p]),
+    "pt_server_scene_unregister": (i32, [vp, u32]),
+    "pt_server_scene_info": (i32, [vp, u32, u64p, C.POINTER(C.c_int)]),
+    "pt_server_submit": (i32, [vp, C.POINTER(abi.pt_server_request), u64p]),
+    "pt_server_wait": (i32, [vp, u64, i32, fp, C.c_size_t, C.POINTER(abi.pt_request_stats)]),
+    "pt_server_release": (i32, [vp, u64]),
+    "pt_server_stats_get": (i32, [vp, C.POINTER(abi.pt_server_stats)]),
     # include/pt_b200_debug.h
     "pt_debug_sobol": (i32, [vp, u32, u32, fp]),
     "pt_debug_pattern": (i32, [vp, u32, u32, fp]),
