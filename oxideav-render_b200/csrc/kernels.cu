@@ -308,7 +308,18 @@ cudaError_t launch_wavefront(const DevRequest *reqs, const WaveSegment *segs, ui
   if (e != cudaSuccess) return e;
   tm.mark(STAGE_RAYGEN, st);
   k_wf_raygen<<<(total + 255) / 256, 256, 0, st>>>(reqs, segs, nseg, total, w);
-  const uint32_t g_ext = (uint32_t)num_sms * 8, g_shade = (uint32_t)num_sms * 6, g_sh = (uint32_t)num_sms * 8;
+  // The traversal kernels are persistent: exactly the blocks that fit at once.
+  static int per_sm_ext = 0, per_sm_sh = 0;
+  if (per_sm_ext == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ext, k_wf_extend, 256, 0) != cudaSuccess ||
+        per_sm_ext < 1)
+      per_sm_ext = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_sh, k_wf_shadow, 256, 0) != cudaSuccess ||
+        per_sm_sh < 1)
+      per_sm_sh = 1;
+  }
+  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext), g_shade = (uint32_t)num_sms * 6,
+                 g_sh = (uint32_t)(num_sms * per_sm_sh);
   for (uint32_t it = 0; it < w.iterations; ++it) {
     tm.mark(STAGE_EXTEND, st);
     k_wf_extend<<<g_ext, 256, 0, st>>>(reqs, w, it, ctr);

@@ -20,6 +20,7 @@
 #pragma once
 
 #include "dev_integrator.cuh"
+#include "dev_traverse.cuh"
 
 namespace ptd {
 
@@ -110,30 +111,56 @@ __global__ void __launch_bounds__(256) k_wf_raygen(const DevRequest *reqs, const
   w.q[0][slot] = slot;
 }
 
-__global__ void __launch_bounds__(256) k_wf_extend(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+// Closest hit of every queued path: persistent lanes, one ray each, refilled
+// from the queue as rays finish (dev_traverse.cuh).
+__global__ void __launch_bounds__(256, 3) k_wf_extend(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
                                                    DevCounters *ctr) {
+  __shared__ int s_stack[kShortStack * 256];
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
+  uint32_t *claim = w.counters + iter * kWfCounterStride + 2;
+  TravStack stk;
+  stk.sm = s_stack + threadIdx.x;
+  stk.stride = blockDim.x;
   ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t slot = q[i];
-    float4 o = w.o[slot], d = w.d[slot];
-    uint4 sd = w.seed[slot];
-    const DevRequest &rq = reqs[sd.w];
-    PathState ps;
-    ps.o = {o.x, o.y, o.z};
-    ps.d = {d.x, d.y, d.z};
-    ps.k = __float_as_uint(o.w);
-    ps.smp.pixel_seed = sd.x;
-    ps.smp.index = sd.y;
-    ps.smp.path_seed = sd.z;
-    Hit h;
-    bool found = trace_extension(rq, ps, h, ts);
-    if (found) {
-      w.hit_tb[slot] = make_float4(h.t, h.b0, h.b1, h.b2);
-      w.hit_g[slot] = (h.g & HIT_G_MASK) | HIT_FOUND | (h.front ? HIT_FRONT : 0u);
-    } else {
-      w.hit_g[slot] = 0u;
+  bool has = false, exhausted = false;
+  uint32_t slot = 0, k = 0;
+  const DevRequest *rq = nullptr;
+  Sampler smp;
+  ClosestRay cr;
+  for (;;) {
+    uint32_t idx = warp_claim(claim, !has, n, exhausted);
+    if (!has && idx < n) {
+      slot = q[idx];
+      float4 o = w.o[slot], d = w.d[slot];
+      uint4 sd = w.seed[slot];
+      rq = reqs + sd.w;
+      smp.pixel_seed = sd.x;
+      smp.index = sd.y;
+      smp.path_seed = sd.z;
+      k = __float_as_uint(o.w);
+      cr.init({o.x, o.y, o.z}, {d.x, d.y, d.z}, 0.0f, inf());
+      has = true;
+      ts.ext_rays++;
+    }
+    if (!__any_sync(0xffffffffu, has)) break;
+    if (has) {
+      const DevScene &s = *rq->scene;
+      AcceptFilter acc{&s, &smp, k << 16, k == 0, 0xffffffffu};
+      uint32_t nodes = 0, tris = 0;
+      bool done = cr.step(s, stk, acc, nodes, tris, ts.err);
+      ts.ext_nodes += nodes;
+      ts.ext_tris += tris;
+      if (done) {
+        if (cr.have) {
+          const Hit &h = cr.best;
+          w.hit_tb[slot] = make_float4(h.t, h.b0, h.b1, h.b2);
+          w.hit_g[slot] = (h.g & HIT_G_MASK) | HIT_FOUND | (h.front ? HIT_FRONT : 0u);
+        } else {
+          w.hit_g[slot] = 0u;
+        }
+        has = false;
+      }
     }
   }
   flush_stats(ctr, ts);
@@ -171,34 +198,70 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevRequest *reqs, WaveBu
   }
 }
 
-__global__ void __launch_bounds__(256) k_wf_shadow(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+// Shadow rays of every queued path, each path's rays in generation order
+// (a visible ray adds its contribution to the path radiance, so the float
+// sum rounds as in the megakernel). Persistent lanes own one path at a time
+// and are refilled from the queue when its last ray finishes.
+__global__ void __launch_bounds__(256, 3) k_wf_shadow(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
                                                    DevCounters *ctr) {
+  __shared__ int s_stack[kShortStack * 256];
   const uint32_t n = w.counters[iter * kWfCounterStride + 1];
+  uint32_t *claim = w.counters + iter * kWfCounterStride + 3;
+  TravStack stk;
+  stk.sm = s_stack + threadIdx.x;
+  stk.stride = blockDim.x;
   ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t slot = w.q_shadow[i];
-    uint4 sd = w.seed[slot];
-    const DevRequest &rq = reqs[sd.w];
-    PathState ps;
-    ps.smp.pixel_seed = sd.x;
-    ps.smp.index = sd.y;
-    ps.smp.path_seed = sd.z;
-    float4 r = w.rad[slot];
-    V3 rad = {r.x, r.y, r.z};
-    uint32_t cnt = w.sh_n[slot];
-    for (uint32_t j = 0; j < cnt; ++j) {
-      size_t k = (size_t)j * w.capacity + slot;
-      float4 so = w.sh_o[k], sdd = w.sh_d[k], sc = w.sh_c[k];
-      ShadowRay sr;
-      sr.o = {so.x, so.y, so.z};
-      sr.tmax = so.w;
-      sr.d = {sdd.x, sdd.y, sdd.z};
-      sr.ray_id = __float_as_uint(sdd.w);
-      sr.contrib = {sc.x, sc.y, sc.z};
-      sr.skip = __float_as_uint(sc.w);
-      if (trace_shadow(rq, ps, sr, ts)) rad = vadd(rad, sr.contrib);
+  bool has = false, exhausted = false;
+  uint32_t slot = 0, j = 0, cnt = 0, ray_id = 0, skip = 0;
+  const DevRequest *rq = nullptr;
+  Sampler smp;
+  V3 rad = vzero(), contrib = vzero();
+  float covered = 0.0f;
+  ShadowTrav tr;
+  auto start_ray = [&]() {
+    size_t e = (size_t)j * w.capacity + slot;
+    float4 so = w.sh_o[e], sdd = w.sh_d[e], sc = w.sh_c[e];
+    tr.init({so.x, so.y, so.z}, {sdd.x, sdd.y, sdd.z}, so.w);
+    ray_id = __float_as_uint(sdd.w);
+    contrib = {sc.x, sc.y, sc.z};
+    skip = __float_as_uint(sc.w);
+    ts.shadow_rays++;
+  };
+  for (;;) {
+    uint32_t idx = warp_claim(claim, !has, n, exhausted);
+    if (!has && idx < n) {
+      slot = w.q_shadow[idx];
+      uint4 sd = w.seed[slot];
+      rq = reqs + sd.w;
+      smp.pixel_seed = sd.x;
+      smp.index = sd.y;
+      smp.path_seed = sd.z;
+      float4 r = w.rad[slot];
+      rad = {r.x, r.y, r.z};
+      covered = r.w;
+      cnt = w.sh_n[slot];
+      j = 0;
+      has = cnt > 0;
+      if (has) start_ray();
     }
-    w.rad[slot] = make_float4(rad.x, rad.y, rad.z, r.w);
+    if (!__any_sync(0xffffffffu, has)) break;
+    if (has) {
+      const DevScene &s = *rq->scene;
+      AcceptFilter acc{&s, &smp, ray_id, false, skip};
+      uint32_t nodes = 0, tris = 0;
+      int res = tr.step(s, stk, acc, nodes, tris, ts.err);
+      ts.sh_nodes += nodes;
+      ts.sh_tris += tris;
+      if (res != 0) {
+        if (res == 1) rad = vadd(rad, contrib);
+        if (++j < cnt) {
+          start_ray();
+        } else {
+          w.rad[slot] = make_float4(rad.x, rad.y, rad.z, covered);
+          has = false;
+        }
+      }
+    }
   }
   flush_stats(ctr, ts);
 }
