@@ -114,6 +114,10 @@ def workload(name: str):
     if name == "c2":
         scene, opts, env = ts.stress_c2()
         return scene, opts, env, "stress_heightfield_spheres 1920x1080 64spp 8 bounces (~4.1M tris, env 512x256)"
+    if name == "soup":
+        scene = ts.random_soup(500_000, seed=107)
+        opts = ts.pt_opts(1024, 16, 8, h=768, scene_camera=0, ambient=0.1)
+        return scene, opts, None, "random_soup 500k tris (mixed-workload scene class) 1024x768 16spp 8 bounces"
     raise SystemExit(f"unknown config {name}")
 
 
@@ -617,7 +621,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2"])
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "soup"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

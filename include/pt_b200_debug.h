@@ -50,6 +50,11 @@ typedef enum pt_schedule { PT_SCHEDULE_MEGAKERNEL = 0, PT_SCHEDULE_WAVEFRONT = 1
 PT_API pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule);
 /* Maximum path slots per wave (device sample buffer 16 B per slot). */
 PT_API pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots);
+/* BVH node layout the wavefront's traversal kernels walk, for extension and
+ * for shadow rays: 2 (two-child 64-byte nodes) or 4 (the same tree as
+ * four-child 128-byte nodes). Default: 4 for both. Hits are identical
+ * either way. */
+PT_API pt_status pt_set_node_width(pt_context *ctx, uint32_t extension_width, uint32_t shadow_width);
 /* Device time in ms of the last refine's path-tracing kernels (CUDA events
  * on the context stream). */
 PT_API pt_status pt_tracer_last_kernel_ms(const pt_tracer *tr, float *ms);

@@ -227,7 +227,8 @@ class pt_server_config(C.Structure):
         ("max_active", C.c_uint32),
         ("megakernel", C.c_uint32),
         ("pipeline_depth", C.c_uint32),
-        ("reserved", C.c_uint32 * 2),
+        ("node_width_extension", C.c_uint32),
+        ("node_width_shadow", C.c_uint32),
     ]
 
 

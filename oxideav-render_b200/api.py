@@ -81,6 +81,10 @@ class Context:
     def set_wave_slots(self, slots: int) -> None:
         self.check(self.lib.pt_set_wave_slots(self.ptr, slots))
 
+    def set_node_width(self, extension: int, shadow: int) -> None:
+        """BVH node layout (2 or 4 children) of extension and shadow rays."""
+        self.check(self.lib.pt_set_node_width(self.ptr, extension, shadow))
+
     def set_stage_timing(self, on: bool) -> None:
         self.check(self.lib.pt_set_stage_timing(self.ptr, 1 if on else 0))
 

@@ -107,6 +107,7 @@ DevRequest make_request(const pt_tracer &t, const SceneHost &sc, const EnvHost *
   rq.strategy = t.opts.path_trace.strategy;
   rq.clamp = t.opts.path_trace.clamp;
   rq.p_env = env ? (sc.dev.em_count > 0 ? 0.5f : 1.0f) : 0.0f;
+  rq.wide_nodes = t.ctx ? t.ctx->wide_nodes : (uint32_t)(WIDE_EXTENSION | WIDE_SHADOW);
   rq.accum = t.d_accum;
   return rq;
 }
@@ -796,6 +797,13 @@ pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule) {
 pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots) {
   if (!ctx || slots == 0) return fail(ctx, PT_ERR_INVALID_ARG, "bad argument");
   ctx->wave_slots = slots;
+  return PT_OK;
+}
+
+pt_status pt_set_node_width(pt_context *ctx, uint32_t extension_width, uint32_t shadow_width) {
+  if (!ctx || (extension_width != 2 && extension_width != 4) || (shadow_width != 2 && shadow_width != 4))
+    return fail(ctx, PT_ERR_INVALID_ARG, "node widths must be 2 or 4");
+  ctx->wide_nodes = (extension_width == 4 ? WIDE_EXTENSION : 0u) | (shadow_width == 4 ? WIDE_SHADOW : 0u);
   return PT_OK;
 }
 

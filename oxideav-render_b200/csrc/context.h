@@ -22,6 +22,9 @@ struct pt_context {
   uint32_t next_id = 1;
   uint32_t schedule = PT_SCHEDULE_MEGAKERNEL;
   uint32_t wave_slots = 1u << 22;
+  // WIDE_* bits: rays that walk the four-child node layout in the wavefront
+  // (default: both kinds).
+  uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   float4 *d_out = nullptr;
   size_t out_cap = 0;
   ptd::WaveSegment *d_segs = nullptr;

@@ -496,8 +496,25 @@ struct Bsdf {
     pdf_out = pdf + probs[LOBE_TRANSMISSION] * pdf_t;
   }
 
-  // Bsdf::sample, src/pathtrace.rs:1216-1279.
+  // Bsdf::sample, src/pathtrace.rs:1216-1279: sample_dir picks the lobe and
+  // direction, eval gives (f, pdf) and sample_accept applies the final
+  // checks. Split so a caller can share one eval call site.
   PT_DEV bool sample(const float u[3], V3 &l_out, V3 &f_out, float &pdf_out) const {
+    V3 l;
+    if (!sample_dir(u, l)) return false;
+    V3 f;
+    float pdf;
+    eval(l, f, pdf);
+    if (!sample_accept(f, pdf)) return false;
+    l_out = l;
+    f_out = f;
+    pdf_out = pdf;
+    return true;
+  }
+  PT_DEV static bool sample_accept(V3 f, float pdf) {
+    return !(pdf <= 0.0f || !isfinite(pdf) || ptd::is_black(f) || !finite3(f));
+  }
+  PT_DEV bool sample_dir(const float u[3], V3 &l_out) const {
     float acc = 0.0f;
     int lobe = -1;
 #pragma unroll
@@ -545,13 +562,7 @@ struct Bsdf {
     bool reflection = vdot(ng, l) > 0.0f;
     bool transmits = lobe == LOBE_TRANSMISSION || lobe == LOBE_DIFFUSE_T;
     if (reflection == transmits) return false;
-    V3 f;
-    float pdf;
-    eval(l, f, pdf);
-    if (pdf <= 0.0f || !isfinite(pdf) || ptd::is_black(f) || !finite3(f)) return false;
     l_out = l;
-    f_out = f;
-    pdf_out = pdf;
     return true;
   }
 };

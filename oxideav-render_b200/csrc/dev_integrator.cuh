@@ -304,131 +304,126 @@ PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hi
   const V3 ng = bsdf.ng;
   const V3 off_pos = offset_ray_origin(p, ng), off_neg = offset_ray_origin(p, vneg(ng));
 
-  // NEE: punctual lights.
-  for (uint32_t j = 0; j < s.light_count; ++j) {
-    LightSample ls;
-    if (!light_sample(s.lights[j], p, ls)) continue;
-    V3 f;
-    float pdf_unused;
-    bsdf.eval(ls.l, f, pdf_unused);
-    if (is_black(f)) continue;
-    ShadowRay sr;
-    sr.contrib = clamp_contrib(rq, vmul(vmul(ps.beta, f), ls.radiance));
-    if (sr.contrib.x == 0.0f && sr.contrib.y == 0.0f && sr.contrib.z == 0.0f) continue;  // adds nothing
-    sr.o = vdot(ls.l, ng) >= 0.0f ? off_pos : off_neg;
-    sr.d = ls.l;
-    sr.tmax = isfinite(ls.distance) ? ls.distance * (1.0f - 1.0e-4f) : inf();
-    sr.ray_id = ray_id | 0x8000u | (j & 0x7fffu);
-    sr.skip = 0xffffffffu;
-    sink.emit(sr);
-  }
-
-  // NEE: the area set (environment / emissive triangles).
-  float pl_u[4];
+  // Next-event estimation and BSDF sampling share one Bsdf::eval call site:
+  // candidate c < light_count is punctual light c, c == light_count the
+  // area-set sample (environment or emissive triangle), the last one the
+  // BSDF-sampled continuation. Shadow rays leave in the reference's order
+  // (punctual lights, then the area sample) and every value is computed as
+  // in Integrator::sample (src/pathtrace.rs:2171-2290); only the code path
+  // to eval is shared, which keeps the kernel's instruction footprint small.
+  float pl_u[4], pb_u[4];
   ps.smp.pattern(2 + 2 * k, pl_u);
-  if (strategy != PT_BSDF_ONLY && (rq.env || s.em_count > 0)) {
-    const float pe = rq.p_env;
-    const uint32_t shadow_id = ray_id | 0xffffu;
-    if (pl_u[2] < pe) {
-      V3 l, le;
-      float pdf;
-      if (rq.env && env_sample(*rq.env, pl_u[0], pl_u[1], l, le, pdf)) {
-        float pl = pe * pdf;
-        V3 f;
-        float pb;
-        bsdf.eval(l, f, pb);
-        if (!is_black(f) && !is_black(le) && pl > 0.0f) {
-          float w = strategy == PT_MIS ? power_heuristic(pl, pb) : 1.0f;
-          ShadowRay sr;
-          sr.contrib = clamp_contrib(rq, vscale(vmul(vmul(ps.beta, f), le), w / pl));
-          if (!(sr.contrib.x == 0.0f && sr.contrib.y == 0.0f && sr.contrib.z == 0.0f)) {
-            sr.o = vdot(l, ng) >= 0.0f ? off_pos : off_neg;
-            sr.d = l;
-            sr.tmax = inf();
-            sr.ray_id = shadow_id;
-            sr.skip = 0xffffffffu;
-            sink.emit(sr);
-          }
-        }
+  ps.smp.pattern(1 + 2 * k, pb_u);
+  const uint32_t nl = s.light_count;
+  const bool area_nee = strategy != PT_BSDF_ONLY && (rq.env || s.em_count > 0);
+  const uint32_t shadow_id = ray_id | 0xffffu;
+  V3 l, f;
+  float pdf;
+  for (uint32_t c = 0;; ++c) {
+    V3 le = vzero();
+    float pl = 0.0f, tmax = inf();
+    uint32_t skip = 0xffffffffu, rid = shadow_id;
+    bool go = false;
+    if (c < nl) {
+      LightSample ls;
+      if (light_sample(s.lights[c], p, ls)) {
+        l = ls.l;
+        le = ls.radiance;
+        tmax = isfinite(ls.distance) ? ls.distance * (1.0f - 1.0e-4f) : inf();
+        rid = ray_id | 0x8000u | (c & 0x7fffu);
+        go = true;
       }
-    } else if (s.em_count > 0) {
-      float us = pe > 0.0f ? clampr((pl_u[2] - pe) / (1.0f - pe), 0.0f, 0.999999f) : pl_u[2];
-      uint32_t li = min(upper_bound(s.em_cdf, s.em_count, us), s.em_count - 1);
-      uint32_t g = __ldg(s.em_tris + li);
-      V3 a, b, c;
-      tri_positions(s, g, a, b, c);
-      bool have_target = false;
-      V3 q = vzero();
-      if (triangle_solid_angle(p, a, b, c) >= 1.0e-4f) {
-        V3 l;
-        if (sample_spherical_triangle(p, a, b, c, pl_u[0], pl_u[1], l)) {
-          V3 n = vcross(vsub(b, a), vsub(c, a));
-          float dn = vdot(l, n);
-          if (dn != 0.0f) {
-            float t = vdot(vsub(a, p), n) / dn;
-            if (t > 0.0f && isfinite(t)) {
-              q = vadd(p, vscale(l, t));
-              have_target = true;
+    } else if (c == nl) {
+      if (!area_nee) continue;
+      const float pe = rq.p_env;
+      if (pl_u[2] < pe) {
+        float epdf;
+        if (rq.env && env_sample(*rq.env, pl_u[0], pl_u[1], l, le, epdf)) {
+          pl = pe * epdf;
+          go = true;
+        }
+      } else if (s.em_count > 0) {
+        float us = pe > 0.0f ? clampr((pl_u[2] - pe) / (1.0f - pe), 0.0f, 0.999999f) : pl_u[2];
+        uint32_t li = min(upper_bound(s.em_cdf, s.em_count, us), s.em_count - 1);
+        uint32_t g = __ldg(s.em_tris + li);
+        V3 a, b, cc;
+        tri_positions(s, g, a, b, cc);
+        bool have_target = false;
+        V3 q = vzero();
+        if (triangle_solid_angle(p, a, b, cc) >= 1.0e-4f) {
+          V3 ld;
+          if (sample_spherical_triangle(p, a, b, cc, pl_u[0], pl_u[1], ld)) {
+            V3 n = vcross(vsub(b, a), vsub(cc, a));
+            float dn = vdot(ld, n);
+            if (dn != 0.0f) {
+              float t = vdot(vsub(a, p), n) / dn;
+              if (t > 0.0f && isfinite(t)) {
+                q = vadd(p, vscale(ld, t));
+                have_target = true;
+              }
             }
           }
+        } else {
+          float su = sqrtf(pl_u[0]);
+          float w0 = 1.0f - su, w1 = su * (1.0f - pl_u[1]), w2 = su * pl_u[1];
+          q = {a.x * w0 + b.x * w1 + cc.x * w2, a.y * w0 + b.y * w1 + cc.y * w2, a.z * w0 + b.z * w1 + cc.z * w2};
+          have_target = true;
         }
-      } else {
-        float su = sqrtf(pl_u[0]);
-        float w0 = 1.0f - su, w1 = su * (1.0f - pl_u[1]), w2 = su * pl_u[1];
-        q = {a.x * w0 + b.x * w1 + c.x * w2, a.y * w0 + b.y * w1 + c.y * w2, a.z * w0 + b.z * w1 + c.z * w2};
-        have_target = true;
-      }
-      if (have_target) {
-        // barycentric_of, src/trace.rs:1120-1133.
-        V3 e1 = vsub(b, a), e2 = vsub(c, a), r = vsub(q, a);
-        float d11 = vdot(e1, e1), d12 = vdot(e1, e2), d22 = vdot(e2, e2);
-        float r1 = vdot(r, e1), r2 = vdot(r, e2);
-        float det = d11 * d22 - d12 * d12;
-        if (isfinite(det) && fabsf(det) > F32_MIN_POSITIVE) {
-          float u = (d22 * r1 - d12 * r2) / det;
-          float vv = (d11 * r2 - d12 * r1) / det;
-          float lb0 = clampr(1.0f - u - vv, 0.0f, 1.0f), lb1 = clampr(u, 0.0f, 1.0f), lb2 = clampr(vv, 0.0f, 1.0f);
-          V3 to = vsub(q, p);
-          float dist2 = vdot(to, to);
-          uint2 linfo = __ldg(s.tri_info + g);
-          const DevMaterial &lmat = s.materials[linfo.x];
-          Surface lsurf = surface(s, g, lb0, lb1, lb2, linfo.y);
-          if (dist2 > 1.0e-12f) {
-            float dist = sqrtf(dist2);
-            V3 l = vscale(to, 1.0f / dist);
-            float cos_l = -vdot(lsurf.ng, l);
-            float pl = tri_pdf(rq, li, g, p, q);
-            if ((cos_l > 0.0f || (lmat.m.double_sided && cos_l < 0.0f)) && pl > 0.0f && isfinite(pl)) {
-              V3 f;
-              float pb;
-              bsdf.eval(l, f, pb);
-              V3 le = emission(s, lmat, g, linfo.y, lb0, lb1, lb2);
-              if (!is_black(f) && !is_black(le)) {
-                float w = strategy == PT_MIS ? power_heuristic(pl, pb) : 1.0f;
-                ShadowRay sr;
-                sr.contrib = clamp_contrib(rq, vscale(vmul(vmul(ps.beta, f), le), w / pl));
-                if (!(sr.contrib.x == 0.0f && sr.contrib.y == 0.0f && sr.contrib.z == 0.0f)) {
-                  sr.o = vdot(l, ng) >= 0.0f ? off_pos : off_neg;
-                  sr.d = l;
-                  sr.tmax = fmaxf(dist * (1.0f - 1.0e-4f), 0.0f);
-                  sr.ray_id = shadow_id;
-                  sr.skip = g;
-                  sink.emit(sr);
-                }
+        if (have_target) {
+          // barycentric_of, src/trace.rs:1120-1133.
+          V3 e1 = vsub(b, a), e2 = vsub(cc, a), r = vsub(q, a);
+          float d11 = vdot(e1, e1), d12 = vdot(e1, e2), d22 = vdot(e2, e2);
+          float r1 = vdot(r, e1), r2 = vdot(r, e2);
+          float det = d11 * d22 - d12 * d12;
+          if (isfinite(det) && fabsf(det) > F32_MIN_POSITIVE) {
+            float u = (d22 * r1 - d12 * r2) / det;
+            float vv = (d11 * r2 - d12 * r1) / det;
+            float lb0 = clampr(1.0f - u - vv, 0.0f, 1.0f), lb1 = clampr(u, 0.0f, 1.0f), lb2 = clampr(vv, 0.0f, 1.0f);
+            V3 to = vsub(q, p);
+            float dist2 = vdot(to, to);
+            uint2 linfo = __ldg(s.tri_info + g);
+            const DevMaterial &lmat = s.materials[linfo.x];
+            Surface lsurf = surface(s, g, lb0, lb1, lb2, linfo.y);
+            if (dist2 > 1.0e-12f) {
+              float dist = sqrtf(dist2);
+              l = vscale(to, 1.0f / dist);
+              float cos_l = -vdot(lsurf.ng, l);
+              pl = tri_pdf(rq, li, g, p, q);
+              if ((cos_l > 0.0f || (lmat.m.double_sided && cos_l < 0.0f)) && pl > 0.0f && isfinite(pl)) {
+                le = emission(s, lmat, g, linfo.y, lb0, lb1, lb2);
+                tmax = fmaxf(dist * (1.0f - 1.0e-4f), 0.0f);
+                skip = g;
+                go = true;
               }
             }
           }
         }
       }
+    } else {
+      if (!bsdf.sample_dir(pb_u, l)) return false;
+      go = true;
     }
+    if (!go) continue;
+    bsdf.eval(l, f, pdf);
+    if (c > nl) break;  // the BSDF sample: continue the path below
+    if (is_black(f)) continue;
+    ShadowRay sr;
+    if (c < nl) {
+      sr.contrib = clamp_contrib(rq, vmul(vmul(ps.beta, f), le));
+    } else {
+      if (is_black(le) || !(pl > 0.0f)) continue;
+      float w = strategy == PT_MIS ? power_heuristic(pl, pdf) : 1.0f;
+      sr.contrib = clamp_contrib(rq, vscale(vmul(vmul(ps.beta, f), le), w / pl));
+    }
+    if (sr.contrib.x == 0.0f && sr.contrib.y == 0.0f && sr.contrib.z == 0.0f) continue;  // adds nothing
+    sr.o = vdot(l, ng) >= 0.0f ? off_pos : off_neg;
+    sr.d = l;
+    sr.tmax = tmax;
+    sr.ray_id = rid;
+    sr.skip = skip;
+    sink.emit(sr);
   }
-
-  // BSDF sampling.
-  float pb_u[4];
-  ps.smp.pattern(1 + 2 * k, pb_u);
-  V3 l, f;
-  float pdf;
-  if (!bsdf.sample(pb_u, l, f, pdf)) return false;
+  if (!Bsdf::sample_accept(f, pdf)) return false;
   ps.beta = vmul(ps.beta, vscale(f, 1.0f / pdf));
   if (!finite3(ps.beta)) return false;
   ps.prev_pdf = pdf;

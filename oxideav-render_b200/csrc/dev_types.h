@@ -2,6 +2,7 @@
 //
 // HBM layout of one resident scene (all arrays 256-byte aligned):
 //   nodes     BvhNode[node_count]        64 B  two child boxes + child refs
+//   nodes4    Bvh4Node[node4_count]     128 B  the same tree, four children per node
 //   tris      float4[3 * tri_count]      48 B  leaf-ordered triangle records:
 //                                              (v0.xyz, global id), v1, v2
 //   tri_info  uint2[tri_count]            8 B  (material, attribute flags) by global id
@@ -30,6 +31,20 @@ struct alignas(16) BvhNode {
   float4 a, b, c;
   int4 d;
 };
+
+// Four-child node, 128 bytes (one cache line), the same tree collapsed so
+// each node holds up to four children, boxes stored by axis:
+//   lo_x / hi_x / lo_y / hi_y / lo_z / hi_z  = that bound of children 0..3
+//   child = child refs as in BvhNode (>= 0 node, < 0 leaf), kEmptyChild
+//           for unused slots.
+struct alignas(128) Bvh4Node {
+  float4 lo_x, hi_x, lo_y, hi_y, lo_z, hi_z;
+  int4 child;
+  int4 pad;
+};
+constexpr int kEmptyChild = 0x7fffffff;
+// Node layout per ray kind in the wavefront (DevRequest::wide_nodes).
+enum WideNodes : uint32_t { WIDE_EXTENSION = 1u, WIDE_SHADOW = 2u };
 
 enum TriFlags : uint32_t {
   TRI_HAS_VN = 1u << 0,       // has_vertex_normals and a normal stream
@@ -78,7 +93,8 @@ struct DevScene {
   const float *em_pmf, *em_cdf;
   const uint32_t *em_lookup;
   uint32_t node_count, tri_count, material_count, texture_count, light_count, em_count;
-  uint32_t max_depth, pad;
+  uint32_t max_depth, node4_count;
+  const Bvh4Node *nodes4;  // the same tree with four-child nodes
 };
 
 struct DevEnv {
@@ -101,7 +117,7 @@ struct DevRequest {
   uint32_t orthographic, max_bounces, rr_start, seed, strategy;
   float clamp;
   float p_env;  // probability the area-light sampler picks the environment
-  uint32_t pad;
+  uint32_t wide_nodes;  // WIDE_* bits: which rays walk the four-child layout
   double *accum;  // width * height * 4 (sum r, g, b, covered count)
 };
 

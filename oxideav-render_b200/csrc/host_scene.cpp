@@ -316,9 +316,10 @@ void pad_box(const float lo[3], const float hi[3], float plo[3], float phi[3]) {
 }  // namespace
 
 void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
-               std::vector<float4> &records, BvhBuildStats &stats, int threads) {
+               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads) {
   auto t0 = std::chrono::steady_clock::now();
   out_nodes.clear();
+  out_nodes4.clear();
   records.clear();
   stats = BvhBuildStats{};
   if (tri_count == 0) return;
@@ -391,6 +392,77 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
       // Right first on the stack so the left subtree is laid out first.
       if (cs[1]->count == 0) st.push_back({nd.left + 1, (uint32_t)r[1]});
       if (cs[0]->count == 0) st.push_back({nd.left, (uint32_t)r[0]});
+    }
+  }
+  // Four-child layout: a node starts from its two binary children and opens
+  // the interior child of largest surface area until it holds four.
+  {
+    auto set_child = [&](Bvh4Node &n, int slot, const BNode *c, int ref) {
+      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      if (c) pad_box(c->lo, c->hi, lo, hi);
+      reinterpret_cast<float *>(&n.lo_x)[slot] = lo[0];
+      reinterpret_cast<float *>(&n.hi_x)[slot] = hi[0];
+      reinterpret_cast<float *>(&n.lo_y)[slot] = lo[1];
+      reinterpret_cast<float *>(&n.hi_y)[slot] = hi[1];
+      reinterpret_cast<float *>(&n.lo_z)[slot] = lo[2];
+      reinterpret_cast<float *>(&n.hi_z)[slot] = hi[2];
+      reinterpret_cast<int *>(&n.child)[slot] = ref;
+    };
+    struct Item {
+      uint32_t bin, gpu;
+    };
+    out_nodes4.push_back(Bvh4Node{});
+    out_nodes4[0].pad = make_int4(0, 0, 0, 0);
+    if (root.count > 0) {
+      set_child(out_nodes4[0], 0, &root, leaf_ref(root.first, root.count));
+      for (int k = 1; k < 4; ++k) set_child(out_nodes4[0], k, nullptr, kEmptyChild);
+    } else {
+      std::vector<Item> st{{0, 0}};
+      while (!st.empty()) {
+        Item it = st.back();
+        st.pop_back();
+        const BNode &nd = b.nodes[it.bin];
+        uint32_t ch[4] = {nd.left, nd.left + 1, 0, 0};
+        int nch = 2;
+        while (nch < 4) {
+          int best = -1;
+          float best_area = -1.0f;
+          for (int i = 0; i < nch; ++i) {
+            const BNode &c = b.nodes[ch[i]];
+            if (c.count > 0) continue;
+            float a = Builder::area(c.lo, c.hi);
+            if (a > best_area) {
+              best_area = a;
+              best = i;
+            }
+          }
+          if (best < 0) break;
+          uint32_t opened = ch[best];
+          for (int i = nch; i > best + 1; --i) ch[i] = ch[i - 1];
+          ch[best] = b.nodes[opened].left;
+          ch[best + 1] = b.nodes[opened].left + 1;
+          ++nch;
+        }
+        std::vector<Item> next;
+        for (int k = 0; k < 4; ++k) {
+          if (k >= nch) {
+            set_child(out_nodes4[it.gpu], k, nullptr, kEmptyChild);
+            continue;
+          }
+          const BNode &c = b.nodes[ch[k]];
+          int ref;
+          if (c.count > 0) {
+            ref = leaf_ref(c.first, c.count);
+          } else {
+            ref = (int)out_nodes4.size();
+            out_nodes4.push_back(Bvh4Node{});
+            out_nodes4.back().pad = make_int4(0, 0, 0, 0);
+            next.push_back({ch[k], (uint32_t)ref});
+          }
+          set_child(out_nodes4[it.gpu], k, &c, ref);
+        }
+        for (auto r = next.rbegin(); r != next.rend(); ++r) st.push_back(*r);
+      }
     }
   }
   records.resize(3 * (size_t)tri_count);
@@ -650,9 +722,10 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
 
   // BVH.
   std::vector<BvhNode> nodes;
+  std::vector<Bvh4Node> nodes4;
   std::vector<float4> records;
   int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  build_bvh(pos.data(), tc, rec_flags.data(), nodes, records, img.bvh, threads);
+  build_bvh(pos.data(), tc, rec_flags.data(), nodes, nodes4, records, img.bvh, threads);
 
   // Lights.
   std::vector<DevLight> lights(desc.light_count);
@@ -712,6 +785,7 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   // One arena.
   ArenaPlan plan;
   size_t p_nodes = plan.add(nodes.data(), nodes.size() * sizeof(BvhNode));
+  size_t p_nodes4 = plan.add(nodes4.data(), nodes4.size() * sizeof(Bvh4Node));
   size_t p_rec = plan.add(records.data(), records.size() * sizeof(float4));
   size_t p_info = plan.add(info.data(), info.size() * sizeof(uint2));
   size_t p_pos = plan.add(pos.data(), pos.size() * 4);
@@ -738,6 +812,7 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   DevScene &d = img.rel;
   std::memset(&d, 0, sizeof d);
   d.nodes = (const BvhNode *)rel(p_nodes, 1);
+  d.nodes4 = (const Bvh4Node *)rel(p_nodes4, nodes4.size());
   d.tris = (const float4 *)rel(p_rec, 1);
   d.tri_info = (const uint2 *)rel(p_info, 1);
   d.pos = (const float *)rel(p_pos, 1);
@@ -754,6 +829,7 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   d.em_cdf = (const float *)rel(p_cdf, 1);
   d.em_lookup = (const uint32_t *)rel(p_lookup, 1);
   d.node_count = (uint32_t)nodes.size();
+  d.node4_count = (uint32_t)nodes4.size();
   d.tri_count = tc;
   d.material_count = desc.material_count;
   d.texture_count = desc.texture_count;
@@ -788,6 +864,7 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
   uint8_t *base = static_cast<uint8_t *>(out.arena.base);
   DevScene d = img.rel;
   rebase(d.nodes, base);
+  rebase(d.nodes4, base);
   rebase(d.tris, base);
   rebase(d.tri_info, base);
   rebase(d.pos, base);

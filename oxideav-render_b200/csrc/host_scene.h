@@ -19,10 +19,11 @@ struct BvhBuildStats {
 };
 
 // Binned-SAH BVH over the soup (positions: 9 floats per triangle), laid out
-// as two-child 64-byte nodes plus 48-byte leaf-ordered triangle records.
+// as two-child 64-byte nodes, as the same tree collapsed to four-child
+// 128-byte nodes, plus 48-byte leaf-ordered triangle records shared by both.
 // `rec_flags[g]` goes into each record (REC_* bits).
 void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &nodes,
-               std::vector<float4> &records, BvhBuildStats &stats, int threads);
+               std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads);
 
 // One device allocation holding a scene (or an environment) plus the
 // device copy of its descriptor. `stream` non-null: the allocation is

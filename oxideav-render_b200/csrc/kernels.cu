@@ -42,7 +42,7 @@ struct ImmediateSink {
 };
 
 // One thread traces one (pixel, sample) path to the end.
-__global__ void __launch_bounds__(128) k_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg,
+__global__ void __launch_bounds__(128, 3) k_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg,
                                                     uint32_t total, float4 *out, DevCounters *ctr) {
   uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
   ThreadStats ts{0, 0, 0, 0, 0, 0, 0};

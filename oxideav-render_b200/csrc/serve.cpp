@@ -584,6 +584,8 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
     if (c.pipeline_depth) s->depth = std::min<uint32_t>(c.pipeline_depth, 8);
     s->eng->schedule = c.megakernel ? PT_SCHEDULE_MEGAKERNEL : PT_SCHEDULE_WAVEFRONT;
     s->eng->wave_slots = s->wave_slots;
+    s->eng->wide_nodes = (c.node_width_extension == 2 ? 0u : WIDE_EXTENSION) |
+                         (c.node_width_shadow == 2 ? 0u : WIDE_SHADOW);
     s->flights.resize(s->depth + 1);
     cudaError_t e = cudaSuccess;
     for (Flight &f : s->flights) {

@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256) k_wf_raygen(const DevRequest *reqs, const
 
 // Closest hit of every queued path: persistent lanes, one ray each, refilled
 // from the queue as rays finish (dev_traverse.cuh).
-__global__ void __launch_bounds__(256, 3) k_wf_extend(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+__global__ void __launch_bounds__(256, 4) k_wf_extend(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
                                                    DevCounters *ctr) {
   __shared__ int s_stack[kShortStack * 256];
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
@@ -139,19 +139,21 @@ __global__ void __launch_bounds__(256, 3) k_wf_extend(const DevRequest *reqs, Wa
       smp.index = sd.y;
       smp.path_seed = sd.z;
       k = __float_as_uint(o.w);
-      cr.init({o.x, o.y, o.z}, {d.x, d.y, d.z}, 0.0f, inf());
+      cr.init(*rq->scene, {o.x, o.y, o.z}, {d.x, d.y, d.z}, 0.0f, inf(), (rq->wide_nodes & WIDE_EXTENSION) != 0);
       has = true;
       ts.ext_rays++;
     }
     if (!__any_sync(0xffffffffu, has)) break;
+    // Node phase: while any lane still looks for its first leaf.
+    while (__any_sync(0xffffffffu, has && cr.core.searching())) {
+      if (has && cr.core.can_step()) cr.node_step(*rq->scene, stk, ts.ext_nodes, ts.err);
+    }
+    // Leaf phase.
     if (has) {
       const DevScene &s = *rq->scene;
       AcceptFilter acc{&s, &smp, k << 16, k == 0, 0xffffffffu};
-      uint32_t nodes = 0, tris = 0;
-      bool done = cr.step(s, stk, acc, nodes, tris, ts.err);
-      ts.ext_nodes += nodes;
-      ts.ext_tris += tris;
-      if (done) {
+      cr.leaf_step(s, acc, ts.ext_tris);
+      if (cr.core.finished()) {
         if (cr.have) {
           const Hit &h = cr.best;
           w.hit_tb[slot] = make_float4(h.t, h.b0, h.b1, h.b2);
@@ -166,7 +168,9 @@ __global__ void __launch_bounds__(256, 3) k_wf_extend(const DevRequest *reqs, Wa
   flush_stats(ctr, ts);
 }
 
-__global__ void __launch_bounds__(128) k_wf_shade(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+// Three 128-thread blocks per SM (168 registers): measured faster than the
+// unconstrained 234-register build despite a few spills.
+__global__ void __launch_bounds__(128, 3) k_wf_shade(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
   uint32_t *q_next = w.q[(iter + 1) & 1u];
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevRequest *reqs, WaveBu
 // (a visible ray adds its contribution to the path radiance, so the float
 // sum rounds as in the megakernel). Persistent lanes own one path at a time
 // and are refilled from the queue when its last ray finishes.
-__global__ void __launch_bounds__(256, 3) k_wf_shadow(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+__global__ void __launch_bounds__(256, 4) k_wf_shadow(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
                                                    DevCounters *ctr) {
   __shared__ int s_stack[kShortStack * 256];
   const uint32_t n = w.counters[iter * kWfCounterStride + 1];
@@ -221,7 +225,7 @@ __global__ void __launch_bounds__(256, 3) k_wf_shadow(const DevRequest *reqs, Wa
   auto start_ray = [&]() {
     size_t e = (size_t)j * w.capacity + slot;
     float4 so = w.sh_o[e], sdd = w.sh_d[e], sc = w.sh_c[e];
-    tr.init({so.x, so.y, so.z}, {sdd.x, sdd.y, sdd.z}, so.w);
+    tr.init(*rq->scene, {so.x, so.y, so.z}, {sdd.x, sdd.y, sdd.z}, so.w, (rq->wide_nodes & WIDE_SHADOW) != 0);
     ray_id = __float_as_uint(sdd.w);
     contrib = {sc.x, sc.y, sc.z};
     skip = __float_as_uint(sc.w);
@@ -245,15 +249,17 @@ __global__ void __launch_bounds__(256, 3) k_wf_shadow(const DevRequest *reqs, Wa
       if (has) start_ray();
     }
     if (!__any_sync(0xffffffffu, has)) break;
+    // Node phase: while any lane still looks for its first leaf.
+    while (__any_sync(0xffffffffu, has && tr.core.searching())) {
+      if (has && tr.core.can_step()) tr.node_step(*rq->scene, stk, ts.sh_nodes, ts.err);
+    }
+    // Leaf phase.
     if (has) {
       const DevScene &s = *rq->scene;
       AcceptFilter acc{&s, &smp, ray_id, false, skip};
-      uint32_t nodes = 0, tris = 0;
-      int res = tr.step(s, stk, acc, nodes, tris, ts.err);
-      ts.sh_nodes += nodes;
-      ts.sh_tris += tris;
-      if (res != 0) {
-        if (res == 1) rad = vadd(rad, contrib);
+      tr.leaf_step(s, acc, ts.sh_tris);
+      if (tr.done()) {
+        if (!tr.occluded) rad = vadd(rad, contrib);
         if (++j < cnt) {
           start_ray();
         } else {

@@ -86,6 +86,7 @@ SIGNATURES = {
     "pt_scene_bvh_stats": (i32, [vp, u32, u32p, u32p, u32p, dp, dp]),
     "pt_set_schedule": (i32, [vp, u32]),
     "pt_set_wave_slots": (i32, [vp, u32]),
+    "pt_set_node_width": (i32, [vp, u32, u32]),
     "pt_tracer_last_kernel_ms": (i32, [vp, fp]),
 }
 

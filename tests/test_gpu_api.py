@@ -81,9 +81,23 @@ def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
     else:
         scene, opts = ts.dispersive_sphere(1.0), ts.pt_opts(48, 8, 8)
     a, ra, ta = _accum_with(ctx, 0, scene, opts, env)
-    b, rb, tb = _accum_with(ctx, 1, scene, opts, env)
-    assert np.array_equal(a, b)
-    assert ra == rb and ta == tb
+    try:
+        # The wavefront on the two-child layout: the same tree, visited at
+        # least as much (its speculative node phase may test boxes against
+        # an older closest hit), identical hits.
+        ctx.set_node_width(2, 2)
+        b, rb, tb = _accum_with(ctx, 1, scene, opts, env)
+        assert np.array_equal(a, b)
+        assert ra == rb and tb[0] >= ta[0] and tb[1] >= ta[1]
+        # On the four-child layout (either ray kind): other node visits,
+        # identical hits.
+        for ext, sh in ((4, 4), (2, 4), (4, 2)):
+            ctx.set_node_width(ext, sh)
+            c, rc, _ = _accum_with(ctx, 1, scene, opts, env)
+            assert np.array_equal(a, c), (ext, sh)
+            assert rc == ra
+    finally:
+        ctx.set_node_width(4, 4)
 
 
 def test_sync_resets_only_on_radiance_changes(ctx):
