@@ -36,9 +36,15 @@ PT_API pt_status pt_tracer_traversal_counts(const pt_tracer *tr, uint64_t *nodes
 PT_API pt_status pt_tracer_traversal_split(const pt_tracer *tr, uint64_t out[4]);
 /* Per-stage device time of refine calls (CUDA events between the kernels of
  * each stage on the context stream), off by default. Stages, in order:
- * ray generation, closest hit, shade, shadow rays, accumulate, megakernel. */
+ * ray generation, closest hit, shade, shadow rays, accumulate, megakernel,
+ * material sort. */
 PT_API pt_status pt_set_stage_timing(pt_context *ctx, int on);
 PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n);
+/* Wavefront shade order: nonzero buckets the active queue by (scene,
+ * material) before each shade launch so warps shade one material at a time
+ * (three small kernels per bounce; on by default). Images are identical
+ * either way. */
+PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
 /* BVH statistics of a resident scene. */
 PT_API pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes, uint32_t *leaves,
                              uint32_t *max_depth, double *sah_cost, double *build_seconds);

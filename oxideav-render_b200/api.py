@@ -81,6 +81,9 @@ class Context:
     def set_wave_slots(self, slots: int) -> None:
         self.check(self.lib.pt_set_wave_slots(self.ptr, slots))
 
+    def set_material_sort(self, on: bool) -> None:
+        self.check(self.lib.pt_set_material_sort(self.ptr, 1 if on else 0))
+
     def set_node_width(self, extension: int, shadow: int) -> None:
         """BVH node layout (2 or 4 children) of extension and shadow rays."""
         self.check(self.lib.pt_set_node_width(self.ptr, extension, shadow))
@@ -249,7 +252,7 @@ class PathTracer:
         self.ctx.check(self.lib.pt_tracer_traversal_counts(self.ptr, C.byref(n), C.byref(t)))
         return n.value, t.value
 
-    STAGES = ("raygen", "extend", "shade", "shadow", "accumulate", "megakernel")
+    STAGES = ("raygen", "extend", "shade", "shadow", "accumulate", "megakernel", "sort")
 
     def stage_ms(self) -> dict:
         """Device ms per stage of the last refine (with stage timing on)."""

@@ -194,7 +194,8 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
                     16 * P, 4 * P,                                           // hit_tb hit_g
                     16 * P * S, 16 * P * S, 16 * P * S, 4 * P,               // sh_o sh_d sh_c sh_n
                     4 * P, 4 * P, 4 * P,                                     // q0 q1 q_shadow
-                    4 * (size_t)kWfCounterStride * (iterations + 1)};
+                    4 * (size_t)kWfCounterStride * (iterations + 1),
+                    4 * P, 4 * 2 * (size_t)kSortBuckets * (iterations + 1)};  // q_sorted sort_counts
   size_t off[sizeof(sizes) / sizeof(sizes[0])], total = 0;
   for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); ++i) {
     total = (total + 255) & ~(size_t)255;
@@ -222,6 +223,8 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   w.q[1] = (uint32_t *)(b + off[k++]);
   w.q_shadow = (uint32_t *)(b + off[k++]);
   w.counters = (uint32_t *)(b + off[k++]);
+  w.q_sorted = (uint32_t *)(b + off[k++]);
+  w.sort_counts = (uint32_t *)(b + off[k++]);
   w.capacity = capacity;
   w.shadow_slots = shadow_slots;
   w.iterations = iterations;
@@ -280,7 +283,7 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
   CK(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
   StageTimer timer;
   if (ctx->stage_timing) {
-    size_t need = waves.size() * (3 * (size_t)max_iter + 3) + 1;
+    size_t need = waves.size() * (4 * (size_t)max_iter + 3) + 1;
     while (ctx->stage_events.size() < need) {
       cudaEvent_t ev;
       CK(ctx, cudaEventCreate(&ev));
@@ -478,6 +481,7 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
   if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
     WaveBuffers w = ctx->wf;
     w.iterations = iters;
+    w.sort_materials = ctx->material_sort ? 1u : 0u;
     CK(ctx, launch_wavefront(d_reqs, d_segs, nseg, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream, timer));
     if (timer) timer->mark(STAGE_ACCUMULATE, ctx->stream);
     CK(ctx, launch_accumulate(d_reqs, d_segs, nseg, max_pix, w.rad, ctx->stream));
@@ -797,6 +801,12 @@ pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule) {
 pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots) {
   if (!ctx || slots == 0) return fail(ctx, PT_ERR_INVALID_ARG, "bad argument");
   ctx->wave_slots = slots;
+  return PT_OK;
+}
+
+pt_status pt_set_material_sort(pt_context *ctx, int on) {
+  if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
+  ctx->material_sort = on != 0;
   return PT_OK;
 }
 

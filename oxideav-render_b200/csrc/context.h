@@ -25,6 +25,7 @@ struct pt_context {
   // WIDE_* bits: rays that walk the four-child node layout in the wavefront
   // (default: both kinds).
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
+  bool material_sort = true;  // bucket each shade queue by material
   float4 *d_out = nullptr;
   size_t out_cap = 0;
   ptd::WaveSegment *d_segs = nullptr;

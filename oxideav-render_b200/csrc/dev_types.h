@@ -147,8 +147,11 @@ struct WaveBuffers {
   uint32_t *q[2];              // active queues (ping-pong by iteration)
   uint32_t *q_shadow;
   uint32_t *counters;          // [iterations][kWfCounterStride]
-  uint32_t capacity, shadow_slots, iterations, pad;
+  uint32_t *q_sorted;          // the active queue bucketed by material (material sort on)
+  uint32_t *sort_counts;       // [iterations][2][kSortBuckets]: bucket sizes, then cursors
+  uint32_t capacity, shadow_slots, iterations, sort_materials;
 };
+constexpr uint32_t kSortBuckets = 256;
 
 // Per-launch device counters (rays traced, traversal work, errors).
 struct DevCounters {
@@ -160,7 +163,7 @@ struct DevCounters {
 
 // Stages timed by the optional per-stage CUDA events.
 enum Stage : int { STAGE_RAYGEN = 0, STAGE_EXTEND, STAGE_SHADE, STAGE_SHADOW, STAGE_ACCUMULATE, STAGE_MEGAKERNEL,
-                   STAGE_END, STAGE_COUNT = STAGE_END };
+                   STAGE_SORT, STAGE_END, STAGE_COUNT = STAGE_END };
 enum ErrorFlags : uint32_t { ERR_STACK_OVERFLOW = 1u };
 
 }  // namespace ptd

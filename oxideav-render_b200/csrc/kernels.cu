@@ -305,6 +305,8 @@ cudaError_t launch_wavefront(const DevRequest *reqs, const WaveSegment *segs, ui
   StageTimer none;
   StageTimer &tm = timer ? *timer : none;
   cudaError_t e = cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * kWfCounterStride * (w.iterations + 1), st);
+  if (e == cudaSuccess && w.sort_materials)
+    e = cudaMemsetAsync(w.sort_counts, 0, sizeof(uint32_t) * 2 * kSortBuckets * (w.iterations + 1), st);
   if (e != cudaSuccess) return e;
   tm.mark(STAGE_RAYGEN, st);
   k_wf_raygen<<<(total + 255) / 256, 256, 0, st>>>(reqs, segs, nseg, total, w);
@@ -323,6 +325,12 @@ cudaError_t launch_wavefront(const DevRequest *reqs, const WaveSegment *segs, ui
   for (uint32_t it = 0; it < w.iterations; ++it) {
     tm.mark(STAGE_EXTEND, st);
     k_wf_extend<<<g_ext, 256, 0, st>>>(reqs, w, it, ctr);
+    if (w.sort_materials) {
+      tm.mark(STAGE_SORT, st);
+      k_wf_sort_count<<<g_shade, 256, 0, st>>>(reqs, w, it);
+      k_wf_sort_scan<<<1, kSortBuckets, 0, st>>>(w, it);
+      k_wf_sort_scatter<<<g_shade, 256, 0, st>>>(reqs, w, it);
+    }
     tm.mark(STAGE_SHADE, st);
     k_wf_shade<<<g_shade, 128, 0, st>>>(reqs, w, it);
     tm.mark(STAGE_SHADOW, st);

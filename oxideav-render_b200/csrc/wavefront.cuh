@@ -168,11 +168,68 @@ __global__ void __launch_bounds__(256, 4) k_wf_extend(const DevRequest *reqs, Wa
   flush_stats(ctr, ts);
 }
 
+// ---- material sort: the active queue bucketed by (scene, material) before
+// shade, stable within each warp's group of equal keys. Bucket 0 holds the
+// paths whose ray missed.
+PT_DEV uint32_t sort_key(const DevRequest *reqs, const WaveBuffers &w, uint32_t slot) {
+  uint32_t hg = w.hit_g[slot];
+  if (!(hg & HIT_FOUND)) return 0;
+  const DevScene *s = reqs[w.seed[slot].w].scene;
+  uint32_t m = __ldg(s->tri_info + (hg & HIT_G_MASK)).x;
+  uint32_t sh = (uint32_t)((uintptr_t)s >> 8) * 0x9E3779B1u;
+  return 1u + (m + sh) % (kSortBuckets - 1u);
+}
+
+__global__ void __launch_bounds__(256) k_wf_sort_count(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+  const uint32_t n = w.counters[iter * kWfCounterStride + 0];
+  const uint32_t *q = w.q[iter & 1u];
+  uint32_t *count = w.sort_counts + (size_t)iter * 2 * kSortBuckets;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t key = sort_key(reqs, w, q[i]);
+    uint32_t peers = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(count + key, (uint32_t)__popc(peers));
+  }
+}
+
+// One block of kSortBuckets threads: bucket sizes -> start cursors.
+__global__ void __launch_bounds__(kSortBuckets) k_wf_sort_scan(WaveBuffers w, uint32_t iter) {
+  __shared__ uint32_t s[kSortBuckets];
+  uint32_t *count = w.sort_counts + (size_t)iter * 2 * kSortBuckets;
+  const uint32_t t = threadIdx.x;
+  const uint32_t own = count[t];
+  s[t] = own;
+  __syncthreads();
+  for (uint32_t off = 1; off < kSortBuckets; off <<= 1) {
+    uint32_t v = t >= off ? s[t - off] : 0u;
+    __syncthreads();
+    s[t] += v;
+    __syncthreads();
+  }
+  count[kSortBuckets + t] = s[t] - own;
+}
+
+__global__ void __launch_bounds__(256) k_wf_sort_scatter(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+  const uint32_t n = w.counters[iter * kWfCounterStride + 0];
+  const uint32_t *q = w.q[iter & 1u];
+  uint32_t *cursor = w.sort_counts + (size_t)iter * 2 * kSortBuckets + kSortBuckets;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t slot = q[i];
+    uint32_t key = sort_key(reqs, w, slot);
+    uint32_t peers = __match_any_sync(__activemask(), key);
+    uint32_t leader = (uint32_t)(__ffs(peers) - 1);
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(cursor + key, (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    w.q_sorted[base + __popc(peers & ((1u << lane) - 1u))] = slot;
+  }
+}
+
 // Three 128-thread blocks per SM (168 registers): measured faster than the
 // unconstrained 234-register build despite a few spills.
 __global__ void __launch_bounds__(128, 3) k_wf_shade(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
-  const uint32_t *q = w.q[iter & 1u];
+  const uint32_t *q = w.sort_materials ? w.q_sorted : w.q[iter & 1u];
   uint32_t *q_next = w.q[(iter + 1) & 1u];
   uint32_t *n_next = w.counters + (iter + 1) * kWfCounterStride + 0;
   uint32_t *n_shadow = w.counters + iter * kWfCounterStride + 1;

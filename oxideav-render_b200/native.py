@@ -87,6 +87,7 @@ SIGNATURES = {
     "pt_set_schedule": (i32, [vp, u32]),
     "pt_set_wave_slots": (i32, [vp, u32]),
     "pt_set_node_width": (i32, [vp, u32, u32]),
+    "pt_set_material_sort": (i32, [vp, i32]),
     "pt_tracer_last_kernel_ms": (i32, [vp, fp]),
 }
 

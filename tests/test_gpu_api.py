@@ -96,8 +96,15 @@ def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
             c, rc, _ = _accum_with(ctx, 1, scene, opts, env)
             assert np.array_equal(a, c), (ext, sh)
             assert rc == ra
+        # Material-sorted shading (the default) reorders work only.
+        for sort in (False, True):
+            ctx.set_material_sort(sort)
+            d, rd, _ = _accum_with(ctx, 1, scene, opts, env)
+            assert np.array_equal(a, d), sort
+            assert rd == ra
     finally:
         ctx.set_node_width(4, 4)
+        ctx.set_material_sort(True)
 
 
 def test_sync_resets_only_on_radiance_changes(ctx):
