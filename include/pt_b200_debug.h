@@ -45,6 +45,30 @@ PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n)
  * (three small kernels per bounce; on by default). Images are identical
  * either way. */
 PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
+
+/* ---- autotuner: one configuration per scene class ----
+ * A scene class groups scenes by triangle-count scale (factors of 4),
+ * emissive triangles, environment map, punctual lights and textures. */
+typedef struct pt_tune_choice {
+  uint32_t schedule;             /* pt_schedule */
+  uint32_t node_width_extension; /* 2 or 4 */
+  uint32_t node_width_shadow;    /* 2 or 4 */
+  uint32_t material_sort;        /* 0 / 1 */
+  uint32_t wave_slots;
+  float samples_per_s;           /* calibration throughput */
+} pt_tune_choice;
+/* Times every candidate (megakernel; wavefront x node widths x material sort
+ * x wave size) on a calibration refine of `samples` spp of the tracer's
+ * scene, camera and options (a scratch accumulator: the tracer's own is
+ * untouched) and records the fastest as the configuration of the scene's
+ * class: later refines of tracers in that class use it. Every candidate
+ * gives bit-identical images. `best` may be NULL. */
+PT_API pt_status pt_autotune(pt_context *ctx, pt_tracer *tr, uint32_t samples, pt_tune_choice *best);
+/* The recorded configuration of the tracer's scene class: PT_OK, or
+ * PT_ERR_NOT_FOUND when the class has not been tuned. */
+PT_API pt_status pt_tune_lookup(pt_context *ctx, const pt_tracer *tr, pt_tune_choice *out);
+/* Forgets every recorded configuration. */
+PT_API pt_status pt_tune_reset(pt_context *ctx);
 /* BVH statistics of a resident scene. */
 PT_API pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes, uint32_t *leaves,
                              uint32_t *max_depth, double *sah_cost, double *build_seconds);

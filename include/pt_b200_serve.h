@@ -51,6 +51,10 @@ typedef struct pt_server_config {
   uint32_t pipeline_depth;   /* waves in flight on the stream; 0 = 2 */
   uint32_t node_width_extension; /* BVH node layout of extension rays: 2 or 4; 0 = 4 */
   uint32_t node_width_shadow;    /* BVH node layout of shadow rays: 2 or 4; 0 = 4 */
+  uint32_t autotune;             /* nonzero: tune each new scene class before its first request runs
+                                    (pt_autotune on the request's camera and options; the node
+                                    layouts of the class's requests follow the result) */
+  uint32_t material_sort_off;    /* nonzero: shade without material sort */
 } pt_server_config;
 
 typedef struct pt_server_request {
@@ -79,6 +83,7 @@ typedef struct pt_server_stats {
   uint64_t scene_evictions;
   uint64_t resident_bytes, peak_resident_bytes;
   uint32_t resident_scenes, active, pending, accumulators;
+  uint64_t tuned_classes;   /* scene classes tuned by the server (config.autotune) */
 } pt_server_stats;
 
 /* A server on `ctx`'s device. `cfg` may be NULL (defaults). The server does

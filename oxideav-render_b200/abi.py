@@ -229,6 +229,8 @@ class pt_server_config(C.Structure):
         ("pipeline_depth", C.c_uint32),
         ("node_width_extension", C.c_uint32),
         ("node_width_shadow", C.c_uint32),
+        ("autotune", C.c_uint32),
+        ("material_sort_off", C.c_uint32),
     ]
 
 
@@ -270,11 +272,24 @@ class pt_server_stats(C.Structure):
         ("active", C.c_uint32),
         ("pending", C.c_uint32),
         ("accumulators", C.c_uint32),
+        ("tuned_classes", C.c_uint64),
+    ]
+
+
+# include/pt_b200_debug.h
+class pt_tune_choice(C.Structure):
+    _fields_ = [
+        ("schedule", C.c_uint32),
+        ("node_width_extension", C.c_uint32),
+        ("node_width_shadow", C.c_uint32),
+        ("material_sort", C.c_uint32),
+        ("wave_slots", C.c_uint32),
+        ("samples_per_s", C.c_float),
     ]
 
 
 ABI_STRUCTS = [
     pt_texture_binding, pt_material, pt_texture, pt_draw_item, pt_light,
     pt_scene_desc, pt_environment, pt_camera, pt_path_trace_options, pt_render_options,
-    pt_server_config, pt_server_request, pt_request_stats, pt_server_stats,
+    pt_server_config, pt_server_request, pt_request_stats, pt_server_stats, pt_tune_choice,
 ]

@@ -81,6 +81,28 @@ class Context:
     def set_wave_slots(self, slots: int) -> None:
         self.check(self.lib.pt_set_wave_slots(self.ptr, slots))
 
+    @staticmethod
+    def _tune_dict(c: abi.pt_tune_choice) -> dict:
+        return {name: getattr(c, name) for name, _ in abi.pt_tune_choice._fields_}
+
+    def autotune(self, tracer: "PathTracer", samples: int = 1) -> dict:
+        """pt_autotune: the fastest configuration for the tracer's scene class
+        (measured on a scratch accumulator); later refines of that class use it."""
+        c = abi.pt_tune_choice()
+        self.check(self.lib.pt_autotune(self.ptr, tracer.ptr, int(samples), C.byref(c)))
+        return self._tune_dict(c)
+
+    def tune_lookup(self, tracer: "PathTracer") -> Optional[dict]:
+        c = abi.pt_tune_choice()
+        st = self.lib.pt_tune_lookup(self.ptr, tracer.ptr, C.byref(c))
+        if st == abi.PT_ERR_NOT_FOUND:
+            return None
+        self.check(st)
+        return self._tune_dict(c)
+
+    def tune_reset(self) -> None:
+        self.check(self.lib.pt_tune_reset(self.ptr))
+
     def set_material_sort(self, on: bool) -> None:
         self.check(self.lib.pt_set_material_sort(self.ptr, 1 if on else 0))
 

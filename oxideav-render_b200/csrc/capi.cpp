@@ -107,7 +107,12 @@ DevRequest make_request(const pt_tracer &t, const SceneHost &sc, const EnvHost *
   rq.strategy = t.opts.path_trace.strategy;
   rq.clamp = t.opts.path_trace.clamp;
   rq.p_env = env ? (sc.dev.em_count > 0 ? 0.5f : 1.0f) : 0.0f;
-  rq.wide_nodes = t.ctx ? t.ctx->wide_nodes : (uint32_t)(WIDE_EXTENSION | WIDE_SHADOW);
+  rq.wide_nodes = (uint32_t)(WIDE_EXTENSION | WIDE_SHADOW);
+  if (t.ctx) {
+    rq.wide_nodes = t.ctx->wide_nodes;
+    auto it = t.ctx->tuned.find(scene_class(sc, env != nullptr));
+    if (it != t.ctx->tuned.end()) rq.wide_nodes = it->second.wide_nodes;
+  }
   rq.accum = t.d_accum;
   return rq;
 }
@@ -156,6 +161,13 @@ std::vector<WaveSegment> pack_wave(std::vector<Job> &jobs, const std::vector<uin
 
 pt_status check_options(pt_context *ctx, const pt_camera *cam, const pt_render_options *o) {
   return validate_opts(ctx, cam, o);
+}
+
+uint32_t scene_class(const SceneHost &sc, bool env) {
+  uint32_t scale = 0;
+  for (uint64_t t = std::max<uint64_t>(sc.tri_count, 1); t >= 4; t >>= 2) ++scale;
+  return scale | (sc.dev.em_count > 0 ? 1u << 8 : 0u) | (env ? 1u << 9 : 0u) | (sc.light_count > 0 ? 1u << 10 : 0u) |
+         (sc.dev.texture_count > 0 ? 1u << 11 : 0u);
 }
 
 float4 bg_linear(const pt_render_options &o) {
@@ -340,15 +352,107 @@ pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_trac
   return PT_OK;
 }
 
+// Applies a tuned configuration's wave-level knobs for one call and
+// restores the context's own afterwards.
+struct KnobScope {
+  pt_context *ctx;
+  uint32_t schedule, wave_slots;
+  bool sort;
+  KnobScope(pt_context *c, const TuneChoice *tc)
+      : ctx(c), schedule(c->schedule), wave_slots(c->wave_slots), sort(c->material_sort) {
+    if (tc) {
+      c->schedule = tc->schedule;
+      c->wave_slots = tc->wave_slots;
+      c->material_sort = tc->material_sort != 0;
+    }
+  }
+  ~KnobScope() {
+    ctx->schedule = schedule;
+    ctx->wave_slots = wave_slots;
+    ctx->material_sort = sort;
+  }
+};
+
 pt_status refine_impl(pt_tracer *t, uint32_t n) {
   if (!t->have_state || n == 0) return PT_OK;
   n = std::min(n, 0xffffffffu - t->samples);
   if (n == 0) return PT_OK;
+  pt_context *ctx = t->ctx;
+  const TuneChoice *tc = nullptr;
+  if (SceneHost *sc = find_scene(ctx, t->scene_id)) {
+    auto it = ctx->tuned.find(scene_class(*sc, t->env != nullptr));
+    if (it != ctx->tuned.end()) tc = &it->second;
+  }
+  KnobScope knobs(ctx, tc);
   std::vector<pt_tracer *> tracers;
   std::vector<Job> jobs;
-  pt_status st = add_job(t->ctx, t, n, tracers, jobs);
+  pt_status st = add_job(ctx, t, n, tracers, jobs);
   if (st != PT_OK) return st;
-  return run_jobs(t->ctx, tracers, jobs, t);
+  return run_jobs(ctx, tracers, jobs, t);
+}
+
+// Calibration refines of `samples` spp of t's scene, camera and options on a
+// scratch accumulator under every candidate configuration; the fastest
+// (device time, best of two runs) becomes the scene class's configuration.
+pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, const EnvHost *env, uint32_t samples,
+                         TuneChoice &best) {
+  samples = std::max(samples, 1u);
+  CK(ctx, cudaSetDevice(ctx->device));
+  pt_tracer s;
+  s.ctx = ctx;
+  s.cam = t->cam;
+  s.opts = t->opts;
+  s.w = t->w;
+  s.h = t->h;
+  s.scene_id = t->scene_id;
+  s.have_state = true;
+  s.dirty = false;
+  const size_t n = (size_t)s.w * s.h * 4;
+  CK(ctx, cudaMalloc(&s.d_accum, n * sizeof(double)));
+  s.accum_cap = n;
+  struct Free {
+    double *p;
+    ~Free() { cudaFree(p); }
+  } free_accum{s.d_accum};
+  const uint32_t cls = scene_class(*sc, env != nullptr);
+  std::vector<TuneChoice> cands;
+  cands.push_back({PT_SCHEDULE_MEGAKERNEL, WIDE_EXTENSION | WIDE_SHADOW, 0, 1u << 22, 0.0f});
+  for (uint32_t wide : {WIDE_EXTENSION | WIDE_SHADOW, (uint32_t)WIDE_SHADOW, 0u, (uint32_t)WIDE_EXTENSION})
+    for (uint32_t sort : {1u, 0u})
+      for (uint32_t slots : {1u << 22, 1u << 20}) cands.push_back({PT_SCHEDULE_WAVEFRONT, wide, sort, slots, 0.0f});
+  KnobScope restore(ctx, nullptr);
+  const double paths = (double)s.w * s.h * samples;
+  best = cands[0];
+  float best_ms = -1.0f;
+  for (TuneChoice &c : cands) {
+    ctx->schedule = c.schedule;
+    ctx->wave_slots = c.wave_slots;
+    ctx->material_sort = c.material_sort != 0;
+    float ms = -1.0f;
+    for (int rep = 0; rep < 2; ++rep) {
+      s.samples = 0;
+      std::vector<pt_tracer *> tr{&s};
+      std::vector<Job> jobs{make_job(s, *sc, env, samples)};
+      jobs[0].req.wide_nodes = c.wide_nodes;
+      pt_status st = run_jobs(ctx, tr, jobs, nullptr);
+      if (st != PT_OK) return st;
+      if (ms < 0.0f || ctx->last_batch_ms < ms) ms = ctx->last_batch_ms;
+    }
+    c.samples_per_s = ms > 0.0f ? (float)(paths / (ms * 1e-3)) : 0.0f;
+    if (best_ms < 0.0f || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  ctx->tuned[cls] = best;
+  return PT_OK;
+}
+
+pt_status autotune_impl(pt_context *ctx, pt_tracer *t, uint32_t samples, TuneChoice &best) {
+  if (!t->have_state) return fail(ctx, PT_ERR_INVALID_ARG, "tracer is not synced");
+  SceneHost *sc = find_scene(ctx, t->scene_id);
+  if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
+  return autotune_scene(ctx, t, sc, t->env.get(), samples, best);
 }
 
 pt_status refine_many_impl(pt_context *ctx, pt_tracer *const *tracers, const uint32_t *samples, uint32_t count) {
@@ -465,6 +569,10 @@ pt_status set_env_impl(pt_tracer *t, const pt_environment *env) {
 namespace ptd {
 pt_status ctx_fail(pt_context *ctx, pt_status st, const std::string &msg) { return fail(ctx, st, msg); }
 SceneHost *ctx_find_scene(pt_context *ctx, uint32_t id) { return find_scene(ctx, id); }
+pt_status autotune(pt_context *ctx, const pt_tracer *t, SceneHost &sc, const EnvHost *env, uint32_t samples,
+                   TuneChoice &best) {
+  return autotune_scene(ctx, t, &sc, env, samples, best);
+}
 
 pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations) {
   if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) return ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations);
@@ -801,6 +909,45 @@ pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule) {
 pt_status pt_set_wave_slots(pt_context *ctx, uint32_t slots) {
   if (!ctx || slots == 0) return fail(ctx, PT_ERR_INVALID_ARG, "bad argument");
   ctx->wave_slots = slots;
+  return PT_OK;
+}
+
+namespace {
+pt_tune_choice to_c(const TuneChoice &c) {
+  pt_tune_choice o;
+  o.schedule = c.schedule;
+  o.node_width_extension = (c.wide_nodes & WIDE_EXTENSION) ? 4u : 2u;
+  o.node_width_shadow = (c.wide_nodes & WIDE_SHADOW) ? 4u : 2u;
+  o.material_sort = c.material_sort;
+  o.wave_slots = c.wave_slots;
+  o.samples_per_s = c.samples_per_s;
+  return o;
+}
+}  // namespace
+
+pt_status pt_autotune(pt_context *ctx, pt_tracer *t, uint32_t samples, pt_tune_choice *best) {
+  if (!ctx || !t || t->ctx != ctx) return fail(ctx, PT_ERR_INVALID_ARG, "bad context / tracer");
+  return guard(ctx, [&]() -> pt_status {
+    TuneChoice c{};
+    pt_status st = autotune_impl(ctx, t, samples, c);
+    if (st == PT_OK && best) *best = to_c(c);
+    return st;
+  });
+}
+
+pt_status pt_tune_lookup(pt_context *ctx, const pt_tracer *t, pt_tune_choice *out) {
+  if (!ctx || !t || !out) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  SceneHost *sc = find_scene(ctx, t->scene_id);
+  if (!sc) return fail(ctx, PT_ERR_NOT_FOUND, "tracer has no resident scene");
+  auto it = ctx->tuned.find(scene_class(*sc, t->env != nullptr));
+  if (it == ctx->tuned.end()) return fail(ctx, PT_ERR_NOT_FOUND, "scene class not tuned");
+  *out = to_c(it->second);
+  return PT_OK;
+}
+
+pt_status pt_tune_reset(pt_context *ctx) {
+  if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
+  ctx->tuned.clear();
   return PT_OK;
 }
 

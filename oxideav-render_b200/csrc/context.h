@@ -14,6 +14,14 @@
 #include "host_scene.h"
 #include "kernels.h"
 
+namespace ptd {
+// An autotuned configuration of one scene class (pt_autotune).
+struct TuneChoice {
+  uint32_t schedule, wide_nodes, material_sort, wave_slots;
+  float samples_per_s;
+};
+}  // namespace ptd
+
 struct pt_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -26,6 +34,7 @@ struct pt_context {
   // (default: both kinds).
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   bool material_sort = true;  // bucket each shade queue by material
+  std::map<uint32_t, ptd::TuneChoice> tuned;  // by scene class (ptd::scene_class)
   float4 *d_out = nullptr;
   size_t out_cap = 0;
   ptd::WaveSegment *d_segs = nullptr;
@@ -116,4 +125,12 @@ pt_status engine_create(int device, pt_context **out);
 float4 bg_linear(const pt_render_options &o);
 // PathTracer::sync's option checks (camera / enum / size limits).
 pt_status check_options(pt_context *ctx, const pt_camera *cam, const pt_render_options *o);
+// Autotuner key of a scene: triangle-count scale (factors of 4), emissive
+// triangles, environment map, punctual lights, textures.
+uint32_t scene_class(const SceneHost &sc, bool env);
+// Times the candidate configurations on a calibration refine of t's camera
+// and options over scene `sc` / environment `env` (own scratch accumulator)
+// and records the fastest for the scene's class.
+pt_status autotune(pt_context *ctx, const pt_tracer *t, SceneHost &sc, const EnvHost *env, uint32_t samples,
+                   TuneChoice &best);
 }  // namespace ptd

@@ -175,6 +175,9 @@ struct pt_server {
   pt_server_stats st{};
   uint64_t tick = 0;
   uint32_t accum_count = 0;
+  bool autotune = false;
+  bool tune_pending = false;  // a request waits for an idle stream to tune its class
+  uint64_t rays_base = 0;     // rays counted before the device counters were last cleared
 };
 
 namespace {
@@ -294,6 +297,28 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
     fail_admission(s, r, PT_ERR_OOM, err);
     return a;
   }
+  if (s->autotune && !s->eng->tuned.count(scene_class(*sc->dev, sc->env_dev != nullptr))) {
+    // A new scene class: tune on an idle stream (no wave launches until the
+    // ones in flight finish), then admit.
+    if (!s->inflight.empty()) {
+      s->tune_pending = true;
+      return Admit::Wait;
+    }
+    sc->pins++;
+    lk.unlock();
+    TuneChoice best{};
+    pt_status tst = autotune(s->eng, &acc.t, *sc->dev, sc->env_dev.get(), 1, best);
+    lk.lock();
+    sc->pins--;
+    // The calibration refines used the engine's counters: restart them.
+    s->rays_base = s->st.rays;
+    cudaMemsetAsync(s->eng->d_ctr, 0, sizeof(DevCounters), s->eng->stream);
+    if (tst != PT_OK) {
+      fail_admission(s, r, tst, "autotune: " + s->eng->err);
+      return Admit::Failed;
+    }
+    s->st.tuned_classes++;
+  }
   cudaStream_t stream = s->eng->stream;
   pt_tracer &t = acc.t;
   if (!t.d_accum) {
@@ -330,6 +355,7 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
 }
 
 void admit(pt_server *s, std::unique_lock<std::mutex> &lk) {
+  s->tune_pending = false;
   for (size_t i = 0; i < s->pending.size() && s->active.size() < s->max_active;) {
     std::shared_ptr<Request> r = s->pending[i];
     Admit a = try_admit(s, r, lk);
@@ -494,7 +520,7 @@ void complete_flight(pt_server *s, size_t fi, cudaError_t e) {
   s->st.gpu_ms += ms;
   s->st.waves++;
   s->st.samples += f.samples;
-  s->st.rays = f.h_ctr->ext_rays + f.h_ctr->shadow_rays;
+  s->st.rays = s->rays_base + f.h_ctr->ext_rays + f.h_ctr->shadow_rays;
   const bool overflow = (f.h_ctr->error_flags & ERR_STACK_OVERFLOW) != 0;
   Clock::time_point now = Clock::now();
   for (auto &r : f.finishing) {
@@ -529,7 +555,7 @@ void worker_main(pt_server *s) {
   for (;;) {
     free_dead(s);
     if (!s->stop && !s->broken) admit(s, lk);
-    if (!s->stop && !s->broken && !s->active.empty() && s->inflight.size() < s->depth) {
+    if (!s->stop && !s->broken && !s->tune_pending && !s->active.empty() && s->inflight.size() < s->depth) {
       launch_next_wave(s);
       continue;
     }
@@ -586,6 +612,8 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
     s->eng->wave_slots = s->wave_slots;
     s->eng->wide_nodes = (c.node_width_extension == 2 ? 0u : WIDE_EXTENSION) |
                          (c.node_width_shadow == 2 ? 0u : WIDE_SHADOW);
+    s->eng->material_sort = c.material_sort_off == 0;
+    s->autotune = c.autotune != 0;
     s->flights.resize(s->depth + 1);
     cudaError_t e = cudaSuccess;
     for (Flight &f : s->flights) {

@@ -25,7 +25,7 @@ def declared_functions():
 
 def test_struct_layout_matches_header():
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pt_b200.h"', '#include "pt_b200_serve.h"',
-             "int main(void) {"]
+             '#include "pt_b200_debug.h"', "int main(void) {"]
     for cls in abi.ABI_STRUCTS:
         n = cls.__name__
         lines.append(f'printf("{n} %zu\\n", sizeof({n}));')
