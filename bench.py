@@ -235,7 +235,7 @@ def run_served(ctx, api, torch, args):
     t0 = time.perf_counter()
     scenes = serving_scenes(args.serve_scenes, 2026)
     gen_s = time.perf_counter() - t0
-    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)))
+    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), autotune=args.autotune)
     t0 = time.perf_counter()
     keys = [srv.register(s, o, api.EnvironmentMap(e) if e is not None else None) for s, o, e in scenes]
     register_s = time.perf_counter() - t0
@@ -502,6 +502,13 @@ def run_b200(args):
     if env is not None:
         tracer.set_environment(api.EnvironmentMap(env))
     tracer.sync(scene, opts)
+    tuned = None
+    if args.autotune:
+        # pt_autotune: calibration refines on a scratch accumulator pick this
+        # scene class's configuration (images are identical under every one).
+        t0 = time.perf_counter()
+        tuned = ctx.autotune(tracer, 0)
+        tuned["seconds"] = time.perf_counter() - t0
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     for _ in range(args.warmup):
         tracer.refine(spp)
@@ -593,7 +600,8 @@ def run_b200(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wname, "samples_per_step": samples_per_step, "global_batch": samples_per_step * ws,
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "flushed (256 MB write) before every timed step", "schedule": args.schedule},
+                       "l2": "flushed (256 MB write) before every timed step", "schedule": args.schedule,
+                       "autotuned": tuned},
             "mrays_per_s": mrays, "rays_per_step": rays / args.steps, "wall_ms_per_step": statistics.mean(wall_ms),
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if v > 0},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -630,6 +638,8 @@ def main():
     ap.add_argument("--ref-spp", type=int, default=8)
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling cases)")
     ap.add_argument("--schedule", default="wavefront", choices=["megakernel", "wavefront"])
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default configuration instead of pt_autotune's per-class choice")
     ap.add_argument("--mixed", type=int, default=64, help="requests in the batched-vs-plain comparison (0: skip)")
     ap.add_argument("--serve-rates", default="5,20,200",
                     help="Poisson arrival rates (requests/s) of the served runs, comma-separated ('' : skip)")

@@ -58,7 +58,8 @@ typedef struct pt_tune_choice {
   float samples_per_s;           /* calibration throughput */
 } pt_tune_choice;
 /* Times every candidate (megakernel; wavefront x node widths x material sort
- * x wave size) on a calibration refine of `samples` spp of the tracer's
+ * x wave size) on a calibration refine of `samples` spp (0: one full wave of
+ * 4,194,304 paths, capped at 4096 spp) of the tracer's
  * scene, camera and options (a scratch accumulator: the tracer's own is
  * untouched) and records the fastest as the configuration of the scene's
  * class: later refines of tracers in that class use it. Every candidate

@@ -85,7 +85,7 @@ class Context:
     def _tune_dict(c: abi.pt_tune_choice) -> dict:
         return {name: getattr(c, name) for name, _ in abi.pt_tune_choice._fields_}
 
-    def autotune(self, tracer: "PathTracer", samples: int = 1) -> dict:
+    def autotune(self, tracer: "PathTracer", samples: int = 0) -> dict:
         """pt_autotune: the fastest configuration for the tracer's scene class
         (measured on a scratch accumulator); later refines of that class use it."""
         c = abi.pt_tune_choice()

@@ -396,7 +396,12 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
 // (device time, best of two runs) becomes the scene class's configuration.
 pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, const EnvHost *env, uint32_t samples,
                          TuneChoice &best) {
-  samples = std::max(samples, 1u);
+  if (samples == 0) {
+    // One full wave (4,194,304 paths): the size real refines run at, where
+    // per-launch costs weigh as they will in use.
+    const uint64_t npix = (uint64_t)std::max(t->w, 1u) * std::max(t->h, 1u);
+    samples = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((1ull << 22) / npix, 1), 4096);
+  }
   CK(ctx, cudaSetDevice(ctx->device));
   pt_tracer s;
   s.ctx = ctx;

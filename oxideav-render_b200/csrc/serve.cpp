@@ -307,7 +307,8 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
     sc->pins++;
     lk.unlock();
     TuneChoice best{};
-    pt_status tst = autotune(s->eng, &acc.t, *sc->dev, sc->env_dev.get(), 1, best);
+    // Calibrate on one full wave whatever the request's size.
+    pt_status tst = autotune(s->eng, &acc.t, *sc->dev, sc->env_dev.get(), 0, best);
     lk.lock();
     sc->pins--;
     // The calibration refines used the engine's counters: restart them.
