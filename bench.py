@@ -429,11 +429,8 @@ def dist_setup():
 def max_over_ranks(x: float, ws: int) -> float:
     if ws == 1:
         return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from oxideav_render_b200 import shard
+    return shard.max_over_ranks(x, device="cuda")
 
 
 def barrier(ws: int):
