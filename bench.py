@@ -514,7 +514,6 @@ def run_b200(args):
     ext = shadow = 0
     split = {"ext_nodes": 0, "ext_tris": 0, "sh_nodes": 0, "sh_tris": 0}
     stage = {k: 0.0 for k in api.PathTracer.STAGES}
-    ctx.set_stage_timing(True)
     with ClockSampler(local if ws > 1 else torch.cuda.current_device()) as clocks:
         for _ in range(args.steps):
             flush.zero_()
@@ -527,10 +526,17 @@ def run_b200(args):
             ext, shadow = ext + e, shadow + s
             for k, v in tracer.traversal_split().items():
                 split[k] += v
-            for k, v in tracer.stage_ms().items():
-                stage[k] += v
-    ctx.set_stage_timing(False)
     barrier(ws)
+    # Stage split: one more (untimed) frame with CUDA events between the
+    # stages. Events need direct launches; the timed frames replay each wave
+    # as one CUDA graph.
+    ctx.set_stage_timing(True)
+    flush.zero_()
+    torch.cuda.synchronize()
+    tracer.refine(spp)
+    stage = {k: v * args.steps for k, v in tracer.stage_ms().items()}
+    stage_frame_ms = tracer.last_kernel_ms()
+    ctx.set_stage_timing(False)
     dev_s = max_over_ranks(sum(kernel_ms) / 1000.0, ws)
     value = samples_per_step * args.steps * ws / dev_s
     ms_per_step = 1000 * dev_s / args.steps
@@ -601,6 +607,7 @@ def run_b200(args):
                        "autotuned": tuned},
             "mrays_per_s": mrays, "rays_per_step": rays / args.steps, "wall_ms_per_step": statistics.mean(wall_ms),
             "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if v > 0},
+            "stage_frame_ms": stage_frame_ms,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": kernel_names[dom],

@@ -45,6 +45,9 @@ PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n)
  * (three small kernels per bounce; on by default). Images are identical
  * either way. */
 PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
+/* Wavefront waves replayed from CUDA graphs (one capture per bounce count
+ * and sort setting; on by default, bypassed while stage timing is on). */
+PT_API pt_status pt_set_wave_graphs(pt_context *ctx, int on);
 
 /* ---- autotuner: one configuration per scene class ----
  * A scene class groups scenes by triangle-count scale (factors of 4),

@@ -103,6 +103,9 @@ class Context:
     def tune_reset(self) -> None:
         self.check(self.lib.pt_tune_reset(self.ptr))
 
+    def set_wave_graphs(self, on: bool) -> None:
+        self.check(self.lib.pt_set_wave_graphs(self.ptr, 1 if on else 0))
+
     def set_material_sort(self, on: bool) -> None:
         self.check(self.lib.pt_set_material_sort(self.ptr, 1 if on else 0))
 

@@ -198,6 +198,9 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
     ctx->wf_arena = nullptr;
     ctx->wf_bytes = 0;
   }
+  // Captured waves point into the old arena.
+  for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
   capacity = std::max(capacity, w.capacity);
   shadow_slots = std::max(shadow_slots, w.shadow_slots);
   iterations = std::max(iterations, w.iterations);
@@ -207,7 +210,8 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
                     16 * P * S, 16 * P * S, 16 * P * S, 4 * P,               // sh_o sh_d sh_c sh_n
                     4 * P, 4 * P, 4 * P,                                     // q0 q1 q_shadow
                     4 * (size_t)kWfCounterStride * (iterations + 1),
-                    4 * P, 4 * 2 * (size_t)kSortBuckets * (iterations + 1)};  // q_sorted sort_counts
+                    4 * P, 4 * 2 * (size_t)kSortBuckets * (iterations + 1),   // q_sorted sort_counts
+                    sizeof(WaveDesc)};
   size_t off[sizeof(sizes) / sizeof(sizes[0])], total = 0;
   for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); ++i) {
     total = (total + 255) & ~(size_t)255;
@@ -237,6 +241,7 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   w.counters = (uint32_t *)(b + off[k++]);
   w.q_sorted = (uint32_t *)(b + off[k++]);
   w.sort_counts = (uint32_t *)(b + off[k++]);
+  w.desc = (WaveDesc *)(b + off[k++]);
   w.capacity = capacity;
   w.shadow_slots = shadow_slots;
   w.iterations = iterations;
@@ -592,12 +597,29 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
     max_pix = std::max(max_pix, s.pixel_count);
   }
   if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
+    if (total == 0) return PT_OK;
     WaveBuffers w = ctx->wf;
     w.iterations = iters;
     w.sort_materials = ctx->material_sort ? 1u : 0u;
-    CK(ctx, launch_wavefront(d_reqs, d_segs, nseg, total, w, ctx->d_ctr, ctx->num_sms, ctx->stream, timer));
-    if (timer) timer->mark(STAGE_ACCUMULATE, ctx->stream);
-    CK(ctx, launch_accumulate(d_reqs, d_segs, nseg, max_pix, w.rad, ctx->stream));
+    // Pageable source: the copy is staged before the call returns and lands
+    // in stream order, after the previous wave has read its descriptor.
+    WaveDesc wd{d_reqs, d_segs, nseg, total, max_pix, 0};
+    CK(ctx, cudaMemcpyAsync(w.desc, &wd, sizeof wd, cudaMemcpyHostToDevice, ctx->stream));
+    const bool timed = timer && timer->events;
+    if (ctx->use_graphs && !timed) {
+      // One captured graph per (bounce count, material sort) replays the
+      // whole wave: one launch instead of ~6 per bounce.
+      const uint32_t key = iters << 1 | w.sort_materials;
+      auto it = ctx->graphs.find(key);
+      if (it == ctx->graphs.end()) {
+        cudaGraphExec_t ge = nullptr;
+        CK(ctx, capture_wavefront(w, ctx->d_ctr, ctx->num_sms, &ge));
+        it = ctx->graphs.emplace(key, ge).first;
+      }
+      CK(ctx, cudaGraphLaunch(it->second, ctx->stream));
+    } else {
+      CK(ctx, launch_wavefront(w, ctx->d_ctr, ctx->num_sms, ctx->stream, timer));
+    }
   } else {
     if (timer) timer->mark(STAGE_MEGAKERNEL, ctx->stream);
     CK(ctx, launch_megakernel(d_reqs, d_segs, nseg, total, ctx->d_out, ctx->d_ctr, ctx->stream));
@@ -652,6 +674,8 @@ void pt_destroy(pt_context *ctx) {
   for (auto &kv : ctx->scenes) release_scene(*kv.second);
   ctx->scenes.clear();
   if (ctx->d_out) cudaFree(ctx->d_out);
+  for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+  ctx->graphs.clear();
   if (ctx->wf_arena) cudaFree(ctx->wf_arena);
   if (ctx->d_segs) cudaFree(ctx->d_segs);
   if (ctx->d_reqs) cudaFree(ctx->d_reqs);
@@ -953,6 +977,12 @@ pt_status pt_tune_lookup(pt_context *ctx, const pt_tracer *t, pt_tune_choice *ou
 pt_status pt_tune_reset(pt_context *ctx) {
   if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
   ctx->tuned.clear();
+  return PT_OK;
+}
+
+pt_status pt_set_wave_graphs(pt_context *ctx, int on) {
+  if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
+  ctx->use_graphs = on != 0;
   return PT_OK;
 }
 

@@ -35,6 +35,9 @@ struct pt_context {
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   bool material_sort = true;  // bucket each shade queue by material
   std::map<uint32_t, ptd::TuneChoice> tuned;  // by scene class (ptd::scene_class)
+  // Wavefront waves replayed as CUDA graphs (bounce count << 1 | sort -> exec).
+  bool use_graphs = true;
+  std::map<uint32_t, cudaGraphExec_t> graphs;
   float4 *d_out = nullptr;
   size_t out_cap = 0;
   ptd::WaveSegment *d_segs = nullptr;

@@ -149,7 +149,17 @@ struct WaveBuffers {
   uint32_t *counters;          // [iterations][kWfCounterStride]
   uint32_t *q_sorted;          // the active queue bucketed by material (material sort on)
   uint32_t *sort_counts;       // [iterations][2][kSortBuckets]: bucket sizes, then cursors
+  struct WaveDesc *desc;       // this wave's requests and segments (written before each wave)
   uint32_t capacity, shadow_slots, iterations, sort_materials;
+};
+
+// What changes from one wave to the next, read by the kernels from device
+// memory, so a wave's launch sequence is the same for every wave of the same
+// bounce count (and can be replayed as one CUDA graph).
+struct WaveDesc {
+  const DevRequest *reqs;
+  const WaveSegment *segs;
+  uint32_t nseg, total, max_pix, pad;
 };
 constexpr uint32_t kSortBuckets = 256;
 

@@ -298,45 +298,69 @@ cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, u
 }
 // One wave of the wavefront schedule: raygen, then `w.iterations` rounds of
 // extend / shade / shadow over device-side queue counters (no host sync).
-cudaError_t launch_wavefront(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
-                             const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
+// The traversal kernels are persistent: exactly the blocks that fit at once
+// (occupancy queried once, outside any stream capture).
+void persistent_blocks(int &per_sm_ext, int &per_sm_sh) {
+  static int ext = 0, sh = 0;
+  if (ext == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext, k_wf_extend, 256, 0) != cudaSuccess || ext < 1) ext = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh, k_wf_shadow, 256, 0) != cudaSuccess || sh < 1) sh = 1;
+  }
+  per_sm_ext = ext;
+  per_sm_sh = sh;
+}
+
+cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
                              StageTimer *timer) {
-  if (total == 0) return cudaSuccess;
   StageTimer none;
   StageTimer &tm = timer ? *timer : none;
   cudaError_t e = cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * kWfCounterStride * (w.iterations + 1), st);
   if (e == cudaSuccess && w.sort_materials)
     e = cudaMemsetAsync(w.sort_counts, 0, sizeof(uint32_t) * 2 * kSortBuckets * (w.iterations + 1), st);
   if (e != cudaSuccess) return e;
-  tm.mark(STAGE_RAYGEN, st);
-  k_wf_raygen<<<(total + 255) / 256, 256, 0, st>>>(reqs, segs, nseg, total, w);
-  // The traversal kernels are persistent: exactly the blocks that fit at once.
-  static int per_sm_ext = 0, per_sm_sh = 0;
-  if (per_sm_ext == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ext, k_wf_extend, 256, 0) != cudaSuccess ||
-        per_sm_ext < 1)
-      per_sm_ext = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_sh, k_wf_shadow, 256, 0) != cudaSuccess ||
-        per_sm_sh < 1)
-      per_sm_sh = 1;
-  }
+  int per_sm_ext, per_sm_sh;
+  persistent_blocks(per_sm_ext, per_sm_sh);
   const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext), g_shade = (uint32_t)num_sms * 6,
-                 g_sh = (uint32_t)(num_sms * per_sm_sh);
+                 g_sh = (uint32_t)(num_sms * per_sm_sh), g_wide = (uint32_t)num_sms * 16;
+  tm.mark(STAGE_RAYGEN, st);
+  k_wf_raygen<<<g_wide, 256, 0, st>>>(w);
   for (uint32_t it = 0; it < w.iterations; ++it) {
     tm.mark(STAGE_EXTEND, st);
-    k_wf_extend<<<g_ext, 256, 0, st>>>(reqs, w, it, ctr);
+    k_wf_extend<<<g_ext, 256, 0, st>>>(w, it, ctr);
     if (w.sort_materials) {
       tm.mark(STAGE_SORT, st);
-      k_wf_sort_count<<<g_shade, 256, 0, st>>>(reqs, w, it);
+      k_wf_sort_count<<<g_shade, 256, 0, st>>>(w, it);
       k_wf_sort_scan<<<1, kSortBuckets, 0, st>>>(w, it);
-      k_wf_sort_scatter<<<g_shade, 256, 0, st>>>(reqs, w, it);
+      k_wf_sort_scatter<<<g_shade, 256, 0, st>>>(w, it);
     }
     tm.mark(STAGE_SHADE, st);
-    k_wf_shade<<<g_shade, 128, 0, st>>>(reqs, w, it);
+    k_wf_shade<<<g_shade, 128, 0, st>>>(w, it);
     tm.mark(STAGE_SHADOW, st);
-    k_wf_shadow<<<g_sh, 256, 0, st>>>(reqs, w, it, ctr);
+    k_wf_shadow<<<g_sh, 256, 0, st>>>(w, it, ctr);
   }
+  tm.mark(STAGE_ACCUMULATE, st);
+  k_wf_accumulate<<<g_wide, 256, 0, st>>>(w);
   return LAUNCH_CHECK();
+}
+
+cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out) {
+  *out = nullptr;
+  int a, b;
+  persistent_blocks(a, b);
+  cudaStream_t cs = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
+  cudaGraph_t g = nullptr;
+  e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    cudaError_t le = launch_wavefront(w, ctr, num_sms, cs, nullptr);
+    e = cudaStreamEndCapture(cs, &g);
+    if (e == cudaSuccess) e = le;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  return e;
 }
 
 cudaError_t launch_accumulate(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t max_pixels,

@@ -86,35 +86,66 @@ struct DeferredSink {
   }
 };
 
-__global__ void __launch_bounds__(256) k_wf_raygen(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg,
-                                                   uint32_t total, WaveBuffers w) {
-  uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot == 0) w.counters[0] = total;
-  if (slot >= total) return;
-  uint32_t lo = 0, hi = nseg;
-  while (hi - lo > 1) {
-    uint32_t mid = (lo + hi) >> 1;
-    if (segs[mid].slot_begin <= slot)
-      lo = mid;
-    else
-      hi = mid;
+// Camera rays for every slot of the wave (grid-stride over the wave's
+// slots, read from the wave descriptor).
+__global__ void __launch_bounds__(256) k_wf_raygen(WaveBuffers w) {
+  const WaveDesc wd = *w.desc;
+  if (blockIdx.x == 0 && threadIdx.x == 0) w.counters[0] = wd.total;
+  for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < wd.total; slot += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = wd.nseg;
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (wd.segs[mid].slot_begin <= slot)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const WaveSegment &seg = wd.segs[lo];
+    const DevRequest &rq = wd.reqs[seg.request];
+    uint32_t local = slot - seg.slot_begin;
+    uint32_t sidx = local / seg.pixel_count, i = local - sidx * seg.pixel_count;
+    uint32_t p = seg.pixel_begin + i;
+    uint32_t y = p / rq.width, x = p - y * rq.width;
+    PathState ps;
+    init_path(rq, x, y, seg.sample_begin + sidx, ps);
+    wf_store(w, slot, ps, seg.request);
+    w.q[0][slot] = slot;
   }
-  const WaveSegment &seg = segs[lo];
-  const DevRequest &rq = reqs[seg.request];
-  uint32_t local = slot - seg.slot_begin;
-  uint32_t s = local / seg.pixel_count, i = local - s * seg.pixel_count;
-  uint32_t p = seg.pixel_begin + i;
-  uint32_t y = p / rq.width, x = p - y * rq.width;
-  PathState ps;
-  init_path(rq, x, y, seg.sample_begin + s, ps);
-  wf_store(w, slot, ps, seg.request);
-  w.q[0][slot] = slot;
+}
+
+// In-order f64 accumulation of the wave's per-slot results into each
+// request's accumulator (a pixel's samples in index order, as the
+// reference's per-pixel loop adds them).
+__global__ void __launch_bounds__(256) k_wf_accumulate(WaveBuffers w) {
+  const WaveDesc wd = *w.desc;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t sg = 0; sg < wd.nseg; ++sg) {
+    const WaveSegment seg = wd.segs[sg];
+    double4 *accum = reinterpret_cast<double4 *>(wd.reqs[seg.request].accum) + seg.pixel_begin;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < seg.pixel_count; i += stride) {
+      double4 a = accum[i];
+      const float4 *src = w.rad + seg.slot_begin + i;
+      for (uint32_t k = 0; k < seg.spp; ++k) {
+        float4 v = src[(size_t)k * seg.pixel_count];
+        if (v.w > 0.0f) {
+          // Non-finite radiance counts as a covered black sample (src/pathtrace.rs:2324-2328).
+          if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) v = make_float4(0.0f, 0.0f, 0.0f, v.w);
+          a.x += (double)v.x;
+          a.y += (double)v.y;
+          a.z += (double)v.z;
+          a.w += 1.0;
+        }
+      }
+      accum[i] = a;
+    }
+  }
 }
 
 // Closest hit of every queued path: persistent lanes, one ray each, refilled
 // from the queue as rays finish (dev_traverse.cuh).
-__global__ void __launch_bounds__(256, 4) k_wf_extend(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+__global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t iter,
                                                    DevCounters *ctr) {
+  const DevRequest *reqs = w.desc->reqs;
   __shared__ int s_stack[kShortStack * 256];
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
@@ -180,7 +211,8 @@ PT_DEV uint32_t sort_key(const DevRequest *reqs, const WaveBuffers &w, uint32_t 
   return 1u + (m + sh) % (kSortBuckets - 1u);
 }
 
-__global__ void __launch_bounds__(256) k_wf_sort_count(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+__global__ void __launch_bounds__(256) k_wf_sort_count(WaveBuffers w, uint32_t iter) {
+  const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
   uint32_t *count = w.sort_counts + (size_t)iter * 2 * kSortBuckets;
@@ -208,7 +240,8 @@ __global__ void __launch_bounds__(kSortBuckets) k_wf_sort_scan(WaveBuffers w, ui
   count[kSortBuckets + t] = s[t] - own;
 }
 
-__global__ void __launch_bounds__(256) k_wf_sort_scatter(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+__global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t iter) {
+  const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
   uint32_t *cursor = w.sort_counts + (size_t)iter * 2 * kSortBuckets + kSortBuckets;
@@ -227,7 +260,8 @@ __global__ void __launch_bounds__(256) k_wf_sort_scatter(const DevRequest *reqs,
 
 // Three 128-thread blocks per SM (168 registers): measured faster than the
 // unconstrained 234-register build despite a few spills.
-__global__ void __launch_bounds__(128, 3) k_wf_shade(const DevRequest *reqs, WaveBuffers w, uint32_t iter) {
+__global__ void __launch_bounds__(128, 3) k_wf_shade(WaveBuffers w, uint32_t iter) {
+  const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.sort_materials ? w.q_sorted : w.q[iter & 1u];
   uint32_t *q_next = w.q[(iter + 1) & 1u];
@@ -263,8 +297,9 @@ __global__ void __launch_bounds__(128, 3) k_wf_shade(const DevRequest *reqs, Wav
 // (a visible ray adds its contribution to the path radiance, so the float
 // sum rounds as in the megakernel). Persistent lanes own one path at a time
 // and are refilled from the queue when its last ray finishes.
-__global__ void __launch_bounds__(256, 4) k_wf_shadow(const DevRequest *reqs, WaveBuffers w, uint32_t iter,
+__global__ void __launch_bounds__(256, 4) k_wf_shadow(WaveBuffers w, uint32_t iter,
                                                    DevCounters *ctr) {
+  const DevRequest *reqs = w.desc->reqs;
   __shared__ int s_stack[kShortStack * 256];
   const uint32_t n = w.counters[iter * kWfCounterStride + 1];
   uint32_t *claim = w.counters + iter * kWfCounterStride + 3;
