@@ -49,6 +49,12 @@ PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
  * and sort setting; on by default, bypassed while stage timing is on). */
 PT_API pt_status pt_set_wave_graphs(pt_context *ctx, int on);
 
+/* Builds a scene's device image on the host only (validation, textures,
+ * BVH, tables; no GPU needed) and reports its host time in seconds:
+ * {total, tables before the BVH, BVH build, tables after it + the image},
+ * and the device bytes the scene would occupy. */
+PT_API pt_status pt_debug_prepare_scene(const pt_scene_desc *desc, double seconds[4], uint64_t *device_bytes);
+
 /* ---- autotuner: one configuration per scene class ----
  * A scene class groups scenes by triangle-count scale (factors of 4),
  * emissive triangles, environment map, punctual lights and textures. */

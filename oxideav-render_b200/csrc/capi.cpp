@@ -954,6 +954,18 @@ pt_tune_choice to_c(const TuneChoice &c) {
 }
 }  // namespace
 
+pt_status pt_debug_prepare_scene(const pt_scene_desc *desc, double seconds[4], uint64_t *device_bytes) {
+  if (!desc || !seconds) return fail(nullptr, PT_ERR_INVALID_ARG, "desc / seconds is NULL");
+  return guard(nullptr, [&]() -> pt_status {
+    SceneImage img;
+    std::string err = build_scene_image(*desc, img);
+    if (!err.empty()) return fail(nullptr, PT_ERR_INVALID_ARG, err);
+    for (int k = 0; k < 4; ++k) seconds[k] = img.seconds[k];
+    if (device_bytes) *device_bytes = img.blob.size();
+    return PT_OK;
+  });
+}
+
 pt_status pt_autotune(pt_context *ctx, pt_tracer *t, uint32_t samples, pt_tune_choice *best) {
   if (!ctx || !t || t->ctx != ctx) return fail(ctx, PT_ERR_INVALID_ARG, "bad context / tracer");
   return guard(ctx, [&]() -> pt_status {

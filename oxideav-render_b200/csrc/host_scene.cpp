@@ -14,6 +14,7 @@
 #include "host_scene.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -84,9 +85,13 @@ struct BNode {
 struct Builder {
   const float *pos;
   uint32_t n;
-  std::vector<float> cen;    // 3 per tri
-  std::vector<float> blo, bhi;
-  std::vector<uint32_t> idx;
+  // Per-triangle bounds in build order: a node's triangles are one
+  // contiguous run, partitioned in place as the tree splits.
+  struct Prim {
+    float lo[3], hi[3], c[3];
+    uint32_t g;
+  };
+  std::vector<Prim> prims;
   std::vector<BNode> nodes;
   std::atomic<uint32_t> node_count{1};
   std::atomic<uint32_t> max_depth{0};
@@ -103,6 +108,8 @@ struct Builder {
   static constexpr int kBins = 16;
   static constexpr uint32_t kMaxLeaf = 8;
   static constexpr uint32_t kLocalThreshold = 32768;
+  static constexpr uint32_t kParallelNode = 65536;
+  int wide = 1;  // threads for one large node's passes
 
   static float area(const float lo[3], const float hi[3]) {
     float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
@@ -116,20 +123,102 @@ struct Builder {
     nd.left = 0;
   }
 
-  // Processes one node; returns the child tasks (0 or 2).
+  // Bin counts and bounds of a run of triangles, per axis (one pass over
+  // the run for all three axes). Merging per-chunk bins gives exactly the
+  // sequential result: sums of counts, min / max of the same values.
+  struct Bins {
+    uint32_t c[3][kBins];
+    float l[3][kBins][3], h[3][kBins][3];
+    void clear() {
+      for (int k = 0; k < 3; ++k)
+        for (int b = 0; b < kBins; ++b) {
+          c[k][b] = 0;
+          for (int a = 0; a < 3; ++a) {
+            l[k][b][a] = INFINITY;
+            h[k][b][a] = -INFINITY;
+          }
+        }
+    }
+    void merge(const Bins &o) {
+      for (int k = 0; k < 3; ++k)
+        for (int b = 0; b < kBins; ++b) {
+          c[k][b] += o.c[k][b];
+          for (int a = 0; a < 3; ++a) {
+            l[k][b][a] = std::min(l[k][b][a], o.l[k][b][a]);
+            h[k][b][a] = std::max(h[k][b][a], o.h[k][b][a]);
+          }
+        }
+    }
+  };
+  void bin_range(Bins &B, uint32_t begin, uint32_t end, const float clo[3], const float scale[3],
+                 const bool use[3]) const {
+    for (uint32_t i = begin; i < end; ++i) {
+      const Prim &pr = prims[i];
+      for (int k = 0; k < 3; ++k) {
+        if (!use[k]) continue;
+        int b = std::min(kBins - 1, (int)((pr.c[k] - clo[k]) * scale[k]));
+        B.c[k][b]++;
+        for (int a = 0; a < 3; ++a) {
+          B.l[k][b][a] = std::min(B.l[k][b][a], pr.lo[a]);
+          B.h[k][b][a] = std::max(B.h[k][b][a], pr.hi[a]);
+        }
+      }
+    }
+  }
+  void bounds_range(uint32_t begin, uint32_t end, float lo[3], float hi[3], float clo[3], float chi[3]) const {
+    for (uint32_t i = begin; i < end; ++i) {
+      const Prim &pr = prims[i];
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], pr.lo[k]);
+        hi[k] = std::max(hi[k], pr.hi[k]);
+        clo[k] = std::min(clo[k], pr.c[k]);
+        chi[k] = std::max(chi[k], pr.c[k]);
+      }
+    }
+  }
+  // Runs fn(chunk, begin, end) over `chunks` slices of [begin, end) on threads.
+  template <class F>
+  static void parallel_chunks(uint32_t begin, uint32_t end, int chunks, F &&fn) {
+    std::vector<std::thread> th;
+    const uint32_t n = end - begin;
+    for (int c = 0; c < chunks; ++c) {
+      uint32_t b = begin + (uint32_t)((uint64_t)n * c / chunks), e = begin + (uint32_t)((uint64_t)n * (c + 1) / chunks);
+      th.emplace_back([&fn, c, b, e] { fn(c, b, e); });
+    }
+    for (auto &x : th) x.join();
+  }
+
+  // Processes one node; returns the child tasks (0 or 2). Nodes of at least
+  // kParallelNode triangles (the top of the tree, before the task pool has
+  // enough subtrees) spread their passes over `wide` threads.
   int split(const Task &t, Task out[2]) {
     BNode &nd = nodes[t.node];
     uint32_t cnt = t.end - t.begin;
+    const int par = cnt >= kParallelNode ? wide : 1;
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t i = t.begin; i < t.end; ++i) {
-      uint32_t g = idx[i];
-      for (int k = 0; k < 3; ++k) {
-        lo[k] = std::min(lo[k], blo[3 * g + k]);
-        hi[k] = std::max(hi[k], bhi[3 * g + k]);
-        clo[k] = std::min(clo[k], cen[3 * g + k]);
-        chi[k] = std::max(chi[k], cen[3 * g + k]);
-      }
+    if (par > 1) {
+      std::vector<std::array<float, 12>> part(par);
+      parallel_chunks(t.begin, t.end, par, [&](int c, uint32_t b, uint32_t e) {
+        float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+        float cl[3] = {INFINITY, INFINITY, INFINITY}, ch[3] = {-INFINITY, -INFINITY, -INFINITY};
+        bounds_range(b, e, l, h, cl, ch);
+        for (int k = 0; k < 3; ++k) {
+          part[c][k] = l[k];
+          part[c][3 + k] = h[k];
+          part[c][6 + k] = cl[k];
+          part[c][9 + k] = ch[k];
+        }
+      });
+      for (int c = 0; c < par; ++c)
+        for (int k = 0; k < 3; ++k) {
+          lo[k] = std::min(lo[k], part[c][k]);
+          hi[k] = std::max(hi[k], part[c][3 + k]);
+          clo[k] = std::min(clo[k], part[c][6 + k]);
+          chi[k] = std::max(chi[k], part[c][9 + k]);
+        }
+    } else {
+      bounds_range(t.begin, t.end, lo, hi, clo, chi);
     }
     for (int k = 0; k < 3; ++k) {
       nd.lo[k] = lo[k];
@@ -151,28 +240,30 @@ struct Builder {
     uint32_t mid = 0;
     int best_bin = 0;
     float best_cost = INFINITY;
+    float scale[3] = {0.0f, 0.0f, 0.0f};
     if (!median) {
       float parent = area(lo, hi);
+      bool use[3];
       for (int k = 0; k < 3; ++k) {
         float span = chi[k] - clo[k];
-        if (!(span > 0.0f)) continue;
-        float scale = (float)kBins / span;
-        uint32_t bc[kBins] = {0};
-        float bl[kBins][3], bh[kBins][3];
-        for (int b = 0; b < kBins; ++b)
-          for (int a = 0; a < 3; ++a) {
-            bl[b][a] = INFINITY;
-            bh[b][a] = -INFINITY;
-          }
-        for (uint32_t i = t.begin; i < t.end; ++i) {
-          uint32_t g = idx[i];
-          int b = std::min(kBins - 1, (int)((cen[3 * g + k] - clo[k]) * scale));
-          bc[b]++;
-          for (int a = 0; a < 3; ++a) {
-            bl[b][a] = std::min(bl[b][a], blo[3 * g + a]);
-            bh[b][a] = std::max(bh[b][a], bhi[3 * g + a]);
-          }
-        }
+        use[k] = span > 0.0f;
+        scale[k] = use[k] ? (float)kBins / span : 0.0f;
+      }
+      Bins B;
+      B.clear();
+      if (par > 1) {
+        std::vector<Bins> part(par);
+        parallel_chunks(t.begin, t.end, par, [&](int c, uint32_t b, uint32_t e) {
+          part[c].clear();
+          bin_range(part[c], b, e, clo, scale, use);
+        });
+        for (int c = 0; c < par; ++c) B.merge(part[c]);
+      } else {
+        bin_range(B, t.begin, t.end, clo, scale, use);
+      }
+      for (int k = 0; k < 3; ++k) {
+        if (!use[k]) continue;
+        const uint32_t *bc = B.c[k];
         float rl[kBins][3], rh[kBins][3];
         uint32_t rc[kBins];
         float accl[3] = {INFINITY, INFINITY, INFINITY}, acch[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -180,8 +271,8 @@ struct Builder {
         for (int b = kBins - 1; b >= 1; --b) {
           acc += bc[b];
           for (int a = 0; a < 3; ++a) {
-            accl[a] = std::min(accl[a], bl[b][a]);
-            acch[a] = std::max(acch[a], bh[b][a]);
+            accl[a] = std::min(accl[a], B.l[k][b][a]);
+            acch[a] = std::max(acch[a], B.h[k][b][a]);
           }
           rc[b] = acc;
           for (int a = 0; a < 3; ++a) {
@@ -194,8 +285,8 @@ struct Builder {
         for (int s = 1; s < kBins; ++s) {
           lc += bc[s - 1];
           for (int a = 0; a < 3; ++a) {
-            ll[a] = std::min(ll[a], bl[s - 1][a]);
-            lh[a] = std::max(lh[a], bh[s - 1][a]);
+            ll[a] = std::min(ll[a], B.l[k][s - 1][a]);
+            lh[a] = std::max(lh[a], B.h[k][s - 1][a]);
           }
           if (lc == 0 || rc[s] == 0) continue;
           float cost = 1.0f + (area(ll, lh) * (float)lc + area(rl[s], rh[s]) * (float)rc[s]) / std::max(parent, 1e-30f);
@@ -212,12 +303,41 @@ struct Builder {
       }
     }
     if (axis >= 0) {
-      float span = chi[axis] - clo[axis];
-      float scale = (float)kBins / span;
-      auto it = std::partition(idx.begin() + t.begin, idx.begin() + t.end, [&](uint32_t g) {
-        return std::min(kBins - 1, (int)((cen[3 * g + axis] - clo[axis]) * scale)) < best_bin;
-      });
-      mid = (uint32_t)(it - idx.begin());
+      const float sc = scale[axis], base = clo[axis];
+      auto left = [&](const Prim &pr) { return std::min(kBins - 1, (int)((pr.c[axis] - base) * sc)) < best_bin; };
+      if (par > 1) {
+        // Two passes: count each chunk's left side, then scatter every chunk
+        // into its place (stable within chunks) and copy back.
+        std::vector<uint32_t> nl(par, 0);
+        parallel_chunks(t.begin, t.end, par, [&](int c, uint32_t b, uint32_t e) {
+          uint32_t k = 0;
+          for (uint32_t i = b; i < e; ++i) k += left(prims[i]) ? 1u : 0u;
+          nl[c] = k;
+        });
+        std::vector<uint32_t> lofs(par), rofs(par);
+        uint32_t total_left = 0;
+        for (int c = 0; c < par; ++c) total_left += nl[c];
+        uint32_t lacc = 0, racc = total_left;
+        for (int c = 0; c < par; ++c) {
+          uint32_t b = t.begin + (uint32_t)((uint64_t)cnt * c / par), e = t.begin + (uint32_t)((uint64_t)cnt * (c + 1) / par);
+          lofs[c] = lacc;
+          rofs[c] = racc;
+          lacc += nl[c];
+          racc += (e - b) - nl[c];
+        }
+        std::vector<Prim> tmp(cnt);
+        parallel_chunks(t.begin, t.end, par, [&](int c, uint32_t b, uint32_t e) {
+          uint32_t li = lofs[c], ri = rofs[c];
+          for (uint32_t i = b; i < e; ++i) tmp[left(prims[i]) ? li++ : ri++] = prims[i];
+        });
+        parallel_chunks(0, cnt, par, [&](int, uint32_t b, uint32_t e) {
+          std::copy(tmp.begin() + b, tmp.begin() + e, prims.begin() + t.begin + b);
+        });
+        mid = t.begin + total_left;
+      } else {
+        auto it = std::partition(prims.begin() + t.begin, prims.begin() + t.end, left);
+        mid = (uint32_t)(it - prims.begin());
+      }
     }
     if (axis < 0 || mid == t.begin || mid == t.end) {
       // Object median along the widest centroid axis (or index halves when
@@ -231,8 +351,8 @@ struct Builder {
         }
       mid = t.begin + cnt / 2;
       if (w > 0.0f)
-        std::nth_element(idx.begin() + t.begin, idx.begin() + mid, idx.begin() + t.end,
-                         [&](uint32_t a, uint32_t b) { return cen[3 * a + ax] < cen[3 * b + ax]; });
+        std::nth_element(prims.begin() + t.begin, prims.begin() + mid, prims.begin() + t.end,
+                         [&](const Prim &a, const Prim &b) { return a.c[ax] < b.c[ax]; });
     }
     uint32_t c = node_count.fetch_add(2);
     nd.left = c;
@@ -326,20 +446,19 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   Builder b;
   b.pos = pos;
   b.n = tri_count;
-  b.cen.resize(3 * (size_t)tri_count);
-  b.blo.resize(3 * (size_t)tri_count);
-  b.bhi.resize(3 * (size_t)tri_count);
-  b.idx.resize(tri_count);
-  std::iota(b.idx.begin(), b.idx.end(), 0u);
+  b.prims.resize(tri_count);
   for (size_t g = 0; g < tri_count; ++g) {
     const float *p = pos + 9 * g;
+    Builder::Prim &pr = b.prims[g];
+    pr.g = (uint32_t)g;
     for (int k = 0; k < 3; ++k) {
       float lo = std::min({p[k], p[3 + k], p[6 + k]}), hi = std::max({p[k], p[3 + k], p[6 + k]});
-      b.blo[3 * g + k] = lo;
-      b.bhi[3 * g + k] = hi;
-      b.cen[3 * g + k] = (lo + hi) * 0.5f;
+      pr.lo[k] = lo;
+      pr.hi[k] = hi;
+      pr.c[k] = (lo + hi) * 0.5f;
     }
   }
+  b.wide = std::max(1, threads);
   b.run(std::max(1, threads));
 
   // Depth-first two-child layout.
@@ -467,7 +586,7 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   }
   records.resize(3 * (size_t)tri_count);
   for (size_t i = 0; i < tri_count; ++i) {
-    uint32_t g = b.idx[i];
+    uint32_t g = b.prims[i].g;
     const float *p = pos + 9 * (size_t)g;
     float gid, fl;
     std::memcpy(&gid, &g, 4);
@@ -602,6 +721,9 @@ void build_mips(const pt_texture &img, bool srgb, MipChain &out) {
 
 // ============================================================ scene upload
 std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
+  using clk = std::chrono::steady_clock;
+  const auto t_start = clk::now();
+  auto since = [](clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); };
   if (desc.item_count && !desc.items) return "pt_scene_desc.items is NULL";
   if (desc.material_count == 0 || !desc.materials) return "pt_scene_desc needs at least one material";
   if (desc.texture_count && !desc.textures) return "pt_scene_desc.textures is NULL";
@@ -725,7 +847,11 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   std::vector<Bvh4Node> nodes4;
   std::vector<float4> records;
   int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  img.seconds[1] = since(t_start);
+  const auto t_bvh = clk::now();
   build_bvh(pos.data(), tc, rec_flags.data(), nodes, nodes4, records, img.bvh, threads);
+  img.seconds[2] = since(t_bvh);
+  const auto t_after = clk::now();
 
   // Lights.
   std::vector<DevLight> lights(desc.light_count);
@@ -804,9 +930,47 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   size_t p_lookup = plan.add(em_lookup.data(), em_lookup.size() * 4);
   DevScene tmp{};
   size_t p_desc = plan.add(&tmp, sizeof(DevScene));
-  img.blob.assign(std::max<size_t>(plan.total, 256), 0);
-  for (size_t i = 0; i < plan.parts.size(); ++i)
-    if (plan.parts[i].second) std::memcpy(img.blob.data() + plan.offsets[i], plan.parts[i].first, plan.parts[i].second);
+  {
+    // Each part lands at its offset; the gaps (alignment padding, the
+    // descriptor slot and the tail) are zeroed. Copies run on several
+    // threads in slices of at most 16 MiB (first touch of the pages included).
+    const size_t total = std::max<size_t>(plan.total, 256);
+    img.blob.allocate(total);
+    uint8_t *dst = img.blob.data();
+    struct Piece {
+      size_t off, bytes;
+      const uint8_t *src;  // nullptr: zero fill
+    };
+    std::vector<Piece> pieces;
+    const size_t kSlice = size_t(16) << 20;
+    auto add = [&](size_t off, size_t bytes, const uint8_t *src) {
+      for (size_t o = 0; o < bytes; o += kSlice)
+        pieces.push_back({off + o, std::min(kSlice, bytes - o), src ? src + o : nullptr});
+    };
+    size_t cursor = 0;
+    for (size_t i = 0; i < plan.parts.size(); ++i) {
+      const size_t off = plan.offsets[i], bytes = plan.parts[i].second;
+      if (off > cursor) add(cursor, off - cursor, nullptr);
+      if (bytes) add(off, bytes, static_cast<const uint8_t *>(plan.parts[i].first));
+      cursor = off + bytes;
+    }
+    if (total > cursor) add(cursor, total - cursor, nullptr);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+      for (size_t k; (k = next.fetch_add(1)) < pieces.size();) {
+        const Piece &pc = pieces[k];
+        if (pc.src)
+          std::memcpy(dst + pc.off, pc.src, pc.bytes);
+        else
+          std::memset(dst + pc.off, 0, pc.bytes);
+      }
+    };
+    const int nt = (int)std::min<size_t>(pieces.size(), (size_t)threads);
+    std::vector<std::thread> pool;
+    for (int k = 1; k < nt; ++k) pool.emplace_back(work);
+    work();
+    for (auto &th : pool) th.join();
+  }
   // Pointer fields hold offset + 1 until commit_scene rebases them.
   auto rel = [&](size_t part, size_t bytes) -> uintptr_t { return bytes ? (uintptr_t)plan.offsets[part] + 1 : 0; };
   DevScene &d = img.rel;
@@ -839,6 +1003,8 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   img.desc_off = plan.offsets[p_desc];
   img.tri_count = tc;
   img.light_count = desc.light_count;
+  img.seconds[3] = since(t_after);
+  img.seconds[0] = since(t_start);
   return "";
 }
 

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -40,13 +41,30 @@ struct DeviceArena {
 // lights, emissive tables) plus a descriptor whose pointer fields hold
 // arena offsets + 1 (0 = absent). Uploading it is one allocation and one
 // copy, so an evicted scene comes back without another BVH build.
+// Uninitialised host bytes (a scene image is written part by part; only the
+// alignment gaps are zeroed).
+struct HostBlob {
+  std::unique_ptr<uint8_t[]> p;
+  size_t n = 0;
+  void allocate(size_t bytes) {
+    p.reset(new uint8_t[bytes]);
+    n = bytes;
+  }
+  uint8_t *data() { return p.get(); }
+  const uint8_t *data() const { return p.get(); }
+  size_t size() const { return n; }
+};
+
 struct SceneImage {
-  std::vector<uint8_t> blob;
+  HostBlob blob;
   DevScene rel{};
   uint64_t desc_off = 0;
   uint64_t tri_count = 0;
   BvhBuildStats bvh;
   uint32_t light_count = 0;
+  // Host time of build_scene_image: total, tables before the BVH (textures,
+  // materials, attribute streams), BVH build, tables after it and the blob.
+  double seconds[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
 struct SceneHost {

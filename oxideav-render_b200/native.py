@@ -89,6 +89,7 @@ SIGNATURES = {
     "pt_set_node_width": (i32, [vp, u32, u32]),
     "pt_set_material_sort": (i32, [vp, i32]),
     "pt_set_wave_graphs": (i32, [vp, i32]),
+    "pt_debug_prepare_scene": (i32, [C.POINTER(abi.pt_scene_desc), dp, u64p]),
     "pt_autotune": (i32, [vp, vp, u32, C.POINTER(abi.pt_tune_choice)]),
     "pt_tune_lookup": (i32, [vp, vp, C.POINTER(abi.pt_tune_choice)]),
     "pt_tune_reset": (i32, [vp]),
