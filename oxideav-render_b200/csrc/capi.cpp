@@ -211,7 +211,7 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
                     4 * P, 4 * P, 4 * P,                                     // q0 q1 q_shadow
                     4 * (size_t)kWfCounterStride * (iterations + 1),
                     4 * P, 4 * 2 * (size_t)kSortBuckets * (iterations + 1),   // q_sorted sort_counts
-                    sizeof(WaveDesc)};
+                    sizeof(WaveDesc), 4 * P};                                  // desc sort_keys
   size_t off[sizeof(sizes) / sizeof(sizes[0])], total = 0;
   for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); ++i) {
     total = (total + 255) & ~(size_t)255;
@@ -242,6 +242,7 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   w.q_sorted = (uint32_t *)(b + off[k++]);
   w.sort_counts = (uint32_t *)(b + off[k++]);
   w.desc = (WaveDesc *)(b + off[k++]);
+  w.sort_keys = (uint32_t *)(b + off[k++]);
   w.capacity = capacity;
   w.shadow_slots = shadow_slots;
   w.iterations = iterations;

@@ -148,6 +148,7 @@ struct WaveBuffers {
   uint32_t *q_shadow;
   uint32_t *counters;          // [iterations][kWfCounterStride]
   uint32_t *q_sorted;          // the active queue bucketed by material (material sort on)
+  uint32_t *sort_keys;         // material-sort key of each active-queue position (set by extend)
   uint32_t *sort_counts;       // [iterations][2][kSortBuckets]: bucket sizes, then cursors
   struct WaveDesc *desc;       // this wave's requests and segments (written before each wave)
   uint32_t capacity, shadow_slots, iterations, sort_materials;

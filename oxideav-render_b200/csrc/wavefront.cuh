@@ -39,9 +39,24 @@ PT_DEV void wf_store(const WaveBuffers &w, uint32_t slot, const PathState &ps, u
   w.seed[slot] = make_uint4(ps.smp.pixel_seed, ps.smp.index, ps.smp.path_seed, request);
 }
 
+// wf_store without the sampler seeds and request, which never change after
+// ray generation (shade writes back only what a vertex can change).
+PT_DEV void wf_store_vertex(const WaveBuffers &w, uint32_t slot, const PathState &ps) {
+  w.o[slot] = make_float4(ps.o.x, ps.o.y, ps.o.z, __uint_as_float(ps.k));
+  w.d[slot] = make_float4(ps.d.x, ps.d.y, ps.d.z, ps.prev_pdf);
+  uint32_t flags = (ps.has_medium ? PF_MEDIUM : 0u) | (ps.covered ? PF_COVERED : 0u) |
+                   ((uint32_t)(ps.hero + 1) << PF_HERO_SHIFT);
+  w.beta[slot] = make_float4(ps.beta.x, ps.beta.y, ps.beta.z, __uint_as_float(flags));
+  w.rad[slot] = make_float4(ps.radiance.x, ps.radiance.y, ps.radiance.z, ps.covered ? 1.0f : 0.0f);
+  w.prev[slot] = make_float4(ps.prev_pos.x, ps.prev_pos.y, ps.prev_pos.z, 0.0f);
+  if (ps.has_medium) w.sigma[slot] = make_float4(ps.sigma.x, ps.sigma.y, ps.sigma.z, 0.0f);
+}
+
 PT_DEV uint32_t wf_load(const WaveBuffers &w, uint32_t slot, PathState &ps) {
-  float4 o = w.o[slot], d = w.d[slot], b = w.beta[slot], r = w.rad[slot], p = w.prev[slot], s = w.sigma[slot];
+  float4 o = w.o[slot], d = w.d[slot], b = w.beta[slot], r = w.rad[slot], p = w.prev[slot];
   uint4 sd = w.seed[slot];
+  // The medium coefficients are read (and written) only inside a medium.
+  const float4 s = (__float_as_uint(b.w) & PF_MEDIUM) ? w.sigma[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   ps.o = {o.x, o.y, o.z};
   ps.k = __float_as_uint(o.w);
   ps.d = {d.x, d.y, d.z};
@@ -141,6 +156,15 @@ __global__ void __launch_bounds__(256) k_wf_accumulate(WaveBuffers w) {
   }
 }
 
+// Computed by extend when the ray finishes and stored by queue position, so
+// the count / scatter passes read keys and slots contiguously.
+PT_DEV uint32_t sort_key(const DevScene *s, bool found, uint32_t g) {
+  if (!found) return 0;
+  uint32_t m = __ldg(s->tri_info + g).x;
+  uint32_t sh = (uint32_t)((uintptr_t)s >> 8) * 0x9E3779B1u;
+  return 1u + (m + sh) % (kSortBuckets - 1u);
+}
+
 // Closest hit of every queued path: persistent lanes, one ray each, refilled
 // from the queue as rays finish (dev_traverse.cuh).
 __global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t iter,
@@ -155,13 +179,14 @@ __global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t it
   stk.stride = blockDim.x;
   ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
   bool has = false, exhausted = false;
-  uint32_t slot = 0, k = 0;
+  uint32_t slot = 0, k = 0, qpos = 0;
   const DevRequest *rq = nullptr;
   Sampler smp;
   ClosestRay cr;
   for (;;) {
     uint32_t idx = warp_claim(claim, !has, n, exhausted);
     if (!has && idx < n) {
+      qpos = idx;
       slot = q[idx];
       float4 o = w.o[slot], d = w.d[slot];
       uint4 sd = w.seed[slot];
@@ -192,6 +217,7 @@ __global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t it
         } else {
           w.hit_g[slot] = 0u;
         }
+        if (w.sort_materials) w.sort_keys[qpos] = sort_key(&s, cr.have, cr.best.g);
         has = false;
       }
     }
@@ -202,22 +228,11 @@ __global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t it
 // ---- material sort: the active queue bucketed by (scene, material) before
 // shade, stable within each warp's group of equal keys. Bucket 0 holds the
 // paths whose ray missed.
-PT_DEV uint32_t sort_key(const DevRequest *reqs, const WaveBuffers &w, uint32_t slot) {
-  uint32_t hg = w.hit_g[slot];
-  if (!(hg & HIT_FOUND)) return 0;
-  const DevScene *s = reqs[w.seed[slot].w].scene;
-  uint32_t m = __ldg(s->tri_info + (hg & HIT_G_MASK)).x;
-  uint32_t sh = (uint32_t)((uintptr_t)s >> 8) * 0x9E3779B1u;
-  return 1u + (m + sh) % (kSortBuckets - 1u);
-}
-
 __global__ void __launch_bounds__(256) k_wf_sort_count(WaveBuffers w, uint32_t iter) {
-  const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
-  const uint32_t *q = w.q[iter & 1u];
   uint32_t *count = w.sort_counts + (size_t)iter * 2 * kSortBuckets;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t key = sort_key(reqs, w, q[i]);
+    uint32_t key = w.sort_keys[i];
     uint32_t peers = __match_any_sync(__activemask(), key);
     if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(count + key, (uint32_t)__popc(peers));
   }
@@ -241,14 +256,13 @@ __global__ void __launch_bounds__(kSortBuckets) k_wf_sort_scan(WaveBuffers w, ui
 }
 
 __global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t iter) {
-  const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
   uint32_t *cursor = w.sort_counts + (size_t)iter * 2 * kSortBuckets + kSortBuckets;
   const uint32_t lane = threadIdx.x & 31u;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t slot = q[i];
-    uint32_t key = sort_key(reqs, w, slot);
+    uint32_t key = w.sort_keys[i];
     uint32_t peers = __match_any_sync(__activemask(), key);
     uint32_t leader = (uint32_t)(__ffs(peers) - 1);
     uint32_t base = 0;
@@ -286,7 +300,7 @@ __global__ void __launch_bounds__(128, 3) k_wf_shade(WaveBuffers w, uint32_t ite
     }
     DeferredSink sink{&w, slot, 0};
     bool alive = shade(rq, ps, found, h, sink);
-    wf_store(w, slot, ps, request);
+    wf_store_vertex(w, slot, ps);
     w.sh_n[slot] = sink.count;
     wf_append(q_next, n_next, alive, slot);
     wf_append(w.q_shadow, n_shadow, sink.count > 0, slot);

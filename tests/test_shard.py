@@ -62,6 +62,8 @@ def test_reductions_over_a_two_rank_gloo_group():
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
-    assert sorted(out[0][0] + out[1][0]) == list(range(10))
-    assert out[0][1] == out[1][1] == 2.5
-    assert out[0][2] == out[1][2] == 10.0
+    got = dict(out)
+    mgr.shutdown()  # stop the manager process here, not at interpreter exit
+    assert sorted(got[0][0] + got[1][0]) == list(range(10))
+    assert got[0][1] == got[1][1] == 2.5
+    assert got[0][2] == got[1][2] == 10.0
