@@ -228,13 +228,27 @@ __global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t it
 // ---- material sort: the active queue bucketed by (scene, material) before
 // shade, stable within each warp's group of equal keys. Bucket 0 holds the
 // paths whose ray missed.
+// Tiles of kSortTile queue entries per block: a shared-memory histogram per
+// tile, then one global atomic per non-empty bucket (the hot buckets - the
+// material most paths hit - would serialise per-warp global atomics).
+constexpr uint32_t kSortPerThread = 8, kSortTile = 256 * kSortPerThread;
+
 __global__ void __launch_bounds__(256) k_wf_sort_count(WaveBuffers w, uint32_t iter) {
+  __shared__ uint32_t hist[kSortBuckets];
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   uint32_t *count = w.sort_counts + (size_t)iter * 2 * kSortBuckets;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t key = w.sort_keys[i];
-    uint32_t peers = __match_any_sync(__activemask(), key);
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(count + key, (uint32_t)__popc(peers));
+  const uint32_t t = threadIdx.x;
+  for (uint32_t base = blockIdx.x * kSortTile; base < n; base += gridDim.x * kSortTile) {
+    hist[t] = 0;
+    __syncthreads();
+#pragma unroll
+    for (uint32_t e = 0; e < kSortPerThread; ++e) {
+      const uint32_t i = base + e * 256 + t;
+      if (i < n) atomicAdd(&hist[w.sort_keys[i]], 1u);
+    }
+    __syncthreads();
+    if (hist[t]) atomicAdd(count + t, hist[t]);
+    __syncthreads();
   }
 }
 
@@ -256,19 +270,30 @@ __global__ void __launch_bounds__(kSortBuckets) k_wf_sort_scan(WaveBuffers w, ui
 }
 
 __global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t iter) {
+  __shared__ uint32_t hist[kSortBuckets], start[kSortBuckets];
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
   uint32_t *cursor = w.sort_counts + (size_t)iter * 2 * kSortBuckets + kSortBuckets;
-  const uint32_t lane = threadIdx.x & 31u;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t slot = q[i];
-    uint32_t key = w.sort_keys[i];
-    uint32_t peers = __match_any_sync(__activemask(), key);
-    uint32_t leader = (uint32_t)(__ffs(peers) - 1);
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(cursor + key, (uint32_t)__popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    w.q_sorted[base + __popc(peers & ((1u << lane) - 1u))] = slot;
+  const uint32_t t = threadIdx.x;
+  for (uint32_t base = blockIdx.x * kSortTile; base < n; base += gridDim.x * kSortTile) {
+    hist[t] = 0;
+    __syncthreads();
+    uint32_t key[kSortPerThread], rank[kSortPerThread];
+#pragma unroll
+    for (uint32_t e = 0; e < kSortPerThread; ++e) {
+      const uint32_t i = base + e * 256 + t;
+      key[e] = i < n ? w.sort_keys[i] : 0u;
+      rank[e] = i < n ? atomicAdd(&hist[key[e]], 1u) : 0u;
+    }
+    __syncthreads();
+    if (hist[t]) start[t] = atomicAdd(cursor + t, hist[t]);
+    __syncthreads();
+#pragma unroll
+    for (uint32_t e = 0; e < kSortPerThread; ++e) {
+      const uint32_t i = base + e * 256 + t;
+      if (i < n) w.q_sorted[start[key[e]] + rank[e]] = q[i];
+    }
+    __syncthreads();
   }
 }
 
