@@ -23,9 +23,12 @@ def test_scenes_prepare_on_the_host():
         st, sec, nbytes, _ = prepare(d.desc)
         assert st == abi.PT_OK
         assert sec[0] >= sec[2] >= 0.0 and nbytes > 0
-    # More triangles, more device bytes.
-    small = prepare(ts.random_soup(1000, seed=1).to_desc(ts.pt_opts(8, 1, 1)).desc)[2]
-    large = prepare(ts.random_soup(20000, seed=1).to_desc(ts.pt_opts(8, 1, 1)).desc)[2]
+    # More triangles, more device bytes. The SceneDesc owns the buffers its
+    # pt_scene_desc points into, so it stays bound across the call.
+    small_desc = ts.random_soup(1000, seed=1).to_desc(ts.pt_opts(8, 1, 1))
+    large_desc = ts.random_soup(20000, seed=1).to_desc(ts.pt_opts(8, 1, 1))
+    small = prepare(small_desc.desc)[2]
+    large = prepare(large_desc.desc)[2]
     assert large > small
 
 
