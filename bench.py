@@ -499,6 +499,10 @@ def run_b200(args):
     if env is not None:
         tracer.set_environment(api.EnvironmentMap(env))
     tracer.sync(scene, opts)
+    # The resident scene's steady state: a large scene's first tree is built
+    # on the device and replaced by the host binned-SAH tree once that is
+    # built in the background (pt_set_bvh_builder AUTO); wait for it.
+    ctx.bvh_wait(tracer._scene_id)
     tuned = None
     if args.autotune:
         # pt_autotune: calibration refines on a scratch accumulator pick this
@@ -585,8 +589,8 @@ def run_b200(args):
         e2e_t = max_over_ranks(sum(e2e_s) / len(e2e_s), ws)
         e2e = {"value": samples_per_step * ws / e2e_t, "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_t,
-               "call": "PathTraceCudaRenderer.render (scene upload incl. host BVH build, refine, "
-                       "sRGB image readback)"}
+               "call": "PathTraceCudaRenderer.render (scene preparation and upload incl. the BVH build, "
+                       "refine, sRGB image readback)"}
         # Where the host part of that time goes (one extra, separately timed upload).
         t0 = time.perf_counter()
         desc = scene.to_desc(opts)
@@ -594,7 +598,8 @@ def run_b200(args):
         sid = ctx.upload(desc)
         t2 = time.perf_counter()
         e2e["host_ms"] = {"flatten": 1000 * (t1 - t0), "prepare_and_upload": 1000 * (t2 - t1),
-                          "bvh_build": 1000 * ctx.bvh_stats(sid)["build_seconds"]}
+                          "bvh_build": 1000 * ctx.bvh_stats(sid)["build_seconds"],
+                          "bvh_on_device": ctx.bvh_on_device(sid)}
         ctx.release(sid)
     mixed = None
     if args.mixed > 0:

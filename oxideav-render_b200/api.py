@@ -75,6 +75,19 @@ class Context:
         return {"nodes": n.value, "leaves": l.value, "max_depth": d.value, "sah_cost": sah.value,
                 "build_seconds": sec.value}
 
+    def set_bvh_builder(self, builder: int) -> None:
+        """pt_set_bvh_builder: abi.PT_BVH_BUILD_AUTO / _HOST / _DEVICE."""
+        self.check(self.lib.pt_set_bvh_builder(self.ptr, builder))
+
+    def bvh_wait(self, scene_id: int) -> None:
+        """pt_scene_bvh_wait: switch the scene to its background host tree."""
+        self.check(self.lib.pt_scene_bvh_wait(self.ptr, scene_id))
+
+    def bvh_on_device(self, scene_id: int) -> bool:
+        v = C.c_int()
+        self.check(self.lib.pt_scene_bvh_on_device(self.ptr, scene_id, C.byref(v)))
+        return bool(v.value)
+
     def set_schedule(self, schedule: int) -> None:
         self.check(self.lib.pt_set_schedule(self.ptr, schedule))
 

@@ -1,0 +1,751 @@
+// Device BVH construction (bvh_build.h): Morton order, radix sort, parallel
+// locally-ordered clustering, SAH leaf collapse, and the two node layouts.
+//
+// Data layout during the build (n triangles, 2n - 1 binary nodes):
+//   node v < n        leaf of the triangle at sorted position v
+//   node v >= n       interior node created by the (v - n)-th merge; merges
+//                     of one clustering round get consecutive ids, so every
+//                     parent has a larger id (and a later round) than its
+//                     children
+//   nlo / nhi         node boxes (float4, w unused)
+//   ncount / ncost    triangles below the node / its SAH cost
+//   nstate            NS_* bits; nfirst / ndepth from the top-down pass
+//   nchild[v - n]     the two children of interior node v
+// The output layouts number the surviving interior nodes in decreasing id
+// order (root first).
+#include <algorithm>
+#include <type_traits>
+#include <chrono>
+#include <cstdio>
+#include <vector>
+
+#include "bvh_build.h"
+#include "dev_types.h"
+
+namespace ptd {
+namespace {
+
+constexpr int kPlocRadius = 16;
+// Morton code bits per axis: 10 (30-bit codes in 32-bit keys) or 21 (63-bit
+// codes in 64-bit keys).
+constexpr int kMortonAxisBits = 10;
+using MortonKey = std::conditional_t<(kMortonAxisBits > 10), unsigned long long, uint32_t>;
+constexpr int kMortonBits = 3 * kMortonAxisBits;
+constexpr uint32_t kMaxLeafTris = 8;
+// SAH weights of a node visit and of a triangle test.
+constexpr float kTraversalCost = 1.0f, kTriangleCost = 1.0f;
+// Smallest scene built on the device; smaller ones build on the host.
+constexpr uint32_t kMinDeviceTris = 64;
+constexpr uint32_t kMaxRounds = 1u << 16;
+
+constexpr int kThreads = 256;
+constexpr int kScanItems = 8, kScanTile = kThreads * kScanItems;
+constexpr int kRadixRounds = 8, kRadixTile = kThreads * kRadixRounds, kRadixBins = 256;
+constexpr uint32_t kLeafShift = 27;
+
+enum NodeState : uint32_t { NS_COVERED = 1u, NS_WIDE = 2u, NS_COLLAPSED = 4u };
+
+__device__ __forceinline__ float box_area(float4 lo, float4 hi) {
+  float dx = fmaxf(hi.x - lo.x, 0.0f), dy = fmaxf(hi.y - lo.y, 0.0f), dz = fmaxf(hi.z - lo.z, 0.0f);
+  float a = dx * dy + dy * dz + dz * dx;
+  return isnan(a) ? INFINITY : a;
+}
+__device__ __forceinline__ float4 fmin4(float4 a, float4 b) {
+  return make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), 0.0f);
+}
+__device__ __forceinline__ float4 fmax4(float4 a, float4 b) {
+  return make_float4(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z), 0.0f);
+}
+// Order-preserving map of floats to unsigned ints (for atomicMin / Max).
+__device__ __forceinline__ uint32_t ord_of(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float float_of(uint32_t u) {
+  return (u & 0x80000000u) ? __uint_as_float(u & 0x7fffffffu) : __uint_as_float(~u);
+}
+// The low `kMortonAxisBits` bits of x spread to every third bit.
+__device__ __forceinline__ MortonKey spread_bits(uint32_t x) {
+  MortonKey r = 0;
+#pragma unroll
+  for (int b = 0; b < kMortonAxisBits; ++b) r |= (MortonKey)((x >> b) & 1u) << (3 * b);
+  return r;
+}
+
+// ---------------------------------------------------------------- scans
+// Exclusive prefix sums in tiles of kScanTile items: each block scans one
+// tile and leaves the tile total in `sums`; a scan of the totals, added
+// back, completes the multi-tile scan.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_scan_tile(const T *in, T *out, uint64_t n, T *sums) {
+  __shared__ T warp_tot[kThreads / 32];
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  T v[kScanItems];
+  T run = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = base + k < n ? in[base + k] : T(0);
+    T x = v[k];
+    v[k] = run;
+    run += x;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  T incl = run;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T y = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d) incl += y;
+  }
+  if (lane == 31) warp_tot[warp] = incl;
+  __syncthreads();
+  T before = 0, total = 0;
+  for (int w = 0; w < kThreads / 32; ++w) {
+    if (w < warp) before += warp_tot[w];
+    total += warp_tot[w];
+  }
+  const T excl = before + incl - run;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < n) out[base + k] = excl + v[k];
+  if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+template <class T>
+__global__ void k_scan_add(T *out, uint64_t n, const T *offs) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] += offs[i / kScanTile];
+}
+
+uint64_t tiles_of(uint64_t n, uint64_t tile) { return (n + tile - 1) / tile; }
+
+// Scratch for every level of a scan of up to `n` items.
+uint64_t scan_scratch_items(uint64_t n) {
+  uint64_t total = 0;
+  do {
+    n = tiles_of(n, kScanTile);
+    total += n + 1;
+  } while (n > 1);
+  return total;
+}
+
+unsigned grid_for(uint64_t n, int per_block = kThreads) {
+  uint64_t g = (n + per_block - 1) / per_block;
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(g, 1u << 20));
+}
+
+// Exclusive scan in -> out (in == out allowed). Returns the device address
+// of the grand total.
+template <class T>
+T *scan_exclusive(const T *in, T *out, uint64_t n, T *scratch, cudaStream_t st) {
+  const uint64_t nt = tiles_of(std::max<uint64_t>(n, 1), kScanTile);
+  T *sums = scratch;
+  k_scan_tile<T><<<(unsigned)nt, kThreads, 0, st>>>(in, out, n, sums);
+  if (nt == 1) return sums;
+  T *total = scan_exclusive<T>(sums, sums, nt, scratch + nt + 1, st);
+  k_scan_add<T><<<grid_for(n), kThreads, 0, st>>>(out, n, sums);
+  return total;
+}
+
+// ---------------------------------------------------------------- radix sort
+__global__ void __launch_bounds__(kThreads) k_radix_hist(const MortonKey *keys, uint32_t n, int shift, uint32_t *hist,
+                                                         uint32_t ntiles) {
+  __shared__ uint32_t h[kRadixBins];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t base = (uint64_t)blockIdx.x * kRadixTile;
+#pragma unroll
+  for (int r = 0; r < kRadixRounds; ++r) {
+    uint64_t i = base + (uint64_t)r * kThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[(uint32_t)(keys[i] >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter of one tile: items are ranked in input order, a round of
+// kThreads items at a time (warp match for equal digits inside a warp,
+// per-warp digit counts across warps, a running count across rounds).
+__global__ void __launch_bounds__(kThreads) k_radix_scatter(const MortonKey *keys, const uint32_t *vals, MortonKey *keys_out,
+                                                            uint32_t *vals_out, uint32_t n, int shift,
+                                                            const uint32_t *offs, uint32_t ntiles) {
+  __shared__ uint32_t run[kRadixBins];
+  __shared__ uint32_t wc[kThreads / 32][kRadixBins];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  run[threadIdx.x] = offs[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; ++w) wc[w][threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint64_t base = (uint64_t)blockIdx.x * kRadixTile;
+  for (int r = 0; r < kRadixRounds; ++r) {
+    const uint64_t i = base + (uint64_t)r * kThreads + threadIdx.x;
+    const bool valid = i < n;
+    MortonKey key = 0;
+    uint32_t val = 0, d = kRadixBins;
+    if (valid) {
+      key = keys[i];
+      val = vals[i];
+      d = (uint32_t)(key >> shift) & 0xffu;
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & lt);
+    const bool leader = lane == __ffs(peers) - 1;
+    if (valid && leader) wc[warp][d] = __popc(peers);
+    __syncthreads();
+    if (valid) {
+      uint32_t pos = run[d] + rank;
+      for (int w = 0; w < warp; ++w) pos += wc[w][d];
+      keys_out[pos] = key;
+      vals_out[pos] = val;
+    }
+    __syncthreads();
+    uint32_t add = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) add += wc[w][threadIdx.x];
+    run[threadIdx.x] += add;
+    __syncthreads();
+    if (valid && leader) wc[warp][d] = 0;
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- primitives
+// Triangle boxes (a triangle with a NaN coordinate gets an empty box: it
+// can never be hit) and the bounds of the finite centroids.
+__global__ void __launch_bounds__(kThreads) k_prim_boxes(const float *pos, uint32_t n, float4 *lo, float4 *hi,
+                                                         uint32_t *cb) {
+  float cl[3] = {INFINITY, INFINITY, INFINITY}, ch[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float *p = pos + 9ull * i;
+    float v[9];
+    bool nan = false;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      v[k] = __ldg(p + k);
+      nan |= isnan(v[k]);
+    }
+    float4 l, h;
+    if (nan) {
+      l = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
+      h = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+    } else {
+      l = make_float4(fminf(fminf(v[0], v[3]), v[6]), fminf(fminf(v[1], v[4]), v[7]), fminf(fminf(v[2], v[5]), v[8]),
+                      0.0f);
+      h = make_float4(fmaxf(fmaxf(v[0], v[3]), v[6]), fmaxf(fmaxf(v[1], v[4]), v[7]), fmaxf(fmaxf(v[2], v[5]), v[8]),
+                      0.0f);
+      float c[3] = {(l.x + h.x) * 0.5f, (l.y + h.y) * 0.5f, (l.z + h.z) * 0.5f};
+      if (isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2]))
+        for (int k = 0; k < 3; ++k) {
+          cl[k] = fminf(cl[k], c[k]);
+          ch[k] = fmaxf(ch[k], c[k]);
+        }
+    }
+    lo[i] = l;
+    hi[i] = h;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    for (int d = 16; d > 0; d >>= 1) {
+      cl[k] = fminf(cl[k], __shfl_xor_sync(0xffffffffu, cl[k], d));
+      ch[k] = fmaxf(ch[k], __shfl_xor_sync(0xffffffffu, ch[k], d));
+    }
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(cb + k, ord_of(cl[k]));
+      atomicMax(cb + 3 + k, ord_of(ch[k]));
+    }
+}
+
+__global__ void k_morton(const float4 *lo, const float4 *hi, uint32_t n, const uint32_t *cb, MortonKey *keys,
+                         uint32_t *vals) {
+  float cmin[3], ext[3];
+  for (int k = 0; k < 3; ++k) {
+    cmin[k] = float_of(cb[k]);
+    ext[k] = float_of(cb[3 + k]) - cmin[k];
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 l = lo[i], h = hi[i];
+    float c[3] = {(l.x + h.x) * 0.5f, (l.y + h.y) * 0.5f, (l.z + h.z) * 0.5f};
+    uint32_t q[3];
+    for (int k = 0; k < 3; ++k) {
+      float x = ext[k] > 0.0f ? (c[k] - cmin[k]) / ext[k] : 0.0f;
+      if (!(x >= 0.0f)) x = 0.0f;
+      x = fminf(x, 1.0f);
+      const uint32_t cells = 1u << kMortonAxisBits;
+      q[k] = min((uint32_t)(x * (float)cells), cells - 1u);
+    }
+    keys[i] = (spread_bits(q[0]) << 2) | (spread_bits(q[1]) << 1) | spread_bits(q[2]);
+    vals[i] = i;
+  }
+}
+
+// ---------------------------------------------------------------- clustering
+struct Nodes {
+  float4 *lo, *hi;
+  uint32_t *count;
+  float *cost;
+  uint32_t *state, *first, *depth;
+  int2 *child;  // indexed v - n
+  uint32_t n;
+};
+
+__global__ void k_leaves(const uint32_t *vals, const float4 *plo, const float4 *phi, Nodes nd, uint32_t *clusters) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd.n; j += gridDim.x * blockDim.x) {
+    uint32_t g = vals[j];
+    float4 l = plo[g], h = phi[g];
+    nd.lo[j] = l;
+    nd.hi[j] = h;
+    nd.count[j] = 1;
+    nd.cost[j] = kTriangleCost * box_area(l, h);
+    nd.state[j] = 0;
+    clusters[j] = j;
+  }
+}
+
+// Nearest neighbour of every cluster within kPlocRadius positions: the
+// smallest area of the merged box, ties to the lower position. Under that
+// order the globally closest pair is mutual, so every round merges.
+__global__ void __launch_bounds__(kThreads) k_nearest(const uint32_t *clusters, uint32_t m, const float4 *nlo,
+                                                      const float4 *nhi, uint32_t *nn) {
+  __shared__ float4 slo[kThreads + 2 * kPlocRadius], shi[kThreads + 2 * kPlocRadius];
+  const int64_t b0 = (int64_t)blockIdx.x * kThreads;
+  for (int t = threadIdx.x; t < kThreads + 2 * kPlocRadius; t += kThreads) {
+    int64_t idx = b0 - kPlocRadius + t;
+    if (idx >= 0 && idx < (int64_t)m) {
+      uint32_t c = clusters[idx];
+      slo[t] = nlo[c];
+      shi[t] = nhi[c];
+    }
+  }
+  __syncthreads();
+  const int64_t i = b0 + threadIdx.x;
+  if (i >= (int64_t)m) return;
+  const float4 l = slo[threadIdx.x + kPlocRadius], h = shi[threadIdx.x + kPlocRadius];
+  const int64_t j0 = i - kPlocRadius > 0 ? i - kPlocRadius : 0;
+  const int64_t j1 = i + kPlocRadius < (int64_t)m - 1 ? i + kPlocRadius : (int64_t)m - 1;
+  float best = INFINITY;
+  uint32_t best_j = 0xffffffffu;
+  for (int64_t j = j0; j <= j1; ++j) {
+    if (j == i) continue;
+    const int t = (int)(j - b0) + kPlocRadius;
+    const float a = box_area(fmin4(l, slo[t]), fmax4(h, shi[t]));
+    if (best_j == 0xffffffffu || a < best) {
+      best = a;
+      best_j = (uint32_t)j;
+    }
+  }
+  nn[i] = best_j;
+}
+
+// keep (high word) and merge (low word) flags of every cluster.
+__global__ void k_mark(const uint32_t *nn, uint32_t m, uint64_t *flags) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    uint32_t j = nn[i];
+    bool mutual = nn[j] == i;
+    uint64_t keep = (mutual && i > j) ? 0u : 1u;
+    uint64_t merge = (mutual && i < j) ? 1u : 0u;
+    flags[i] = (keep << 32) | merge;
+  }
+}
+
+__global__ void k_compact(const uint32_t *clusters, uint32_t *next, uint32_t m, const uint32_t *nn,
+                          const uint64_t *flags, const uint64_t *offs, uint32_t merged_before, Nodes nd) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    const uint64_t f = flags[i];
+    if (!(f >> 32)) continue;
+    const uint64_t o = offs[i];
+    const uint32_t pos = (uint32_t)(o >> 32);
+    if (!(f & 1u)) {
+      next[pos] = clusters[i];
+      continue;
+    }
+    const uint32_t a = clusters[i], b = clusters[nn[i]];
+    const uint32_t k = merged_before + (uint32_t)o;
+    const uint32_t v = nd.n + k;
+    const float4 l = fmin4(nd.lo[a], nd.lo[b]), h = fmax4(nd.hi[a], nd.hi[b]);
+    const uint32_t cnt = nd.count[a] + nd.count[b];
+    const float area = box_area(l, h);
+    const float split = kTraversalCost * area + nd.cost[a] + nd.cost[b];
+    const float leaf = kTriangleCost * (float)cnt * area;
+    const bool collapse = cnt <= kMaxLeafTris && leaf <= split;
+    nd.lo[v] = l;
+    nd.hi[v] = h;
+    nd.count[v] = cnt;
+    nd.cost[v] = collapse ? leaf : split;
+    nd.state[v] = collapse ? NS_COLLAPSED : 0u;
+    nd.child[k] = make_int2((int)a, (int)b);
+    next[pos] = v;
+  }
+}
+
+// ---------------------------------------------------------------- layouts
+__device__ __forceinline__ bool interior(const Nodes &nd, uint32_t c) {
+  return c >= nd.n && !(nd.state[c] & NS_COLLAPSED);
+}
+
+// Children of the four-child node of interior node v: start from its two
+// children and open the interior child of largest surface area until there
+// are four (or none is left to open).
+__device__ int wide_children(const Nodes &nd, uint32_t v, uint32_t ch[4]) {
+  const int2 c = nd.child[v - nd.n];
+  ch[0] = (uint32_t)c.x;
+  ch[1] = (uint32_t)c.y;
+  int nch = 2;
+  while (nch < 4) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (int i = 0; i < nch; ++i) {
+      if (!interior(nd, ch[i])) continue;
+      float a = box_area(nd.lo[ch[i]], nd.hi[ch[i]]);
+      if (a > best_area) {
+        best_area = a;
+        best = i;
+      }
+    }
+    if (best < 0) break;
+    const int2 oc = nd.child[ch[best] - nd.n];
+    for (int i = nch; i > best + 1; --i) ch[i] = ch[i - 1];
+    ch[best] = (uint32_t)oc.x;
+    ch[best + 1] = (uint32_t)oc.y;
+    ++nch;
+  }
+  return nch;
+}
+
+__global__ void k_root(Nodes nd, uint32_t root) {
+  nd.first[root] = 0;
+  nd.depth[root] = 0;
+  nd.state[root] |= NS_WIDE;
+}
+
+// Top-down pass over the interior nodes of one clustering round (parents of
+// later rounds are done): record offsets, depths, coverage by a collapsed
+// ancestor, and the four-child node marks.
+__global__ void k_topdown(Nodes nd, uint32_t v0, uint32_t v1, uint32_t *max_depth, uint32_t *leaves) {
+  for (uint32_t v = v0 + blockIdx.x * blockDim.x + threadIdx.x; v < v1; v += gridDim.x * blockDim.x) {
+    const uint32_t st = nd.state[v];
+    const int2 c = nd.child[v - nd.n];
+    const uint32_t a = (uint32_t)c.x, b = (uint32_t)c.y;
+    const uint32_t f = nd.first[v], d = nd.depth[v];
+    nd.first[a] = f;
+    nd.first[b] = f + nd.count[a];
+    nd.depth[a] = d + 1;
+    nd.depth[b] = d + 1;
+    if (st & (NS_COVERED | NS_COLLAPSED)) {
+      nd.state[a] |= NS_COVERED;
+      nd.state[b] |= NS_COVERED;
+      continue;
+    }
+    uint32_t leaf_kids = 0;
+    if (!interior(nd, a)) ++leaf_kids;
+    if (!interior(nd, b)) ++leaf_kids;
+    if (leaf_kids) {
+      atomicMax(max_depth, d + 1);
+      atomicAdd(leaves, leaf_kids);
+    }
+    if (st & NS_WIDE) {
+      uint32_t ch[4];
+      const int nch = wide_children(nd, v, ch);
+      for (int i = 0; i < nch; ++i)
+        if (interior(nd, ch[i])) nd.state[ch[i]] |= NS_WIDE;
+    }
+  }
+}
+
+// In decreasing id order: (two-child node) << 32 | (four-child node).
+__global__ void k_layout_flags(Nodes nd, uint64_t *flags) {
+  const uint32_t m = nd.n - 1;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x) {
+    const uint32_t v = 2 * nd.n - 2 - p;
+    const uint32_t st = nd.state[v];
+    const uint64_t two = (st & (NS_COVERED | NS_COLLAPSED)) ? 0u : 1u;
+    const uint64_t four = (two && (st & NS_WIDE)) ? 1u : 0u;
+    flags[p] = (two << 32) | four;
+  }
+}
+
+__device__ __forceinline__ void pad_box(float4 lo, float4 hi, float plo[3], float phi[3]) {
+  const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+  float ext = 0.0f;
+  for (int k = 0; k < 3; ++k) ext = fmaxf(fmaxf(ext, h[k] - l[k]), fmaxf(fabsf(l[k]), fabsf(h[k])));
+  const float pad = ext * 1.0e-5f + 1.0e-30f;
+  for (int k = 0; k < 3; ++k) {
+    plo[k] = l[k] - pad;
+    phi[k] = h[k] + pad;
+  }
+}
+
+// Reference to child c from a two-child node (`wide` false: the index in
+// the two-child array) or a four-child node (the index in the four-child
+// array); leaves encode their record range.
+__device__ __forceinline__ int child_ref(const Nodes &nd, const uint64_t *offs, uint32_t c, bool wide,
+                                         uint32_t &count) {
+  if (interior(nd, c)) {
+    count = 0;
+    const uint64_t o = offs[2 * nd.n - 2 - c];
+    return (int)(wide ? (uint32_t)o : (uint32_t)(o >> 32));
+  }
+  count = nd.count[c];
+  return (int)~(nd.first[c] | (count << kLeafShift));
+}
+
+__global__ void k_write_nodes(Nodes nd, const uint64_t *offs, BvhNode *out2, Bvh4Node *out4) {
+  const uint32_t m = nd.n - 1;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x) {
+    const uint32_t v = 2 * nd.n - 2 - p;
+    const uint32_t st = nd.state[v];
+    if (st & (NS_COVERED | NS_COLLAPSED)) continue;
+    const uint64_t o = offs[p];
+    const int2 c = nd.child[v - nd.n];
+    {
+      float l0[3], h0[3], l1[3], h1[3];
+      pad_box(nd.lo[c.x], nd.hi[c.x], l0, h0);
+      pad_box(nd.lo[c.y], nd.hi[c.y], l1, h1);
+      uint32_t n0, n1;
+      const int r0 = child_ref(nd, offs, (uint32_t)c.x, false, n0), r1 = child_ref(nd, offs, (uint32_t)c.y, false, n1);
+      BvhNode g;
+      g.a = make_float4(l0[0], h0[0], l0[1], h0[1]);
+      g.b = make_float4(l1[0], h1[0], l1[1], h1[1]);
+      g.c = make_float4(l0[2], h0[2], l1[2], h1[2]);
+      g.d = make_int4(r0, r1, (int)n0, (int)n1);
+      out2[o >> 32] = g;
+    }
+    if (st & NS_WIDE) {
+      uint32_t ch[4];
+      const int nch = wide_children(nd, v, ch);
+      float bl[3][4], bh[3][4];
+      int ref[4];
+      for (int i = 0; i < 4; ++i) {
+        if (i < nch) {
+          float l[3], h[3];
+          pad_box(nd.lo[ch[i]], nd.hi[ch[i]], l, h);
+          for (int k = 0; k < 3; ++k) {
+            bl[k][i] = l[k];
+            bh[k][i] = h[k];
+          }
+          uint32_t cnt;
+          ref[i] = child_ref(nd, offs, ch[i], true, cnt);
+        } else {
+          for (int k = 0; k < 3; ++k) {
+            bl[k][i] = INFINITY;
+            bh[k][i] = -INFINITY;
+          }
+          ref[i] = kEmptyChild;
+        }
+      }
+      Bvh4Node q;
+      q.lo_x = make_float4(bl[0][0], bl[0][1], bl[0][2], bl[0][3]);
+      q.hi_x = make_float4(bh[0][0], bh[0][1], bh[0][2], bh[0][3]);
+      q.lo_y = make_float4(bl[1][0], bl[1][1], bl[1][2], bl[1][3]);
+      q.hi_y = make_float4(bh[1][0], bh[1][1], bh[1][2], bh[1][3]);
+      q.lo_z = make_float4(bl[2][0], bl[2][1], bl[2][2], bl[2][3]);
+      q.hi_z = make_float4(bh[2][0], bh[2][1], bh[2][2], bh[2][3]);
+      q.child = make_int4(ref[0], ref[1], ref[2], ref[3]);
+      q.pad = make_int4(0, 0, 0, 0);
+      out4[(uint32_t)o] = q;
+    }
+  }
+}
+
+// Leaf-ordered triangle records: (v0, global id), (v1, REC_* flags), (v2, 0).
+__global__ void k_write_records(Nodes nd, const uint32_t *vals, const float *pos, const uint2 *tri_info,
+                                const DevMaterial *materials, float4 *records) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nd.n; j += gridDim.x * blockDim.x) {
+    const uint32_t g = vals[j];
+    const uint32_t r = nd.first[j];
+    const float *p = pos + 9ull * g;
+    const pt_material &m = materials[__ldg(&tri_info[g].x)].m;
+    const uint32_t fl = (m.alpha_mode == PT_ALPHA_OPAQUE ? REC_OPAQUE : 0u) | (m.double_sided ? REC_DOUBLE_SIDED : 0u);
+    records[3ull * r] = make_float4(p[0], p[1], p[2], __uint_as_float(g));
+    records[3ull * r + 1] = make_float4(p[3], p[4], p[5], __uint_as_float(fl));
+    records[3ull * r + 2] = make_float4(p[6], p[7], p[8], 0.0f);
+  }
+}
+
+// ---------------------------------------------------------------- host side
+struct Scratch {
+  std::vector<void *> ptrs;
+  cudaStream_t st;
+  bool oom = false;
+  std::string err;
+  template <class T>
+  T *get(uint64_t count) {
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, std::max<uint64_t>(count, 1) * sizeof(T), st);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      if (err.empty()) err = std::string("device BVH scratch allocation failed: ") + cudaGetErrorString(e);
+      oom = oom || e == cudaErrorMemoryAllocation;
+      return nullptr;
+    }
+    ptrs.push_back(p);
+    return static_cast<T *>(p);
+  }
+  ~Scratch() {
+    for (void *p : ptrs) cudaFreeAsync(p, st);
+  }
+};
+
+uint64_t align256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
+
+}  // namespace
+
+std::string device_build_bvh(SceneHost &sc, cudaStream_t st, uint32_t max_depth_allowed, bool &oom,
+                             DeviceBuildInfo *info) {
+  oom = false;
+  const auto t0 = std::chrono::steady_clock::now();
+  const uint64_t n64 = sc.tri_count;
+  if (n64 < kMinDeviceTris) return "too few triangles for the device builder";
+  if (n64 >= (1ull << kLeafShift)) return "too many triangles for the leaf encoding";
+  const uint32_t n = (uint32_t)n64;
+  const uint32_t total_nodes = 2 * n - 1;
+
+  Scratch s{{}, st};
+  float4 *plo = s.get<float4>(n), *phi = s.get<float4>(n);
+  uint32_t *cb = s.get<uint32_t>(6);
+  MortonKey *keys = s.get<MortonKey>(n), *keys2 = s.get<MortonKey>(n);
+  uint32_t *vals = s.get<uint32_t>(n), *vals2 = s.get<uint32_t>(n);
+  const uint32_t ntiles = (uint32_t)tiles_of(n, kRadixTile);
+  uint32_t *hist = s.get<uint32_t>((uint64_t)kRadixBins * ntiles);
+  uint32_t *scan32 = s.get<uint32_t>(scan_scratch_items((uint64_t)kRadixBins * ntiles));
+  Nodes nd;
+  nd.n = n;
+  nd.lo = s.get<float4>(total_nodes);
+  nd.hi = s.get<float4>(total_nodes);
+  nd.count = s.get<uint32_t>(total_nodes);
+  nd.cost = s.get<float>(total_nodes);
+  nd.state = s.get<uint32_t>(total_nodes);
+  nd.first = s.get<uint32_t>(total_nodes);
+  nd.depth = s.get<uint32_t>(total_nodes);
+  nd.child = s.get<int2>(n - 1);
+  uint32_t *ca = s.get<uint32_t>(n), *cbuf = s.get<uint32_t>(n), *nn = s.get<uint32_t>(n);
+  uint64_t *flags = s.get<uint64_t>(n), *offs = s.get<uint64_t>(n);
+  uint64_t *scan64 = s.get<uint64_t>(scan_scratch_items(n));
+  uint32_t *counters = s.get<uint32_t>(2);  // max depth, leaves
+  if (!s.err.empty()) {
+    oom = s.oom;
+    return s.err;
+  }
+  auto check = [&](const char *what) -> std::string {
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? std::string() : std::string(what) + ": " + cudaGetErrorString(e);
+  };
+
+  // Boxes, Morton codes, sort.
+  const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  cudaMemcpyAsync(cb, init, sizeof init, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), st);
+  const float *pos = sc.dev.pos;
+  k_prim_boxes<<<grid_for(n), kThreads, 0, st>>>(pos, n, plo, phi, cb);
+  k_morton<<<grid_for(n), kThreads, 0, st>>>(plo, phi, n, cb, keys, vals);
+  for (int shift = 0; shift < kMortonBits; shift += 8) {
+    k_radix_hist<<<ntiles, kThreads, 0, st>>>(keys, n, shift, hist, ntiles);
+    scan_exclusive<uint32_t>(hist, hist, (uint64_t)kRadixBins * ntiles, scan32, st);
+    k_radix_scatter<<<ntiles, kThreads, 0, st>>>(keys, vals, keys2, vals2, n, shift, hist, ntiles);
+    std::swap(keys, keys2);
+    std::swap(vals, vals2);
+  }
+  std::string err = check("device BVH sort");
+  if (!err.empty()) return err;
+
+  // Clustering rounds.
+  k_leaves<<<grid_for(n), kThreads, 0, st>>>(vals, plo, phi, nd, ca);
+  std::vector<uint32_t> round_begin{0};
+  uint32_t m = n, merged = 0;
+  while (m > 1) {
+    if (round_begin.size() > kMaxRounds) return "device BVH clustering did not converge";
+    const unsigned g = (unsigned)tiles_of(m, kThreads);
+    k_nearest<<<g, kThreads, 0, st>>>(ca, m, nd.lo, nd.hi, nn);
+    k_mark<<<grid_for(m), kThreads, 0, st>>>(nn, m, flags);
+    uint64_t *tot = scan_exclusive<uint64_t>(flags, offs, m, scan64, st);
+    k_compact<<<grid_for(m), kThreads, 0, st>>>(ca, cbuf, m, nn, flags, offs, merged, nd);
+    uint64_t t = 0;
+    cudaError_t e = cudaMemcpyAsync(&t, tot, sizeof t, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return std::string("device BVH clustering: ") + cudaGetErrorString(e);
+    const uint32_t new_m = (uint32_t)(t >> 32), merges = (uint32_t)t;
+    if (merges == 0 || new_m + merges != m) return "device BVH clustering made no progress";
+    merged += merges;
+    round_begin.push_back(merged);
+    m = new_m;
+    std::swap(ca, cbuf);
+  }
+  if (merged != n - 1) return "device BVH clustering left more than one root";
+
+  // Top-down pass, latest round first.
+  const uint32_t root = 2 * n - 2;
+  k_root<<<1, 1, 0, st>>>(nd, root);
+  for (size_t r = round_begin.size() - 1; r >= 1; --r) {
+    const uint32_t v0 = n + round_begin[r - 1], v1 = n + round_begin[r];
+    k_topdown<<<grid_for(v1 - v0), kThreads, 0, st>>>(nd, v0, v1, counters, counters + 1);
+  }
+  k_layout_flags<<<grid_for(n - 1), kThreads, 0, st>>>(nd, flags);
+  uint64_t *tot = scan_exclusive<uint64_t>(flags, offs, n - 1, scan64, st);
+  uint64_t t = 0;
+  uint32_t cnt[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(&t, tot, sizeof t, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, counters, sizeof cnt, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return std::string("device BVH layout: ") + cudaGetErrorString(e);
+  const uint32_t n2 = (uint32_t)(t >> 32), n4 = (uint32_t)t;
+  if (cnt[0] > max_depth_allowed)
+    return "depth " + std::to_string(cnt[0]) + " of the device-built tree exceeds " + std::to_string(max_depth_allowed);
+  if (n2 == 0 || n4 == 0) return "device BVH has no interior node";
+
+  // The tree's own allocation: nodes, four-child nodes, records.
+  const uint64_t off4 = align256((uint64_t)n2 * sizeof(BvhNode));
+  const uint64_t offr = off4 + align256((uint64_t)n4 * sizeof(Bvh4Node));
+  const uint64_t bytes = offr + align256(3ull * n * sizeof(float4));
+  DeviceArena arena;
+  e = cudaMalloc(&arena.base, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    oom = e == cudaErrorMemoryAllocation;
+    return std::string("device allocation of ") + std::to_string(bytes) + " BVH bytes failed: " + cudaGetErrorString(e);
+  }
+  arena.bytes = bytes;
+  uint8_t *base = static_cast<uint8_t *>(arena.base);
+  BvhNode *out2 = reinterpret_cast<BvhNode *>(base);
+  Bvh4Node *out4 = reinterpret_cast<Bvh4Node *>(base + off4);
+  float4 *records = reinterpret_cast<float4 *>(base + offr);
+  k_write_nodes<<<grid_for(n - 1), kThreads, 0, st>>>(nd, offs, out2, out4);
+  k_write_records<<<grid_for(n), kThreads, 0, st>>>(nd, vals, pos, sc.dev.tri_info, sc.dev.materials, records);
+  float root_cost = 0.0f;
+  float4 rb[2];
+  e = cudaMemcpyAsync(&root_cost, nd.cost + root, sizeof root_cost, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&rb[0], nd.lo + root, sizeof(float4), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&rb[1], nd.hi + root, sizeof(float4), cudaMemcpyDeviceToHost, st);
+  DevScene d = sc.dev;
+  d.nodes = out2;
+  d.nodes4 = out4;
+  d.tris = records;
+  d.node_count = n2;
+  d.node4_count = n4;
+  d.max_depth = cnt[0];
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sc.d_desc, &d, sizeof d, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    arena.release();
+    return std::string("device BVH write: ") + cudaGetErrorString(e);
+  }
+  sc.dev = d;
+  sc.bvh_arena.release();
+  sc.bvh_arena = arena;
+  arena.base = nullptr;  // owned by the scene now
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  sc.bvh = BvhBuildStats{};
+  sc.bvh.nodes = n2;
+  sc.bvh.leaves = cnt[1];
+  sc.bvh.max_depth = cnt[0];
+  const float dx = rb[1].x - rb[0].x, dy = rb[1].y - rb[0].y, dz = rb[1].z - rb[0].z;
+  const double ra = (double)dx * dy + (double)dy * dz + (double)dz * dx;
+  sc.bvh.sah_cost = ra > 0.0 ? (double)root_cost / ra : 0.0;
+  sc.bvh.seconds = secs;
+  if (info) {
+    info->iterations = (uint32_t)round_begin.size() - 1;
+    info->ms = 1000.0 * secs;
+  }
+  return "";
+}
+
+}  // namespace ptd

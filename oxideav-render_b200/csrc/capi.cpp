@@ -353,6 +353,9 @@ pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_trac
                   std::vector<Job> &jobs) {
   SceneHost *sc = find_scene(ctx, t->scene_id);
   if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
+  // A finished background host tree replaces the device-built one (no wave
+  // of this batch is queued yet; hits do not depend on the tree).
+  adopt_pending_tree(*sc, ctx->stream, false);
   tracers.push_back(t);
   jobs.push_back(make_job(*t, *sc, t->env.get(), n));
   return PT_OK;
@@ -463,6 +466,8 @@ pt_status autotune_impl(pt_context *ctx, pt_tracer *t, uint32_t samples, TuneCho
   if (!t->have_state) return fail(ctx, PT_ERR_INVALID_ARG, "tracer is not synced");
   SceneHost *sc = find_scene(ctx, t->scene_id);
   if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
+  // Tune on the tree the scene keeps.
+  adopt_pending_tree(*sc, ctx->stream, true);
   return autotune_scene(ctx, t, sc, t->env.get(), samples, best);
 }
 
@@ -697,7 +702,7 @@ pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *
     CK(ctx, cudaSetDevice(ctx->device));
     auto sc = std::make_unique<SceneHost>();
     bool oom = false;
-    std::string err = upload_scene(*desc, *sc, oom);
+    std::string err = upload_scene(*desc, *sc, oom, ctx->bvh_builder, ctx->stream);
     if (!err.empty()) return fail(ctx, oom ? PT_ERR_OOM : PT_ERR_INVALID_ARG, err);
     uint32_t id = ctx->next_id++;
     ctx->scenes[id] = std::move(sc);
@@ -723,7 +728,7 @@ pt_status pt_scene_device_bytes(pt_context *ctx, uint32_t scene_id, uint64_t *by
   if (!ctx || !bytes) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
   SceneHost *s = find_scene(ctx, scene_id);
   if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
-  *bytes = s->arena.bytes;
+  *bytes = s->device_bytes();
   return PT_OK;
 }
 
@@ -745,6 +750,32 @@ pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes
   if (max_depth) *max_depth = s->bvh.max_depth;
   if (sah_cost) *sah_cost = s->bvh.sah_cost;
   if (build_seconds) *build_seconds = s->bvh.seconds;
+  return PT_OK;
+}
+
+pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (builder > PT_BVH_BUILD_DEVICE) return fail(ctx, PT_ERR_INVALID_ARG, "unknown BVH builder");
+  ctx->bvh_builder = (int)builder;
+  return PT_OK;
+}
+
+pt_status pt_scene_bvh_wait(pt_context *ctx, uint32_t scene_id) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  return guard(ctx, [&]() -> pt_status {
+    SceneHost *s = find_scene(ctx, scene_id);
+    if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+    CK(ctx, cudaSetDevice(ctx->device));
+    adopt_pending_tree(*s, ctx->stream, true);
+    return PT_OK;
+  });
+}
+
+pt_status pt_scene_bvh_on_device(pt_context *ctx, uint32_t scene_id, int *on_device) {
+  if (!ctx || !on_device) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  SceneHost *s = find_scene(ctx, scene_id);
+  if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+  *on_device = s->device_bvh ? 1 : 0;
   return PT_OK;
 }
 

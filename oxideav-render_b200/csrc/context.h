@@ -34,6 +34,7 @@ struct pt_context {
   // (default: both kinds).
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   bool material_sort = true;  // bucket each shade queue by material
+  int bvh_builder = ptd::BVH_BUILD_AUTO;  // where pt_scene_upload builds the BVH (ptd::BvhBuilder)
   std::map<uint32_t, ptd::TuneChoice> tuned;  // by scene class (ptd::scene_class)
   // Wavefront waves replayed as CUDA graphs (bounce count << 1 | sort -> exec).
   bool use_graphs = true;

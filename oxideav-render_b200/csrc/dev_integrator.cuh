@@ -181,13 +181,10 @@ PT_DEV void tri_positions(const DevScene &s, uint32_t g, V3 &a, V3 &b, V3 &c) {
   c = ld3(p + 6);
 }
 
-// Integrator::tri_pdf, src/pathtrace.rs:1972-1991.
-PT_DEV float tri_pdf(const DevRequest &rq, uint32_t li, uint32_t g, V3 p, V3 q) {
-  const DevScene &s = *rq.scene;
-  V3 a, b, c;
-  tri_positions(s, g, a, b, c);
-  float sel = (1.0f - rq.p_env) * __ldg(s.em_pmf + li);
-  float omega = triangle_solid_angle(p, a, b, c);
+// Integrator::tri_pdf, src/pathtrace.rs:1972-1991, for emitter li with
+// corners a, b, c whose solid angle seen from p is omega.
+PT_DEV float tri_pdf_omega(const DevRequest &rq, uint32_t li, V3 a, V3 b, V3 c, float omega, V3 p, V3 q) {
+  float sel = (1.0f - rq.p_env) * __ldg(rq.scene->em_pmf + li);
   if (omega >= 1.0e-4f) return sel / omega;
   V3 cr = vcross(vsub(b, a), vsub(c, a));
   float len = sqrtf(vdot(cr, cr));
@@ -197,6 +194,11 @@ PT_DEV float tri_pdf(const DevRequest &rq, uint32_t li, uint32_t g, V3 p, V3 q) 
   float cs = fabsf(vdot(cr, to) / (len * sqrtf(d2)));
   if (cs <= 0.0f) return 0.0f;
   return sel * d2 / (0.5f * len * cs);
+}
+PT_DEV float tri_pdf(const DevRequest &rq, uint32_t li, uint32_t g, V3 p, V3 q) {
+  V3 a, b, c;
+  tri_positions(*rq.scene, g, a, b, c);
+  return tri_pdf_omega(rq, li, a, b, c, triangle_solid_angle(p, a, b, c), p, q);
 }
 
 // Shade vertex k of the path whose extension ray produced (found, hit).
@@ -350,7 +352,10 @@ PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hi
         tri_positions(s, g, a, b, cc);
         bool have_target = false;
         V3 q = vzero();
-        if (triangle_solid_angle(p, a, b, cc) >= 1.0e-4f) {
+        // The solid angle picks the sampling method and is the pdf's
+        // denominator (one evaluation serves both).
+        const float omega = triangle_solid_angle(p, a, b, cc);
+        if (omega >= 1.0e-4f) {
           V3 ld;
           if (sample_spherical_triangle(p, a, b, cc, pl_u[0], pl_u[1], ld)) {
             V3 n = vcross(vsub(b, a), vsub(cc, a));
@@ -388,7 +393,7 @@ PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hi
               float dist = sqrtf(dist2);
               l = vscale(to, 1.0f / dist);
               float cos_l = -vdot(lsurf.ng, l);
-              pl = tri_pdf(rq, li, g, p, q);
+              pl = tri_pdf_omega(rq, li, a, b, cc, omega, p, q);
               if ((cos_l > 0.0f || (lmat.m.double_sided && cos_l < 0.0f)) && pl > 0.0f && isfinite(pl)) {
                 le = emission(s, lmat, g, linfo.y, lb0, lb1, lb2);
                 tmax = fmaxf(dist * (1.0f - 1.0e-4f), 0.0f);

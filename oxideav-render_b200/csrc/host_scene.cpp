@@ -12,6 +12,7 @@
 // SAH-based Bounding Volume Hierarchies", 2007), built in parallel over
 // subtrees, emitted depth-first as two-child nodes.
 #include "host_scene.h"
+#include "bvh_build.h"
 
 #include <algorithm>
 #include <array>
@@ -95,6 +96,8 @@ struct Builder {
   std::vector<BNode> nodes;
   std::atomic<uint32_t> node_count{1};
   std::atomic<uint32_t> max_depth{0};
+  const std::atomic<bool> *cancel = nullptr;  // set: stop splitting
+  bool cancelled() const { return cancel && cancel->load(std::memory_order_relaxed); }
 
   struct Task {
     uint32_t node, begin, end, depth;
@@ -364,7 +367,7 @@ struct Builder {
 
   void local_build(Task t) {
     std::vector<Task> st{t};
-    while (!st.empty()) {
+    while (!st.empty() && !cancelled()) {
       Task cur = st.back();
       st.pop_back();
       Task ch[2];
@@ -386,7 +389,9 @@ struct Builder {
         stack.pop_back();
         ++active;
       }
-      if (t.end - t.begin <= kLocalThreshold) {
+      if (cancelled()) {
+        // Drain: take tasks without splitting them.
+      } else if (t.end - t.begin <= kLocalThreshold) {
         local_build(t);
       } else {
         Task ch[2];
@@ -435,15 +440,17 @@ void pad_box(const float lo[3], const float hi[3], float plo[3], float phi[3]) {
 
 }  // namespace
 
-void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
-               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads) {
+bool build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
+               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads,
+               const std::atomic<bool> *cancel) {
   auto t0 = std::chrono::steady_clock::now();
   out_nodes.clear();
   out_nodes4.clear();
   records.clear();
   stats = BvhBuildStats{};
-  if (tri_count == 0) return;
+  if (tri_count == 0) return true;
   Builder b;
+  b.cancel = cancel;
   b.pos = pos;
   b.n = tri_count;
   b.prims.resize(tri_count);
@@ -460,6 +467,7 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   }
   b.wide = std::max(1, threads);
   b.run(std::max(1, threads));
+  if (b.cancelled()) return false;
 
   // Depth-first two-child layout.
   auto leaf_ref = [](uint32_t first, uint32_t count) { return (int)~(first | (count << 27)); };
@@ -607,6 +615,7 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   }
   stats.sah_cost = cost;
   stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return true;
 }
 
 // ============================================================ arena
@@ -720,7 +729,7 @@ void build_mips(const pt_texture &img, bool srgb, MipChain &out) {
 }  // namespace
 
 // ============================================================ scene upload
-std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh) {
   using clk = std::chrono::steady_clock;
   const auto t_start = clk::now();
   auto since = [](clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); };
@@ -849,7 +858,7 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   img.seconds[1] = since(t_start);
   const auto t_bvh = clk::now();
-  build_bvh(pos.data(), tc, rec_flags.data(), nodes, nodes4, records, img.bvh, threads);
+  if (with_bvh) build_bvh(pos.data(), tc, rec_flags.data(), nodes, nodes4, records, img.bvh, threads);
   img.seconds[2] = since(t_bvh);
   const auto t_after = clk::now();
 
@@ -1003,6 +1012,10 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img) {
   img.desc_off = plan.offsets[p_desc];
   img.tri_count = tc;
   img.light_count = desc.light_count;
+  if (!with_bvh) {
+    img.bvh_pos = std::move(pos);
+    img.bvh_flags = std::move(rec_flags);
+  }
   img.seconds[3] = since(t_after);
   img.seconds[0] = since(t_start);
   return "";
@@ -1067,8 +1080,42 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
   return "";
 }
 
-std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
+std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder, cudaStream_t stream) {
   oom = false;
+  uint64_t tris = 0;
+  for (uint32_t i = 0; desc.items && i < desc.item_count; ++i) tris += desc.items[i].triangle_count;
+  const bool device = builder == BVH_BUILD_DEVICE || (builder == BVH_BUILD_AUTO && tris >= kAutoDeviceBuildTris);
+  if (device && tris >= 64) {
+    SceneImage img;
+    std::string err = build_scene_image(desc, img, false);
+    if (!err.empty()) return err;
+    err = commit_scene(img, out, oom);
+    if (!err.empty()) return err;
+    err = device_build_bvh(out, stream, kMaxTreeDepth, oom);
+    if (err.empty()) {
+      out.device_bvh = true;
+      if (builder == BVH_BUILD_AUTO) {
+        auto p = std::make_shared<PendingTree>();
+        p->pos = std::move(img.bvh_pos);
+        p->flags = std::move(img.bvh_flags);
+        const uint32_t tc = (uint32_t)out.tri_count;
+        const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        PendingTree *raw = p.get();
+        p->th = std::thread([raw, tc, threads] {
+          raw->ok = build_bvh(raw->pos.data(), tc, raw->flags.data(), raw->nodes, raw->nodes4, raw->records,
+                              raw->stats, threads, &raw->cancel);
+          raw->pos = std::vector<float>();
+          raw->flags = std::vector<uint32_t>();
+          raw->done.store(true, std::memory_order_release);
+        });
+        out.pending = std::move(p);
+      }
+      return "";
+    }
+    release_scene(out);
+    if (err.rfind("depth", 0) != 0) return err;
+    oom = false;
+  }
   SceneImage img;
   std::string err = build_scene_image(desc, img);
   if (!err.empty()) return err;
@@ -1076,8 +1123,65 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom) {
 }
 
 void release_scene(SceneHost &s) {
+  s.pending.reset();
   s.arena.release();
+  s.bvh_arena.release();
   s.d_desc = nullptr;
+  s.device_bvh = false;
+}
+
+PendingTree::~PendingTree() {
+  cancel.store(true);
+  if (th.joinable()) th.join();
+}
+
+bool adopt_pending_tree(SceneHost &sc, cudaStream_t stream, bool wait) {
+  if (!sc.pending) return false;
+  PendingTree &p = *sc.pending;
+  if (!wait && !p.done.load(std::memory_order_acquire)) return false;
+  if (p.th.joinable()) p.th.join();
+  if (!p.ok || p.nodes.empty() || p.nodes4.empty() || sc.d_desc == nullptr) {
+    sc.pending.reset();
+    return false;
+  }
+  auto al = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+  const uint64_t b2 = p.nodes.size() * sizeof(BvhNode), b4 = p.nodes4.size() * sizeof(Bvh4Node);
+  const uint64_t br = p.records.size() * sizeof(float4);
+  const uint64_t off4 = al(b2), offr = off4 + al(b4), total = offr + al(br);
+  DeviceArena a;
+  if (cudaStreamSynchronize(stream) != cudaSuccess || cudaMalloc(&a.base, total) != cudaSuccess) {
+    cudaGetLastError();
+    a.base = nullptr;
+    sc.pending.reset();
+    return false;
+  }
+  a.bytes = total;
+  uint8_t *base = static_cast<uint8_t *>(a.base);
+  DevScene d = sc.dev;
+  d.nodes = reinterpret_cast<const BvhNode *>(base);
+  d.nodes4 = reinterpret_cast<const Bvh4Node *>(base + off4);
+  d.tris = reinterpret_cast<const float4 *>(base + offr);
+  d.node_count = (uint32_t)p.nodes.size();
+  d.node4_count = (uint32_t)p.nodes4.size();
+  d.max_depth = p.stats.max_depth;
+  cudaError_t e = cudaMemcpy(base, p.nodes.data(), b2, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(base + off4, p.nodes4.data(), b4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(base + offr, p.records.data(), br, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(sc.d_desc, &d, sizeof d, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    // The descriptor still points at the device tree (its copy is last).
+    cudaGetLastError();
+    a.release();
+    sc.pending.reset();
+    return false;
+  }
+  sc.bvh_arena.release();
+  sc.bvh_arena = a;
+  sc.dev = d;
+  sc.bvh = p.stats;
+  sc.device_bvh = false;
+  sc.pending.reset();
+  return true;
 }
 
 // ============================================================ environment

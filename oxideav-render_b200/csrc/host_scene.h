@@ -5,8 +5,10 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <memory>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -23,8 +25,10 @@ struct BvhBuildStats {
 // as two-child 64-byte nodes, as the same tree collapsed to four-child
 // 128-byte nodes, plus 48-byte leaf-ordered triangle records shared by both.
 // `rec_flags[g]` goes into each record (REC_* bits).
-void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &nodes,
-               std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads);
+// Returns false (outputs unspecified) when `cancel` became true mid-build.
+bool build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &nodes,
+               std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads,
+               const std::atomic<bool> *cancel = nullptr);
 
 // One device allocation holding a scene (or an environment) plus the
 // device copy of its descriptor. `stream` non-null: the allocation is
@@ -57,6 +61,10 @@ struct HostBlob {
 
 struct SceneImage {
   HostBlob blob;
+  // Without a BVH (build_scene_image with_bvh false): the soup positions
+  // and record flags a host build needs.
+  std::vector<float> bvh_pos;
+  std::vector<uint32_t> bvh_flags;
   DevScene rel{};
   uint64_t desc_off = 0;
   uint64_t tri_count = 0;
@@ -67,24 +75,63 @@ struct SceneImage {
   double seconds[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
+// The host binned-SAH tree of a scene whose first tree was built on the
+// device, built on host threads in the background. The destructor cancels
+// a build still running and joins it.
+struct PendingTree {
+  std::thread th;
+  std::atomic<bool> done{false}, cancel{false};
+  bool ok = false;
+  std::vector<float> pos;
+  std::vector<uint32_t> flags;
+  std::vector<BvhNode> nodes;
+  std::vector<Bvh4Node> nodes4;
+  std::vector<float4> records;
+  BvhBuildStats stats;
+  ~PendingTree();
+};
+
 struct SceneHost {
-  DevScene dev{};           // pointers into `arena`
+  DevScene dev{};           // pointers into `arena` (and `bvh_arena`)
   DevScene *d_desc = nullptr;
   DeviceArena arena;
+  DeviceArena bvh_arena;    // nodes and records of a device-built BVH
   uint64_t tri_count = 0;
   BvhBuildStats bvh;
   uint32_t light_count = 0;
+  bool device_bvh = false;  // the BVH was built on the GPU
+  std::shared_ptr<PendingTree> pending;  // host tree on its way (BVH_BUILD_AUTO)
+  uint64_t device_bytes() const { return arena.bytes + bvh_arena.bytes; }
 };
 
 // Validates `desc` and builds its device image on the host. Returns an
-// empty string on success, else an error message.
-std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img);
+// empty string on success, else an error message. `with_bvh` false leaves
+// the BVH parts out (node counts 0) for a build on the device.
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh = true);
 // Allocates the arena and copies `img` into it (stream-ordered when `stream`
 // is non-null). `oom` is set when the failure was a device allocation.
 std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaStream_t stream = nullptr);
-// build_scene_image + commit_scene.
-std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom);
+// Deepest leaf a tree may have: the traversal stacks hold 64 two-child
+// entries and 3 * 56 + 8 four-child entries.
+constexpr uint32_t kMaxTreeDepth = 56;
+// Where upload_scene builds the BVH.
+// BVH_BUILD_AUTO: scenes of at least kAutoDeviceBuildTris triangles get a
+// device-built tree at once and the host binned-SAH tree (fewer node visits
+// per ray) in the background, adopted by adopt_pending_tree; smaller scenes
+// build on the host.
+enum BvhBuilder : int { BVH_BUILD_AUTO = 0, BVH_BUILD_HOST = 1, BVH_BUILD_DEVICE = 2 };
+constexpr uint64_t kAutoDeviceBuildTris = 16384;
+// build_scene_image + commit_scene, with the BVH built where `builder`
+// says (`stream`: the device build's stream). A device-built tree deeper
+// than the traversal stacks allow is rebuilt on the host.
+std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder = BVH_BUILD_HOST,
+                         cudaStream_t stream = nullptr);
 void release_scene(SceneHost &s);
+// Replaces the device-built tree of `sc` by its finished background host
+// tree (waiting for it when `wait`). Synchronises `stream` first, so no
+// queued wave still reads the old tree. Returns true when a tree was
+// adopted; a failed allocation keeps the device tree.
+bool adopt_pending_tree(SceneHost &sc, cudaStream_t stream, bool wait);
 
 struct EnvHost {
   DevEnv dev{};

@@ -255,7 +255,7 @@ Admit make_resident(pt_server *s, const std::shared_ptr<SceneEntry> &e, std::uni
     err = msg;
     return Admit::Failed;
   }
-  e->dev_bytes = dev->arena.bytes + (env_dev ? env_dev->arena.bytes : 0);
+  e->dev_bytes = dev->device_bytes() + (env_dev ? env_dev->arena.bytes : 0);
   e->est_bytes = e->dev_bytes;
   e->dev = std::move(dev);
   e->env_dev = std::move(env_dev);

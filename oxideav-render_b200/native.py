@@ -75,6 +75,9 @@ SIGNATURES = {
     "pt_server_release": (i32, [vp, u64]),
     "pt_server_stats_get": (i32, [vp, C.POINTER(abi.pt_server_stats)]),
     # include/pt_b200_debug.h
+    "pt_set_bvh_builder": (i32, [vp, u32]),
+    "pt_scene_bvh_on_device": (i32, [vp, u32, C.POINTER(C.c_int)]),
+    "pt_scene_bvh_wait": (i32, [vp, u32]),
     "pt_debug_sobol": (i32, [vp, u32, u32, fp]),
     "pt_debug_pattern": (i32, [vp, u32, u32, fp]),
     "pt_debug_primary_hits": (i32, [vp, u32, u32p, fp]),

@@ -80,6 +80,9 @@ def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
         scene, opts = ts.alpha_planes(), ts.pt_opts(48, 8, 4)
     else:
         scene, opts = ts.dispersive_sphere(1.0), ts.pt_opts(48, 8, 8)
+    # Host-built trees throughout: the traversal counts below compare
+    # schedules on one tree.
+    ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST)
     a, ra, ta = _accum_with(ctx, 0, scene, opts, env)
     try:
         # The wavefront on the two-child layout: the same tree, visited at
@@ -105,6 +108,7 @@ def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
     finally:
         ctx.set_node_width(4, 4)
         ctx.set_material_sort(True)
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
 
 
 def test_sync_resets_only_on_radiance_changes(ctx):

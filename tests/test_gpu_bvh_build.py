@@ -1,0 +1,152 @@
+"""Device-built BVHs (pt_set_bvh_builder): a scene whose tree is built on the
+GPU renders the same accumulator, bit for bit, as with the host-built tree
+(closest hit = smallest t, ties to the lowest global id, so hits do not
+depend on the tree), on both schedules and both node layouts, and the tree
+respects the traversal stacks' depth limit. Under AUTO a scene starts on its
+device tree and switches to the background host tree between refines."""
+import numpy as np
+import pytest
+
+from oxideav_render_b200 import abi, api, testscenes as ts
+from oxideav_render_b200.options import PathTraceOptions
+from oxideav_render_b200.scene import Primitive
+
+pytestmark = pytest.mark.gpu
+
+
+def with_cloud(scene, tris: int, seed: int, center, size: float):
+    """`scene` plus `tris` small diffuse triangles in a cube around `center`
+    (enough triangles for the device builder, inside the camera's view)."""
+    rng = np.random.default_rng(seed)
+    m = scene.add_material(ts.diffuse_material((0.6, 0.6, 0.6), 1.0))
+    c = np.asarray(center, np.float32) + (rng.random((tris, 1, 3)) - 0.5) * size
+    d = rng.normal(size=(tris, 3, 3))
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    pos = (c + d * rng.uniform(0.003, 0.03, (tris, 1, 1))).astype(np.float32).reshape(-1, 3)
+    scene.add_primitive(Primitive(np.ascontiguousarray(pos), material=m))
+    return scene
+
+
+def case(name):
+    if name == "spheres":
+        return ts.sphere_grid_c1(64, 2) + (None,)
+    if name == "soup":
+        return ts.random_soup(30000, seed=11), ts.pt_opts(48, 2, 6), None
+    if name == "materials":
+        return ts.material_extensions(), ts.pt_opts(48, 2, 6), None
+    if name == "env":
+        env = ts.env_noise(64, 32, np.random.default_rng(4))
+        return with_cloud(ts.area_light_scene(0.35, 0.5), 3000, 1, (0, 0, 0), 1.0), ts.pt_opts(40, 4, 4), env
+    if name == "alpha":
+        return with_cloud(ts.alpha_planes(), 2000, 2, (0, 0, -0.5), 1.5), ts.pt_opts(40, 4, 4), None
+    if name == "dispersion":
+        return ts.dispersive_sphere(1.0), ts.pt_opts(40, 4, 8), None
+    raise KeyError(name)
+
+
+def render(ctx, builder, scene, opts, env, schedule):
+    ctx.set_bvh_builder(builder)
+    ctx.set_schedule(schedule)
+    try:
+        t = api.PathTracer(ctx)
+        if env is not None:
+            t.set_environment(api.EnvironmentMap(env))
+        t.sync(scene, opts)
+        t.refine(opts.path_trace.samples_per_pixel)
+        sid = t._scene_id
+        out = t.accum(), t.ray_counts(), ctx.bvh_stats(sid), ctx.bvh_on_device(sid)
+        t.close()
+        return out
+    finally:
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
+        ctx.set_schedule(0)
+
+
+@pytest.mark.parametrize("name", ["spheres", "soup", "materials", "env", "alpha", "dispersion"])
+def test_device_tree_renders_identically(ctx, name):
+    scene, opts, env = case(name)
+    a, ra, sa, da = render(ctx, abi.PT_BVH_BUILD_HOST, scene, opts, env, 0)
+    assert not da
+    for schedule in (0, 1):
+        b, rb, sb, db = render(ctx, abi.PT_BVH_BUILD_DEVICE, scene, opts, env, schedule)
+        assert db, "scene not built on the device"
+        assert np.array_equal(a, b), (name, schedule)
+        assert ra == rb
+        assert 0 < sb["max_depth"] <= 56 and sb["nodes"] > 0 and sb["leaves"] > 0
+        assert sb["build_seconds"] > 0.0
+    try:
+        # The two-child layout of the device tree, for both ray kinds.
+        ctx.set_node_width(2, 2)
+        c, rc, _, _ = render(ctx, abi.PT_BVH_BUILD_DEVICE, scene, opts, env, 1)
+        assert np.array_equal(a, c) and rc == ra
+    finally:
+        ctx.set_node_width(4, 4)
+
+
+def test_builder_selection(ctx):
+    # Tiny scenes stay on the host even when the device builder is asked for;
+    # AUTO builds large scenes on the device.
+    small, o = ts.cornell_c0()
+    o = o.replace(width=16, height=16, path_trace=PathTraceOptions(samples_per_pixel=1, max_bounces=2))
+    assert not render(ctx, abi.PT_BVH_BUILD_DEVICE, small, o, None, 1)[3]
+    big = ts.random_soup(20000, seed=3)
+    assert render(ctx, abi.PT_BVH_BUILD_AUTO, big, ts.pt_opts(8, 1, 2), None, 1)[3]
+    assert not render(ctx, abi.PT_BVH_BUILD_AUTO, ts.random_soup(2000, seed=3), ts.pt_opts(8, 1, 2), None, 1)[3]
+    with pytest.raises(api.RenderError) as ei:
+        ctx.set_bvh_builder(7)
+    assert ei.value.status == abi.PT_ERR_INVALID_ARG
+
+
+def test_device_tree_is_deterministic(ctx):
+    scene = ts.random_soup(50000, seed=5)
+    desc = scene.to_desc(ts.pt_opts(8, 1, 1))
+    ctx.set_bvh_builder(abi.PT_BVH_BUILD_DEVICE)
+    try:
+        stats = []
+        for _ in range(2):
+            sid = ctx.upload(desc)
+            assert ctx.bvh_on_device(sid)
+            st = ctx.bvh_stats(sid)
+            stats.append((st["nodes"], st["leaves"], st["max_depth"], st["sah_cost"], ctx.scene_bytes(sid)))
+            ctx.release(sid)
+        assert stats[0] == stats[1]
+    finally:
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
+
+
+def test_auto_switches_to_the_host_tree_between_refines(ctx):
+    scene, opts = ts.sphere_grid_c1(48, 6)
+    ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST)
+    try:
+        ref = api.PathTracer(ctx)
+        ref.sync(scene, opts)
+        ref.refine(6)
+        want = ref.accum()
+        ref.close()
+    finally:
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
+    t = api.PathTracer(ctx)
+    t.sync(scene, opts)
+    sid = t._scene_id
+    assert ctx.bvh_on_device(sid)
+    t.refine(2)  # on the device tree (or the host one, if it was already done)
+    ctx.bvh_wait(sid)
+    assert not ctx.bvh_on_device(sid)
+    st = ctx.bvh_stats(sid)
+    assert 0 < st["max_depth"] <= 64 and st["nodes"] > 0
+    t.refine(4)
+    assert np.array_equal(t.accum(), want)
+    t.close()
+
+
+def test_release_while_the_host_tree_builds(ctx):
+    # Releasing (or replacing) a scene cancels its background build.
+    desc = ts.random_soup(400000, seed=8).to_desc(ts.pt_opts(8, 1, 1))
+    for _ in range(3):
+        sid = ctx.upload(desc)
+        assert ctx.bvh_on_device(sid)
+        ctx.release(sid)
+    sid = ctx.upload(desc)
+    ctx.bvh_wait(sid)
+    assert not ctx.bvh_on_device(sid)
+    ctx.release(sid)
