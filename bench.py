@@ -599,7 +599,8 @@ def run_b200(args):
         t2 = time.perf_counter()
         e2e["host_ms"] = {"flatten": 1000 * (t1 - t0), "prepare_and_upload": 1000 * (t2 - t1),
                           "bvh_build": 1000 * ctx.bvh_stats(sid)["build_seconds"],
-                          "bvh_on_device": ctx.bvh_on_device(sid)}
+                          "bvh_on_device": ctx.bvh_on_device(sid),
+                          "upload_phases": {k: 1000 * v for k, v in ctx.upload_seconds(sid).items()}}
         ctx.release(sid)
     mixed = None
     if args.mixed > 0:

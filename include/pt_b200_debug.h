@@ -51,7 +51,8 @@ PT_API pt_status pt_set_wave_graphs(pt_context *ctx, int on);
 
 /* Builds a scene's device image on the host only (validation, textures,
  * BVH, tables; no GPU needed) and reports its host time in seconds:
- * {total, tables before the BVH, BVH build, tables after it + the image},
+ * {total, tables (textures and mips, materials, lights, emissive tables),
+ * BVH build, the image fill (corner streams and tables copied into place)},
  * and the device bytes the scene would occupy. */
 PT_API pt_status pt_debug_prepare_scene(const pt_scene_desc *desc, double seconds[4], uint64_t *device_bytes);
 
@@ -101,6 +102,17 @@ typedef enum pt_bvh_builder {
 PT_API pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder);
 /* 1 when the scene's current BVH was built on the device. */
 PT_API pt_status pt_scene_bvh_on_device(pt_context *ctx, uint32_t scene_id, int *on_device);
+/* Host wall time in seconds of the scene's pt_scene_upload: [0] the host
+ * image (validation, attribute streams, materials, texture mips, tables,
+ * and the host BVH when built there), [1] device allocation + copy, [2] the
+ * device BVH build (0 when built on the host), [3] total. */
+PT_API pt_status pt_scene_upload_seconds(pt_context *ctx, uint32_t scene_id, double seconds[4]);
+/* The scene's texel pool as generated on the device: for each texture in
+ * order, for each mip level, the sRGB-decoded level then the linear level
+ * (RGBA f32). Copies at most `capacity` texels to `out` (may be NULL) and
+ * reports the pool's texel count in `total`. */
+PT_API pt_status pt_debug_scene_texels(pt_context *ctx, uint32_t scene_id, float *out, uint64_t capacity,
+                                       uint64_t *total);
 /* Waits for the scene's background host tree (BVH_BUILD_AUTO) and switches
  * the scene to it; PT_OK at once when none is pending. */
 PT_API pt_status pt_scene_bvh_wait(pt_context *ctx, uint32_t scene_id);

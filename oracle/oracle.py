@@ -51,6 +51,7 @@ def lib():
                 "oracle_surface": (None, [vp, u32, fp, fp, fp, fp]),
                 "oracle_material_base": (None, [vp, u32, fp, fp]),
                 "oracle_texture_sample": (None, [vp, f32, f32, f32, i32, fp, u32p, fp]),
+                "oracle_texture_mips": (C.c_uint64, [vp, i32, fp, C.c_uint64]),
                 "oracle_emissive_table": (None, [vp, u32p, C.POINTER(u32p), C.POINTER(fp), C.POINTER(fp)]),
                 "oracle_sobol_owen_4d": (None, [u32, u32, fp]),
                 "oracle_sobol": (u32, [u32, u32]),
@@ -287,6 +288,20 @@ def texture_sample(pixels: np.ndarray, sampler, u: float, v: float, lod: float, 
     lib().oracle_texture_sample(C.addressof(t), u, v, lod, 1 if srgb else 0, out.ctypes.data_as(C.POINTER(C.c_float)),
                                 C.byref(levels), top.ctypes.data_as(C.POINTER(C.c_float)))
     return out, levels.value, top
+
+
+def texture_mips(pixels: np.ndarray, srgb: bool) -> np.ndarray:
+    """Every level of one mip chain (build_mips), concatenated, (n, 4) f32."""
+    a = _abi()
+    px = np.ascontiguousarray(pixels)
+    fmt = a.PT_PIXELS_RGBA8 if px.dtype == np.uint8 else a.PT_PIXELS_RGBA_F32
+    if fmt == a.PT_PIXELS_RGBA_F32:
+        px = np.ascontiguousarray(px, dtype=np.float32)
+    t = a.pt_texture(px.shape[1], px.shape[0], fmt, px.ctypes.data, 0, 0, 0, 0)
+    n = lib().oracle_texture_mips(C.addressof(t), 1 if srgb else 0, None, 0)
+    out = np.zeros((n, 4), np.float32)
+    lib().oracle_texture_mips(C.addressof(t), 1 if srgb else 0, out.ctypes.data_as(C.POINTER(C.c_float)), n)
+    return out
 
 
 def sobol_owen_4d(index: int, seed: int) -> np.ndarray:

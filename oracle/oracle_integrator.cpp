@@ -709,6 +709,29 @@ void oracle_texture_sample(const pt_texture *t, float u, float v, float lod, int
     for (int k = 0; k < 4; ++k) top[k] = mips.back().texels[0][k];
 }
 
+// Every level of one chain of a texture (build_mips, src/texture.rs:324-383),
+// concatenated level by level as RGBA f32; returns the texel count and
+// writes at most `cap` texels.
+uint64_t oracle_texture_mips(const pt_texture *t, int srgb, float *out, uint64_t cap) {
+  pt_material m{};
+  m.base_color_texture.texture = -1;
+  pt_scene_desc d{};
+  d.material_count = 1;
+  d.materials = &m;
+  d.texture_count = 1;
+  d.textures = t;
+  Scene sc(d);
+  const std::vector<MipLevel> &mips = sc.textures[0]->mips(srgb != 0);
+  uint64_t n = 0;
+  for (const MipLevel &lv : mips)
+    for (const auto &px : lv.texels) {
+      if (n < cap)
+        for (int k = 0; k < 4; ++k) out[4 * n + k] = px[k];
+      ++n;
+    }
+  return n;
+}
+
 void oracle_sobol_owen_4d(uint32_t index, uint32_t seed, float out[4]) { sobol_owen_4d(index, seed, out); }
 uint32_t oracle_sobol(uint32_t index, uint32_t dim) { return sobol(index, (int)dim); }
 void oracle_sampler_pattern(uint32_t seed, uint32_t x, uint32_t y, uint32_t index, uint32_t pattern, float out[4]) {

@@ -79,6 +79,21 @@ class Context:
         """pt_set_bvh_builder: abi.PT_BVH_BUILD_AUTO / _HOST / _DEVICE."""
         self.check(self.lib.pt_set_bvh_builder(self.ptr, builder))
 
+    def upload_seconds(self, scene_id: int) -> dict:
+        """pt_scene_upload_seconds: where the scene's upload time went."""
+        s = (C.c_double * 4)()
+        self.check(self.lib.pt_scene_upload_seconds(self.ptr, scene_id, s))
+        return {"host_image": s[0], "device_copy": s[1], "device_bvh": s[2], "total": s[3]}
+
+    def scene_texels(self, scene_id: int) -> np.ndarray:
+        """pt_debug_scene_texels: the scene's device texel pool, (n, 4) f32."""
+        total = C.c_uint64()
+        self.check(self.lib.pt_debug_scene_texels(self.ptr, scene_id, None, 0, C.byref(total)))
+        out = np.zeros((total.value, 4), np.float32)
+        self.check(self.lib.pt_debug_scene_texels(self.ptr, scene_id, out.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  total.value, C.byref(total)))
+        return out
+
     def bvh_wait(self, scene_id: int) -> None:
         """pt_scene_bvh_wait: switch the scene to its background host tree."""
         self.check(self.lib.pt_scene_bvh_wait(self.ptr, scene_id))

@@ -760,6 +760,30 @@ pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder) {
   return PT_OK;
 }
 
+pt_status pt_scene_upload_seconds(pt_context *ctx, uint32_t scene_id, double seconds[4]) {
+  if (!ctx || !seconds) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  SceneHost *s = find_scene(ctx, scene_id);
+  if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+  for (int k = 0; k < 4; ++k) seconds[k] = s->upload_seconds[k];
+  return PT_OK;
+}
+
+pt_status pt_debug_scene_texels(pt_context *ctx, uint32_t scene_id, float *out, uint64_t capacity, uint64_t *total) {
+  if (!ctx || !total) return fail(ctx, PT_ERR_INVALID_ARG, "NULL argument");
+  return guard(ctx, [&]() -> pt_status {
+    SceneHost *s = find_scene(ctx, scene_id);
+    if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
+    *total = s->pool_texels;
+    const uint64_t n = std::min(capacity, s->pool_texels);
+    if (n && out) {
+      CK(ctx, cudaSetDevice(ctx->device));
+      CK(ctx, cudaStreamSynchronize(ctx->stream));
+      CK(ctx, cudaMemcpy(out, s->dev.texels, n * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
+    return PT_OK;
+  });
+}
+
 pt_status pt_scene_bvh_wait(pt_context *ctx, uint32_t scene_id) {
   if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
   return guard(ctx, [&]() -> pt_status {
@@ -993,7 +1017,7 @@ pt_status pt_debug_prepare_scene(const pt_scene_desc *desc, double seconds[4], u
     std::string err = build_scene_image(*desc, img);
     if (!err.empty()) return fail(nullptr, PT_ERR_INVALID_ARG, err);
     for (int k = 0; k < 4; ++k) seconds[k] = img.seconds[k];
-    if (device_bytes) *device_bytes = img.blob.size();
+    if (device_bytes) *device_bytes = img.device_bytes();
     return PT_OK;
   });
 }

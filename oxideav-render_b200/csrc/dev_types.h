@@ -64,6 +64,10 @@ struct DevTexture {
   uint32_t mag, min, wrap_s, wrap_t, pad;
   uint32_t lw[kMaxMipLevels], lh[kMaxMipLevels];
   uint64_t srgb_off[kMaxMipLevels], lin_off[kMaxMipLevels];  // texel offsets into the pool
+  // The uploaded source texels the chains are generated from: byte offset
+  // in the scene's source-texel part, PT_PIXELS_* format.
+  uint64_t src_off;
+  uint32_t src_format, pad2;
 };
 
 // pt_material plus values the host precomputes so the device never

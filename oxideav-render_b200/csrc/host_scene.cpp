@@ -13,6 +13,7 @@
 // subtrees, emitted depth-first as two-child nodes.
 #include "host_scene.h"
 #include "bvh_build.h"
+#include "mip_build.h"
 
 #include <algorithm>
 #include <array>
@@ -21,6 +22,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <numeric>
 #include <thread>
@@ -747,35 +749,34 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
   if (T >= (1ull << 27)) return "scene has " + std::to_string(T) + " triangles; the limit is 134217727";
   const uint32_t tc = (uint32_t)T;
 
-  // Textures: mip chains in one texel pool.
+  // Textures: each chain's level sizes and texel offsets in the pool (the
+  // pool itself is generated on the device from the source texels).
   std::vector<DevTexture> texs(desc.texture_count);
-  std::vector<float4> pool;
   std::vector<bool> tex_ok(desc.texture_count, false);
+  uint64_t pool_texels = 0, src_bytes = 0;
   for (uint32_t i = 0; i < desc.texture_count; ++i) {
     const pt_texture &t = desc.textures[i];
     DevTexture &d = texs[i];
     std::memset(&d, 0, sizeof d);
     if (!t.pixels || t.width == 0 || t.height == 0) continue;
     if (t.format > PT_PIXELS_RGBA_F32) return "texture " + std::to_string(i) + " has an unknown pixel format";
-    MipChain s, l;
-    build_mips(t, true, s);
-    build_mips(t, false, l);
-    if (s.levels.size() > (size_t)kMaxMipLevels) return "texture " + std::to_string(i) + " is too large";
+    if (mip_levels(t.width, t.height) > (uint32_t)kMaxMipLevels) return "texture " + std::to_string(i) + " is too large";
     d.img_w = t.width;
     d.img_h = t.height;
-    d.levels = (uint32_t)s.levels.size();
+    d.levels = mip_levels(t.width, t.height, d.lw, d.lh, kMaxMipLevels);
     d.mag = t.mag_filter;
     d.min = t.min_filter;
     d.wrap_s = t.wrap_s;
     d.wrap_t = t.wrap_t;
     for (uint32_t k = 0; k < d.levels; ++k) {
-      d.lw[k] = s.w[k];
-      d.lh[k] = s.h[k];
-      d.srgb_off[k] = pool.size();
-      pool.insert(pool.end(), s.levels[k].begin(), s.levels[k].end());
-      d.lin_off[k] = pool.size();
-      pool.insert(pool.end(), l.levels[k].begin(), l.levels[k].end());
+      const uint64_t n = (uint64_t)d.lw[k] * d.lh[k];
+      d.srgb_off[k] = pool_texels;
+      d.lin_off[k] = pool_texels + n;
+      pool_texels += 2 * n;
     }
+    d.src_format = t.format;
+    d.src_off = src_bytes;
+    src_bytes += ((uint64_t)t.width * t.height * (t.format == PT_PIXELS_RGBA8 ? 4 : 16) + 15) & ~uint64_t(15);
     tex_ok[i] = true;
   }
   auto fix_binding = [&](pt_texture_binding &b) {
@@ -803,64 +804,18 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
     dm.emissive_nonblack = (dm.m.emissive[0] > 0.0f || dm.m.emissive[1] > 0.0f || dm.m.emissive[2] > 0.0f) ? 1u : 0u;
   }
 
-  // Attribute streams by global triangle id.
+  // Which optional corner streams the scene has, and each item's first
+  // global triangle id.
   bool any_vn = false, any_tan = false, any_col = false, any_uv[PT_MAX_UV_SETS] = {false, false, false, false};
+  std::vector<uint64_t> first_tri(desc.item_count + 1, 0);
   for (uint32_t i = 0; i < desc.item_count; ++i) {
     const pt_draw_item &it = desc.items[i];
     any_vn |= it.normals && it.has_vertex_normals;
     any_tan |= it.tangents != nullptr;
     any_col |= it.colors != nullptr;
     for (int s = 0; s < PT_MAX_UV_SETS; ++s) any_uv[s] |= it.uvs[s] != nullptr;
+    first_tri[i + 1] = first_tri[i] + it.triangle_count;
   }
-  std::vector<float> pos(9 * (size_t)tc), nrm(any_vn ? 9 * (size_t)tc : 0), tan(any_tan ? 12 * (size_t)tc : 0),
-      col(any_col ? 12 * (size_t)tc : 0);
-  std::vector<float> uv[PT_MAX_UV_SETS];
-  for (int s = 0; s < PT_MAX_UV_SETS; ++s)
-    if (any_uv[s]) uv[s].assign(6 * (size_t)tc, 0.0f);
-  std::vector<uint2> info(tc);
-  std::vector<uint32_t> rec_flags(tc);
-  size_t g0 = 0;
-  for (uint32_t i = 0; i < desc.item_count; ++i) {
-    const pt_draw_item &it = desc.items[i];
-    size_t n = it.triangle_count;
-    std::memcpy(pos.data() + 9 * g0, it.positions, 36 * n);
-    uint32_t flags = 0;
-    if (it.normals && it.has_vertex_normals) {
-      std::memcpy(nrm.data() + 9 * g0, it.normals, 36 * n);
-      flags |= TRI_HAS_VN;
-    }
-    if (it.tangents) {
-      std::memcpy(tan.data() + 12 * g0, it.tangents, 48 * n);
-      flags |= TRI_HAS_TANGENTS;
-    }
-    if (it.colors) {
-      std::memcpy(col.data() + 12 * g0, it.colors, 48 * n);
-      flags |= TRI_HAS_COLORS;
-    }
-    for (int s = 0; s < PT_MAX_UV_SETS; ++s)
-      if (it.uvs[s]) {
-        std::memcpy(uv[s].data() + 6 * g0, it.uvs[s], 24 * n);
-        flags |= TRI_UV0 << s;
-      }
-    const pt_material &mm = desc.materials[it.material];
-    uint32_t rf = (mm.alpha_mode == PT_ALPHA_OPAQUE ? REC_OPAQUE : 0u) | (mm.double_sided ? REC_DOUBLE_SIDED : 0u);
-    for (size_t t = 0; t < n; ++t) {
-      info[g0 + t] = make_uint2(it.material, flags);
-      rec_flags[g0 + t] = rf;
-    }
-    g0 += n;
-  }
-
-  // BVH.
-  std::vector<BvhNode> nodes;
-  std::vector<Bvh4Node> nodes4;
-  std::vector<float4> records;
-  int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  img.seconds[1] = since(t_start);
-  const auto t_bvh = clk::now();
-  if (with_bvh) build_bvh(pos.data(), tc, rec_flags.data(), nodes, nodes4, records, img.bvh, threads);
-  img.seconds[2] = since(t_bvh);
-  const auto t_after = clk::now();
 
   // Lights.
   std::vector<DevLight> lights(desc.light_count);
@@ -870,8 +825,15 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
     lights[j].cos_inner = std::cos(desc.lights[j].inner_cone_angle);
   }
 
-  // EmissiveLights::build.
+  // EmissiveLights::build: the mean emitted radiance of each material, then
+  // every emitting triangle of positive area (read from the items' own
+  // position arrays) in global id order.
+  // An emissive texture's mean is its 1x1 colour level, built here on the
+  // host for the textures bound as emission (the same texels the device
+  // chain holds).
   std::vector<float> mean_e(3 * (size_t)desc.material_count);
+  std::vector<float4> tex_mean(desc.texture_count);
+  std::vector<bool> have_mean(desc.texture_count, false);
   for (uint32_t m = 0; m < desc.material_count; ++m) {
     const pt_material &mt = mats[m].m;
     float e[3] = {0.0f, 0.0f, 0.0f};
@@ -881,8 +843,13 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
       e[2] = mt.emissive[2];
       int ti = mt.emissive_texture.texture;
       if (ti >= 0) {
-        const DevTexture &d = texs[ti];
-        const float4 &c = pool[d.srgb_off[d.levels - 1]];
+        if (!have_mean[ti]) {
+          MipChain s;
+          build_mips(desc.textures[ti], true, s);
+          tex_mean[ti] = s.levels.back()[0];
+          have_mean[ti] = true;
+        }
+        const float4 &c = tex_mean[ti];
         e[0] = e[0] * c.x;
         e[1] = e[1] * c.y;
         e[2] = e[2] * c.z;
@@ -890,109 +857,194 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
     }
     std::memcpy(&mean_e[3 * m], e, sizeof e);
   }
-  std::vector<uint32_t> em_tris, em_lookup(tc, 0xffffffffu);
+  std::vector<uint32_t> em_tris;
   std::vector<float> power;
-  for (uint32_t g = 0; g < tc; ++g) {
-    const float *e = &mean_e[3 * (size_t)info[g].x];
+  for (uint32_t i = 0; i < desc.item_count; ++i) {
+    const pt_draw_item &it = desc.items[i];
+    const float *e = &mean_e[3 * (size_t)it.material];
     float lum = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2];
     if (std::isnan(lum) || lum <= 0.0f) continue;
-    const float *p = pos.data() + 9 * (size_t)g;
-    float e1[3] = {p[3] - p[0], p[4] - p[1], p[5] - p[2]}, e2[3] = {p[6] - p[0], p[7] - p[1], p[8] - p[2]};
-    float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-    float ar = 0.5f * std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-    if (std::isnan(ar) || ar <= 0.0f || !std::isfinite(ar)) continue;
-    float sides = mats[info[g].x].m.double_sided ? 2.0f : 1.0f;
-    em_lookup[g] = (uint32_t)em_tris.size();
-    em_tris.push_back(g);
-    power.push_back(ar * lum * sides);
+    const float sides = mats[it.material].m.double_sided ? 2.0f : 1.0f;
+    for (uint64_t t = 0; t < it.triangle_count; ++t) {
+      const float *p = it.positions + 9 * t;
+      float e1[3] = {p[3] - p[0], p[4] - p[1], p[5] - p[2]}, e2[3] = {p[6] - p[0], p[7] - p[1], p[8] - p[2]};
+      float cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      float ar = 0.5f * std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      if (std::isnan(ar) || ar <= 0.0f || !std::isfinite(ar)) continue;
+      em_tris.push_back((uint32_t)(first_tri[i] + t));
+      power.push_back(ar * lum * sides);
+    }
   }
-  double total = 0.0;
-  for (float p : power) total += (double)p;
+  double total_power = 0.0;
+  for (float p : power) total_power += (double)p;
   std::vector<float> pmf, cdf;
   double acc = 0.0;
   for (float pw : power) {
-    pmf.push_back((float)((double)pw / total));
-    acc += (double)pw / total;
+    pmf.push_back((float)((double)pw / total_power));
+    acc += (double)pw / total_power;
     cdf.push_back((float)acc);
   }
   if (!cdf.empty()) cdf.back() = 1.0f;
+  img.seconds[1] = since(t_start);
 
-  // One arena.
-  ArenaPlan plan;
-  size_t p_nodes = plan.add(nodes.data(), nodes.size() * sizeof(BvhNode));
-  size_t p_nodes4 = plan.add(nodes4.data(), nodes4.size() * sizeof(Bvh4Node));
-  size_t p_rec = plan.add(records.data(), records.size() * sizeof(float4));
-  size_t p_info = plan.add(info.data(), info.size() * sizeof(uint2));
-  size_t p_pos = plan.add(pos.data(), pos.size() * 4);
-  size_t p_nrm = plan.add(nrm.data(), nrm.size() * 4);
-  size_t p_tan = plan.add(tan.data(), tan.size() * 4);
-  size_t p_col = plan.add(col.data(), col.size() * 4);
-  size_t p_uv[PT_MAX_UV_SETS];
-  for (int s = 0; s < PT_MAX_UV_SETS; ++s) p_uv[s] = plan.add(uv[s].data(), uv[s].size() * 4);
-  size_t p_mat = plan.add(mats.data(), mats.size() * sizeof(DevMaterial));
-  size_t p_tex = plan.add(texs.data(), texs.size() * sizeof(DevTexture));
-  size_t p_pool = plan.add(pool.data(), pool.size() * sizeof(float4));
-  size_t p_lights = plan.add(lights.data(), lights.size() * sizeof(DevLight));
-  size_t p_emt = plan.add(em_tris.data(), em_tris.size() * 4);
-  size_t p_pmf = plan.add(pmf.data(), pmf.size() * 4);
-  size_t p_cdf = plan.add(cdf.data(), cdf.size() * 4);
-  size_t p_lookup = plan.add(em_lookup.data(), em_lookup.size() * 4);
-  DevScene tmp{};
-  size_t p_desc = plan.add(&tmp, sizeof(DevScene));
-  {
-    // Each part lands at its offset; the gaps (alignment padding, the
-    // descriptor slot and the tail) are zeroed. Copies run on several
-    // threads in slices of at most 16 MiB (first touch of the pages included).
-    const size_t total = std::max<size_t>(plan.total, 256);
-    img.blob.allocate(total);
-    uint8_t *dst = img.blob.data();
-    struct Piece {
-      size_t off, bytes;
-      const uint8_t *src;  // nullptr: zero fill
-    };
-    std::vector<Piece> pieces;
-    const size_t kSlice = size_t(16) << 20;
-    auto add = [&](size_t off, size_t bytes, const uint8_t *src) {
-      for (size_t o = 0; o < bytes; o += kSlice)
-        pieces.push_back({off + o, std::min(kSlice, bytes - o), src ? src + o : nullptr});
-    };
-    size_t cursor = 0;
-    for (size_t i = 0; i < plan.parts.size(); ++i) {
-      const size_t off = plan.offsets[i], bytes = plan.parts[i].second;
-      if (off > cursor) add(cursor, off - cursor, nullptr);
-      if (bytes) add(off, bytes, static_cast<const uint8_t *>(plan.parts[i].first));
-      cursor = off + bytes;
+  // The arena plan: every part's offset (256-byte aligned) from its size.
+  struct Plan {
+    std::vector<size_t> off, bytes;
+    size_t total = 0;
+    size_t add(size_t b) {
+      size_t o = (total + 255) & ~(size_t)255;
+      off.push_back(o);
+      bytes.push_back(b);
+      total = o + b;
+      return off.size() - 1;
     }
-    if (total > cursor) add(cursor, total - cursor, nullptr);
+  } plan;
+  const size_t p_info = plan.add(T * sizeof(uint2));
+  const size_t p_pos = plan.add(T * 36);
+  const size_t p_nrm = plan.add(any_vn ? T * 36 : 0);
+  const size_t p_tan = plan.add(any_tan ? T * 48 : 0);
+  const size_t p_col = plan.add(any_col ? T * 48 : 0);
+  size_t p_uv[PT_MAX_UV_SETS];
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s) p_uv[s] = plan.add(any_uv[s] ? T * 24 : 0);
+  const size_t p_mat = plan.add(mats.size() * sizeof(DevMaterial));
+  const size_t p_tex = plan.add(texs.size() * sizeof(DevTexture));
+  const size_t p_src = plan.add(src_bytes);
+  const size_t p_lights = plan.add(lights.size() * sizeof(DevLight));
+  const size_t p_emt = plan.add(em_tris.size() * 4);
+  const size_t p_pmf = plan.add(pmf.size() * 4);
+  const size_t p_cdf = plan.add(cdf.size() * 4);
+  const size_t p_lookup = plan.add(T * 4);
+  const size_t p_desc = plan.add(sizeof(DevScene));
+  // The texel pool comes last and exists on the device only: the host
+  // image ends where it starts.
+  const size_t p_pool = plan.add(pool_texels * sizeof(float4));
+  const size_t total = std::max<size_t>(plan.off[p_pool], 256);
+  const auto t_fill = clk::now();
+  const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  img.blob.allocate(total);
+  uint8_t *const dst = img.blob.data();
+  std::vector<uint32_t> rec_flags(T);
+
+  // Fill: every byte of the blob is written once, by tasks spread over
+  // threads (copies in slices of at most 16 MiB, first touch included).
+  std::vector<std::function<void()>> tasks;
+  const size_t kSlice = size_t(16) << 20;
+  auto copy_task = [&](size_t off, const void *src, size_t bytes) {
+    for (size_t o = 0; o < bytes; o += kSlice) {
+      const size_t b = std::min(kSlice, bytes - o);
+      const uint8_t *s = src ? static_cast<const uint8_t *>(src) + o : nullptr;
+      tasks.push_back([dst, off, o, s, b] {
+        if (s)
+          std::memcpy(dst + off + o, s, b);
+        else
+          std::memset(dst + off + o, 0, b);
+      });
+    }
+  };
+  {
+    size_t cursor = 0;  // zero the alignment gaps and the tail
+    for (size_t k = 0; k < p_pool; ++k) {
+      if (plan.off[k] > cursor) copy_task(cursor, nullptr, plan.off[k] - cursor);
+      cursor = plan.off[k] + plan.bytes[k];
+    }
+    if (total > cursor) copy_task(cursor, nullptr, total - cursor);
+  }
+  copy_task(plan.off[p_mat], mats.data(), plan.bytes[p_mat]);
+  copy_task(plan.off[p_tex], texs.data(), plan.bytes[p_tex]);
+  for (uint32_t i = 0; i < desc.texture_count; ++i)
+    if (tex_ok[i]) {
+      const pt_texture &tx = desc.textures[i];
+      const size_t b = (size_t)tx.width * tx.height * (tx.format == PT_PIXELS_RGBA8 ? 4 : 16);
+      copy_task(plan.off[p_src] + texs[i].src_off, tx.pixels, b);
+    }
+  copy_task(plan.off[p_lights], lights.data(), plan.bytes[p_lights]);
+  copy_task(plan.off[p_emt], em_tris.data(), plan.bytes[p_emt]);
+  copy_task(plan.off[p_pmf], pmf.data(), plan.bytes[p_pmf]);
+  copy_task(plan.off[p_cdf], cdf.data(), plan.bytes[p_cdf]);
+  copy_task(plan.off[p_desc], nullptr, plan.bytes[p_desc]);
+  // Corner streams by global triangle id: each item's array, or zeros for
+  // an item without it.
+  for (uint32_t i = 0; i < desc.item_count; ++i) {
+    const pt_draw_item &it = desc.items[i];
+    const size_t g0 = first_tri[i], n = it.triangle_count;
+    copy_task(plan.off[p_pos] + 36 * g0, it.positions, 36 * n);
+    if (any_vn) copy_task(plan.off[p_nrm] + 36 * g0, it.normals && it.has_vertex_normals ? it.normals : nullptr, 36 * n);
+    if (any_tan) copy_task(plan.off[p_tan] + 48 * g0, it.tangents, 48 * n);
+    if (any_col) copy_task(plan.off[p_col] + 48 * g0, it.colors, 48 * n);
+    for (int s = 0; s < PT_MAX_UV_SETS; ++s)
+      if (any_uv[s]) copy_task(plan.off[p_uv[s]] + 24 * g0, it.uvs[s], 24 * n);
+    // (material, attribute flags) and the record flags of its triangles.
+    uint32_t flags = 0;
+    if (it.normals && it.has_vertex_normals) flags |= TRI_HAS_VN;
+    if (it.tangents) flags |= TRI_HAS_TANGENTS;
+    if (it.colors) flags |= TRI_HAS_COLORS;
+    for (int s = 0; s < PT_MAX_UV_SETS; ++s)
+      if (it.uvs[s]) flags |= TRI_UV0 << s;
+    const pt_material &mm = desc.materials[it.material];
+    const uint32_t rf = (mm.alpha_mode == PT_ALPHA_OPAQUE ? REC_OPAQUE : 0u) | (mm.double_sided ? REC_DOUBLE_SIDED : 0u);
+    const uint2 inf = make_uint2(it.material, flags);
+    uint2 *info = reinterpret_cast<uint2 *>(dst + plan.off[p_info]);
+    uint32_t *rec = rec_flags.data();
+    const size_t kTris = size_t(1) << 20;
+    for (size_t a = 0; a < n; a += kTris) {
+      const size_t b = std::min(n, a + kTris);
+      tasks.push_back([info, rec, inf, rf, g0, a, b] {
+        for (size_t t = a; t < b; ++t) {
+          info[g0 + t] = inf;
+          rec[g0 + t] = rf;
+        }
+      });
+    }
+  }
+  // Emissive lookup by global id: "none" everywhere, then the emitters.
+  {
+    uint32_t *lookup = reinterpret_cast<uint32_t *>(dst + plan.off[p_lookup]);
+    const size_t kTris = size_t(4) << 20;
+    for (size_t a = 0; a < T; a += kTris) {
+      const size_t b = std::min(T, a + kTris);
+      tasks.push_back([lookup, a, b] { std::fill(lookup + a, lookup + b, 0xffffffffu); });
+    }
+  }
+  {
     std::atomic<size_t> next{0};
     auto work = [&] {
-      for (size_t k; (k = next.fetch_add(1)) < pieces.size();) {
-        const Piece &pc = pieces[k];
-        if (pc.src)
-          std::memcpy(dst + pc.off, pc.src, pc.bytes);
-        else
-          std::memset(dst + pc.off, 0, pc.bytes);
-      }
+      for (size_t k; (k = next.fetch_add(1)) < tasks.size();) tasks[k]();
     };
-    const int nt = (int)std::min<size_t>(pieces.size(), (size_t)threads);
-    std::vector<std::thread> pool;
-    for (int k = 1; k < nt; ++k) pool.emplace_back(work);
+    const int nt = (int)std::min<size_t>(tasks.size(), (size_t)threads);
+    std::vector<std::thread> pool_threads;
+    for (int k = 1; k < nt; ++k) pool_threads.emplace_back(work);
     work();
-    for (auto &th : pool) th.join();
+    for (auto &th : pool_threads) th.join();
   }
-  // Pointer fields hold offset + 1 until commit_scene rebases them.
-  auto rel = [&](size_t part, size_t bytes) -> uintptr_t { return bytes ? (uintptr_t)plan.offsets[part] + 1 : 0; };
+  {
+    uint32_t *lookup = reinterpret_cast<uint32_t *>(dst + plan.off[p_lookup]);
+    for (size_t k = 0; k < em_tris.size(); ++k) lookup[em_tris[k]] = (uint32_t)k;
+  }
+  img.seconds[3] = since(t_fill);
+
+  // BVH (host build) from the positions now in the blob.
+  const auto t_bvh = clk::now();
+  const float *pos = reinterpret_cast<const float *>(dst + plan.off[p_pos]);
+  if (with_bvh) build_bvh(pos, tc, rec_flags.data(), img.tree.nodes, img.tree.nodes4, img.tree.records, img.bvh, threads);
+  img.seconds[2] = since(t_bvh);
+  img.pos_off = plan.off[p_pos];
+  img.textures = texs;
+  img.tex_src_off = plan.off[p_src];
+  img.pool_off = plan.off[p_pool];
+  img.pool_bytes = plan.bytes[p_pool];
+  if (!with_bvh) img.rec_flags = std::move(rec_flags);
+
+  // Pointer fields hold offset + 1 until commit_scene rebases them; the
+  // tree's are set when it is committed.
+  auto rel = [&](size_t part, size_t bytes) -> uintptr_t { return bytes ? (uintptr_t)plan.off[part] + 1 : 0; };
   DevScene &d = img.rel;
   std::memset(&d, 0, sizeof d);
-  d.nodes = (const BvhNode *)rel(p_nodes, 1);
-  d.nodes4 = (const Bvh4Node *)rel(p_nodes4, nodes4.size());
-  d.tris = (const float4 *)rel(p_rec, 1);
   d.tri_info = (const uint2 *)rel(p_info, 1);
   d.pos = (const float *)rel(p_pos, 1);
-  d.nrm = (const float *)rel(p_nrm, nrm.size());
-  d.tan = (const float *)rel(p_tan, tan.size());
-  d.col = (const float *)rel(p_col, col.size());
-  for (int s = 0; s < PT_MAX_UV_SETS; ++s) d.uv[s] = (const float *)rel(p_uv[s], uv[s].size());
+  d.nrm = (const float *)rel(p_nrm, plan.bytes[p_nrm]);
+  d.tan = (const float *)rel(p_tan, plan.bytes[p_tan]);
+  d.col = (const float *)rel(p_col, plan.bytes[p_col]);
+  for (int s = 0; s < PT_MAX_UV_SETS; ++s) d.uv[s] = (const float *)rel(p_uv[s], plan.bytes[p_uv[s]]);
   d.materials = (const DevMaterial *)rel(p_mat, 1);
   d.textures = (const DevTexture *)rel(p_tex, 1);
   d.texels = (const float4 *)rel(p_pool, 1);
@@ -1001,36 +1053,72 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
   d.em_pmf = (const float *)rel(p_pmf, 1);
   d.em_cdf = (const float *)rel(p_cdf, 1);
   d.em_lookup = (const uint32_t *)rel(p_lookup, 1);
-  d.node_count = (uint32_t)nodes.size();
-  d.node4_count = (uint32_t)nodes4.size();
   d.tri_count = tc;
   d.material_count = desc.material_count;
   d.texture_count = desc.texture_count;
   d.light_count = desc.light_count;
   d.em_count = (uint32_t)em_tris.size();
-  d.max_depth = img.bvh.max_depth;
-  img.desc_off = plan.offsets[p_desc];
+  img.desc_off = plan.off[p_desc];
   img.tri_count = tc;
   img.light_count = desc.light_count;
-  if (!with_bvh) {
-    img.bvh_pos = std::move(pos);
-    img.bvh_flags = std::move(rec_flags);
-  }
-  img.seconds[3] = since(t_after);
   img.seconds[0] = since(t_start);
   return "";
 }
 
-namespace {
-template <class T>
-void rebase(const T *&p, uint8_t *base) {
-  p = p ? reinterpret_cast<const T *>(base + (reinterpret_cast<uintptr_t>(p) - 1)) : nullptr;
+uint64_t HostTree::bytes() const {
+  auto al = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+  return al(nodes.size() * sizeof(BvhNode)) + al(nodes4.size() * sizeof(Bvh4Node)) + al(records.size() * sizeof(float4));
 }
+
+namespace {
+
+template <class P>
+void rebase(const P *&p, uint8_t *base) {
+  p = p ? reinterpret_cast<const P *>(base + (reinterpret_cast<uintptr_t>(p) - 1)) : nullptr;
+}
+
+// Allocates `a` for `t` and copies it (stream-ordered when `stream` is
+// non-null), pointing d's tree fields into it.
+std::string commit_tree(const HostTree &t, uint32_t max_depth, DeviceArena &a, DevScene &d, bool &oom,
+                        cudaStream_t stream) {
+  auto al = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+  const uint64_t b2 = t.nodes.size() * sizeof(BvhNode), b4 = t.nodes4.size() * sizeof(Bvh4Node);
+  const uint64_t br = t.records.size() * sizeof(float4);
+  const uint64_t off4 = al(b2), offr = off4 + al(b4), total = std::max<uint64_t>(offr + al(br), 256);
+  cudaError_t e = stream ? cudaMallocAsync(&a.base, total, stream) : cudaMalloc(&a.base, total);
+  if (e != cudaSuccess) {
+    oom = e == cudaErrorMemoryAllocation;
+    a.base = nullptr;
+    cudaGetLastError();
+    return std::string("device allocation of ") + std::to_string(total) + " BVH bytes failed: " + cudaGetErrorString(e);
+  }
+  a.bytes = total;
+  a.stream = stream;
+  uint8_t *base = static_cast<uint8_t *>(a.base);
+  const void *src[3] = {t.nodes.data(), t.nodes4.data(), t.records.data()};
+  const uint64_t off[3] = {0, off4, offr}, len[3] = {b2, b4, br};
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+    if (len[k])
+      e = stream ? cudaMemcpyAsync(base + off[k], src[k], len[k], cudaMemcpyHostToDevice, stream)
+                 : cudaMemcpy(base + off[k], src[k], len[k], cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    a.release();
+    return std::string("BVH upload failed: ") + cudaGetErrorString(e);
+  }
+  d.nodes = t.nodes.empty() ? nullptr : reinterpret_cast<const BvhNode *>(base);
+  d.nodes4 = t.nodes4.empty() ? nullptr : reinterpret_cast<const Bvh4Node *>(base + off4);
+  d.tris = reinterpret_cast<const float4 *>(base + offr);
+  d.node_count = (uint32_t)t.nodes.size();
+  d.node4_count = (uint32_t)t.nodes4.size();
+  d.max_depth = max_depth;
+  return "";
+}
+
 }  // namespace
 
 std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaStream_t stream) {
   oom = false;
-  const size_t total = img.blob.size();
+  const size_t total = std::max<uint64_t>(img.blob.size(), img.pool_off + img.pool_bytes);
   cudaError_t e = stream ? cudaMallocAsync(&out.arena.base, total, stream) : cudaMalloc(&out.arena.base, total);
   if (e != cudaSuccess) {
     oom = e == cudaErrorMemoryAllocation;
@@ -1042,9 +1130,6 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
   out.arena.stream = stream;
   uint8_t *base = static_cast<uint8_t *>(out.arena.base);
   DevScene d = img.rel;
-  rebase(d.nodes, base);
-  rebase(d.nodes4, base);
-  rebase(d.tris, base);
   rebase(d.tri_info, base);
   rebase(d.pos, base);
   rebase(d.nrm, base);
@@ -1059,22 +1144,50 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
   rebase(d.em_pmf, base);
   rebase(d.em_cdf, base);
   rebase(d.em_lookup, base);
-  out.dev = d;
   out.d_desc = reinterpret_cast<DevScene *>(base + img.desc_off);
-  if (stream) {
-    // Pageable sources: both calls return once the bytes are staged, and
-    // the copies run in the stream's order (before any later wave).
-    e = cudaMemcpyAsync(base, img.blob.data(), total, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice, stream);
-  } else {
-    e = cudaMemcpy(base, img.blob.data(), total, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice);
-  }
+  // Pageable sources: the copies return once the bytes are staged, and run
+  // in the stream's order (before any later wave).
+  e = stream ? cudaMemcpyAsync(base, img.blob.data(), img.blob.size(), cudaMemcpyHostToDevice, stream)
+             : cudaMemcpy(base, img.blob.data(), img.blob.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     out.arena.release();
     return std::string("scene upload failed: ") + cudaGetErrorString(e);
   }
+  if (img.pool_bytes) {
+    static float decode[256];
+    static bool init = [] {
+      for (int i = 0; i < 256; ++i) decode[i] = host_srgb_to_linear((float)i / 255.0f);
+      return true;
+    }();
+    (void)init;
+    std::string err = device_build_mips(img.textures, d.textures, base + img.tex_src_off,
+                                        reinterpret_cast<float4 *>(base + img.pool_off), decode, stream);
+    // Without a stream the commit is synchronous: the chains are done when
+    // it returns (later work may run on any stream).
+    if (err.empty() && !stream && cudaStreamSynchronize(nullptr) != cudaSuccess)
+      err = std::string("mip generation failed: ") + cudaGetErrorString(cudaGetLastError());
+    if (!err.empty()) {
+      out.arena.release();
+      return err;
+    }
+  }
+  if (!img.tree.nodes.empty()) {
+    std::string err = commit_tree(img.tree, img.bvh.max_depth, out.bvh_arena, d, oom, stream);
+    if (!err.empty()) {
+      out.arena.release();
+      return err;
+    }
+  }
+  e = stream ? cudaMemcpyAsync(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice, stream)
+             : cudaMemcpy(out.d_desc, &d, sizeof(DevScene), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    out.arena.release();
+    out.bvh_arena.release();
+    return std::string("scene upload failed: ") + cudaGetErrorString(e);
+  }
+  out.dev = d;
   out.tri_count = img.tri_count;
+  out.pool_texels = img.pool_bytes / sizeof(float4);
   out.bvh = img.bvh;
   out.light_count = img.light_count;
   return "";
@@ -1082,6 +1195,9 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
 
 std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder, cudaStream_t stream) {
   oom = false;
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
   uint64_t tris = 0;
   for (uint32_t i = 0; desc.items && i < desc.item_count; ++i) tris += desc.items[i].triangle_count;
   const bool device = builder == BVH_BUILD_DEVICE || (builder == BVH_BUILD_AUTO && tris >= kAutoDeviceBuildTris);
@@ -1089,22 +1205,33 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
     SceneImage img;
     std::string err = build_scene_image(desc, img, false);
     if (!err.empty()) return err;
+    const auto t1 = clk::now();
     err = commit_scene(img, out, oom);
     if (!err.empty()) return err;
+    const auto t2 = clk::now();
     err = device_build_bvh(out, stream, kMaxTreeDepth, oom);
     if (err.empty()) {
+      const auto t3 = clk::now();
+      out.upload_seconds[0] = secs(t0, t1);
+      out.upload_seconds[1] = secs(t1, t2);
+      out.upload_seconds[2] = secs(t2, t3);
+      out.upload_seconds[3] = secs(t0, t3);
       out.device_bvh = true;
       if (builder == BVH_BUILD_AUTO) {
+        // The host tree, built from the positions in the (now uploaded)
+        // host image, which the background build keeps alive.
         auto p = std::make_shared<PendingTree>();
-        p->pos = std::move(img.bvh_pos);
-        p->flags = std::move(img.bvh_flags);
+        p->blob = std::move(img.blob);
+        p->pos_off = img.pos_off;
+        p->flags = std::move(img.rec_flags);
         const uint32_t tc = (uint32_t)out.tri_count;
         const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
         PendingTree *raw = p.get();
         p->th = std::thread([raw, tc, threads] {
-          raw->ok = build_bvh(raw->pos.data(), tc, raw->flags.data(), raw->nodes, raw->nodes4, raw->records,
+          const float *pos = reinterpret_cast<const float *>(raw->blob.data() + raw->pos_off);
+          raw->ok = build_bvh(pos, tc, raw->flags.data(), raw->tree.nodes, raw->tree.nodes4, raw->tree.records,
                               raw->stats, threads, &raw->cancel);
-          raw->pos = std::vector<float>();
+          raw->blob = HostBlob();
           raw->flags = std::vector<uint32_t>();
           raw->done.store(true, std::memory_order_release);
         });
@@ -1117,9 +1244,17 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
     oom = false;
   }
   SceneImage img;
+  const auto t1 = clk::now();
   std::string err = build_scene_image(desc, img);
   if (!err.empty()) return err;
-  return commit_scene(img, out, oom);
+  const auto t2 = clk::now();
+  err = commit_scene(img, out, oom);
+  const auto t3 = clk::now();
+  out.upload_seconds[0] = secs(t1, t2);
+  out.upload_seconds[1] = secs(t2, t3);
+  out.upload_seconds[2] = 0.0;
+  out.upload_seconds[3] = secs(t0, t3);
+  return err;
 }
 
 void release_scene(SceneHost &s) {
@@ -1140,38 +1275,23 @@ bool adopt_pending_tree(SceneHost &sc, cudaStream_t stream, bool wait) {
   PendingTree &p = *sc.pending;
   if (!wait && !p.done.load(std::memory_order_acquire)) return false;
   if (p.th.joinable()) p.th.join();
-  if (!p.ok || p.nodes.empty() || p.nodes4.empty() || sc.d_desc == nullptr) {
-    sc.pending.reset();
-    return false;
-  }
-  auto al = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
-  const uint64_t b2 = p.nodes.size() * sizeof(BvhNode), b4 = p.nodes4.size() * sizeof(Bvh4Node);
-  const uint64_t br = p.records.size() * sizeof(float4);
-  const uint64_t off4 = al(b2), offr = off4 + al(b4), total = offr + al(br);
-  DeviceArena a;
-  if (cudaStreamSynchronize(stream) != cudaSuccess || cudaMalloc(&a.base, total) != cudaSuccess) {
+  if (!p.ok || p.tree.nodes.empty() || p.tree.nodes4.empty() || sc.d_desc == nullptr ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
     cudaGetLastError();
-    a.base = nullptr;
     sc.pending.reset();
     return false;
   }
-  a.bytes = total;
-  uint8_t *base = static_cast<uint8_t *>(a.base);
+  DeviceArena a;
   DevScene d = sc.dev;
-  d.nodes = reinterpret_cast<const BvhNode *>(base);
-  d.nodes4 = reinterpret_cast<const Bvh4Node *>(base + off4);
-  d.tris = reinterpret_cast<const float4 *>(base + offr);
-  d.node_count = (uint32_t)p.nodes.size();
-  d.node4_count = (uint32_t)p.nodes4.size();
-  d.max_depth = p.stats.max_depth;
-  cudaError_t e = cudaMemcpy(base, p.nodes.data(), b2, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(base + off4, p.nodes4.data(), b4, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(base + offr, p.records.data(), br, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(sc.d_desc, &d, sizeof d, cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
+  bool oom = false;
+  std::string err = commit_tree(p.tree, p.stats.max_depth, a, d, oom, nullptr);
+  if (err.empty() && cudaMemcpy(sc.d_desc, &d, sizeof d, cudaMemcpyHostToDevice) != cudaSuccess) {
     // The descriptor still points at the device tree (its copy is last).
     cudaGetLastError();
     a.release();
+    err = "descriptor update failed";
+  }
+  if (!err.empty()) {
     sc.pending.reset();
     return false;
   }

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <memory>
@@ -41,11 +42,12 @@ struct DeviceArena {
 };
 
 // A scene fully prepared on the host: the exact bytes of its device arena
-// (BVH nodes, triangle records, attribute streams, materials, texel pool,
-// lights, emissive tables) plus a descriptor whose pointer fields hold
-// arena offsets + 1 (0 = absent). Uploading it is one allocation and one
-// copy, so an evicted scene comes back without another BVH build.
-// Uninitialised host bytes (a scene image is written part by part; only the
+// (attribute streams, materials, texel pool, lights, emissive tables), its
+// BVH (nodes and triangle records, a second device allocation) and a
+// descriptor whose pointer fields hold arena offsets + 1 (0 = absent).
+// Uploading it is two allocations and a few copies, so an evicted scene
+// comes back without another BVH build.
+// Uninitialised host bytes (a scene image is written part by part; the
 // alignment gaps are zeroed).
 struct HostBlob {
   std::unique_ptr<uint8_t[]> p;
@@ -59,19 +61,34 @@ struct HostBlob {
   size_t size() const { return n; }
 };
 
+// A BVH in its device layouts, in host memory.
+struct HostTree {
+  std::vector<BvhNode> nodes;
+  std::vector<Bvh4Node> nodes4;
+  std::vector<float4> records;
+  uint64_t bytes() const;  // of its device allocation
+};
+
 struct SceneImage {
-  HostBlob blob;
-  // Without a BVH (build_scene_image with_bvh false): the soup positions
-  // and record flags a host build needs.
-  std::vector<float> bvh_pos;
-  std::vector<uint32_t> bvh_flags;
+  HostBlob blob;   // everything but the BVH
+  HostTree tree;   // empty when built without a BVH
+  uint64_t pos_off = 0;  // the soup positions' offset in `blob`
+  // Textures: the table (as in the blob), the source texels' offset in the
+  // blob, and the device-only texel pool that follows the blob in the arena
+  // (its mip chains are generated on the device at commit).
+  std::vector<DevTexture> textures;
+  uint64_t tex_src_off = 0, pool_off = 0, pool_bytes = 0;
+  uint64_t device_bytes() const { return std::max<uint64_t>(blob.size(), pool_off + pool_bytes) + tree.bytes(); }
+  // Without a BVH: the record flags a later host build needs.
+  std::vector<uint32_t> rec_flags;
   DevScene rel{};
   uint64_t desc_off = 0;
   uint64_t tri_count = 0;
   BvhBuildStats bvh;
   uint32_t light_count = 0;
-  // Host time of build_scene_image: total, tables before the BVH (textures,
-  // materials, attribute streams), BVH build, tables after it and the blob.
+  // Host time of build_scene_image: total, tables (textures and their mips,
+  // materials, lights, emissive tables), BVH build, the blob fill (corner
+  // streams and tables copied into place).
   double seconds[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
@@ -82,11 +99,10 @@ struct PendingTree {
   std::thread th;
   std::atomic<bool> done{false}, cancel{false};
   bool ok = false;
-  std::vector<float> pos;
+  HostBlob blob;         // the scene's host image (its positions)
+  uint64_t pos_off = 0;
   std::vector<uint32_t> flags;
-  std::vector<BvhNode> nodes;
-  std::vector<Bvh4Node> nodes4;
-  std::vector<float4> records;
+  HostTree tree;
   BvhBuildStats stats;
   ~PendingTree();
 };
@@ -97,10 +113,14 @@ struct SceneHost {
   DeviceArena arena;
   DeviceArena bvh_arena;    // nodes and records of a device-built BVH
   uint64_t tri_count = 0;
+  uint64_t pool_texels = 0;  // texels of every mip chain (dev.texels)
   BvhBuildStats bvh;
   uint32_t light_count = 0;
   bool device_bvh = false;  // the BVH was built on the GPU
   std::shared_ptr<PendingTree> pending;  // host tree on its way (BVH_BUILD_AUTO)
+  // Host wall time of upload_scene: host image, arena allocation + copy,
+  // device BVH build, total.
+  double upload_seconds[4] = {0.0, 0.0, 0.0, 0.0};
   uint64_t device_bytes() const { return arena.bytes + bvh_arena.bytes; }
 };
 

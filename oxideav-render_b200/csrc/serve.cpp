@@ -681,7 +681,7 @@ pt_status pt_server_scene_register(pt_server *s, const pt_scene_desc *desc, cons
     auto e = std::make_shared<SceneEntry>();
     std::string err = build_scene_image(*desc, e->img);
     if (!err.empty()) return sfail(PT_ERR_INVALID_ARG, err);
-    e->est_bytes = e->img.blob.size();
+    e->est_bytes = e->img.device_bytes();
     if (env) {
       e->has_env = true;
       e->env = *env;
