@@ -1,0 +1,60 @@
+"""Frame sources over the PathTraceCuda renderer (src/source.rs tests
+:222-313 with this backend): a rendered frame reaches the video plane with
+pixels other than the background, and every frame of an animated source
+equals a direct render of the scene at that frame's time."""
+import numpy as np
+import pytest
+
+from oxideav_render_b200 import api, testscenes as ts
+from oxideav_render_b200.options import BackgroundColor, CameraSpec
+from oxideav_render_b200.scene import PreparedScene, Primitive
+from oxideav_render_b200.source import AnimatedRenderSource, Eof, RenderSource
+
+pytestmark = pytest.mark.gpu
+
+
+def one_triangle(shift: float = 0.0) -> PreparedScene:
+    s = PreparedScene()
+    m = s.add_material(ts.diffuse_material((0.8, 0.3, 0.2), 1.0))
+    tri = np.array([[-0.5 + shift, -0.5, 0.0], [0.5 + shift, -0.5, 0.0], [shift, 0.5, 0.0]], np.float32)
+    s.add_primitive(Primitive(tri, np.array([0, 1, 2], np.uint32), material=m))
+    return s
+
+
+def opts(w=32, h=None):
+    return ts.pt_opts(w, 4, 2, h=h, background=BackgroundColor((255, 255, 255, 255)), scene_camera=None,
+                      camera=CameraSpec(0.0, 0.0, 3.0), ambient=1.0)
+
+
+def test_rendered_frame_has_non_background_pixels(ctx):
+    src = RenderSource(one_triangle(), api.PathTraceCudaRenderer(ctx), opts())
+    f = src.next_frame()
+    px = np.frombuffer(f.planes[0].data, np.uint8).reshape(32, 32, 4)
+    assert f.planes[0].stride == 32 * 4
+    assert np.any(np.any(px != 255, axis=2))
+    with pytest.raises(Eof):
+        src.next_frame()
+
+
+def test_non_square_frames(ctx):
+    src = RenderSource(one_triangle(), api.PathTraceCudaRenderer(ctx), opts(48, 24))
+    f = src.next_frame()
+    assert f.planes[0].stride == 48 * 4 and len(f.planes[0].data) == 48 * 24 * 4
+
+
+def test_animated_frames_equal_direct_renders(ctx):
+    o = opts(40, 24)
+    src = AnimatedRenderSource(lambda t: one_triangle(0.3 * t), api.PathTraceCudaRenderer(ctx), o, frames=3,
+                               fps=(2, 1))
+    frames = []
+    for k in range(3):
+        f = src.next_frame()
+        assert f.pts == k
+        t = k / 2
+        want = api.PathTraceCudaRenderer(ctx).render(one_triangle(0.3 * t), o.replace(time=t))
+        got = np.frombuffer(f.planes[0].data, np.uint8).reshape(24, 40, 4)
+        assert np.array_equal(got, want), k
+        frames.append(got)
+    assert not np.array_equal(frames[0], frames[2])
+    with pytest.raises(Eof):
+        src.next_frame()
