@@ -288,6 +288,8 @@ typedef struct pt_context pt_context;
 
 /* Create a context on CUDA device `device` (one per GPU). */
 PT_API pt_status pt_create(pt_context **out, int device);
+/* Destroys the context and its resident scenes; destroy its tracers first
+ * (a tracer refers to its context). */
 PT_API void pt_destroy(pt_context *ctx);
 /* Message of the last failing call on ctx (or of pt_create when ctx is NULL). */
 PT_API const char *pt_last_error(const pt_context *ctx);

@@ -18,6 +18,7 @@ the camera is `Camera.resolve` of the options, exactly as the reference's
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -39,9 +40,12 @@ class Context:
             raise RenderError(st, (self.lib.pt_last_error(None) or b"").decode())
         self.ptr = p
         self.device = device
+        self._tracers = weakref.WeakSet()  # destroyed before the context
 
     def close(self):
         if getattr(self, "ptr", None):
+            for t in list(self._tracers):
+                t.close()
             self.lib.pt_destroy(self.ptr)
             self.ptr = None
 
@@ -196,6 +200,7 @@ class PathTracer:
         p = C.c_void_p()
         self.ctx.check(self.lib.pt_tracer_create(self.ctx.ptr, C.byref(p)))
         self.ptr = p
+        self.ctx._tracers.add(self)
         self.opts = RenderOptions()
         self._scene = None
         self._scene_key = None
@@ -207,7 +212,8 @@ class PathTracer:
 
     def close(self):
         if getattr(self, "ptr", None):
-            self.lib.pt_tracer_destroy(self.ptr)
+            if self.ctx.ptr:  # a tracer never outlives its context's native object
+                self.lib.pt_tracer_destroy(self.ptr)
             self.ptr = None
         if self._scene_id is not None and self.ctx.ptr:
             self.ctx.release(self._scene_id)

@@ -305,8 +305,19 @@ __global__ void k_leaves(const uint32_t *vals, const float4 *plo, const float4 *
 // Nearest neighbour of every cluster within kPlocRadius positions: the
 // smallest area of the merged box, ties to the lower position. Under that
 // order the globally closest pair is mutual, so every round merges.
-__global__ void __launch_bounds__(kThreads) k_nearest(const uint32_t *clusters, uint32_t m, const float4 *nlo,
+// Clustering state on the device, so rounds run back to back without the
+// host reading the cluster count in between.
+struct PlocState {
+  uint32_t m;        // clusters left
+  uint32_t merged;   // interior nodes created so far
+  uint32_t rounds;   // rounds done (round r created nodes n + round_begin[r-1] ..)
+  uint32_t error;    // a round merged nothing
+};
+
+__global__ void __launch_bounds__(kThreads) k_nearest(const uint32_t *clusters, const PlocState *ps, const float4 *nlo,
                                                       const float4 *nhi, uint32_t *nn) {
+  const uint32_t m = ps->m;
+  if (m <= 1 || (uint64_t)blockIdx.x * kThreads >= m) return;
   __shared__ float4 slo[kThreads + 2 * kPlocRadius], shi[kThreads + 2 * kPlocRadius];
   const int64_t b0 = (int64_t)blockIdx.x * kThreads;
   for (int t = threadIdx.x; t < kThreads + 2 * kPlocRadius; t += kThreads) {
@@ -337,9 +348,15 @@ __global__ void __launch_bounds__(kThreads) k_nearest(const uint32_t *clusters, 
   nn[i] = best_j;
 }
 
-// keep (high word) and merge (low word) flags of every cluster.
-__global__ void k_mark(const uint32_t *nn, uint32_t m, uint64_t *flags) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+// keep (high word) and merge (low word) flags of every cluster; zeros for
+// positions from m up to `bound` (the scan covers the host's bound).
+__global__ void k_mark(const uint32_t *nn, const PlocState *ps, uint32_t bound, uint64_t *flags) {
+  const uint32_t m = ps->m;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < bound; i += gridDim.x * blockDim.x) {
+    if (m <= 1 || i >= m) {
+      flags[i] = 0;
+      continue;
+    }
     uint32_t j = nn[i];
     bool mutual = nn[j] == i;
     uint64_t keep = (mutual && i > j) ? 0u : 1u;
@@ -348,8 +365,10 @@ __global__ void k_mark(const uint32_t *nn, uint32_t m, uint64_t *flags) {
   }
 }
 
-__global__ void k_compact(const uint32_t *clusters, uint32_t *next, uint32_t m, const uint32_t *nn,
-                          const uint64_t *flags, const uint64_t *offs, uint32_t merged_before, Nodes nd) {
+__global__ void k_compact(const uint32_t *clusters, uint32_t *next, const PlocState *ps, const uint32_t *nn,
+                          const uint64_t *flags, const uint64_t *offs, Nodes nd) {
+  const uint32_t m = ps->m, merged_before = ps->merged;
+  if (m <= 1) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
     const uint64_t f = flags[i];
     if (!(f >> 32)) continue;
@@ -376,6 +395,22 @@ __global__ void k_compact(const uint32_t *clusters, uint32_t *next, uint32_t m, 
     nd.child[k] = make_int2((int)a, (int)b);
     next[pos] = v;
   }
+}
+
+// Ends a round: the scan total gives the clusters kept and the merges made.
+__global__ void k_advance(PlocState *ps, const uint64_t *total, uint32_t *round_begin, uint32_t max_rounds) {
+  if (ps->m <= 1 || ps->error) return;
+  const uint64_t t = *total;
+  const uint32_t kept = (uint32_t)(t >> 32), merges = (uint32_t)t;
+  if (merges == 0 || kept + merges != ps->m || ps->rounds >= max_rounds) {
+    ps->error = 1;
+    ps->m = 1;
+    return;
+  }
+  ps->merged += merges;
+  ps->m = kept;
+  ps->rounds += 1;
+  round_begin[ps->rounds] = ps->merged;
 }
 
 // ---------------------------------------------------------------- layouts
@@ -622,6 +657,8 @@ std::string device_build_bvh(SceneHost &sc, cudaStream_t st, uint32_t max_depth_
   uint64_t *flags = s.get<uint64_t>(n), *offs = s.get<uint64_t>(n);
   uint64_t *scan64 = s.get<uint64_t>(scan_scratch_items(n));
   uint32_t *counters = s.get<uint32_t>(2);  // max depth, leaves
+  PlocState *pstate = s.get<PlocState>(1);
+  uint32_t *round_dev = s.get<uint32_t>(kMaxRounds + 1);
   if (!s.err.empty()) {
     oom = s.oom;
     return s.err;
@@ -648,29 +685,37 @@ std::string device_build_bvh(SceneHost &sc, cudaStream_t st, uint32_t max_depth_
   std::string err = check("device BVH sort");
   if (!err.empty()) return err;
 
-  // Clustering rounds.
+  // Clustering rounds, in batches launched back to back; the host reads
+  // the cluster count once per batch (grids are sized by that bound).
   k_leaves<<<grid_for(n), kThreads, 0, st>>>(vals, plo, phi, nd, ca);
-  std::vector<uint32_t> round_begin{0};
-  uint32_t m = n, merged = 0;
-  while (m > 1) {
-    if (round_begin.size() > kMaxRounds) return "device BVH clustering did not converge";
-    const unsigned g = (unsigned)tiles_of(m, kThreads);
-    k_nearest<<<g, kThreads, 0, st>>>(ca, m, nd.lo, nd.hi, nn);
-    k_mark<<<grid_for(m), kThreads, 0, st>>>(nn, m, flags);
-    uint64_t *tot = scan_exclusive<uint64_t>(flags, offs, m, scan64, st);
-    k_compact<<<grid_for(m), kThreads, 0, st>>>(ca, cbuf, m, nn, flags, offs, merged, nd);
-    uint64_t t = 0;
-    cudaError_t e = cudaMemcpyAsync(&t, tot, sizeof t, cudaMemcpyDeviceToHost, st);
+  PlocState init_state{n, 0, 0, 0};
+  cudaMemcpyAsync(pstate, &init_state, sizeof init_state, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(round_dev, 0, sizeof(uint32_t), st);
+  uint32_t bound = n;
+  PlocState hs = init_state;
+  for (uint32_t batch = 0;; ++batch) {
+    const uint32_t per_batch = bound > 65536 ? 4 : 16;
+    for (uint32_t r = 0; r < per_batch; ++r) {
+      k_nearest<<<(unsigned)tiles_of(bound, kThreads), kThreads, 0, st>>>(ca, pstate, nd.lo, nd.hi, nn);
+      k_mark<<<grid_for(bound), kThreads, 0, st>>>(nn, pstate, bound, flags);
+      uint64_t *tot = scan_exclusive<uint64_t>(flags, offs, bound, scan64, st);
+      k_compact<<<grid_for(bound), kThreads, 0, st>>>(ca, cbuf, pstate, nn, flags, offs, nd);
+      k_advance<<<1, 1, 0, st>>>(pstate, tot, round_dev, kMaxRounds);
+      std::swap(ca, cbuf);
+    }
+    cudaError_t e = cudaMemcpyAsync(&hs, pstate, sizeof hs, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return std::string("device BVH clustering: ") + cudaGetErrorString(e);
-    const uint32_t new_m = (uint32_t)(t >> 32), merges = (uint32_t)t;
-    if (merges == 0 || new_m + merges != m) return "device BVH clustering made no progress";
-    merged += merges;
-    round_begin.push_back(merged);
-    m = new_m;
-    std::swap(ca, cbuf);
+    if (hs.error) return "device BVH clustering made no progress";
+    if (hs.m <= 1) break;
+    bound = hs.m;
   }
+  const uint32_t merged = hs.merged;
   if (merged != n - 1) return "device BVH clustering left more than one root";
+  std::vector<uint32_t> round_begin(hs.rounds + 1);
+  if (cudaMemcpy(round_begin.data(), round_dev, round_begin.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return "device BVH clustering: round table read failed";
 
   // Top-down pass, latest round first.
   const uint32_t root = 2 * n - 2;

@@ -690,6 +690,7 @@ void pt_destroy(pt_context *ctx) {
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->staging.release();
   delete ctx;
 }
 
@@ -702,7 +703,7 @@ pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *
     CK(ctx, cudaSetDevice(ctx->device));
     auto sc = std::make_unique<SceneHost>();
     bool oom = false;
-    std::string err = upload_scene(*desc, *sc, oom, ctx->bvh_builder, ctx->stream);
+    std::string err = upload_scene(*desc, *sc, oom, ctx->bvh_builder, ctx->stream, &ctx->staging);
     if (!err.empty()) return fail(ctx, oom ? PT_ERR_OOM : PT_ERR_INVALID_ARG, err);
     uint32_t id = ctx->next_id++;
     ctx->scenes[id] = std::move(sc);

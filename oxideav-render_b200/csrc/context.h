@@ -35,6 +35,7 @@ struct pt_context {
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   bool material_sort = true;  // bucket each shade queue by material
   int bvh_builder = ptd::BVH_BUILD_AUTO;  // where pt_scene_upload builds the BVH (ptd::BvhBuilder)
+  ptd::HostStaging staging;  // pinned host image buffer of pt_scene_upload
   std::map<uint32_t, ptd::TuneChoice> tuned;  // by scene class (ptd::scene_class)
   // Wavefront waves replayed as CUDA graphs (bounce count << 1 | sort -> exec).
   bool use_graphs = true;

@@ -731,7 +731,28 @@ void build_mips(const pt_texture &img, bool srgb, MipChain &out) {
 }  // namespace
 
 // ============================================================ scene upload
-std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh) {
+uint8_t *HostStaging::reserve(size_t bytes) {
+  if (bytes > kMaxStagingBytes) return nullptr;
+  if (bytes <= cap) return p;
+  release();
+  size_t want = std::max(bytes, std::min(kMaxStagingBytes, cap * 2));
+  void *q = nullptr;
+  if (cudaHostAlloc(&q, want, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  p = static_cast<uint8_t *>(q);
+  cap = want;
+  return p;
+}
+
+void HostStaging::release() {
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+}
+
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh, HostStaging *staging) {
   using clk = std::chrono::steady_clock;
   const auto t_start = clk::now();
   auto since = [](clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); };
@@ -921,7 +942,10 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
   const size_t total = std::max<size_t>(plan.off[p_pool], 256);
   const auto t_fill = clk::now();
   const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  img.blob.allocate(total);
+  if (uint8_t *pinned = staging ? staging->reserve(total) : nullptr)
+    img.blob.use(pinned, total);
+  else
+    img.blob.allocate(total);
   uint8_t *const dst = img.blob.data();
   std::vector<uint32_t> rec_flags(T);
 
@@ -1193,7 +1217,8 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
   return "";
 }
 
-std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder, cudaStream_t stream) {
+std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder, cudaStream_t stream,
+                         HostStaging *staging) {
   oom = false;
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
@@ -1203,7 +1228,7 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
   const bool device = builder == BVH_BUILD_DEVICE || (builder == BVH_BUILD_AUTO && tris >= kAutoDeviceBuildTris);
   if (device && tris >= 64) {
     SceneImage img;
-    std::string err = build_scene_image(desc, img, false);
+    std::string err = build_scene_image(desc, img, false, staging);
     if (!err.empty()) return err;
     const auto t1 = clk::now();
     err = commit_scene(img, out, oom);
@@ -1218,20 +1243,28 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
       out.upload_seconds[3] = secs(t0, t3);
       out.device_bvh = true;
       if (builder == BVH_BUILD_AUTO) {
-        // The host tree, built from the positions in the (now uploaded)
-        // host image, which the background build keeps alive.
+        // The host tree, built in the background from the positions read
+        // back from the scene's arena (the host image may be a staging
+        // buffer the next upload reuses).
         auto p = std::make_shared<PendingTree>();
-        p->blob = std::move(img.blob);
-        p->pos_off = img.pos_off;
+        cudaGetDevice(&p->device);
+        p->d_pos = out.dev.pos;
         p->flags = std::move(img.rec_flags);
         const uint32_t tc = (uint32_t)out.tri_count;
         const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
         PendingTree *raw = p.get();
         p->th = std::thread([raw, tc, threads] {
-          const float *pos = reinterpret_cast<const float *>(raw->blob.data() + raw->pos_off);
-          raw->ok = build_bvh(pos, tc, raw->flags.data(), raw->tree.nodes, raw->tree.nodes4, raw->tree.records,
-                              raw->stats, threads, &raw->cancel);
-          raw->blob = HostBlob();
+          std::vector<float> pos(9 * (size_t)tc);
+          cudaStream_t s = nullptr;
+          bool read = cudaSetDevice(raw->device) == cudaSuccess &&
+                      cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+                      cudaMemcpyAsync(pos.data(), raw->d_pos, pos.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                      s) == cudaSuccess &&
+                      cudaStreamSynchronize(s) == cudaSuccess;
+          if (s) cudaStreamDestroy(s);
+          if (!read) cudaGetLastError();
+          raw->ok = read && build_bvh(pos.data(), tc, raw->flags.data(), raw->tree.nodes, raw->tree.nodes4,
+                                      raw->tree.records, raw->stats, threads, &raw->cancel);
           raw->flags = std::vector<uint32_t>();
           raw->done.store(true, std::memory_order_release);
         });

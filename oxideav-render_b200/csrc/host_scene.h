@@ -51,14 +51,34 @@ struct DeviceArena {
 // alignment gaps are zeroed).
 struct HostBlob {
   std::unique_ptr<uint8_t[]> p;
+  uint8_t *ext = nullptr;  // borrowed memory (a HostStaging buffer) instead of p
   size_t n = 0;
   void allocate(size_t bytes) {
     p.reset(new uint8_t[bytes]);
+    ext = nullptr;
     n = bytes;
   }
-  uint8_t *data() { return p.get(); }
-  const uint8_t *data() const { return p.get(); }
+  void use(uint8_t *q, size_t bytes) {
+    p.reset();
+    ext = q;
+    n = bytes;
+  }
+  uint8_t *data() { return ext ? ext : p.get(); }
+  const uint8_t *data() const { return ext ? ext : p.get(); }
   size_t size() const { return n; }
+};
+
+// Page-locked host memory reused by every upload of a context (grow-only,
+// up to kMaxStagingBytes): the image is written straight into it and the
+// copy to the device runs at DMA speed.
+struct HostStaging {
+  static constexpr size_t kMaxStagingBytes = size_t(4) << 30;
+  uint8_t *p = nullptr;
+  size_t cap = 0;
+  // `bytes` of pinned memory, or nullptr (too large, or pinning failed).
+  uint8_t *reserve(size_t bytes);
+  void release();
+  ~HostStaging() { release(); }
 };
 
 // A BVH in its device layouts, in host memory.
@@ -99,8 +119,8 @@ struct PendingTree {
   std::thread th;
   std::atomic<bool> done{false}, cancel{false};
   bool ok = false;
-  HostBlob blob;         // the scene's host image (its positions)
-  uint64_t pos_off = 0;
+  int device = 0;
+  const float *d_pos = nullptr;  // the scene's positions on the device (read back by the build)
   std::vector<uint32_t> flags;
   HostTree tree;
   BvhBuildStats stats;
@@ -127,7 +147,8 @@ struct SceneHost {
 // Validates `desc` and builds its device image on the host. Returns an
 // empty string on success, else an error message. `with_bvh` false leaves
 // the BVH parts out (node counts 0) for a build on the device.
-std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh = true);
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh = true,
+                              HostStaging *staging = nullptr);
 // Allocates the arena and copies `img` into it (stream-ordered when `stream`
 // is non-null). `oom` is set when the failure was a device allocation.
 std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaStream_t stream = nullptr);
@@ -145,7 +166,7 @@ constexpr uint64_t kAutoDeviceBuildTris = 16384;
 // says (`stream`: the device build's stream). A device-built tree deeper
 // than the traversal stacks allow is rebuilt on the host.
 std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder = BVH_BUILD_HOST,
-                         cudaStream_t stream = nullptr);
+                         cudaStream_t stream = nullptr, HostStaging *staging = nullptr);
 void release_scene(SceneHost &s);
 // Replaces the device-built tree of `sc` by its finished background host
 // tree (waiting for it when `wait`). Synchronises `stream` first, so no

@@ -13,10 +13,10 @@ from oxideav_render_b200.source import AnimatedRenderSource, Eof, RenderSource
 pytestmark = pytest.mark.gpu
 
 
-def one_triangle(shift: float = 0.0) -> PreparedScene:
+def one_triangle(green: float = 0.3) -> PreparedScene:
     s = PreparedScene()
-    m = s.add_material(ts.diffuse_material((0.8, 0.3, 0.2), 1.0))
-    tri = np.array([[-0.5 + shift, -0.5, 0.0], [0.5 + shift, -0.5, 0.0], [shift, 0.5, 0.0]], np.float32)
+    m = s.add_material(ts.diffuse_material((0.8, green, 0.2), 1.0))
+    tri = np.array([[-0.5, -0.5, 0.0], [0.5, -0.5, 0.0], [0.0, 0.5, 0.0]], np.float32)
     s.add_primitive(Primitive(tri, np.array([0, 1, 2], np.uint32), material=m))
     return s
 
@@ -44,14 +44,16 @@ def test_non_square_frames(ctx):
 
 def test_animated_frames_equal_direct_renders(ctx):
     o = opts(40, 24)
-    src = AnimatedRenderSource(lambda t: one_triangle(0.3 * t), api.PathTraceCudaRenderer(ctx), o, frames=3,
+    # The colour animates (the orbit camera frames the scene's bounds, so a
+    # moving lone triangle would look the same in every frame).
+    src = AnimatedRenderSource(lambda t: one_triangle(0.3 + 0.4 * t), api.PathTraceCudaRenderer(ctx), o, frames=3,
                                fps=(2, 1))
     frames = []
     for k in range(3):
         f = src.next_frame()
         assert f.pts == k
         t = k / 2
-        want = api.PathTraceCudaRenderer(ctx).render(one_triangle(0.3 * t), o.replace(time=t))
+        want = api.PathTraceCudaRenderer(ctx).render(one_triangle(0.3 + 0.4 * t), o.replace(time=t))
         got = np.frombuffer(f.planes[0].data, np.uint8).reshape(24, 40, 4)
         assert np.array_equal(got, want), k
         frames.append(got)
