@@ -305,11 +305,16 @@ def run_served(ctx, api, torch, args):
 
     # Plain per-request path on the saturated run's requests (new ones, in
     # arrival order) within a time budget: one-shot render (scene prepared
-    # and uploaded per request, PathTraceRenderer::render_hdr semantics) and,
-    # separately, refine + hdr on a tracer whose scene is already uploaded.
+    # and uploaded per request, PathTraceRenderer::render_hdr semantics),
+    # once with this library's default preparation (device BVH for large
+    # scenes) and once with the BVH built on the host as the reference's
+    # TraceScene::new does; and refine + hdr on a tracer whose scene is
+    # already uploaded.
+    from oxideav_render_b200 import abi
     spec, arrivals, images = sample_reqs
     renderer = api.PathTraceCudaRenderer(ctx)
     plain_t, plain_n, resident_t, identical, arr = [], [], [], [], []
+    host_t = []
     budget_end = time.perf_counter() + args.plain_seconds
     for i, sp in enumerate(spec):
         if sp[0] != "new":
@@ -334,16 +339,29 @@ def run_served(ctx, api, torch, args):
         tr.refine(o.path_trace.samples_per_pixel)
         tr.hdr()
         resident_t.append(time.perf_counter() - t0)
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST)
+        try:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            renderer.render_hdr(s, o)
+            host_t.append(time.perf_counter() - t0)
+        finally:
+            ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
     renderer.tracer.close()
     # Latency of the plain path under the same arrivals: one request at a
     # time, first come first served (Lindley recursion on measured times).
-    free_at, plain_lat = 0.0, []
-    for a, s_ in zip(arr, plain_t):
-        begin = max(a, free_at)
-        free_at = begin + s_
-        plain_lat.append(1000.0 * (free_at - a))
+    def fcfs_latency(times):
+        free_at, lat = 0.0, []
+        for a, s_ in zip(arr, times):
+            begin = max(a, free_at)
+            free_at = begin + s_
+            lat.append(1000.0 * (free_at - a))
+        return lat
+
+    plain_lat, host_lat = fcfs_latency(plain_t), fcfs_latency(host_t)
     sat = max(runs, key=lambda r: r["rate_per_s"])
     plain_sps = sum(plain_n) / sum(plain_t)
+    host_sps = sum(plain_n) / sum(host_t)
     resident_sps = sum(plain_n) / sum(resident_t)
     return {
         "scenes": len(scenes), "budget_gb": args.serve_budget_gb, "scene_gen_s": gen_s, "register_s": register_s,
@@ -354,9 +372,14 @@ def run_served(ctx, api, torch, args):
         "plain_render": {"requests": len(plain_t), "samples_per_s": plain_sps,
                          "p50_ms": float(np.percentile(plain_lat, 50)), "p99_ms": float(np.percentile(plain_lat, 99)),
                          "call": "PathTraceCudaRenderer.render_hdr per request (scene prepared + uploaded per call)"},
+        "plain_render_host_bvh": {"requests": len(host_t), "samples_per_s": host_sps,
+                                  "p50_ms": float(np.percentile(host_lat, 50)),
+                                  "p99_ms": float(np.percentile(host_lat, 99)),
+                                  "call": "the same one-shot render with the BVH built on the host per call"},
         "plain_resident": {"requests": len(resident_t), "samples_per_s": resident_sps,
                            "call": "PathTracer.refine + hdr per request, scene already on the device"},
         "speedup_vs_plain_render": sat["samples_per_s"] / plain_sps,
+        "speedup_vs_plain_render_host_bvh": sat["samples_per_s"] / host_sps,
         "speedup_vs_plain_resident": sat["samples_per_s"] / resident_sps,
         "bit_identical_checked": len(identical), "bit_identical": all(identical) if identical else None,
     }
@@ -477,6 +500,26 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def run_uploads(args):
+    """Profiling case: uploads the workload's scene `--upload-only` times
+    (device BVH build and device mip chains) and prints the phase times."""
+    import torch
+    entry.load_package()
+    from oxideav_render_b200 import abi, api
+    scene, opts, env, wname = workload(args.config)
+    ctx = api.Context(torch.cuda.current_device())
+    ctx.set_bvh_builder(abi.PT_BVH_BUILD_DEVICE)
+    desc = scene.to_desc(opts)
+    runs = []
+    for _ in range(args.upload_only):
+        sid = ctx.upload(desc)
+        runs.append({k: 1000 * v for k, v in ctx.upload_seconds(sid).items()})
+        runs[-1]["bvh"] = ctx.bvh_stats(sid)
+        ctx.release(sid)
+    print(json.dumps({"workload": wname, "uploads_ms": runs}))
+    ctx.close()
 
 
 def run_b200(args):
@@ -668,11 +711,15 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
     ap.add_argument("--plain-seconds", type=float, default=15.0, help="time budget of the plain-path sample")
+    ap.add_argument("--upload-only", type=int, default=0,
+                    help="profiling case: upload the scene this many times (device BVH, device mips) and exit")
     args = ap.parse_args()
     args.serve_rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.upload_only > 0:
+        run_uploads(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

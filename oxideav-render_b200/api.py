@@ -237,9 +237,12 @@ class PathTracer:
         need_prepare = self._dirty or self._scene is not scene or self._scene_key != key
         if need_prepare:
             desc = scene.to_desc(opts)
-            sid = self.ctx.upload(desc)
+            # The old scene goes first: its device memory and any background
+            # host BVH build of it are freed before the new upload runs.
             if self._scene_id is not None:
                 self.ctx.release(self._scene_id)
+                self._scene_id = None
+            sid = self.ctx.upload(desc)
             self._scene_id, self._desc, self._scene, self._scene_key = sid, desc, scene, key
             self._dirty = False
             self.lib.pt_tracer_invalidate_scene(self.ptr)

@@ -1251,7 +1251,9 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
         p->d_pos = out.dev.pos;
         p->flags = std::move(img.rec_flags);
         const uint32_t tc = (uint32_t)out.tri_count;
-        const int threads = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        // Leave two hardware threads to the caller (launches, the next upload).
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int threads = (int)std::max(1u, std::min(32u, hw > 4 ? hw - 2 : 1u));
         PendingTree *raw = p.get();
         p->th = std::thread([raw, tc, threads] {
           std::vector<float> pos(9 * (size_t)tc);
