@@ -295,10 +295,12 @@ PT_API void pt_destroy(pt_context *ctx);
 PT_API const char *pt_last_error(const pt_context *ctx);
 PT_API uint32_t pt_abi_version(void);
 
-/* Upload a prepared scene: builds the BVH on the host (binned SAH), the
- * emissive-triangle table (EmissiveLights::build, src/pathtrace.rs:1479-1543)
- * and the texture mip chains, and copies everything to device memory, where it
- * stays until pt_scene_release (or until the serving cache evicts it). */
+/* Upload a prepared scene: the emissive-triangle table (EmissiveLights::build,
+ * src/pathtrace.rs:1479-1543) on the host; the BVH (on the device for large
+ * scenes, replaced by a host binned-SAH tree built in the background; see
+ * pt_set_bvh_builder) and the texture mip chains on the device. The scene
+ * stays in device memory until pt_scene_release (or until the serving cache
+ * evicts it). */
 PT_API pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *scene_id);
 PT_API pt_status pt_scene_release(pt_context *ctx, uint32_t scene_id);
 /* Device bytes held by a resident scene. */
@@ -378,6 +380,48 @@ PT_API pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const pt_
 PT_API pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                           const pt_render_options *opts, const pt_environment *env,
                           uint8_t *out_rgba, size_t out_bytes);
+
+/* ------------------------------------------------------------------ raycast */
+
+/* ShadingMode (src/options.rs:150-187). */
+typedef enum pt_shading_mode {
+  PT_SHADE_FLAT = 0,
+  PT_SHADE_GOURAUD = 1,
+  PT_SHADE_PHONG = 2,
+  PT_SHADE_WIREFRAME = 3,
+  PT_SHADE_NORMAL_DEBUG = 4,
+  PT_SHADE_DEPTH_DEBUG = 5,
+  PT_SHADE_PBR = 6
+} pt_shading_mode;
+
+/* What the raycast backend reads of RenderOptions (src/options.rs) plus the
+ * camera's clip planes (Camera::near / far, src/camera.rs:80-84). */
+typedef struct pt_raycast_options {
+  uint32_t width, height;  /* output pixels */
+  uint32_t aa;             /* SSAA factor per axis, 1..=8 */
+  uint32_t shading;        /* pt_shading_mode */
+  float light_azimuth_deg, light_elevation_deg, light_intensity; /* LightSpec */
+  uint8_t background[4];
+  uint32_t tone_map;       /* pt_tone_map */
+  float exposure;
+  uint32_t max_ray_depth;  /* capped at 16 */
+  float near_plane, far_plane;
+} pt_raycast_options;
+
+/* The Whitted ray tracer behind RenderBackend::Raycast (src/raycast.rs:145-560)
+ * on a resident scene: one ray per render sample (width·aa × height·aa,
+ * through Camera::primary_ray at the sample centre, `camera` resolved for
+ * that resolution), the legacy shading modes (Flat, Gouraud, Phong with
+ * Whitted's shadow, mirror and refraction rays up to max_ray_depth,
+ * Wireframe, NormalDebug, DepthDebug), then the scanline backend's frame
+ * resolve (src/scanline.rs:124-221): SSAA box filter, premultiplied
+ * averages, exposure + tone map + sRGB for RGBA8. Writes the scene-linear
+ * HDR image (width*height*4 floats) and/or the RGBA8 image
+ * (width*height*4 bytes); either pointer may be NULL. PT_SHADE_PBR is not
+ * built: PT_ERR_INVALID_ARG. */
+PT_API pt_status pt_raycast_render(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+                                   const pt_raycast_options *opts, float *out_hdr, size_t hdr_floats,
+                                   uint8_t *out_rgba, size_t rgba_bytes);
 
 #ifdef __cplusplus
 }

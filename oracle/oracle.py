@@ -52,6 +52,7 @@ def lib():
                 "oracle_material_base": (None, [vp, u32, fp, fp]),
                 "oracle_texture_sample": (None, [vp, f32, f32, f32, i32, fp, u32p, fp]),
                 "oracle_texture_mips": (C.c_uint64, [vp, i32, fp, C.c_uint64]),
+                "oracle_raycast": (i32, [vp, vp, vp, fp, C.POINTER(C.c_uint8)]),
                 "oracle_emissive_table": (None, [vp, u32p, C.POINTER(u32p), C.POINTER(fp), C.POINTER(fp)]),
                 "oracle_sobol_owen_4d": (None, [u32, u32, fp]),
                 "oracle_sobol": (u32, [u32, u32]),
@@ -288,6 +289,24 @@ def texture_sample(pixels: np.ndarray, sampler, u: float, v: float, lod: float, 
     lib().oracle_texture_sample(C.addressof(t), u, v, lod, 1 if srgb else 0, out.ctypes.data_as(C.POINTER(C.c_float)),
                                 C.byref(levels), top.ctypes.data_as(C.POINTER(C.c_float)))
     return out, levels.value, top
+
+
+def raycast(scene, opts):
+    """RenderBackend::Raycast render of a PreparedScene (legacy shading
+    modes): (HDR (h, w, 4) f32, RGBA8 (h, w, 4) u8)."""
+    from oxideav_render_b200.scene import Camera
+    w, h, aa = max(opts.width, 1), max(opts.height, 1), int(opts.aa)
+    cam = Camera.resolve(scene, opts, w * aa, h * aa)
+    desc = scene.to_desc(opts)
+    c = cam.to_c()
+    o = opts.to_raycast_c(cam.near, cam.far)
+    hdr = np.zeros((h, w, 4), np.float32)
+    rgba = np.zeros((h, w, 4), np.uint8)
+    st = lib().oracle_raycast(C.addressof(desc.desc), C.addressof(c), C.addressof(o),
+                              hdr.ctypes.data_as(C.POINTER(C.c_float)), rgba.ctypes.data_as(C.POINTER(C.c_uint8)))
+    if st != 0:
+        raise ValueError("the oracle's raycast covers the legacy shading modes only")
+    return hdr, rgba
 
 
 def texture_mips(pixels: np.ndarray, srgb: bool) -> np.ndarray:

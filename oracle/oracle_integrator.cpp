@@ -460,11 +460,295 @@ static bool resolve_pixel(const double *a, uint32_t samples, const float bg[4], 
   return true;
 }
 
+// ---- RenderBackend::Raycast, legacy shading modes ------------------------
+// Ctx::pixel / legacy / whitted (src/raycast.rs:349-516) with shade_pixel and
+// build_light (src/shade.rs:26-50), reflect / refract / schlick
+// (src/trace.rs:1087-1116), normal_to_byte / depth_to_byte
+// (src/scanline.rs:840-858), Camera::ndc_z / view_depth
+// (src/camera.rs:521-543), and the frame resolve (src/scanline.rs:124-221).
+namespace {
+constexpr float kAmbient = 0.2f;
+constexpr float kSecondary = 1.0e-2f;
+constexpr float kWireEdge = 0.03f;
+constexpr uint32_t kDepthCap = 16;
+
+V3 interp3v(const std::vector<V3> &v, size_t base, const float b[3]) {
+  V3 x = v[base], y = v[base + 1], z = v[base + 2];
+  return {x.x * b[0] + y.x * b[1] + z.x * b[2], x.y * b[0] + y.y * b[1] + z.y * b[2],
+          x.z * b[0] + y.z * b[1] + z.z * b[2]};
+}
+
+struct Raycaster {
+  const Scene *ts;
+  pt_camera cam;
+  uint32_t rw, rh, mode, max_depth;
+  V3 light;
+  float intensity, near_p, far_p;
+  float lut[256];
+
+  V3 cv(const float *a) const { return {a[0], a[1], a[2]}; }
+  void primary_ray(float px, float py, V3 &o, V3 &d) const {
+    float ndc_x = (px / fmaxr((float)rw, 1.0f)) * 2.0f - 1.0f;
+    float ndc_y = 1.0f - (py / fmaxr((float)rh, 1.0f)) * 2.0f;
+    V3 off = add(scale(cv(cam.side), ndc_x * cam.half_w), scale(cv(cam.up), ndc_y * cam.half_h));
+    if (cam.projection == PT_PERSPECTIVE) {
+      o = cv(cam.eye);
+      d = normalise(add(off, cv(cam.forward)));
+    } else {
+      o = add(cv(cam.eye), off);
+      d = cv(cam.forward);
+    }
+  }
+  V4 shade_pixel(V4 base, V3 n) const {
+    float cos_theta = fmaxr(dot(n, light), 0.0f);
+    float diffuse = kAmbient + (1.0f - kAmbient) * cos_theta * intensity;
+    float f = clampr(diffuse, 0.0f, 1.0f);
+    return V4{{base[0] * f, base[1] * f, base[2] * f, base[3]}};
+  }
+  V3 corner_normal(const Item &it, size_t c, const Hit &h) const {
+    if (it.normals.size() > c) return it.normals[c];
+    return ts->surface(h).geometric_normal;
+  }
+  V3 hit_normal(const Item &it, const Hit &h) const {
+    if (it.normals.size() == it.positions.size()) return interp3v(it.normals, 3 * (size_t)h.tri, h.bary);
+    return ts->surface(h).geometric_normal;
+  }
+  static V3 reflect(V3 d, V3 n) {
+    float k = 2.0f * dot(d, n);
+    return {d.x - k * n.x, d.y - k * n.y, d.z - k * n.z};
+  }
+  static bool refract(V3 d, V3 n, float eta, V3 &out) {
+    float cos_i = clampr(-dot(d, n), -1.0f, 1.0f);
+    float sin2_t = eta * eta * (1.0f - cos_i * cos_i);
+    if (sin2_t > 1.0f) return false;
+    float cos_t = std::sqrt(1.0f - sin2_t);
+    float k = eta * cos_i - cos_t;
+    out = normalise({eta * d.x + k * n.x, eta * d.y + k * n.y, eta * d.z + k * n.z});
+    return true;
+  }
+  static float schlick(float f0, float c) { return f0 + (1.0f - f0) * powi5(1.0f - clampr(c, 0.0f, 1.0f)); }
+  static uint32_t normal_byte(float n) {
+    if (!std::isfinite(n)) return 128;
+    float v = std::round((clampr(n, -1.0f, 1.0f) + 1.0f) * 0.5f * 255.0f);
+    return (uint32_t)clampr(v, 0.0f, 255.0f);
+  }
+  static uint32_t depth_byte(float z) {
+    if (!std::isfinite(z)) return 0;
+    float zc = clampr(z, -1.0f, 1.0f);
+    float v = std::round((1.0f - (zc * 0.5f + 0.5f)) * 255.0f);
+    return (uint32_t)clampr(v, 0.0f, 255.0f);
+  }
+  float ndc_z(float vd) const {
+    if (cam.projection == PT_PERSPECTIVE) {
+      float nf = 1.0f / (near_p - far_p);
+      float d = fmaxr(vd, FLT_MIN);
+      return -(far_p + near_p) * nf + 2.0f * far_p * near_p * nf / d;
+    }
+    float fne = far_p - near_p;
+    if (std::fabs(fne) < FLT_EPSILON) return 0.0f;
+    return (2.0f * vd - (far_p + near_p)) / fne;
+  }
+
+  V4 whitted(V3 d, const Hit &hit, uint32_t depth) const {
+    const Item &it = ts->item_of(hit);
+    const pt_material &mat = ts->material_of(hit);
+    const V4 a{{mat.base_color[0], mat.base_color[1], mat.base_color[2], mat.base_color[3]}};
+    if (mat.unlit) return a;
+    V3 raw = normalise(hit_normal(it, hit));
+    bool entering = dot(d, raw) < 0.0f;
+    V3 n = entering ? raw : scale(raw, -1.0f);
+    V3 p = interp3v(it.positions, 3 * (size_t)hit.tri, hit.bary);
+    uint32_t skip = hit.global;
+    auto not_self = [&](const Hit &h) { return h.global != skip; };
+    V3 so = Integrator::offset_ray_origin(p, n);
+    bool shadowed = ts->occluded_filtered(so, light, 0.0f, INF, not_self);
+    V4 out = shadowed ? V4{{a[0] * kAmbient, a[1] * kAmbient, a[2] * kAmbient, a[3]}} : shade_pixel(a, n);
+    for (int k = 0; k < 3; ++k) out[k] += mat.emissive[k];
+    if (depth >= max_depth) return out;
+    float cos_in = clampr(-dot(d, n), 0.0f, 1.0f);
+    auto trace = [&](V3 o, V3 dir, V4 &c) {
+      Hit h;
+      if (!ts->closest_hit_filtered(o, dir, 0.0f, INF, not_self, h)) return false;
+      c = whitted(dir, h, depth + 1);
+      return true;
+    };
+    float gloss = mat.metallic * (1.0f - mat.roughness);
+    if (gloss > kSecondary) {
+      float f0 = 0.04f + 0.96f * mat.metallic;
+      float kr = clampr(schlick(f0, cos_in), 0.0f, 1.0f) * gloss;
+      V4 rc{{0.0f, 0.0f, 0.0f, 1.0f}};
+      trace(so, reflect(d, n), rc);
+      for (int k = 0; k < 3; ++k) out[k] = out[k] * (1.0f - kr) + rc[k] * a[k] * kr;
+    }
+    float kt = (mat.ext_flags & PT_EXT_TRANSMISSION) ? clampr(mat.transmission_factor, 0.0f, 1.0f) : 0.0f;
+    if (kt > kSecondary) {
+      float eta = entering ? 1.0f / mat.ior : mat.ior;
+      V3 tdir;
+      if (refract(d, n, eta, tdir)) {
+        V3 ro = Integrator::offset_ray_origin(p, scale(n, -1.0f));
+        V4 tc{{0.0f, 0.0f, 0.0f, 0.0f}};
+        trace(ro, tdir, tc);
+        for (int k = 0; k < 3; ++k) out[k] = out[k] * (1.0f - kt) + tc[k] * a[k] * kt;
+      } else {
+        V4 rc;
+        if (trace(so, reflect(d, n), rc))
+          for (int k = 0; k < 3; ++k) out[k] = out[k] * (1.0f - kt) + rc[k] * kt;
+      }
+    }
+    return out;
+  }
+
+  bool legacy(V3 o, V3 d, V4 &c) const {
+    Hit hit;
+    if (!ts->closest_hit_filtered(o, d, 0.0f, INF, [](const Hit &) { return true; }, hit)) return false;
+    const Item &it = ts->item_of(hit);
+    const pt_material &mat = ts->material_of(hit);
+    const V4 base{{mat.base_color[0], mat.base_color[1], mat.base_color[2], mat.base_color[3]}};
+    const size_t b0 = 3 * (size_t)hit.tri;
+    switch (mode) {
+      case PT_SHADE_FLAT:
+        c = base;
+        return true;
+      case PT_SHADE_WIREFRAME: {
+        float m = INF;
+        for (int k = 0; k < 3; ++k) m = fminr(m, hit.bary[k]);
+        if (m > kWireEdge) return false;
+        c = base;
+        return true;
+      }
+      case PT_SHADE_GOURAUD: {
+        V4 ca = shade_pixel(base, corner_normal(it, b0, hit));
+        V4 cb = shade_pixel(base, corner_normal(it, b0 + 1, hit));
+        V4 cc = shade_pixel(base, corner_normal(it, b0 + 2, hit));
+        for (int k = 0; k < 4; ++k) c[k] = ca[k] * hit.bary[0] + cb[k] * hit.bary[1] + cc[k] * hit.bary[2];
+        return true;
+      }
+      case PT_SHADE_NORMAL_DEBUG: {
+        V3 n = normalise(hit_normal(it, hit));
+        c = V4{{lut[normal_byte(n.x)], lut[normal_byte(n.y)], lut[normal_byte(n.z)], 1.0f}};
+        return true;
+      }
+      case PT_SHADE_DEPTH_DEBUG: {
+        V3 pp = interp3v(it.positions, b0, hit.bary);
+        float g = lut[depth_byte(ndc_z(dot(sub(pp, cv(cam.eye)), cv(cam.forward))))];
+        c = V4{{g, g, g, 1.0f}};
+        return true;
+      }
+      default:
+        c = whitted(d, hit, 0);
+        return true;
+    }
+  }
+};
+}  // namespace
+
 }  // namespace oracle
 
 using namespace oracle;
 
 extern "C" {
+
+// RenderBackend::Raycast render (legacy modes): HDR (w*h*4 floats) and/or
+// RGBA8 (w*h*4 bytes); returns 0, or -1 for options it does not cover.
+int oracle_raycast(const pt_scene_desc *desc, const pt_camera *cam, const pt_raycast_options *o, float *hdr,
+                   uint8_t *rgba) {
+  if (o->shading >= PT_SHADE_PBR || o->aa < 1 || o->aa > 8) return -1;
+  Scene sc(*desc);
+  Raycaster rc;
+  rc.ts = &sc;
+  rc.cam = *cam;
+  rc.rw = o->width * o->aa;
+  rc.rh = o->height * o->aa;
+  rc.mode = o->shading;
+  rc.max_depth = std::min(o->max_ray_depth, kDepthCap);
+  {
+    const float deg = 3.14159265358979323846f / 180.0f;
+    float az = o->light_azimuth_deg * deg, el = o->light_elevation_deg * deg;
+    float cos_el = std::cos(el);
+    rc.light = normalise({cos_el * std::sin(az), std::sin(el), cos_el * std::cos(az)});
+  }
+  rc.intensity = o->light_intensity;
+  rc.near_p = o->near_plane;
+  rc.far_p = o->far_plane;
+  for (int i = 0; i < 256; ++i) rc.lut[i] = srgb_to_linear_f((float)i / 255.0f);
+  const size_t ns = (size_t)rc.rw * rc.rh;
+  std::vector<V4> col(ns);
+  std::vector<uint8_t> cov(ns, 0);
+  const unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t y; (y = next.fetch_add(1)) < rc.rh;)
+      for (uint32_t x = 0; x < rc.rw; ++x) {
+        V3 ro, rd;
+        rc.primary_ray((float)x + 0.5f, (float)y + 0.5f, ro, rd);
+        V4 c{{0, 0, 0, 0}};
+        bool hit = rc.legacy(ro, rd, c);
+        col[y * rc.rw + x] = hit ? c : V4{{0, 0, 0, 0}};
+        cov[y * rc.rw + x] = hit ? 1 : 0;
+      }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned k = 1; k < nt; ++k) pool.emplace_back(work);
+  work();
+  for (auto &th : pool) th.join();
+  const bool display = o->shading == PT_SHADE_NORMAL_DEBUG || o->shading == PT_SHADE_DEPTH_DEBUG;
+  const uint32_t tm = display ? (uint32_t)PT_TONE_CLAMP : o->tone_map;
+  const float exposure = display ? 1.0f : o->exposure;
+  float bg[4] = {rc.lut[o->background[0]], rc.lut[o->background[1]], rc.lut[o->background[2]],
+                 (float)o->background[3] / 255.0f};
+  const uint32_t aa = o->aa;
+  const float n = (float)(aa * aa);
+  for (uint32_t oy = 0; oy < o->height; ++oy)
+    for (uint32_t ox = 0; ox < o->width; ++ox) {
+      float pre_h[3] = {0, 0, 0}, str_h[3] = {0, 0, 0}, a_h = 0.0f;
+      float pre_d[3] = {0, 0, 0}, str_d[3] = {0, 0, 0}, a_d = 0.0f;
+      for (uint32_t j = 0; j < aa; ++j)
+        for (uint32_t i = 0; i < aa; ++i) {
+          size_t si = ((size_t)oy * aa + j) * rc.rw + (size_t)ox * aa + i;
+          float ch[4] = {bg[0], bg[1], bg[2], bg[3]}, cd[4] = {bg[0], bg[1], bg[2], bg[3]};
+          if (cov[si]) {
+            const V4 &c = col[si];
+            for (int k = 0; k < 4; ++k) ch[k] = c[k];
+            V3 m = tone_apply(tm, {c[0] * exposure, c[1] * exposure, c[2] * exposure});
+            cd[0] = m.x;
+            cd[1] = m.y;
+            cd[2] = m.z;
+            cd[3] = clampr(c[3], 0.0f, 1.0f);
+          }
+          for (int k = 0; k < 3; ++k) {
+            pre_h[k] += ch[k] * ch[3];
+            str_h[k] += ch[k];
+            pre_d[k] += cd[k] * cd[3];
+            str_d[k] += cd[k];
+          }
+          a_h += ch[3];
+          a_d += cd[3];
+        }
+      const size_t op = (size_t)oy * o->width + ox;
+      float oh[4], od[4];
+      if (a_h > 0.0f) {
+        for (int k = 0; k < 3; ++k) oh[k] = pre_h[k] / a_h;
+        oh[3] = a_h / n;
+      } else {
+        for (int k = 0; k < 3; ++k) oh[k] = str_h[k] / n;
+        oh[3] = 0.0f;
+      }
+      if (a_d > 0.0f) {
+        for (int k = 0; k < 3; ++k) od[k] = pre_d[k] / a_d;
+        od[3] = a_d / n;
+      } else {
+        for (int k = 0; k < 3; ++k) od[k] = str_d[k] / n;
+        od[3] = 0.0f;
+      }
+      if (hdr)
+        for (int k = 0; k < 4; ++k) hdr[4 * op + k] = oh[k];
+      if (rgba) {
+        for (int k = 0; k < 3; ++k) rgba[4 * op + k] = linear_to_srgb_byte(od[k]);
+        rgba[4 * op + 3] = (uint8_t)std::round(clampr(od[3], 0.0f, 1.0f) * 255.0f);
+      }
+    }
+  return 0;
+}
 
 void *oracle_scene_create(const pt_scene_desc *desc) {
   try {

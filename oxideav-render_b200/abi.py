@@ -220,6 +220,28 @@ class pt_render_options(C.Structure):
     ]
 
 
+PT_SHADE_FLAT, PT_SHADE_GOURAUD, PT_SHADE_PHONG, PT_SHADE_WIREFRAME = 0, 1, 2, 3
+PT_SHADE_NORMAL_DEBUG, PT_SHADE_DEPTH_DEBUG, PT_SHADE_PBR = 4, 5, 6
+
+
+class pt_raycast_options(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("aa", C.c_uint32),
+        ("shading", C.c_uint32),
+        ("light_azimuth_deg", C.c_float),
+        ("light_elevation_deg", C.c_float),
+        ("light_intensity", C.c_float),
+        ("background", C.c_uint8 * 4),
+        ("tone_map", C.c_uint32),
+        ("exposure", C.c_float),
+        ("max_ray_depth", C.c_uint32),
+        ("near_plane", C.c_float),
+        ("far_plane", C.c_float),
+    ]
+
+
 # include/pt_b200_serve.h
 class pt_server_config(C.Structure):
     _fields_ = [
@@ -291,6 +313,6 @@ class pt_tune_choice(C.Structure):
 
 ABI_STRUCTS = [
     pt_texture_binding, pt_material, pt_texture, pt_draw_item, pt_light,
-    pt_scene_desc, pt_environment, pt_camera, pt_path_trace_options, pt_render_options,
+    pt_scene_desc, pt_environment, pt_camera, pt_path_trace_options, pt_render_options, pt_raycast_options,
     pt_server_config, pt_server_request, pt_request_stats, pt_server_stats, pt_tune_choice,
 ]

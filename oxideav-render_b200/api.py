@@ -389,12 +389,57 @@ class PathTraceCudaRenderer:
         return self.tracer.hdr()
 
 
+class RaycastCudaRenderer:
+    """Renderer for RenderBackend::Raycast (src/raycast.rs) on the device:
+    every call prepares and uploads the scene (as the reference's
+    `render` builds its PreparedScene and TraceScene per call), resolves the
+    camera at the SSAA resolution, traces one ray per sample and resolves the
+    frame. The legacy shading modes are built (Flat, Gouraud, Phong with
+    Whitted's shadow / mirror / refraction rays, Wireframe, NormalDebug,
+    DepthDebug); `ShadingMode.Pbr` raises RenderError."""
+
+    def __init__(self, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.lib = self.ctx.lib
+
+    def _run(self, scene: PreparedScene, opts: RenderOptions, hdr: bool) -> np.ndarray:
+        opts.validate()
+        w, h, aa = max(opts.width, 1), max(opts.height, 1), int(opts.aa)
+        cam = Camera.resolve(scene, opts, w * aa, h * aa)
+        desc = scene.to_desc(opts)
+        sid = self.ctx.upload(desc)
+        try:
+            o = opts.to_raycast_c(cam.near, cam.far)
+            c = cam.to_c()
+            if hdr:
+                out = np.zeros((h, w, 4), np.float32)
+                st = self.lib.pt_raycast_render(self.ctx.ptr, sid, C.byref(c), C.byref(o),
+                                                out.ctypes.data_as(C.POINTER(C.c_float)), out.size, None, 0)
+            else:
+                out = np.zeros((h, w, 4), np.uint8)
+                st = self.lib.pt_raycast_render(self.ctx.ptr, sid, C.byref(c), C.byref(o), None, 0,
+                                                out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size)
+            self.ctx.check(st)
+            return out
+        finally:
+            self.ctx.release(sid)
+
+    def render(self, scene: PreparedScene, opts: RenderOptions) -> np.ndarray:
+        return self._run(scene, opts, False)
+
+    def render_hdr(self, scene: PreparedScene, opts: RenderOptions) -> np.ndarray:
+        return self._run(scene, opts, True)
+
+
 def make_renderer(backend: RenderBackend, ctx: Optional[Context] = None):
-    """make_renderer (src/lib.rs:174-180) for the backend this library provides."""
+    """make_renderer (src/lib.rs:174-180) for the backends this library provides."""
     if backend == RenderBackend.PathTraceCuda:
         return PathTraceCudaRenderer(ctx)
+    if backend == RenderBackend.Raycast:
+        return RaycastCudaRenderer(ctx)
     raise NotImplementedError(f"{backend} is served by the reference crate, not by this library")
 
 
-__all__ = ["Context", "EnvironmentMap", "PathTracer", "PathTraceCudaRenderer", "make_renderer", "RenderError",
+__all__ = ["Context", "EnvironmentMap", "PathTracer", "PathTraceCudaRenderer", "RaycastCudaRenderer", "make_renderer",
+           "RenderError",
            "radiance_key"]

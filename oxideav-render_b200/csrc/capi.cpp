@@ -6,6 +6,7 @@
 // accumulator resident on the device. No exception crosses the ABI: every
 // entry point catches and maps failures to a pt_status plus a message.
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -981,6 +982,84 @@ pt_status pt_render_hdr(pt_context *ctx, uint32_t scene_id, const pt_camera *cam
 pt_status pt_render_image(pt_context *ctx, uint32_t scene_id, const pt_camera *camera, const pt_render_options *opts,
                           const pt_environment *env, uint8_t *out, size_t n) {
   return guard(ctx, [&] { return render_impl(ctx, scene_id, camera, opts, env, out, n, true); });
+}
+
+// ---------------------------------------------------------------- raycast
+namespace {
+// build_light, src/shade.rs:26-35: azimuth / elevation in degrees to a unit
+// direction toward the light (f32 throughout, as the reference).
+void legacy_light(const pt_raycast_options &o, float dir[3]) {
+  const float deg = 3.14159265358979323846f / 180.0f;
+  float az = o.light_azimuth_deg * deg, el = o.light_elevation_deg * deg;
+  float cos_el = std::cos(el);
+  float d[3] = {cos_el * std::sin(az), std::sin(el), cos_el * std::cos(az)};
+  float len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  for (int k = 0; k < 3; ++k) dir[k] = len < 1.1920929e-7f ? 0.0f : d[k] / len;
+}
+}  // namespace
+
+pt_status pt_raycast_render(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+                            const pt_raycast_options *opts, float *out_hdr, size_t hdr_floats, uint8_t *out_rgba,
+                            size_t rgba_bytes) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (!camera || !opts) return fail(ctx, PT_ERR_INVALID_ARG, "camera / options is NULL");
+  const pt_raycast_options &o = *opts;
+  if (o.width == 0 || o.height == 0) return fail(ctx, PT_ERR_INVALID_ARG, "width and height must be positive");
+  if (o.aa < 1 || o.aa > 8) return fail(ctx, PT_ERR_INVALID_ARG, "aa must be in 1..=8");
+  if (o.shading > PT_SHADE_PBR) return fail(ctx, PT_ERR_INVALID_ARG, "unknown shading mode");
+  if (o.shading == PT_SHADE_PBR)
+    return fail(ctx, PT_ERR_INVALID_ARG, "Pbr shading on the raycast backend is not built (legacy modes are)");
+  if (o.tone_map > PT_TONE_ACES) return fail(ctx, PT_ERR_INVALID_ARG, "unknown tone map");
+  const uint64_t rw = (uint64_t)o.width * o.aa, rh = (uint64_t)o.height * o.aa;
+  if (rw * rh > (1ull << 30)) return fail(ctx, PT_ERR_INVALID_ARG, "render resolution too large");
+  const uint64_t npx = (uint64_t)o.width * o.height;
+  if (out_hdr && hdr_floats < 4 * npx) return fail(ctx, PT_ERR_INVALID_ARG, "HDR buffer too small");
+  if (out_rgba && rgba_bytes < 4 * npx) return fail(ctx, PT_ERR_INVALID_ARG, "RGBA buffer too small");
+  return guard(ctx, [&]() -> pt_status {
+    SceneHost *sc = find_scene(ctx, scene_id);
+    if (!sc) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene " + std::to_string(scene_id));
+    CK(ctx, cudaSetDevice(ctx->device));
+    adopt_pending_tree(*sc, ctx->stream, false);
+    static float decode[256];
+    static bool init = [] {
+      for (int i = 0; i < 256; ++i) decode[i] = host_srgb_to_linear((float)i / 255.0f);
+      return true;
+    }();
+    (void)init;
+    float light[3];
+    legacy_light(o, light);
+    const bool display = o.shading == PT_SHADE_NORMAL_DEBUG || o.shading == PT_SHADE_DEPTH_DEBUG;
+    float4 bg = make_float4(decode[o.background[0]], decode[o.background[1]], decode[o.background[2]],
+                            (float)o.background[3] / 255.0f);
+    const uint64_t ns = rw * rh;
+    // One stream-ordered allocation: samples, coverage, error word, outputs.
+    auto al = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
+    const uint64_t off_cov = al(ns * sizeof(float4)), off_err = off_cov + al(ns);
+    const uint64_t off_hdr = off_err + 256, off_rgba = off_hdr + al(npx * sizeof(float4));
+    const uint64_t total = off_rgba + al(npx * 4);
+    void *buf = nullptr;
+    CK(ctx, cudaMallocAsync(&buf, total, ctx->stream));
+    std::unique_ptr<void, std::function<void(void *)>> hold(buf, [ctx](void *q) { cudaFreeAsync(q, ctx->stream); });
+    uint8_t *b = static_cast<uint8_t *>(buf);
+    uint32_t *d_err = reinterpret_cast<uint32_t *>(b + off_err);
+    CK(ctx, cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream));
+    CK(ctx, launch_raycast(sc->dev, *camera, (uint32_t)rw, (uint32_t)rh, o.shading, o.max_ray_depth, light,
+                           o.light_intensity, o.near_plane, o.far_plane, decode, reinterpret_cast<float4 *>(b),
+                           b + off_cov, d_err, ctx->num_sms, ctx->stream));
+    float4 *d_hdr = out_hdr ? reinterpret_cast<float4 *>(b + off_hdr) : nullptr;
+    uchar4 *d_rgba = out_rgba ? reinterpret_cast<uchar4 *>(b + off_rgba) : nullptr;
+    CK(ctx, launch_raycast_resolve(reinterpret_cast<float4 *>(b), b + off_cov, o.width, o.height, o.aa, bg,
+                                   display ? (uint32_t)PT_TONE_CLAMP : o.tone_map, display ? 1.0f : o.exposure, d_hdr,
+                                   d_rgba, ctx->stream));
+    uint32_t err = 0;
+    CK(ctx, cudaMemcpyAsync(&err, d_err, sizeof err, cudaMemcpyDeviceToHost, ctx->stream));
+    if (d_hdr)
+      CK(ctx, cudaMemcpyAsync(out_hdr, d_hdr, npx * sizeof(float4), cudaMemcpyDeviceToHost, ctx->stream));
+    if (d_rgba) CK(ctx, cudaMemcpyAsync(out_rgba, d_rgba, npx * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (err & ERR_STACK_OVERFLOW) return fail(ctx, PT_ERR_DEVICE, "BVH traversal stack overflow");
+    return PT_OK;
+  });
 }
 
 // ---------------------------------------------------------------- debug hooks

@@ -831,7 +831,7 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
   std::vector<uint64_t> first_tri(desc.item_count + 1, 0);
   for (uint32_t i = 0; i < desc.item_count; ++i) {
     const pt_draw_item &it = desc.items[i];
-    any_vn |= it.normals && it.has_vertex_normals;
+    any_vn |= it.normals != nullptr;
     any_tan |= it.tangents != nullptr;
     any_col |= it.colors != nullptr;
     for (int s = 0; s < PT_MAX_UV_SETS; ++s) any_uv[s] |= it.uvs[s] != nullptr;
@@ -992,7 +992,10 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
     const pt_draw_item &it = desc.items[i];
     const size_t g0 = first_tri[i], n = it.triangle_count;
     copy_task(plan.off[p_pos] + 36 * g0, it.positions, 36 * n);
-    if (any_vn) copy_task(plan.off[p_nrm] + 36 * g0, it.normals && it.has_vertex_normals ? it.normals : nullptr, 36 * n);
+    // Every item's corner normals (face normals when it has no vertex
+    // normals: the raycast backend shades with them); TRI_HAS_VN tells the
+    // path tracer which are vertex normals.
+    if (any_vn) copy_task(plan.off[p_nrm] + 36 * g0, it.normals, 36 * n);
     if (any_tan) copy_task(plan.off[p_tan] + 48 * g0, it.tangents, 48 * n);
     if (any_col) copy_task(plan.off[p_col] + 48 * g0, it.colors, 48 * n);
     for (int s = 0; s < PT_MAX_UV_SETS; ++s)

@@ -1,5 +1,6 @@
 // Kernels of the plain (one path per thread) schedule, the in-order f64
 // accumulator, the resolve kernels and the test hooks.
+#include <algorithm>
 #include <cstdio>
 
 #include "dev_integrator.cuh"
@@ -146,6 +147,12 @@ PT_DEV uint8_t srgb_byte(float c) {
   }
   return (uint8_t)lo;
 }
+
+}  // namespace ptd
+
+#include "raycast.cuh"
+
+namespace ptd {
 
 // PathTracer::hdr, src/pathtrace.rs:2717-2734.
 __global__ void k_resolve_hdr(const double *accum, uint32_t n, uint32_t samples, float4 bg, float4 *out) {
@@ -400,6 +407,41 @@ cudaError_t launch_debug_bsdf(const float *params, const float *dirs, const floa
                               cudaStream_t st) {
   k_debug_bsdf<<<(n + 127) / 128, 128, 0, st>>>(params, dirs, us, n, out);
   return LAUNCH_CHECK();
+}
+
+// RenderBackend::Raycast: trace every render sample, then resolve.
+cudaError_t launch_raycast(const DevScene &s, const pt_camera &cam, uint32_t rw, uint32_t rh, uint32_t mode,
+                           uint32_t max_depth, const float light_dir[3], float light_intensity, float near_plane,
+                           float far_plane, const float decode[256], float4 *samples, uint8_t *covered,
+                           uint32_t *err, int num_sms, cudaStream_t st) {
+  RaycastParams p;
+  p.s = s;
+  p.cam = cam;
+  p.rw = rw;
+  p.rh = rh;
+  p.mode = mode;
+  p.max_depth = max_depth < kRayDepthCap ? max_depth : kRayDepthCap;
+  p.light_dir = {light_dir[0], light_dir[1], light_dir[2]};
+  p.light_intensity = light_intensity;
+  p.near_plane = near_plane;
+  p.far_plane = far_plane;
+  for (int k = 0; k < 256; ++k) p.decode[k] = decode[k];
+  p.samples = samples;
+  p.covered = covered;
+  p.err = err;
+  const uint64_t n = (uint64_t)rw * rh;
+  const uint64_t blocks = std::min<uint64_t>((n + 127) / 128, (uint64_t)num_sms * 16);
+  k_raycast<<<(unsigned)std::max<uint64_t>(blocks, 1), 128, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_raycast_resolve(const float4 *samples, const uint8_t *covered, uint32_t out_w, uint32_t out_h,
+                                   uint32_t aa, float4 bg, uint32_t tone, float exposure, float4 *hdr, uchar4 *rgba,
+                                   cudaStream_t st) {
+  const uint64_t n = (uint64_t)out_w * out_h;
+  const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 1u << 16));
+  k_raycast_resolve<<<blocks, 256, 0, st>>>(samples, covered, out_w, out_h, aa, bg, tone, exposure, hdr, rgba);
+  return cudaGetLastError();
 }
 
 }  // namespace ptd

@@ -41,6 +41,15 @@ cudaError_t launch_resolve_hdr(const double *accum, uint32_t n, uint32_t samples
 cudaError_t launch_resolve_image(const double *accum, uint32_t n, uint32_t samples, float4 bg, uchar4 bg_bytes,
                                  uint32_t tone_map, float exposure, uchar4 *out, cudaStream_t st);
 cudaError_t launch_debug_sobol(uint32_t n, uint32_t seed, float4 *out, cudaStream_t st);
+// RenderBackend::Raycast (raycast.cuh): one sample per render pixel
+// (rw x rh), then the aa x aa box resolve into HDR and / or RGBA8.
+cudaError_t launch_raycast(const DevScene &s, const pt_camera &cam, uint32_t rw, uint32_t rh, uint32_t mode,
+                           uint32_t max_depth, const float light_dir[3], float light_intensity, float near_plane,
+                           float far_plane, const float decode[256], float4 *samples, uint8_t *covered,
+                           uint32_t *err, int num_sms, cudaStream_t st);
+cudaError_t launch_raycast_resolve(const float4 *samples, const uint8_t *covered, uint32_t out_w, uint32_t out_h,
+                                   uint32_t aa, float4 bg, uint32_t tone, float exposure, float4 *hdr, uchar4 *rgba,
+                                   cudaStream_t st);
 cudaError_t launch_debug_pattern(const DevRequest *rq, uint32_t npix, uint32_t index, uint32_t pattern, float4 *out,
                                  cudaStream_t st);
 cudaError_t launch_debug_primary(const DevRequest *rq, uint32_t npix, uint32_t index, uint32_t *out_g, float4 *out_tb,

@@ -63,6 +63,8 @@ SIGNATURES = {
                               C.POINTER(abi.pt_environment), u8p, C.c_size_t]),
     "pt_refine_noalloc": (i32, [vp, u32, C.POINTER(abi.pt_camera), C.POINTER(abi.pt_render_options), u32, u32,
                                 C.c_void_p]),
+    "pt_raycast_render": (i32, [vp, u32, C.POINTER(abi.pt_camera), C.POINTER(abi.pt_raycast_options), fp,
+                                C.c_size_t, u8p, C.c_size_t]),
     # include/pt_b200_serve.h
     "pt_server_create": (i32, [vp, C.POINTER(abi.pt_server_config), C.POINTER(vp)]),
     "pt_server_destroy": (None, [vp]),

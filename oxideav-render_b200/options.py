@@ -155,6 +155,25 @@ class RenderOptions:
         o.path_trace = self.path_trace.to_c()
         return o
 
+    def to_raycast_c(self, near_plane: float, far_plane: float) -> abi.pt_raycast_options:
+        """The raycast backend's options (include/pt_b200.h pt_raycast_options)."""
+        o = abi.pt_raycast_options()
+        o.width = max(int(self.width), 1)
+        o.height = max(int(self.height), 1)
+        o.aa = int(self.aa)
+        o.shading = int(self.shading.value)
+        o.light_azimuth_deg = float(self.light.azimuth_deg)
+        o.light_elevation_deg = float(self.light.elevation_deg)
+        o.light_intensity = float(self.light.intensity)
+        for k in range(4):
+            o.background[k] = int(self.background.rgba[k]) & 0xFF
+        o.tone_map = int(self.tone_map)
+        o.exposure = float(self.exposure)
+        o.max_ray_depth = int(self.max_ray_depth)
+        o.near_plane = float(near_plane)
+        o.far_plane = float(far_plane)
+        return o
+
     def validate(self) -> None:
         """RenderOptions::validate (src/options.rs:643-757)."""
 

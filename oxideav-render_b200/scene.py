@@ -285,6 +285,8 @@ class SceneCamera:
     perspective: bool = True
     yfov: float = math.pi / 3
     ymag: float = 1.0
+    znear: float = 0.01
+    zfar: Optional[float] = None  # None: infinite (perspective) / unset
 
 
 def _normalise(v):
@@ -649,6 +651,8 @@ class Camera:
     half_w: float
     half_h: float
     projection: Projection = Projection.Perspective
+    near: float = 0.01   # clip planes (DepthDebug): Camera::near / far
+    far: float = 1000.0
 
     def to_c(self) -> abi.pt_camera:
         c = abi.pt_camera()
@@ -662,8 +666,9 @@ class Camera:
         return c
 
     @staticmethod
-    def from_scene_camera(cam: SceneCamera, width: int, height: int) -> "Camera":
-        """Camera::from_scene_camera (src/camera.rs:208-332)."""
+    def from_scene_camera(cam: SceneCamera, width: int, height: int, mn=None, mx=None) -> "Camera":
+        """Camera::from_scene_camera (src/camera.rs:208-332); `mn` / `mx`
+        bound the scene (the far plane of an infinite or unset zfar)."""
         w = cam.world
         eye = w[:3, 3]
         forward = _normalise(-w[:3, 2])
@@ -677,12 +682,28 @@ class Camera:
                 side = np.array([1.0, 0.0, 0.0])
         up = np.cross(side, forward)
         aspect = max(width, 1) / max(height, 1)
+        far_extent = 0.0
+        if mn is not None and mx is not None:
+            for i in range(8):
+                c = np.array([mx[0] if i & 1 else mn[0], mx[1] if i & 2 else mn[1], mx[2] if i & 4 else mn[2]], float)
+                d = float(np.dot(c - eye, forward))
+                if math.isfinite(d):
+                    far_extent = max(far_extent, d)
+        zfar = cam.zfar
         if cam.perspective:
             yfov = cam.yfov if (math.isfinite(cam.yfov) and 1e-4 < cam.yfov < math.pi - 1e-3) else math.pi / 3
             th = math.tan(yfov * 0.5)
-            return Camera(tuple(eye), tuple(forward), tuple(side), tuple(up), th * aspect, th, Projection.Perspective)
+            near = cam.znear if (math.isfinite(cam.znear) and cam.znear > 0.0) else 0.01
+            far = zfar if (zfar is not None and math.isfinite(zfar) and zfar > near) else \
+                max(far_extent * 1.05, near * 2.0 + 1e-3)
+            return Camera(tuple(eye), tuple(forward), tuple(side), tuple(up), th * aspect, th, Projection.Perspective,
+                          near, far)
         hh = abs(cam.ymag) if (math.isfinite(cam.ymag) and abs(cam.ymag) > 1e-6) else 1.0
-        return Camera(tuple(eye), tuple(forward), tuple(side), tuple(up), hh * aspect, hh, Projection.Orthographic)
+        near = cam.znear if math.isfinite(cam.znear) else 0.0
+        far = zfar if (zfar is not None and math.isfinite(zfar) and zfar > near) else \
+            max(far_extent * 1.05, near + 1e-3)
+        return Camera(tuple(eye), tuple(forward), tuple(side), tuple(up), hh * aspect, hh, Projection.Orthographic,
+                      near, far)
 
     @staticmethod
     def build(width: int, height: int, mn, mx, opts: RenderOptions) -> "Camera":
@@ -703,6 +724,7 @@ class Camera:
             d = np.array([math.cos(el) * math.sin(az), math.sin(el), math.cos(el) * math.cos(az)])
             eye = center + d * dist
         else:
+            dist = auto
             eye = center + np.array([0.0, 0.0, auto])
         forward = _normalise(center - eye)
         side = _normalise(np.cross(forward, [0.0, 1.0, 0.0]))
@@ -715,13 +737,17 @@ class Camera:
                                             and opts.camera.distance > 0) else 1.0
             half = radius * zoom
             hw, hh = (half * aspect, half) if aspect >= 1.0 else (half, half / aspect)
+        if persp:
+            near, far = max(dist - extent, extent * 0.01), dist + extent * 2.0
+        else:
+            near, far = min(dist - extent * 2.0, -extent), dist + extent * 2.0
         return Camera(tuple(eye), tuple(forward), tuple(side), tuple(up), hw, hh,
-                      Projection.Perspective if persp else Projection.Orthographic)
+                      Projection.Perspective if persp else Projection.Orthographic, near, far)
 
     @staticmethod
     def resolve(scene: PreparedScene, opts: RenderOptions, width: int, height: int) -> "Camera":
         """Camera::resolve (src/camera.rs:177-188)."""
         mn, mx = scene.bounds_or_unit()
         if opts.scene_camera is not None and 0 <= opts.scene_camera < len(scene.cameras):
-            return Camera.from_scene_camera(scene.cameras[opts.scene_camera], width, height)
+            return Camera.from_scene_camera(scene.cameras[opts.scene_camera], width, height, mn, mx)
         return Camera.build(width, height, mn, mx, opts)
