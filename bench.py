@@ -502,6 +502,57 @@ def run_reference(args):
     }))
 
 
+def run_raycast(ctx, api, torch, scene, opts, cpu: bool, steps: int = 3):
+    """RenderBackend::Raycast (Phong / Whitted, the default shading mode) on
+    the workload's scene and camera: one-shot renders through
+    RaycastCudaRenderer (scene prepared + uploaded per call, as the
+    reference's render does) and raycasts of an already-uploaded scene, plus
+    the oracle's CPU restatement of the same frame."""
+    import ctypes as C
+    from oxideav_render_b200.options import ShadingMode
+    from oxideav_render_b200.scene import Camera
+    o = opts.replace(shading=ShadingMode.Phong, aa=1)
+    samples = o.width * o.height * o.aa * o.aa
+    r = api.RaycastCudaRenderer(ctx)
+    img = r.render(scene, o)
+    one_shot = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img = r.render(scene, o)
+        one_shot.append(time.perf_counter() - t0)
+    cam = Camera.resolve(scene, o, o.width * o.aa, o.height * o.aa)
+    desc = scene.to_desc(o)
+    sid = ctx.upload(desc)
+    ctx.bvh_wait(sid)
+    c, ro = cam.to_c(), o.to_raycast_c(cam.near, cam.far)
+    out = np.zeros((o.height, o.width, 4), np.uint8)
+    resident = []
+    for i in range(steps + 1):
+        t0 = time.perf_counter()
+        ctx.check(ctx.lib.pt_raycast_render(ctx.ptr, sid, C.byref(c), C.byref(ro), None, 0,
+                                            out.ctypes.data_as(C.POINTER(C.c_uint8)), out.size))
+        if i > 0:
+            resident.append(time.perf_counter() - t0)
+    ctx.release(sid)
+    res = {"workload": f"Phong (Whitted: shadow, mirror and refraction rays, depth {o.max_ray_depth}) "
+                       f"{o.width}x{o.height}, aa {o.aa}",
+           "samples_per_frame": samples,
+           "one_shot_ms": 1000 * statistics.median(one_shot),
+           "one_shot_samples_per_s": samples / statistics.median(one_shot),
+           "resident_ms": 1000 * statistics.median(resident),
+           "resident_samples_per_s": samples / statistics.median(resident),
+           "identical_to_oracle": None, "cpu_ms": None}
+    if cpu:
+        oracle = entry.load_oracle()
+        t0 = time.perf_counter()
+        _, want = oracle.raycast(scene, o)
+        res["cpu_ms"] = 1000 * (time.perf_counter() - t0)
+        res["cpu_threads"] = min(64, os.cpu_count() or 1)
+        res["identical_to_oracle"] = bool(np.array_equal(img, want))
+    return res
+
+
 def run_uploads(args):
     """Profiling case: uploads the workload's scene `--upload-only` times
     (device BVH build and device mip chains) and prints the phase times."""
@@ -645,6 +696,9 @@ def run_b200(args):
                           "bvh_on_device": ctx.bvh_on_device(sid),
                           "upload_phases": {k: 1000 * v for k, v in ctx.upload_seconds(sid).items()}}
         ctx.release(sid)
+    raycast = None
+    if args.raycast:
+        raycast = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline)
     mixed = None
     if args.mixed > 0:
         mixed = run_mixed(ctx, api, torch, args.mixed, 2026 + rank)
@@ -673,6 +727,7 @@ def run_b200(args):
                          "ms_per_launch": stage[dom] / max(launches_of_dom, 1)},
             "e2e": e2e,
             "batched_mixed": mixed,
+            "raycast": raycast,
             "served": served,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
@@ -711,6 +766,8 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
     ap.add_argument("--plain-seconds", type=float, default=15.0, help="time budget of the plain-path sample")
+    ap.add_argument("--no-raycast", dest="raycast", action="store_false",
+                    help="skip the RenderBackend::Raycast measurement")
     ap.add_argument("--upload-only", type=int, default=0,
                     help="profiling case: upload the scene this many times (device BVH, device mips) and exit")
     args = ap.parse_args()
