@@ -524,7 +524,6 @@ def run_raycast(ctx, api, torch, scene, opts, cpu: bool, steps: int = 3):
     cam = Camera.resolve(scene, o, o.width * o.aa, o.height * o.aa)
     desc = scene.to_desc(o)
     sid = ctx.upload(desc)
-    ctx.bvh_wait(sid)
     c, ro = cam.to_c(), o.to_raycast_c(cam.near, cam.far)
     out = np.zeros((o.height, o.width, 4), np.uint8)
     resident = []
@@ -593,10 +592,6 @@ def run_b200(args):
     if env is not None:
         tracer.set_environment(api.EnvironmentMap(env))
     tracer.sync(scene, opts)
-    # The resident scene's steady state: a large scene's first tree is built
-    # on the device and replaced by the host binned-SAH tree once that is
-    # built in the background (pt_set_bvh_builder AUTO); wait for it.
-    ctx.bvh_wait(tracer._scene_id)
     tuned = None
     if args.autotune:
         # pt_autotune: calibration refines on a scratch accumulator pick this

@@ -84,20 +84,20 @@ PT_API pt_status pt_tune_reset(pt_context *ctx);
 PT_API pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes, uint32_t *leaves,
                              uint32_t *max_depth, double *sah_cost, double *build_seconds);
 
-/* Where pt_scene_upload builds a scene's BVH: on the host (binned SAH),
- * on the device (Morton order + parallel locally-ordered clustering with an
- * SAH leaf collapse, for scenes of at least 64 triangles), or AUTO (the
- * default): scenes of at least 16,384 triangles get a device-built tree at
- * once while the host binned-SAH tree (fewer node visits per ray) is built
- * on host threads in the background; the next refine after it finishes
- * (or pt_autotune, or pt_scene_bvh_wait) switches the scene to it. Smaller
- * scenes build on the host. A device-built tree deeper than the traversal
- * stacks allow is rebuilt on the host. Images are identical whichever tree
- * a scene has. */
+/* Where pt_scene_upload builds a scene's BVH: on the host (binned SAH, 16
+ * bins per axis), on the device with the same split rule (DEVICE: the
+ * host's tree, built level by level on the GPU), on the device by
+ * parallel locally-ordered clustering over Morton order with an SAH leaf
+ * collapse (DEVICE_PLOC: faster to build, 3-12 % more node visits per ray),
+ * or AUTO (the default): DEVICE for scenes of at least 16,384 triangles,
+ * the host below. The device builders take scenes of at least 64
+ * triangles; a device-built tree deeper than the traversal stacks allow is
+ * rebuilt on the host. Images are identical whichever tree a scene has. */
 typedef enum pt_bvh_builder {
   PT_BVH_BUILD_AUTO = 0,
   PT_BVH_BUILD_HOST = 1,
-  PT_BVH_BUILD_DEVICE = 2
+  PT_BVH_BUILD_DEVICE = 2,
+  PT_BVH_BUILD_DEVICE_PLOC = 3
 } pt_bvh_builder;
 PT_API pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder);
 /* 1 when the scene's current BVH was built on the device. */
@@ -113,9 +113,6 @@ PT_API pt_status pt_scene_upload_seconds(pt_context *ctx, uint32_t scene_id, dou
  * reports the pool's texel count in `total`. */
 PT_API pt_status pt_debug_scene_texels(pt_context *ctx, uint32_t scene_id, float *out, uint64_t capacity,
                                        uint64_t *total);
-/* Waits for the scene's background host tree (BVH_BUILD_AUTO) and switches
- * the scene to it; PT_OK at once when none is pending. */
-PT_API pt_status pt_scene_bvh_wait(pt_context *ctx, uint32_t scene_id);
 
 /* Schedule of the hot loop: one path per thread (megakernel), or the
  * wavefront (extend / shade / shadow kernels over compacted queues). Both

@@ -46,7 +46,7 @@ PT_LIGHT_DIRECTIONAL, PT_LIGHT_POINT, PT_LIGHT_SPOT = 0, 1, 2
 PT_PERSPECTIVE, PT_ORTHOGRAPHIC = 0, 1
 PT_MIS, PT_LIGHT_ONLY, PT_BSDF_ONLY = 0, 1, 2
 PT_TONE_CLAMP, PT_TONE_REINHARD, PT_TONE_ACES = 0, 1, 2
-PT_BVH_BUILD_AUTO, PT_BVH_BUILD_HOST, PT_BVH_BUILD_DEVICE = 0, 1, 2
+PT_BVH_BUILD_AUTO, PT_BVH_BUILD_HOST, PT_BVH_BUILD_DEVICE, PT_BVH_BUILD_DEVICE_PLOC = 0, 1, 2, 3
 
 f3 = C.c_float * 3
 f4 = C.c_float * 4

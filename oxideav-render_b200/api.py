@@ -80,7 +80,7 @@ class Context:
                 "build_seconds": sec.value}
 
     def set_bvh_builder(self, builder: int) -> None:
-        """pt_set_bvh_builder: abi.PT_BVH_BUILD_AUTO / _HOST / _DEVICE."""
+        """pt_set_bvh_builder: abi.PT_BVH_BUILD_AUTO / _HOST / _DEVICE / _DEVICE_PLOC."""
         self.check(self.lib.pt_set_bvh_builder(self.ptr, builder))
 
     def upload_seconds(self, scene_id: int) -> dict:
@@ -97,10 +97,6 @@ class Context:
         self.check(self.lib.pt_debug_scene_texels(self.ptr, scene_id, out.ctypes.data_as(C.POINTER(C.c_float)),
                                                   total.value, C.byref(total)))
         return out
-
-    def bvh_wait(self, scene_id: int) -> None:
-        """pt_scene_bvh_wait: switch the scene to its background host tree."""
-        self.check(self.lib.pt_scene_bvh_wait(self.ptr, scene_id))
 
     def bvh_on_device(self, scene_id: int) -> bool:
         v = C.c_int()

@@ -597,6 +597,498 @@ __global__ void k_write_records(Nodes nd, const uint32_t *vals, const float *pos
   }
 }
 
+// ---------------------------------------------------------------- binned SAH, top down
+// The host builder's split rule, level by level on the device: per active
+// node the bounds of its triangles and centroids, 16 bins per axis of the
+// centroid extent, the sweep for the cheapest split (cost 1 + (A_L n_L +
+// A_R n_R) / A_parent, leaf when at most 8 triangles cost no more), a
+// stable partition, the children. Nodes near the depth limit, or without a
+// valid split, halve their range by index.
+constexpr int kSahBins = 16;
+constexpr uint32_t kSahNone = 0xffffffffu;
+constexpr uint32_t kSahHalve = 0xfffffffeu;
+constexpr int kSahBinWords = 3 * kSahBins * 7;  // per axis and bin: count, lo.xyz, hi.xyz
+
+struct SahNodes {
+  float4 *lo, *hi;          // node bounds
+  uint32_t *begin, *count;  // triangle range
+  uint32_t *depth;
+  int *left;                // first of two consecutive children, -1 for a leaf
+  uint32_t *state;          // NS_WIDE marks (four-child layout)
+};
+
+struct SahLevel {
+  const uint32_t *act;  // active node ids, ranges in increasing order
+  uint32_t m;           // active nodes
+  uint32_t *bnd;        // 12 per active node: ord(lo), ord(hi), ord(clo), ord(chi)
+  uint32_t *bins;       // kSahBinWords per active node
+  uint32_t *split;      // per active node: axis << 8 | bin, kSahNone (leaf) or kSahHalve
+};
+
+// Builder::area of the host build (0 for an empty or NaN box).
+__device__ __forceinline__ float host_area(float4 lo, float4 hi) {
+  float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+  if (!(dx >= 0.0f) || !(dy >= 0.0f) || !(dz >= 0.0f)) return 0.0f;
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Bin of a centroid offset times the bin scale: truncation, clamped to the
+// bins (a NaN offset lands in bin 0).
+__device__ __forceinline__ int sah_bin(float f) { return f >= 1.0f ? min(kSahBins - 1, (int)fminf(f, 16.0f)) : 0; }
+
+// Active node of every triangle (binary search of the sorted ranges).
+__global__ void k_sah_seg(SahNodes nd, SahLevel lv, uint32_t n, uint32_t *seg) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = lv.m;
+    while (hi - lo > 1) {
+      uint32_t mid = (lo + hi) >> 1;
+      if (nd.begin[lv.act[mid]] <= i)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint32_t v = lv.act[lo];
+    seg[i] = (i >= nd.begin[v] && i < nd.begin[v] + nd.count[v]) ? lo : kSahNone;
+  }
+}
+
+__device__ __forceinline__ void prim_box(const float4 *plo, const float4 *phi, uint32_t i, float l[3], float h[3],
+                                         float c[3]) {
+  const float4 a = plo[i], b = phi[i];
+  l[0] = a.x, l[1] = a.y, l[2] = a.z;
+  h[0] = b.x, h[1] = b.y, h[2] = b.z;
+  for (int k = 0; k < 3; ++k) c[k] = (l[k] + h[k]) * 0.5f;
+}
+
+// Bounds of every active node: a warp whose 32 triangles share a node
+// reduces them first (one atomic per bound), others update per lane.
+__global__ void k_sah_bounds(const float4 *plo, const float4 *phi, const uint32_t *seg, uint32_t n, SahLevel lv) {
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t s = i < n ? seg[i] : kSahNone;
+    float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float cl[3] = {INFINITY, INFINITY, INFINITY}, ch[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (s != kSahNone) {
+      float c[3];
+      prim_box(plo, phi, i, l, h, c);
+      for (int k = 0; k < 3; ++k) cl[k] = ch[k] = c[k];
+    }
+    const uint32_t s0 = __shfl_sync(0xffffffffu, s, 0);
+    if (__all_sync(0xffffffffu, s == s0)) {
+      if (s0 == kSahNone) continue;
+      for (int k = 0; k < 3; ++k)
+        for (int d = 16; d > 0; d >>= 1) {
+          l[k] = fminf(l[k], __shfl_xor_sync(0xffffffffu, l[k], d));
+          h[k] = fmaxf(h[k], __shfl_xor_sync(0xffffffffu, h[k], d));
+          cl[k] = fminf(cl[k], __shfl_xor_sync(0xffffffffu, cl[k], d));
+          ch[k] = fmaxf(ch[k], __shfl_xor_sync(0xffffffffu, ch[k], d));
+        }
+      if ((threadIdx.x & 31) != 0) continue;
+    } else if (s == kSahNone) {
+      continue;
+    }
+    uint32_t *b = lv.bnd + 12ull * s;
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(b + k, ord_of(l[k]));
+      atomicMax(b + 3 + k, ord_of(h[k]));
+      atomicMin(b + 6 + k, ord_of(cl[k]));
+      atomicMax(b + 9 + k, ord_of(ch[k]));
+    }
+  }
+}
+
+__device__ __forceinline__ void node_binning(const uint32_t *b, float clo[3], float scale[3], bool use[3]) {
+  for (int k = 0; k < 3; ++k) {
+    clo[k] = float_of(b[6 + k]);
+    float span = float_of(b[9 + k]) - clo[k];
+    use[k] = span > 0.0f;
+    scale[k] = use[k] ? (float)kSahBins / span : 0.0f;
+  }
+}
+
+// Bin counts and bounds: a tile of triangles of one node accumulates in
+// shared memory and flushes once; tiles spanning several nodes (small
+// nodes) update the nodes' bins directly.
+__global__ void __launch_bounds__(kThreads) k_sah_bins(const float4 *plo, const float4 *phi, const uint32_t *seg,
+                                                       uint32_t n, SahLevel lv) {
+  __shared__ uint32_t sb[kSahBinWords];
+  constexpr uint32_t kTile = kThreads * 8;
+  for (uint32_t t0 = blockIdx.x * kTile; t0 < n; t0 += gridDim.x * kTile) {
+    const uint32_t t1 = min(n, t0 + kTile);
+    const uint32_t sa = seg[t0], sz = seg[t1 - 1];
+    const bool uniform = sa == sz && sa != kSahNone;
+    if (uniform) {
+      for (int w = threadIdx.x; w < kSahBinWords; w += kThreads) {
+        const int f = w % 7;
+        sb[w] = (f >= 1 && f <= 3) ? 0xffffffffu : 0u;
+      }
+      __syncthreads();
+    }
+    for (uint32_t i = t0 + threadIdx.x; i < t1; i += kThreads) {
+      const uint32_t s = seg[i];
+      if (s == kSahNone) continue;
+      float clo[3], scale[3];
+      bool use[3];
+      node_binning(lv.bnd + 12ull * s, clo, scale, use);
+      float l[3], h[3], c[3];
+      prim_box(plo, phi, i, l, h, c);
+      uint32_t *dst = uniform ? sb : lv.bins + (uint64_t)kSahBinWords * s;
+      for (int k = 0; k < 3; ++k) {
+        if (!use[k]) continue;
+        const int bin = sah_bin((c[k] - clo[k]) * scale[k]);
+        uint32_t *w = dst + (k * kSahBins + bin) * 7;
+        atomicAdd(w, 1u);
+        for (int a = 0; a < 3; ++a) {
+          atomicMin(w + 1 + a, ord_of(l[a]));
+          atomicMax(w + 4 + a, ord_of(h[a]));
+        }
+      }
+    }
+    if (uniform) {
+      __syncthreads();
+      uint32_t *g = lv.bins + (uint64_t)kSahBinWords * sa;
+      for (int w = threadIdx.x; w < kSahBinWords; w += kThreads) {
+        const int f = w % 7;
+        if (f == 0) {
+          if (sb[w]) atomicAdd(g + w, sb[w]);
+        } else if (f <= 3) {
+          if (sb[w] != 0xffffffffu) atomicMin(g + w, sb[w]);
+        } else if (sb[w]) {
+          atomicMax(g + w, sb[w]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void k_sah_init_bins(SahLevel lv) {
+  const uint64_t total = (uint64_t)lv.m * kSahBinWords;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+    const int f = (int)(w % 7);
+    lv.bins[w] = (f >= 1 && f <= 3) ? 0xffffffffu : 0u;
+  }
+  const uint64_t tb = (uint64_t)lv.m * 12;
+  for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < tb; w += (uint64_t)gridDim.x * blockDim.x) {
+    const int f = (int)(w % 12);
+    lv.bnd[w] = (f < 3 || (f >= 6 && f < 9)) ? 0xffffffffu : 0u;
+  }
+}
+
+// The split of every active node (the host builder's sweep).
+__global__ void k_sah_split(SahNodes nd, SahLevel lv, uint32_t *max_depth) {
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < lv.m; a += gridDim.x * blockDim.x) {
+    const uint32_t v = lv.act[a];
+    const uint32_t *b = lv.bnd + 12ull * a;
+    const float4 lo = make_float4(float_of(b[0]), float_of(b[1]), float_of(b[2]), 0.0f);
+    const float4 hi = make_float4(float_of(b[3]), float_of(b[4]), float_of(b[5]), 0.0f);
+    nd.lo[v] = lo;
+    nd.hi[v] = hi;
+    const uint32_t cnt = nd.count[v], depth = nd.depth[v];
+    if (cnt <= 1) {
+      lv.split[a] = kSahNone;
+      atomicMax(max_depth, depth);
+      continue;
+    }
+    uint32_t need = 0;
+    for (uint32_t c = cnt; c > kMaxLeafTris; c = (c + 1) / 2) ++need;
+    const bool median = depth + need >= 56;
+    int axis = -1, best_bin = 0;
+    float best_cost = INFINITY;
+    if (!median) {
+      const float parent = host_area(lo, hi);
+      bool use[3];
+      float clo[3], scale[3];
+      node_binning(b, clo, scale, use);
+      const uint32_t *bins = lv.bins + (uint64_t)kSahBinWords * a;
+      for (int k = 0; k < 3; ++k) {
+        if (!use[k]) continue;
+        float rl[kSahBins][3], rh[kSahBins][3];
+        uint32_t rc[kSahBins];
+        float accl[3] = {INFINITY, INFINITY, INFINITY}, acch[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t acc = 0;
+        for (int bb = kSahBins - 1; bb >= 1; --bb) {
+          const uint32_t *w = bins + (k * kSahBins + bb) * 7;
+          acc += w[0];
+          if (w[0])
+            for (int q = 0; q < 3; ++q) {
+              accl[q] = fminf(accl[q], float_of(w[1 + q]));
+              acch[q] = fmaxf(acch[q], float_of(w[4 + q]));
+            }
+          rc[bb] = acc;
+          for (int q = 0; q < 3; ++q) {
+            rl[bb][q] = accl[q];
+            rh[bb][q] = acch[q];
+          }
+        }
+        float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+        uint32_t lc = 0;
+        for (int s = 1; s < kSahBins; ++s) {
+          const uint32_t *w = bins + (k * kSahBins + s - 1) * 7;
+          lc += w[0];
+          if (w[0])
+            for (int q = 0; q < 3; ++q) {
+              ll[q] = fminf(ll[q], float_of(w[1 + q]));
+              lh[q] = fmaxf(lh[q], float_of(w[4 + q]));
+            }
+          if (lc == 0 || rc[s] == 0) continue;
+          const float4 l4 = make_float4(ll[0], ll[1], ll[2], 0.0f), h4 = make_float4(lh[0], lh[1], lh[2], 0.0f);
+          const float4 r4l = make_float4(rl[s][0], rl[s][1], rl[s][2], 0.0f);
+          const float4 r4h = make_float4(rh[s][0], rh[s][1], rh[s][2], 0.0f);
+          const float cost =
+              1.0f + (host_area(l4, h4) * (float)lc + host_area(r4l, r4h) * (float)rc[s]) / fmaxf(parent, 1e-30f);
+          if (cost < best_cost) {
+            best_cost = cost;
+            axis = k;
+            best_bin = s;
+          }
+        }
+      }
+      if (cnt <= kMaxLeafTris && (axis < 0 || (float)cnt <= best_cost)) {
+        lv.split[a] = kSahNone;
+        atomicMax(max_depth, depth);
+        continue;
+      }
+    }
+    lv.split[a] = axis >= 0 ? ((uint32_t)axis << 8 | (uint32_t)best_bin) : kSahHalve;
+  }
+}
+
+// Left flags of the triangles of SAH-split nodes.
+__global__ void k_sah_flags(const float4 *plo, const float4 *phi, const uint32_t *seg, uint32_t n, SahLevel lv,
+                            uint32_t *flag) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = seg[i];
+    uint32_t f = 0;
+    if (s != kSahNone) {
+      const uint32_t sp = lv.split[s];
+      if (sp < kSahHalve) {
+        const int axis = (int)(sp >> 8), bin = (int)(sp & 0xffu);
+        float clo[3], scale[3];
+        bool use[3];
+        node_binning(lv.bnd + 12ull * s, clo, scale, use);
+        float l[3], h[3], c[3];
+        prim_box(plo, phi, i, l, h, c);
+        f = sah_bin((c[axis] - clo[axis]) * scale[axis]) < bin ? 1u : 0u;
+      }
+    }
+    flag[i] = f;
+  }
+}
+
+// Left triangles of a split node's range from the exclusive scan of the
+// flags (`end` may be n).
+__device__ __forceinline__ uint32_t left_count(const uint32_t *scan, const uint32_t *flag, uint32_t n, uint32_t b0,
+                                               uint32_t e0) {
+  return (e0 < n ? scan[e0] : scan[n - 1] + flag[n - 1]) - scan[b0];
+}
+
+// Stable partition of the split nodes' ranges (others keep their order).
+__global__ void k_sah_scatter(const float4 *plo, const float4 *phi, float4 *qlo, float4 *qhi, const uint32_t *seg,
+                              const uint32_t *flag, const uint32_t *scan, uint32_t n, SahNodes nd, SahLevel lv) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t s = seg[i];
+    uint32_t dst = i;
+    if (s != kSahNone && lv.split[s] < kSahHalve) {
+      const uint32_t v = lv.act[s], b0 = nd.begin[v], e0 = b0 + nd.count[v];
+      const uint32_t total_left = left_count(scan, flag, n, b0, e0);
+      const uint32_t lrank = scan[i] - scan[b0];
+      dst = flag[i] ? b0 + lrank : b0 + total_left + (i - b0 - lrank);
+    }
+    qlo[dst] = plo[i];
+    qhi[dst] = phi[i];
+  }
+}
+
+__global__ void k_sah_split_flags(SahLevel lv, uint32_t *out) {
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < lv.m; a += gridDim.x * blockDim.x)
+    out[a] = lv.split[a] != kSahNone ? 1u : 0u;
+}
+
+// Children of the split nodes: ids from a scan of the split flags.
+__global__ void k_sah_children(SahNodes nd, SahLevel lv, const uint32_t *split_scan, uint32_t next_id,
+                               const uint32_t *scan, const uint32_t *flag, uint32_t n, uint32_t *next_act) {
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < lv.m; a += gridDim.x * blockDim.x) {
+    const uint32_t v = lv.act[a], sp = lv.split[a];
+    if (sp == kSahNone) {
+      nd.left[v] = -1;
+      continue;
+    }
+    const uint32_t b0 = nd.begin[v], cnt = nd.count[v];
+    const uint32_t nl = sp == kSahHalve ? cnt / 2 : left_count(scan, flag, n, b0, b0 + cnt);
+    const uint32_t k = split_scan[a];
+    const uint32_t c = next_id + 2 * k;
+    nd.left[v] = (int)c;
+    nd.begin[c] = b0;
+    nd.count[c] = nl;
+    nd.begin[c + 1] = b0 + nl;
+    nd.count[c + 1] = cnt - nl;
+    nd.depth[c] = nd.depth[c + 1] = nd.depth[v] + 1;
+    nd.state[c] = nd.state[c + 1] = 0;
+    next_act[2 * k] = c;
+    next_act[2 * k + 1] = c + 1;
+  }
+}
+
+__device__ __forceinline__ bool sah_interior(const SahNodes &nd, uint32_t c) { return nd.left[c] >= 0; }
+
+// Children of the four-child node of interior node v (the host layout's
+// rule: open the interior child of largest surface area until four).
+__device__ int sah_wide_children(const SahNodes &nd, uint32_t v, uint32_t ch[4]) {
+  ch[0] = (uint32_t)nd.left[v];
+  ch[1] = ch[0] + 1;
+  int nch = 2;
+  while (nch < 4) {
+    int best = -1;
+    float best_area = -1.0f;
+    for (int i = 0; i < nch; ++i) {
+      if (!sah_interior(nd, ch[i])) continue;
+      float a = host_area(nd.lo[ch[i]], nd.hi[ch[i]]);
+      if (a > best_area) {
+        best_area = a;
+        best = i;
+      }
+    }
+    if (best < 0) break;
+    const uint32_t oc = (uint32_t)nd.left[ch[best]];
+    for (int i = nch; i > best + 1; --i) ch[i] = ch[i - 1];
+    ch[best] = oc;
+    ch[best + 1] = oc + 1;
+    ++nch;
+  }
+  return nch;
+}
+
+// Four-child marks, one level of node ids at a time (parents first).
+__global__ void k_sah_mark(SahNodes nd, uint32_t v0, uint32_t v1) {
+  for (uint32_t v = v0 + blockIdx.x * blockDim.x + threadIdx.x; v < v1; v += gridDim.x * blockDim.x) {
+    if (!sah_interior(nd, v) || !(nd.state[v] & NS_WIDE)) continue;
+    uint32_t ch[4];
+    const int nch = sah_wide_children(nd, v, ch);
+    for (int i = 0; i < nch; ++i)
+      if (sah_interior(nd, ch[i])) nd.state[ch[i]] |= NS_WIDE;
+  }
+}
+
+// (two-child node) << 32 | (four-child node), in id order.
+__global__ void k_sah_layout_flags(SahNodes nd, uint32_t total, uint64_t *flags) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+    const uint64_t two = sah_interior(nd, v) ? 1u : 0u;
+    const uint64_t four = (two && (nd.state[v] & NS_WIDE)) ? 1u : 0u;
+    flags[v] = (two << 32) | four;
+  }
+}
+
+__device__ __forceinline__ int sah_ref(const SahNodes &nd, const uint64_t *offs, uint32_t c, bool wide,
+                                       uint32_t &count) {
+  if (sah_interior(nd, c)) {
+    count = 0;
+    const uint64_t o = offs[c];
+    return (int)(wide ? (uint32_t)o : (uint32_t)(o >> 32));
+  }
+  count = nd.count[c];
+  return (int)~(nd.begin[c] | (count << kLeafShift));
+}
+
+__global__ void k_sah_write_nodes(SahNodes nd, uint32_t total, const uint64_t *offs, BvhNode *out2, Bvh4Node *out4) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+    if (!sah_interior(nd, v)) continue;
+    const uint64_t o = offs[v];
+    const uint32_t c0 = (uint32_t)nd.left[v], c1 = c0 + 1;
+    float l0[3], h0[3], l1[3], h1[3];
+    pad_box(nd.lo[c0], nd.hi[c0], l0, h0);
+    pad_box(nd.lo[c1], nd.hi[c1], l1, h1);
+    uint32_t n0, n1;
+    const int r0 = sah_ref(nd, offs, c0, false, n0), r1 = sah_ref(nd, offs, c1, false, n1);
+    BvhNode g;
+    g.a = make_float4(l0[0], h0[0], l0[1], h0[1]);
+    g.b = make_float4(l1[0], h1[0], l1[1], h1[1]);
+    g.c = make_float4(l0[2], h0[2], l1[2], h1[2]);
+    g.d = make_int4(r0, r1, (int)n0, (int)n1);
+    out2[o >> 32] = g;
+    if (!(nd.state[v] & NS_WIDE)) continue;
+    uint32_t ch[4];
+    const int nch = sah_wide_children(nd, v, ch);
+    float bl[3][4], bh[3][4];
+    int ref[4];
+    for (int i = 0; i < 4; ++i) {
+      if (i < nch) {
+        float l[3], h[3];
+        pad_box(nd.lo[ch[i]], nd.hi[ch[i]], l, h);
+        for (int k = 0; k < 3; ++k) {
+          bl[k][i] = l[k];
+          bh[k][i] = h[k];
+        }
+        uint32_t cnt;
+        ref[i] = sah_ref(nd, offs, ch[i], true, cnt);
+      } else {
+        for (int k = 0; k < 3; ++k) {
+          bl[k][i] = INFINITY;
+          bh[k][i] = -INFINITY;
+        }
+        ref[i] = kEmptyChild;
+      }
+    }
+    Bvh4Node q;
+    q.lo_x = make_float4(bl[0][0], bl[0][1], bl[0][2], bl[0][3]);
+    q.hi_x = make_float4(bh[0][0], bh[0][1], bh[0][2], bh[0][3]);
+    q.lo_y = make_float4(bl[1][0], bl[1][1], bl[1][2], bl[1][3]);
+    q.hi_y = make_float4(bh[1][0], bh[1][1], bh[1][2], bh[1][3]);
+    q.lo_z = make_float4(bl[2][0], bl[2][1], bl[2][2], bl[2][3]);
+    q.hi_z = make_float4(bh[2][0], bh[2][1], bh[2][2], bh[2][3]);
+    q.child = make_int4(ref[0], ref[1], ref[2], ref[3]);
+    q.pad = make_int4(0, 0, 0, 0);
+    out4[(uint32_t)o] = q;
+  }
+}
+
+// Triangle boxes (min / max of the three corners, as the host build), with
+// the global id in lo.w.
+__global__ void k_sah_prims(const float *pos, uint32_t n, float4 *lo, float4 *hi) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float *p = pos + 9ull * i;
+    float l[3], h[3];
+    for (int k = 0; k < 3; ++k) {
+      const float a = __ldg(p + k), b = __ldg(p + 3 + k), c = __ldg(p + 6 + k);
+      l[k] = fminf(fminf(a, b), c);
+      h[k] = fmaxf(fmaxf(a, b), c);
+    }
+    lo[i] = make_float4(l[0], l[1], l[2], __uint_as_float(i));
+    hi[i] = make_float4(h[0], h[1], h[2], 0.0f);
+  }
+}
+
+__global__ void k_sah_records(const float4 *plo, uint32_t n, const float *pos, const uint2 *tri_info,
+                              const DevMaterial *materials, float4 *records) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const uint32_t g = __float_as_uint(plo[r].w);
+    const float *p = pos + 9ull * g;
+    const pt_material &m = materials[__ldg(&tri_info[g].x)].m;
+    const uint32_t fl = (m.alpha_mode == PT_ALPHA_OPAQUE ? REC_OPAQUE : 0u) | (m.double_sided ? REC_DOUBLE_SIDED : 0u);
+    records[3ull * r] = make_float4(p[0], p[1], p[2], __uint_as_float(g));
+    records[3ull * r + 1] = make_float4(p[3], p[4], p[5], __uint_as_float(fl));
+    records[3ull * r + 2] = make_float4(p[6], p[7], p[8], 0.0f);
+  }
+}
+
+// SAH cost contribution of every node (traversal 1, intersection 1,
+// relative to the root box), summed by a scan.
+__global__ void k_sah_cost(SahNodes nd, uint32_t total, double *out) {
+  const double root = fmax((double)host_area(nd.lo[0], nd.hi[0]), 1e-30);
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < total; v += gridDim.x * blockDim.x) {
+    const double a = (double)host_area(nd.lo[v], nd.hi[v]) / root;
+    out[v] = sah_interior(nd, v) ? a : a * (double)nd.count[v];
+  }
+}
+
+__global__ void k_sah_root(SahNodes nd, uint32_t n, uint32_t *act) {
+  nd.begin[0] = 0;
+  nd.count[0] = n;
+  nd.depth[0] = 0;
+  nd.state[0] = NS_WIDE;
+  act[0] = 0;
+}
+
 // ---------------------------------------------------------------- host side
 struct Scratch {
   std::vector<void *> ptrs;
@@ -624,6 +1116,155 @@ struct Scratch {
 uint64_t align256(uint64_t x) { return (x + 255) & ~uint64_t(255); }
 
 }  // namespace
+
+std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_depth_allowed, bool &oom,
+                                 DeviceBuildInfo *info) {
+  oom = false;
+  const auto t0 = std::chrono::steady_clock::now();
+  const uint64_t n64 = sc.tri_count;
+  if (n64 < kMinDeviceTris) return "too few triangles for the device builder";
+  if (n64 >= (1ull << kLeafShift)) return "too many triangles for the leaf encoding";
+  const uint32_t n = (uint32_t)n64;
+  const uint32_t cap = 2 * n;  // nodes of a binary tree with non-empty leaves
+
+  Scratch s{{}, st};
+  float4 *plo = s.get<float4>(n), *phi = s.get<float4>(n), *qlo = s.get<float4>(n), *qhi = s.get<float4>(n);
+  uint32_t *seg = s.get<uint32_t>(n), *flag = s.get<uint32_t>(n), *pscan = s.get<uint32_t>(n);
+  uint32_t *scan32 = s.get<uint32_t>(scan_scratch_items(n));
+  SahNodes nd;
+  nd.lo = s.get<float4>(cap);
+  nd.hi = s.get<float4>(cap);
+  nd.begin = s.get<uint32_t>(cap);
+  nd.count = s.get<uint32_t>(cap);
+  nd.depth = s.get<uint32_t>(cap);
+  nd.left = s.get<int>(cap);
+  nd.state = s.get<uint32_t>(cap);
+  uint32_t *act = s.get<uint32_t>(n), *act2 = s.get<uint32_t>(n);
+  uint32_t *split = s.get<uint32_t>(n), *split_scan = s.get<uint32_t>(n), *split_flag = s.get<uint32_t>(n);
+  uint64_t *flags64 = s.get<uint64_t>(cap), *offs = s.get<uint64_t>(cap);
+  uint64_t *scan64 = s.get<uint64_t>(scan_scratch_items(cap));
+  uint32_t *counters = s.get<uint32_t>(2);  // max leaf depth
+  double *cost = s.get<double>(cap), *cost_scan = s.get<double>(scan_scratch_items(cap));
+  if (!s.err.empty()) {
+    oom = s.oom;
+    return s.err;
+  }
+  // Bounds and bins of the widest level so far, grown on demand.
+  uint32_t *bnd = nullptr, *bins = nullptr;
+  uint32_t level_cap = 0;
+  auto grow = [&](uint32_t m) -> bool {
+    if (m <= level_cap) return true;
+    const uint32_t want = std::max<uint32_t>(m, std::min<uint32_t>(n, level_cap * 2 + 1024));
+    bnd = s.get<uint32_t>(12ull * want);
+    bins = s.get<uint32_t>((uint64_t)kSahBinWords * want);
+    level_cap = want;
+    return s.err.empty();
+  };
+
+  const float *pos = sc.dev.pos;
+  cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), st);
+  k_sah_prims<<<grid_for(n), kThreads, 0, st>>>(pos, n, plo, phi);
+  k_sah_root<<<1, 1, 0, st>>>(nd, n, act);
+  std::vector<uint32_t> level_begin{0};
+  uint32_t m = 1, next_id = 1;
+  while (m > 0) {
+    if (level_begin.size() > 64) return "device SAH build exceeded 64 levels";
+    if (!grow(m)) {
+      oom = s.oom;
+      return s.err;
+    }
+    SahLevel lv{act, m, bnd, bins, split};
+    k_sah_init_bins<<<grid_for((uint64_t)m * kSahBinWords), kThreads, 0, st>>>(lv);
+    k_sah_seg<<<grid_for(n), kThreads, 0, st>>>(nd, lv, n, seg);
+    k_sah_bounds<<<grid_for(n), kThreads, 0, st>>>(plo, phi, seg, n, lv);
+    k_sah_bins<<<(unsigned)std::min<uint64_t>(tiles_of(n, kThreads * 8), 1u << 16), kThreads, 0, st>>>(plo, phi, seg,
+                                                                                                  n, lv);
+    k_sah_split<<<grid_for(m), kThreads, 0, st>>>(nd, lv, counters);
+    k_sah_flags<<<grid_for(n), kThreads, 0, st>>>(plo, phi, seg, n, lv, flag);
+    scan_exclusive<uint32_t>(flag, pscan, n, scan32, st);
+    k_sah_scatter<<<grid_for(n), kThreads, 0, st>>>(plo, phi, qlo, qhi, seg, flag, pscan, n, nd, lv);
+    k_sah_split_flags<<<grid_for(m), kThreads, 0, st>>>(lv, split_flag);
+    uint32_t *tot = scan_exclusive<uint32_t>(split_flag, split_scan, m, scan32, st);
+    k_sah_children<<<grid_for(m), kThreads, 0, st>>>(nd, lv, split_scan, next_id, pscan, flag, n, act2);
+    std::swap(plo, qlo);
+    std::swap(phi, qhi);
+    std::swap(act, act2);
+    uint32_t splits = 0;
+    cudaError_t e = cudaMemcpyAsync(&splits, tot, sizeof splits, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return std::string("device SAH build: ") + cudaGetErrorString(e);
+    if (next_id + 2ull * splits > cap) return "device SAH build ran out of nodes";
+    level_begin.push_back(next_id);
+    next_id += 2 * splits;
+    m = 2 * splits;
+  }
+  const uint32_t total = next_id;
+  // Four-child marks level by level (parents first), then both numberings.
+  for (size_t l = 0; l + 1 < level_begin.size(); ++l)
+    k_sah_mark<<<grid_for(level_begin[l + 1] - level_begin[l]), kThreads, 0, st>>>(nd, level_begin[l],
+                                                                                   level_begin[l + 1]);
+  k_sah_layout_flags<<<grid_for(total), kThreads, 0, st>>>(nd, total, flags64);
+  uint64_t *tot = scan_exclusive<uint64_t>(flags64, offs, total, scan64, st);
+  k_sah_cost<<<grid_for(total), kThreads, 0, st>>>(nd, total, cost);
+  double *cost_total = scan_exclusive<double>(cost, cost, total, cost_scan, st);
+  uint64_t t = 0;
+  uint32_t depth = 0;
+  double sah_cost = 0.0;
+  cudaError_t e = cudaMemcpyAsync(&t, tot, sizeof t, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&sah_cost, cost_total, sizeof sah_cost, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&depth, counters, sizeof depth, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return std::string("device SAH layout: ") + cudaGetErrorString(e);
+  const uint32_t n2 = (uint32_t)(t >> 32), n4 = (uint32_t)t;
+  if (depth > max_depth_allowed)
+    return "depth " + std::to_string(depth) + " of the device-built tree exceeds " + std::to_string(max_depth_allowed);
+  if (n2 == 0 || n4 == 0) return "device BVH has no interior node";
+  const uint64_t off4 = align256((uint64_t)n2 * sizeof(BvhNode));
+  const uint64_t offr = off4 + align256((uint64_t)n4 * sizeof(Bvh4Node));
+  const uint64_t bytes = offr + align256(3ull * n * sizeof(float4));
+  DeviceArena arena;
+  e = cudaMalloc(&arena.base, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    oom = e == cudaErrorMemoryAllocation;
+    return std::string("device allocation of ") + std::to_string(bytes) + " BVH bytes failed: " + cudaGetErrorString(e);
+  }
+  arena.bytes = bytes;
+  uint8_t *base = static_cast<uint8_t *>(arena.base);
+  BvhNode *out2 = reinterpret_cast<BvhNode *>(base);
+  Bvh4Node *out4 = reinterpret_cast<Bvh4Node *>(base + off4);
+  float4 *records = reinterpret_cast<float4 *>(base + offr);
+  k_sah_write_nodes<<<grid_for(total), kThreads, 0, st>>>(nd, total, offs, out2, out4);
+  k_sah_records<<<grid_for(n), kThreads, 0, st>>>(plo, n, pos, sc.dev.tri_info, sc.dev.materials, records);
+  DevScene d = sc.dev;
+  d.nodes = out2;
+  d.nodes4 = out4;
+  d.tris = records;
+  d.node_count = n2;
+  d.node4_count = n4;
+  d.max_depth = depth;
+  e = cudaMemcpyAsync(sc.d_desc, &d, sizeof d, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    arena.release();
+    return std::string("device BVH write: ") + cudaGetErrorString(e);
+  }
+  sc.dev = d;
+  sc.bvh_arena.release();
+  sc.bvh_arena = arena;
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  sc.bvh = BvhBuildStats{};
+  sc.bvh.nodes = n2;
+  sc.bvh.leaves = total - n2;
+  sc.bvh.max_depth = depth;
+  sc.bvh.sah_cost = sah_cost;
+  sc.bvh.seconds = secs;
+  if (info) {
+    info->iterations = (uint32_t)level_begin.size() - 1;
+    info->ms = 1000.0 * secs;
+  }
+  return "";
+}
 
 std::string device_build_bvh(SceneHost &sc, cudaStream_t st, uint32_t max_depth_allowed, bool &oom,
                              DeviceBuildInfo *info) {

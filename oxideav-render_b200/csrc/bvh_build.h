@@ -41,4 +41,13 @@ struct DeviceBuildInfo {
 std::string device_build_bvh(SceneHost &sc, cudaStream_t stream, uint32_t max_depth, bool &oom,
                              DeviceBuildInfo *info = nullptr);
 
+// The same contract with the host builder's binned-SAH split rule, built
+// top down one tree level per round: per active node its bounds, 16 bins
+// per axis of its centroid extent, the sweep for the cheapest split (or a
+// leaf of at most 8 triangles), a stable partition and the children. Nodes
+// at the depth limit or without a valid split halve their range by index
+// (the host splits at the centroid median there).
+std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t stream, uint32_t max_depth, bool &oom,
+                                 DeviceBuildInfo *info = nullptr);
+
 }  // namespace ptd

@@ -354,9 +354,6 @@ pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_trac
                   std::vector<Job> &jobs) {
   SceneHost *sc = find_scene(ctx, t->scene_id);
   if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
-  // A finished background host tree replaces the device-built one (no wave
-  // of this batch is queued yet; hits do not depend on the tree).
-  adopt_pending_tree(*sc, ctx->stream, false);
   tracers.push_back(t);
   jobs.push_back(make_job(*t, *sc, t->env.get(), n));
   return PT_OK;
@@ -467,8 +464,6 @@ pt_status autotune_impl(pt_context *ctx, pt_tracer *t, uint32_t samples, TuneCho
   if (!t->have_state) return fail(ctx, PT_ERR_INVALID_ARG, "tracer is not synced");
   SceneHost *sc = find_scene(ctx, t->scene_id);
   if (!sc) return fail(ctx, PT_ERR_EVICTED, "scene " + std::to_string(t->scene_id) + " is no longer resident");
-  // Tune on the tree the scene keeps.
-  adopt_pending_tree(*sc, ctx->stream, true);
   return autotune_scene(ctx, t, sc, t->env.get(), samples, best);
 }
 
@@ -757,7 +752,7 @@ pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes
 
 pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder) {
   if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
-  if (builder > PT_BVH_BUILD_DEVICE) return fail(ctx, PT_ERR_INVALID_ARG, "unknown BVH builder");
+  if (builder > PT_BVH_BUILD_DEVICE_PLOC) return fail(ctx, PT_ERR_INVALID_ARG, "unknown BVH builder");
   ctx->bvh_builder = (int)builder;
   return PT_OK;
 }
@@ -782,17 +777,6 @@ pt_status pt_debug_scene_texels(pt_context *ctx, uint32_t scene_id, float *out, 
       CK(ctx, cudaStreamSynchronize(ctx->stream));
       CK(ctx, cudaMemcpy(out, s->dev.texels, n * sizeof(float4), cudaMemcpyDeviceToHost));
     }
-    return PT_OK;
-  });
-}
-
-pt_status pt_scene_bvh_wait(pt_context *ctx, uint32_t scene_id) {
-  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
-  return guard(ctx, [&]() -> pt_status {
-    SceneHost *s = find_scene(ctx, scene_id);
-    if (!s) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene");
-    CK(ctx, cudaSetDevice(ctx->device));
-    adopt_pending_tree(*s, ctx->stream, true);
     return PT_OK;
   });
 }
@@ -1019,7 +1003,6 @@ pt_status pt_raycast_render(pt_context *ctx, uint32_t scene_id, const pt_camera 
     SceneHost *sc = find_scene(ctx, scene_id);
     if (!sc) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene " + std::to_string(scene_id));
     CK(ctx, cudaSetDevice(ctx->device));
-    adopt_pending_tree(*sc, ctx->stream, false);
     static float decode[256];
     static bool init = [] {
       for (int i = 0; i < 256; ++i) decode[i] = host_srgb_to_linear((float)i / 255.0f);

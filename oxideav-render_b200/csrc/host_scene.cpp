@@ -98,8 +98,6 @@ struct Builder {
   std::vector<BNode> nodes;
   std::atomic<uint32_t> node_count{1};
   std::atomic<uint32_t> max_depth{0};
-  const std::atomic<bool> *cancel = nullptr;  // set: stop splitting
-  bool cancelled() const { return cancel && cancel->load(std::memory_order_relaxed); }
 
   struct Task {
     uint32_t node, begin, end, depth;
@@ -116,6 +114,9 @@ struct Builder {
   static constexpr uint32_t kParallelNode = 65536;
   int wide = 1;  // threads for one large node's passes
 
+  // Bin of a centroid offset times the bin scale: truncation, clamped to
+  // the bins (a NaN offset lands in bin 0).
+  static int bin_of(float f) { return f >= 1.0f ? std::min(kBins - 1, (int)std::min(f, 16.0f)) : 0; }
   static float area(const float lo[3], const float hi[3]) {
     float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
     if (!(dx >= 0.0f) || !(dy >= 0.0f) || !(dz >= 0.0f)) return 0.0f;
@@ -161,7 +162,7 @@ struct Builder {
       const Prim &pr = prims[i];
       for (int k = 0; k < 3; ++k) {
         if (!use[k]) continue;
-        int b = std::min(kBins - 1, (int)((pr.c[k] - clo[k]) * scale[k]));
+        int b = bin_of((pr.c[k] - clo[k]) * scale[k]);
         B.c[k][b]++;
         for (int a = 0; a < 3; ++a) {
           B.l[k][b][a] = std::min(B.l[k][b][a], pr.lo[a]);
@@ -309,7 +310,7 @@ struct Builder {
     }
     if (axis >= 0) {
       const float sc = scale[axis], base = clo[axis];
-      auto left = [&](const Prim &pr) { return std::min(kBins - 1, (int)((pr.c[axis] - base) * sc)) < best_bin; };
+      auto left = [&](const Prim &pr) { return bin_of((pr.c[axis] - base) * sc) < best_bin; };
       if (par > 1) {
         // Two passes: count each chunk's left side, then scatter every chunk
         // into its place (stable within chunks) and copy back.
@@ -369,7 +370,7 @@ struct Builder {
 
   void local_build(Task t) {
     std::vector<Task> st{t};
-    while (!st.empty() && !cancelled()) {
+    while (!st.empty()) {
       Task cur = st.back();
       st.pop_back();
       Task ch[2];
@@ -391,9 +392,7 @@ struct Builder {
         stack.pop_back();
         ++active;
       }
-      if (cancelled()) {
-        // Drain: take tasks without splitting them.
-      } else if (t.end - t.begin <= kLocalThreshold) {
+      if (t.end - t.begin <= kLocalThreshold) {
         local_build(t);
       } else {
         Task ch[2];
@@ -442,17 +441,15 @@ void pad_box(const float lo[3], const float hi[3], float plo[3], float phi[3]) {
 
 }  // namespace
 
-bool build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
-               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads,
-               const std::atomic<bool> *cancel) {
+void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
+               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads) {
   auto t0 = std::chrono::steady_clock::now();
   out_nodes.clear();
   out_nodes4.clear();
   records.clear();
   stats = BvhBuildStats{};
-  if (tri_count == 0) return true;
+  if (tri_count == 0) return;
   Builder b;
-  b.cancel = cancel;
   b.pos = pos;
   b.n = tri_count;
   b.prims.resize(tri_count);
@@ -469,7 +466,6 @@ bool build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   }
   b.wide = std::max(1, threads);
   b.run(std::max(1, threads));
-  if (b.cancelled()) return false;
 
   // Depth-first two-child layout.
   auto leaf_ref = [](uint32_t first, uint32_t count) { return (int)~(first | (count << 27)); };
@@ -617,7 +613,6 @@ bool build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   }
   stats.sah_cost = cost;
   stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  return true;
 }
 
 // ============================================================ arena
@@ -1054,12 +1049,10 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
   const float *pos = reinterpret_cast<const float *>(dst + plan.off[p_pos]);
   if (with_bvh) build_bvh(pos, tc, rec_flags.data(), img.tree.nodes, img.tree.nodes4, img.tree.records, img.bvh, threads);
   img.seconds[2] = since(t_bvh);
-  img.pos_off = plan.off[p_pos];
   img.textures = texs;
   img.tex_src_off = plan.off[p_src];
   img.pool_off = plan.off[p_pool];
   img.pool_bytes = plan.bytes[p_pool];
-  if (!with_bvh) img.rec_flags = std::move(rec_flags);
 
   // Pointer fields hold offset + 1 until commit_scene rebases them; the
   // tree's are set when it is committed.
@@ -1228,7 +1221,8 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
   auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
   uint64_t tris = 0;
   for (uint32_t i = 0; desc.items && i < desc.item_count; ++i) tris += desc.items[i].triangle_count;
-  const bool device = builder == BVH_BUILD_DEVICE || (builder == BVH_BUILD_AUTO && tris >= kAutoDeviceBuildTris);
+  const bool device = builder == BVH_BUILD_DEVICE || builder == BVH_BUILD_DEVICE_PLOC ||
+                      (builder == BVH_BUILD_AUTO && tris >= kAutoDeviceBuildTris);
   if (device && tris >= 64) {
     SceneImage img;
     std::string err = build_scene_image(desc, img, false, staging);
@@ -1237,7 +1231,8 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
     err = commit_scene(img, out, oom);
     if (!err.empty()) return err;
     const auto t2 = clk::now();
-    err = device_build_bvh(out, stream, kMaxTreeDepth, oom);
+    err = builder == BVH_BUILD_DEVICE_PLOC ? device_build_bvh(out, stream, kMaxTreeDepth, oom)
+                                           : device_build_bvh_sah(out, stream, kMaxTreeDepth, oom);
     if (err.empty()) {
       const auto t3 = clk::now();
       out.upload_seconds[0] = secs(t0, t1);
@@ -1245,36 +1240,6 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
       out.upload_seconds[2] = secs(t2, t3);
       out.upload_seconds[3] = secs(t0, t3);
       out.device_bvh = true;
-      if (builder == BVH_BUILD_AUTO) {
-        // The host tree, built in the background from the positions read
-        // back from the scene's arena (the host image may be a staging
-        // buffer the next upload reuses).
-        auto p = std::make_shared<PendingTree>();
-        cudaGetDevice(&p->device);
-        p->d_pos = out.dev.pos;
-        p->flags = std::move(img.rec_flags);
-        const uint32_t tc = (uint32_t)out.tri_count;
-        // Leave two hardware threads to the caller (launches, the next upload).
-        const unsigned hw = std::thread::hardware_concurrency();
-        const int threads = (int)std::max(1u, std::min(32u, hw > 4 ? hw - 2 : 1u));
-        PendingTree *raw = p.get();
-        p->th = std::thread([raw, tc, threads] {
-          std::vector<float> pos(9 * (size_t)tc);
-          cudaStream_t s = nullptr;
-          bool read = cudaSetDevice(raw->device) == cudaSuccess &&
-                      cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
-                      cudaMemcpyAsync(pos.data(), raw->d_pos, pos.size() * sizeof(float), cudaMemcpyDeviceToHost,
-                                      s) == cudaSuccess &&
-                      cudaStreamSynchronize(s) == cudaSuccess;
-          if (s) cudaStreamDestroy(s);
-          if (!read) cudaGetLastError();
-          raw->ok = read && build_bvh(pos.data(), tc, raw->flags.data(), raw->tree.nodes, raw->tree.nodes4,
-                                      raw->tree.records, raw->stats, threads, &raw->cancel);
-          raw->flags = std::vector<uint32_t>();
-          raw->done.store(true, std::memory_order_release);
-        });
-        out.pending = std::move(p);
-      }
       return "";
     }
     release_scene(out);
@@ -1296,50 +1261,10 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
 }
 
 void release_scene(SceneHost &s) {
-  s.pending.reset();
   s.arena.release();
   s.bvh_arena.release();
   s.d_desc = nullptr;
   s.device_bvh = false;
-}
-
-PendingTree::~PendingTree() {
-  cancel.store(true);
-  if (th.joinable()) th.join();
-}
-
-bool adopt_pending_tree(SceneHost &sc, cudaStream_t stream, bool wait) {
-  if (!sc.pending) return false;
-  PendingTree &p = *sc.pending;
-  if (!wait && !p.done.load(std::memory_order_acquire)) return false;
-  if (p.th.joinable()) p.th.join();
-  if (!p.ok || p.tree.nodes.empty() || p.tree.nodes4.empty() || sc.d_desc == nullptr ||
-      cudaStreamSynchronize(stream) != cudaSuccess) {
-    cudaGetLastError();
-    sc.pending.reset();
-    return false;
-  }
-  DeviceArena a;
-  DevScene d = sc.dev;
-  bool oom = false;
-  std::string err = commit_tree(p.tree, p.stats.max_depth, a, d, oom, nullptr);
-  if (err.empty() && cudaMemcpy(sc.d_desc, &d, sizeof d, cudaMemcpyHostToDevice) != cudaSuccess) {
-    // The descriptor still points at the device tree (its copy is last).
-    cudaGetLastError();
-    a.release();
-    err = "descriptor update failed";
-  }
-  if (!err.empty()) {
-    sc.pending.reset();
-    return false;
-  }
-  sc.bvh_arena.release();
-  sc.bvh_arena = a;
-  sc.dev = d;
-  sc.bvh = p.stats;
-  sc.device_bvh = false;
-  sc.pending.reset();
-  return true;
 }
 
 // ============================================================ environment

@@ -6,10 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <cstdint>
 #include <memory>
-#include <thread>
 #include <string>
 #include <vector>
 
@@ -26,10 +24,8 @@ struct BvhBuildStats {
 // as two-child 64-byte nodes, as the same tree collapsed to four-child
 // 128-byte nodes, plus 48-byte leaf-ordered triangle records shared by both.
 // `rec_flags[g]` goes into each record (REC_* bits).
-// Returns false (outputs unspecified) when `cancel` became true mid-build.
-bool build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &nodes,
-               std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads,
-               const std::atomic<bool> *cancel = nullptr);
+void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &nodes,
+               std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads);
 
 // One device allocation holding a scene (or an environment) plus the
 // device copy of its descriptor. `stream` non-null: the allocation is
@@ -92,15 +88,12 @@ struct HostTree {
 struct SceneImage {
   HostBlob blob;   // everything but the BVH
   HostTree tree;   // empty when built without a BVH
-  uint64_t pos_off = 0;  // the soup positions' offset in `blob`
   // Textures: the table (as in the blob), the source texels' offset in the
   // blob, and the device-only texel pool that follows the blob in the arena
   // (its mip chains are generated on the device at commit).
   std::vector<DevTexture> textures;
   uint64_t tex_src_off = 0, pool_off = 0, pool_bytes = 0;
   uint64_t device_bytes() const { return std::max<uint64_t>(blob.size(), pool_off + pool_bytes) + tree.bytes(); }
-  // Without a BVH: the record flags a later host build needs.
-  std::vector<uint32_t> rec_flags;
   DevScene rel{};
   uint64_t desc_off = 0;
   uint64_t tri_count = 0;
@@ -110,21 +103,6 @@ struct SceneImage {
   // materials, lights, emissive tables), BVH build, the blob fill (corner
   // streams and tables copied into place).
   double seconds[4] = {0.0, 0.0, 0.0, 0.0};
-};
-
-// The host binned-SAH tree of a scene whose first tree was built on the
-// device, built on host threads in the background. The destructor cancels
-// a build still running and joins it.
-struct PendingTree {
-  std::thread th;
-  std::atomic<bool> done{false}, cancel{false};
-  bool ok = false;
-  int device = 0;
-  const float *d_pos = nullptr;  // the scene's positions on the device (read back by the build)
-  std::vector<uint32_t> flags;
-  HostTree tree;
-  BvhBuildStats stats;
-  ~PendingTree();
 };
 
 struct SceneHost {
@@ -137,7 +115,6 @@ struct SceneHost {
   BvhBuildStats bvh;
   uint32_t light_count = 0;
   bool device_bvh = false;  // the BVH was built on the GPU
-  std::shared_ptr<PendingTree> pending;  // host tree on its way (BVH_BUILD_AUTO)
   // Host wall time of upload_scene: host image, arena allocation + copy,
   // device BVH build, total.
   double upload_seconds[4] = {0.0, 0.0, 0.0, 0.0};
@@ -156,11 +133,11 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
 // entries and 3 * 56 + 8 four-child entries.
 constexpr uint32_t kMaxTreeDepth = 56;
 // Where upload_scene builds the BVH.
-// BVH_BUILD_AUTO: scenes of at least kAutoDeviceBuildTris triangles get a
-// device-built tree at once and the host binned-SAH tree (fewer node visits
-// per ray) in the background, adopted by adopt_pending_tree; smaller scenes
-// build on the host.
-enum BvhBuilder : int { BVH_BUILD_AUTO = 0, BVH_BUILD_HOST = 1, BVH_BUILD_DEVICE = 2 };
+// BVH_BUILD_AUTO: scenes of at least kAutoDeviceBuildTris triangles build
+// on the device with the binned-SAH rule (the host builder's tree, in
+// milliseconds), smaller ones on the host. BVH_BUILD_DEVICE_PLOC clusters
+// on the device instead (faster to build, 3-12 % more node visits).
+enum BvhBuilder : int { BVH_BUILD_AUTO = 0, BVH_BUILD_HOST = 1, BVH_BUILD_DEVICE = 2, BVH_BUILD_DEVICE_PLOC = 3 };
 constexpr uint64_t kAutoDeviceBuildTris = 16384;
 // build_scene_image + commit_scene, with the BVH built where `builder`
 // says (`stream`: the device build's stream). A device-built tree deeper
@@ -168,12 +145,6 @@ constexpr uint64_t kAutoDeviceBuildTris = 16384;
 std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder = BVH_BUILD_HOST,
                          cudaStream_t stream = nullptr, HostStaging *staging = nullptr);
 void release_scene(SceneHost &s);
-// Replaces the device-built tree of `sc` by its finished background host
-// tree (waiting for it when `wait`). Synchronises `stream` first, so no
-// queued wave still reads the old tree. Returns true when a tree was
-// adopted; a failed allocation keeps the device tree.
-bool adopt_pending_tree(SceneHost &sc, cudaStream_t stream, bool wait);
-
 struct EnvHost {
   DevEnv dev{};
   DevEnv *d_desc = nullptr;

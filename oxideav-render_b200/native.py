@@ -79,7 +79,6 @@ SIGNATURES = {
     # include/pt_b200_debug.h
     "pt_set_bvh_builder": (i32, [vp, u32]),
     "pt_scene_bvh_on_device": (i32, [vp, u32, C.POINTER(C.c_int)]),
-    "pt_scene_bvh_wait": (i32, [vp, u32]),
     "pt_scene_upload_seconds": (i32, [vp, u32, dp]),
     "pt_debug_scene_texels": (i32, [vp, u32, fp, u64, u64p]),
     "pt_debug_sobol": (i32, [vp, u32, u32, fp]),

@@ -1,9 +1,10 @@
 """Device-built BVHs (pt_set_bvh_builder): a scene whose tree is built on the
-GPU renders the same accumulator, bit for bit, as with the host-built tree
-(closest hit = smallest t, ties to the lowest global id, so hits do not
-depend on the tree), on both schedules and both node layouts, and the tree
-respects the traversal stacks' depth limit. Under AUTO a scene starts on its
-device tree and switches to the background host tree between refines."""
+GPU — by the level-by-level binned-SAH build or by clustering — renders the
+same accumulator, bit for bit, as with the host-built tree (closest hit =
+smallest t, ties to the lowest global id, so hits do not depend on the
+tree), on both schedules and both node layouts; the trees respect the
+traversal stacks' depth limit and are deterministic, and the device
+binned-SAH build gives the host builder's tree."""
 import numpy as np
 import pytest
 
@@ -67,20 +68,21 @@ def test_device_tree_renders_identically(ctx, name):
     scene, opts, env = case(name)
     a, ra, sa, da = render(ctx, abi.PT_BVH_BUILD_HOST, scene, opts, env, 0)
     assert not da
-    for schedule in (0, 1):
-        b, rb, sb, db = render(ctx, abi.PT_BVH_BUILD_DEVICE, scene, opts, env, schedule)
-        assert db, "scene not built on the device"
-        assert np.array_equal(a, b), (name, schedule)
-        assert ra == rb
-        assert 0 < sb["max_depth"] <= 56 and sb["nodes"] > 0 and sb["leaves"] > 0
-        assert sb["build_seconds"] > 0.0
-    try:
-        # The two-child layout of the device tree, for both ray kinds.
-        ctx.set_node_width(2, 2)
-        c, rc, _, _ = render(ctx, abi.PT_BVH_BUILD_DEVICE, scene, opts, env, 1)
-        assert np.array_equal(a, c) and rc == ra
-    finally:
-        ctx.set_node_width(4, 4)
+    for builder in (abi.PT_BVH_BUILD_DEVICE, abi.PT_BVH_BUILD_DEVICE_PLOC):
+        for schedule in (0, 1):
+            b, rb, sb, db = render(ctx, builder, scene, opts, env, schedule)
+            assert db, "scene not built on the device"
+            assert np.array_equal(a, b), (name, builder, schedule)
+            assert ra == rb
+            assert 0 < sb["max_depth"] <= 56 and sb["nodes"] > 0 and sb["leaves"] > 0
+            assert sb["build_seconds"] > 0.0 and sb["sah_cost"] > 0.0
+        try:
+            # The two-child layout of the device tree, for both ray kinds.
+            ctx.set_node_width(2, 2)
+            c, rc, _, _ = render(ctx, builder, scene, opts, env, 1)
+            assert np.array_equal(a, c) and rc == ra
+        finally:
+            ctx.set_node_width(4, 4)
 
 
 def test_builder_selection(ctx):
@@ -97,56 +99,39 @@ def test_builder_selection(ctx):
     assert ei.value.status == abi.PT_ERR_INVALID_ARG
 
 
-def test_device_tree_is_deterministic(ctx):
+def test_device_trees_are_deterministic(ctx):
     scene = ts.random_soup(50000, seed=5)
     desc = scene.to_desc(ts.pt_opts(8, 1, 1))
-    ctx.set_bvh_builder(abi.PT_BVH_BUILD_DEVICE)
     try:
-        stats = []
-        for _ in range(2):
+        for builder in (abi.PT_BVH_BUILD_DEVICE, abi.PT_BVH_BUILD_DEVICE_PLOC):
+            ctx.set_bvh_builder(builder)
+            stats = []
+            for _ in range(2):
+                sid = ctx.upload(desc)
+                assert ctx.bvh_on_device(sid)
+                st = ctx.bvh_stats(sid)
+                stats.append((st["nodes"], st["leaves"], st["max_depth"], st["sah_cost"], ctx.scene_bytes(sid)))
+                ctx.release(sid)
+            assert stats[0] == stats[1], builder
+    finally:
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
+
+
+@pytest.mark.parametrize("name", ["spheres", "soup"])
+def test_device_sah_build_gives_the_host_tree(ctx, name):
+    # Same split rule, same float arithmetic: the same nodes and leaves
+    # (these scenes never fall back to median splits).
+    scene, opts, _ = case(name)
+    desc = scene.to_desc(opts)
+    got = {}
+    try:
+        for builder in (abi.PT_BVH_BUILD_HOST, abi.PT_BVH_BUILD_DEVICE):
+            ctx.set_bvh_builder(builder)
             sid = ctx.upload(desc)
-            assert ctx.bvh_on_device(sid)
-            st = ctx.bvh_stats(sid)
-            stats.append((st["nodes"], st["leaves"], st["max_depth"], st["sah_cost"], ctx.scene_bytes(sid)))
+            got[builder] = ctx.bvh_stats(sid)
             ctx.release(sid)
-        assert stats[0] == stats[1]
     finally:
         ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
-
-
-def test_auto_switches_to_the_host_tree_between_refines(ctx):
-    scene, opts = ts.sphere_grid_c1(48, 6)
-    ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST)
-    try:
-        ref = api.PathTracer(ctx)
-        ref.sync(scene, opts)
-        ref.refine(6)
-        want = ref.accum()
-        ref.close()
-    finally:
-        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
-    t = api.PathTracer(ctx)
-    t.sync(scene, opts)
-    sid = t._scene_id
-    assert ctx.bvh_on_device(sid)
-    t.refine(2)  # on the device tree (or the host one, if it was already done)
-    ctx.bvh_wait(sid)
-    assert not ctx.bvh_on_device(sid)
-    st = ctx.bvh_stats(sid)
-    assert 0 < st["max_depth"] <= 64 and st["nodes"] > 0
-    t.refine(4)
-    assert np.array_equal(t.accum(), want)
-    t.close()
-
-
-def test_release_while_the_host_tree_builds(ctx):
-    # Releasing (or replacing) a scene cancels its background build.
-    desc = ts.random_soup(400000, seed=8).to_desc(ts.pt_opts(8, 1, 1))
-    for _ in range(3):
-        sid = ctx.upload(desc)
-        assert ctx.bvh_on_device(sid)
-        ctx.release(sid)
-    sid = ctx.upload(desc)
-    ctx.bvh_wait(sid)
-    assert not ctx.bvh_on_device(sid)
-    ctx.release(sid)
+    h, d = got[abi.PT_BVH_BUILD_HOST], got[abi.PT_BVH_BUILD_DEVICE]
+    assert (h["nodes"], h["leaves"], h["max_depth"]) == (d["nodes"], d["leaves"], d["max_depth"])
+    assert abs(h["sah_cost"] - d["sah_cost"]) <= 1e-6 * h["sah_cost"]
