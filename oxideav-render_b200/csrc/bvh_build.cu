@@ -1071,6 +1071,210 @@ __global__ void k_sah_records(const float4 *plo, uint32_t n, const float *pos, c
   }
 }
 
+// ---- small subtrees: nodes of at most kSahSmall triangles leave the level
+// rounds and are built whole by one thread each (the same split rule, an
+// in-place partition), in node ids reserved for them (2c - 2 per node of c
+// triangles; unused ids stay empty leaves that nothing references).
+constexpr uint32_t kSahSmall = 32;
+
+// Splits the children of the last round into the next round's active list
+// and the deferred (small) list: flags, then a scatter after their scan.
+__global__ void k_sah_route_flags(const uint32_t *kids, uint32_t nk, SahNodes nd, uint32_t *flag) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x)
+    flag[k] = nd.count[kids[k]] > kSahSmall ? 1u : 0u;
+}
+__global__ void k_sah_route(const uint32_t *kids, uint32_t nk, const uint32_t *flag, const uint32_t *scan,
+                            uint32_t *act_next, uint32_t *deferred, uint32_t def_base) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
+    if (flag[k])
+      act_next[scan[k]] = kids[k];
+    else
+      deferred[def_base + (k - scan[k])] = kids[k];
+  }
+}
+
+__global__ void k_sah_small_reserve(const uint32_t *deferred, uint32_t nd_count, SahNodes nd, uint32_t *need) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd_count; k += gridDim.x * blockDim.x) {
+    const uint32_t c = nd.count[deferred[k]];
+    need[k] = c > 1 ? 2 * c - 2 : 0;
+  }
+}
+
+__global__ void k_add_base(uint32_t *v, uint32_t n, uint32_t base) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) v[k] += base;
+}
+
+__global__ void k_sah_small_clear(SahNodes nd, uint32_t v0, uint32_t v1) {
+  for (uint32_t v = v0 + blockIdx.x * blockDim.x + threadIdx.x; v < v1; v += gridDim.x * blockDim.x) {
+    nd.lo[v] = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
+    nd.hi[v] = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+    nd.begin[v] = 0;
+    nd.count[v] = 0;
+    nd.depth[v] = 0;
+    nd.left[v] = -1;
+    nd.state[v] = 0;
+  }
+}
+
+// The whole subtree of one small node, depth first (the host builder's
+// split of a node, sequentially: bounds, 16 bins per axis, the sweep, leaf
+// or split, then an in-place partition).
+__global__ void k_sah_small(const uint32_t *deferred, uint32_t nd_count, const uint32_t *first_id, SahNodes nd,
+                            float4 *plo, float4 *phi, uint32_t *used, uint32_t *max_depth) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd_count; k += gridDim.x * blockDim.x) {
+    const uint32_t root = deferred[k];
+    uint32_t next = first_id[k];
+    const uint32_t id0 = next;
+    struct Task {
+      uint32_t v, b, c, d;
+    } st[2 * kSahSmall];
+    int sp = 0;
+    st[sp++] = {root, nd.begin[root], nd.count[root], nd.depth[root]};
+    while (sp > 0) {
+      const Task t = st[--sp];
+      float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.0f), hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+      float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (uint32_t i = t.b; i < t.b + t.c; ++i) {
+        float l[3], h[3], c[3];
+        prim_box(plo, phi, i, l, h, c);
+        lo = make_float4(fminf(lo.x, l[0]), fminf(lo.y, l[1]), fminf(lo.z, l[2]), 0.0f);
+        hi = make_float4(fmaxf(hi.x, h[0]), fmaxf(hi.y, h[1]), fmaxf(hi.z, h[2]), 0.0f);
+        for (int q = 0; q < 3; ++q) {
+          clo[q] = fminf(clo[q], c[q]);
+          chi[q] = fmaxf(chi[q], c[q]);
+        }
+      }
+      nd.lo[t.v] = lo;
+      nd.hi[t.v] = hi;
+      nd.left[t.v] = -1;
+      if (t.c <= 1) {
+        atomicMax(max_depth, t.d);
+        continue;
+      }
+      uint32_t need = 0;
+      for (uint32_t c = t.c; c > kMaxLeafTris; c = (c + 1) / 2) ++need;
+      const bool median = t.d + need >= 56;
+      int axis = -1, best_bin = 0;
+      float best_cost = INFINITY, scale[3] = {0.0f, 0.0f, 0.0f};
+      if (!median) {
+        const float parent = host_area(lo, hi);
+        for (int ax = 0; ax < 3; ++ax) {
+          const float span = chi[ax] - clo[ax];
+          if (!(span > 0.0f)) continue;
+          scale[ax] = (float)kSahBins / span;
+          uint32_t bc[kSahBins];
+          float bl[kSahBins][3], bh[kSahBins][3];
+          for (int b = 0; b < kSahBins; ++b) {
+            bc[b] = 0;
+            for (int q = 0; q < 3; ++q) {
+              bl[b][q] = INFINITY;
+              bh[b][q] = -INFINITY;
+            }
+          }
+          for (uint32_t i = t.b; i < t.b + t.c; ++i) {
+            float l[3], h[3], c[3];
+            prim_box(plo, phi, i, l, h, c);
+            const int b = sah_bin((c[ax] - clo[ax]) * scale[ax]);
+            bc[b]++;
+            for (int q = 0; q < 3; ++q) {
+              bl[b][q] = fminf(bl[b][q], l[q]);
+              bh[b][q] = fmaxf(bh[b][q], h[q]);
+            }
+          }
+          float rl[kSahBins][3], rh[kSahBins][3];
+          uint32_t rc[kSahBins];
+          float accl[3] = {INFINITY, INFINITY, INFINITY}, acch[3] = {-INFINITY, -INFINITY, -INFINITY};
+          uint32_t acc = 0;
+          for (int b = kSahBins - 1; b >= 1; --b) {
+            acc += bc[b];
+            for (int q = 0; q < 3; ++q) {
+              accl[q] = fminf(accl[q], bl[b][q]);
+              acch[q] = fmaxf(acch[q], bh[b][q]);
+              rl[b][q] = accl[q];
+              rh[b][q] = acch[q];
+            }
+            rc[b] = acc;
+          }
+          float ll[3] = {INFINITY, INFINITY, INFINITY}, lh[3] = {-INFINITY, -INFINITY, -INFINITY};
+          uint32_t lc = 0;
+          for (int s = 1; s < kSahBins; ++s) {
+            lc += bc[s - 1];
+            for (int q = 0; q < 3; ++q) {
+              ll[q] = fminf(ll[q], bl[s - 1][q]);
+              lh[q] = fmaxf(lh[q], bh[s - 1][q]);
+            }
+            if (lc == 0 || rc[s] == 0) continue;
+            const float cost = 1.0f + (host_area(make_float4(ll[0], ll[1], ll[2], 0.0f), make_float4(lh[0], lh[1], lh[2], 0.0f)) *
+                                           (float)lc +
+                                       host_area(make_float4(rl[s][0], rl[s][1], rl[s][2], 0.0f),
+                                                 make_float4(rh[s][0], rh[s][1], rh[s][2], 0.0f)) *
+                                           (float)rc[s]) /
+                                          fmaxf(parent, 1e-30f);
+            if (cost < best_cost) {
+              best_cost = cost;
+              axis = ax;
+              best_bin = s;
+            }
+          }
+        }
+        if (t.c <= kMaxLeafTris && (axis < 0 || (float)t.c <= best_cost)) {
+          atomicMax(max_depth, t.d);
+          continue;
+        }
+      }
+      uint32_t mid;
+      if (axis >= 0) {
+        uint32_t i = t.b, j = t.b + t.c;  // [t.b, i) left, [j, end) right
+        while (i < j) {
+          float l[3], h[3], c[3];
+          prim_box(plo, phi, i, l, h, c);
+          if (sah_bin((c[axis] - clo[axis]) * scale[axis]) < best_bin) {
+            ++i;
+          } else {
+            --j;
+            const float4 a = plo[i], b = phi[i];
+            plo[i] = plo[j];
+            phi[i] = phi[j];
+            plo[j] = a;
+            phi[j] = b;
+          }
+        }
+        mid = i - t.b;
+      } else {
+        mid = t.c / 2;
+      }
+      const uint32_t c0 = next;
+      next += 2;
+      nd.left[t.v] = (int)c0;
+      nd.begin[c0] = t.b;
+      nd.count[c0] = mid;
+      nd.begin[c0 + 1] = t.b + mid;
+      nd.count[c0 + 1] = t.c - mid;
+      nd.depth[c0] = nd.depth[c0 + 1] = t.d + 1;
+      st[sp++] = {c0 + 1, t.b + mid, t.c - mid, t.d + 1};
+      st[sp++] = {c0, t.b, mid, t.d + 1};
+    }
+    used[k] = next - id0;
+  }
+}
+
+// Four-child marks inside the small subtrees: the root, then its nodes in
+// id order (a parent's id precedes its children's).
+__global__ void k_sah_small_mark(const uint32_t *deferred, uint32_t nd_count, const uint32_t *first_id,
+                                 const uint32_t *used, SahNodes nd) {
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nd_count; k += gridDim.x * blockDim.x) {
+    const uint32_t root = deferred[k], id0 = first_id[k], id1 = id0 + used[k];
+    for (uint32_t w = 0; w <= id1 - id0; ++w) {
+      const uint32_t v = w == 0 ? root : id0 + w - 1;
+      if (!sah_interior(nd, v) || !(nd.state[v] & NS_WIDE)) continue;
+      uint32_t ch[4];
+      const int nch = sah_wide_children(nd, v, ch);
+      for (int i = 0; i < nch; ++i)
+        if (sah_interior(nd, ch[i])) nd.state[ch[i]] |= NS_WIDE;
+    }
+  }
+}
+
 // SAH cost contribution of every node (traversal 1, intersection 1,
 // relative to the root box), summed by a scan.
 __global__ void k_sah_cost(SahNodes nd, uint32_t total, double *out) {
@@ -1139,12 +1343,14 @@ std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_de
   nd.depth = s.get<uint32_t>(cap);
   nd.left = s.get<int>(cap);
   nd.state = s.get<uint32_t>(cap);
-  uint32_t *act = s.get<uint32_t>(n), *act2 = s.get<uint32_t>(n);
+  uint32_t *act = s.get<uint32_t>(n);
   uint32_t *split = s.get<uint32_t>(n), *split_scan = s.get<uint32_t>(n), *split_flag = s.get<uint32_t>(n);
   uint64_t *flags64 = s.get<uint64_t>(cap), *offs = s.get<uint64_t>(cap);
   uint64_t *scan64 = s.get<uint64_t>(scan_scratch_items(cap));
   uint32_t *counters = s.get<uint32_t>(2);  // max leaf depth
   double *cost = s.get<double>(cap), *cost_scan = s.get<double>(scan_scratch_items(cap));
+  uint32_t *kids = s.get<uint32_t>(n), *route = s.get<uint32_t>(n), *route_scan = s.get<uint32_t>(n);
+  uint32_t *deferred = s.get<uint32_t>(n), *first_id = s.get<uint32_t>(n), *used = s.get<uint32_t>(n);
   if (!s.err.empty()) {
     oom = s.oom;
     return s.err;
@@ -1166,7 +1372,7 @@ std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_de
   k_sah_prims<<<grid_for(n), kThreads, 0, st>>>(pos, n, plo, phi);
   k_sah_root<<<1, 1, 0, st>>>(nd, n, act);
   std::vector<uint32_t> level_begin{0};
-  uint32_t m = 1, next_id = 1;
+  uint32_t m = 1, next_id = 1, n_deferred = 0;
   while (m > 0) {
     if (level_begin.size() > 64) return "device SAH build exceeded 64 levels";
     if (!grow(m)) {
@@ -1185,10 +1391,9 @@ std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_de
     k_sah_scatter<<<grid_for(n), kThreads, 0, st>>>(plo, phi, qlo, qhi, seg, flag, pscan, n, nd, lv);
     k_sah_split_flags<<<grid_for(m), kThreads, 0, st>>>(lv, split_flag);
     uint32_t *tot = scan_exclusive<uint32_t>(split_flag, split_scan, m, scan32, st);
-    k_sah_children<<<grid_for(m), kThreads, 0, st>>>(nd, lv, split_scan, next_id, pscan, flag, n, act2);
+    k_sah_children<<<grid_for(m), kThreads, 0, st>>>(nd, lv, split_scan, next_id, pscan, flag, n, kids);
     std::swap(plo, qlo);
     std::swap(phi, qhi);
-    std::swap(act, act2);
     uint32_t splits = 0;
     cudaError_t e = cudaMemcpyAsync(&splits, tot, sizeof splits, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1196,13 +1401,42 @@ std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_de
     if (next_id + 2ull * splits > cap) return "device SAH build ran out of nodes";
     level_begin.push_back(next_id);
     next_id += 2 * splits;
-    m = 2 * splits;
+    // The children: large ones stay in the rounds, small ones wait for the
+    // subtree kernel.
+    const uint32_t nk = 2 * splits;
+    uint32_t active = 0;
+    if (nk) {
+      k_sah_route_flags<<<grid_for(nk), kThreads, 0, st>>>(kids, nk, nd, route);
+      uint32_t *rt = scan_exclusive<uint32_t>(route, route_scan, nk, scan32, st);
+      k_sah_route<<<grid_for(nk), kThreads, 0, st>>>(kids, nk, route, route_scan, act, deferred, n_deferred);
+      e = cudaMemcpyAsync(&active, rt, sizeof active, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return std::string("device SAH build: ") + cudaGetErrorString(e);
+    }
+    n_deferred += nk - active;
+    m = active;
+  }
+  // Small subtrees, one thread each, in reserved node ids.
+  if (n_deferred) {
+    k_sah_small_reserve<<<grid_for(n_deferred), kThreads, 0, st>>>(deferred, n_deferred, nd, route);
+    uint32_t *rt = scan_exclusive<uint32_t>(route, first_id, n_deferred, scan32, st);
+    uint32_t reserved = 0;
+    cudaError_t e = cudaMemcpyAsync(&reserved, rt, sizeof reserved, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return std::string("device SAH build: ") + cudaGetErrorString(e);
+    if ((uint64_t)next_id + reserved > cap) return "device SAH build ran out of nodes";
+    if (reserved) k_sah_small_clear<<<grid_for(reserved), kThreads, 0, st>>>(nd, next_id, next_id + reserved);
+    k_add_base<<<grid_for(n_deferred), kThreads, 0, st>>>(first_id, n_deferred, next_id);
+    k_sah_small<<<grid_for(n_deferred, 64), 64, 0, st>>>(deferred, n_deferred, first_id, nd, plo, phi, used, counters);
+    next_id += reserved;
   }
   const uint32_t total = next_id;
   // Four-child marks level by level (parents first), then both numberings.
   for (size_t l = 0; l + 1 < level_begin.size(); ++l)
     k_sah_mark<<<grid_for(level_begin[l + 1] - level_begin[l]), kThreads, 0, st>>>(nd, level_begin[l],
                                                                                    level_begin[l + 1]);
+  if (n_deferred)
+    k_sah_small_mark<<<grid_for(n_deferred, 64), 64, 0, st>>>(deferred, n_deferred, first_id, used, nd);
   k_sah_layout_flags<<<grid_for(total), kThreads, 0, st>>>(nd, total, flags64);
   uint64_t *tot = scan_exclusive<uint64_t>(flags64, offs, total, scan64, st);
   k_sah_cost<<<grid_for(total), kThreads, 0, st>>>(nd, total, cost);
@@ -1255,7 +1489,7 @@ std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_de
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   sc.bvh = BvhBuildStats{};
   sc.bvh.nodes = n2;
-  sc.bvh.leaves = total - n2;
+  sc.bvh.leaves = n2 + 1;  // a binary tree: one leaf more than interior nodes
   sc.bvh.max_depth = depth;
   sc.bvh.sah_cost = sah_cost;
   sc.bvh.seconds = secs;
