@@ -671,7 +671,8 @@ __global__ void k_sah_bounds(const float4 *plo, const float4 *phi, const uint32_
     if (s != kSahNone) {
       float c[3];
       prim_box(plo, phi, i, l, h, c);
-      for (int k = 0; k < 3; ++k) cl[k] = ch[k] = c[k];
+      for (int k = 0; k < 3; ++k)
+        if (isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2])) cl[k] = ch[k] = c[k];
     }
     const uint32_t s0 = __shfl_sync(0xffffffffu, s, 0);
     if (__all_sync(0xffffffffu, s == s0)) {
@@ -1048,11 +1049,18 @@ __global__ void k_sah_prims(const float *pos, uint32_t n, float4 *lo, float4 *hi
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float *p = pos + 9ull * i;
     float l[3], h[3];
+    bool nan = false;
     for (int k = 0; k < 3; ++k) {
       const float a = __ldg(p + k), b = __ldg(p + 3 + k), c = __ldg(p + 6 + k);
+      nan |= isnan(a) || isnan(b) || isnan(c);
       l[k] = fminf(fminf(a, b), c);
       h[k] = fmaxf(fmaxf(a, b), c);
     }
+    if (nan)  // never hit: an empty box, outside every node's bounds
+      for (int k = 0; k < 3; ++k) {
+        l[k] = INFINITY;
+        h[k] = -INFINITY;
+      }
     lo[i] = make_float4(l[0], l[1], l[2], __uint_as_float(i));
     hi[i] = make_float4(h[0], h[1], h[2], 0.0f);
   }
@@ -1139,10 +1147,11 @@ __global__ void k_sah_small(const uint32_t *deferred, uint32_t nd_count, const u
         prim_box(plo, phi, i, l, h, c);
         lo = make_float4(fminf(lo.x, l[0]), fminf(lo.y, l[1]), fminf(lo.z, l[2]), 0.0f);
         hi = make_float4(fmaxf(hi.x, h[0]), fmaxf(hi.y, h[1]), fmaxf(hi.z, h[2]), 0.0f);
-        for (int q = 0; q < 3; ++q) {
-          clo[q] = fminf(clo[q], c[q]);
-          chi[q] = fmaxf(chi[q], c[q]);
-        }
+        if (isfinite(c[0]) && isfinite(c[1]) && isfinite(c[2]))
+          for (int q = 0; q < 3; ++q) {
+            clo[q] = fminf(clo[q], c[q]);
+            chi[q] = fmaxf(chi[q], c[q]);
+          }
       }
       nd.lo[t.v] = lo;
       nd.hi[t.v] = hi;

@@ -135,3 +135,25 @@ def test_device_sah_build_gives_the_host_tree(ctx, name):
     h, d = got[abi.PT_BVH_BUILD_HOST], got[abi.PT_BVH_BUILD_DEVICE]
     assert (h["nodes"], h["leaves"], h["max_depth"]) == (d["nodes"], d["leaves"], d["max_depth"])
     assert abs(h["sah_cost"] - d["sah_cost"]) <= 1e-6 * h["sah_cost"]
+
+
+def test_hostile_geometry_on_every_builder(ctx):
+    # Triangles with NaN or huge coordinates, zero-area and duplicated
+    # triangles among ordinary ones: every builder's tree gives the host
+    # tree's accumulator, and no device build fails.
+    rng = np.random.default_rng(21)
+    s = with_cloud(ts.area_light_scene(0.35, 0.5), 3000, 4, (0, 0, 0), 1.0)
+    m = s.add_material(ts.diffuse_material((0.5, 0.7, 0.3), 1.0))
+    bad = (rng.random((40, 3, 3)) - 0.5).astype(np.float32)
+    bad[:10, 0, 0] = np.nan                  # NaN corners
+    bad[10:20] = bad[10:11, :1]              # zero-area (all corners equal)
+    bad[20:30] *= 1e30                       # enormous
+    bad[30:40] = bad[30]                     # identical triangles
+    s.add_primitive(Primitive(np.ascontiguousarray(bad.reshape(-1, 3)), material=m))
+    o = ts.pt_opts(32, 2, 3)
+    a, ra, _, _ = render(ctx, abi.PT_BVH_BUILD_HOST, s, o, None, 1)
+    for builder in (abi.PT_BVH_BUILD_DEVICE, abi.PT_BVH_BUILD_DEVICE_PLOC):
+        b, rb, st, on_device = render(ctx, builder, s, o, None, 1)
+        assert on_device and st["max_depth"] <= 56
+        assert np.array_equal(a, b), builder
+        assert rb == ra
