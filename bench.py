@@ -502,16 +502,18 @@ def run_reference(args):
     }))
 
 
-def run_raycast(ctx, api, torch, scene, opts, cpu: bool, steps: int = 3):
-    """RenderBackend::Raycast (Phong / Whitted, the default shading mode) on
-    the workload's scene and camera: one-shot renders through
-    RaycastCudaRenderer (scene prepared + uploaded per call, as the
-    reference's render does) and raycasts of an already-uploaded scene, plus
-    the oracle's CPU restatement of the same frame."""
+def run_raycast(ctx, api, torch, scene, opts, cpu: bool, steps: int = 3, pbr: bool = False):
+    """RenderBackend::Raycast on the workload's scene and camera — Phong /
+    Whitted (the default shading mode), or Pbr with ray-traced shadows:
+    one-shot renders through RaycastCudaRenderer (scene prepared + uploaded
+    per call, as the reference's render does) and raycasts of an
+    already-uploaded scene, plus the oracle's CPU restatement of the same
+    frame."""
     import ctypes as C
     from oxideav_render_b200.options import ShadingMode
     from oxideav_render_b200.scene import Camera
-    o = opts.replace(shading=ShadingMode.Phong, aa=1)
+    o = opts.replace(shading=ShadingMode.Pbr, aa=1, shadows=True) if pbr else \
+        opts.replace(shading=ShadingMode.Phong, aa=1)
     samples = o.width * o.height * o.aa * o.aa
     r = api.RaycastCudaRenderer(ctx)
     img = r.render(scene, o)
@@ -534,8 +536,10 @@ def run_raycast(ctx, api, torch, scene, opts, cpu: bool, steps: int = 3):
         if i > 0:
             resident.append(time.perf_counter() - t0)
     ctx.release(sid)
-    res = {"workload": f"Phong (Whitted: shadow, mirror and refraction rays, depth {o.max_ray_depth}) "
-                       f"{o.width}x{o.height}, aa {o.aa}",
+    what = (f"Pbr (glTF direct light with shadow rays, mirror / refraction / BLEND rays, depth {o.max_ray_depth}, "
+            f"reflection cut-off {o.reflection_roughness_cutoff})" if pbr else
+            f"Phong (Whitted: shadow, mirror and refraction rays, depth {o.max_ray_depth})")
+    res = {"workload": f"{what} {o.width}x{o.height}, aa {o.aa}",
            "samples_per_frame": samples,
            "one_shot_ms": 1000 * statistics.median(one_shot),
            "one_shot_samples_per_s": samples / statistics.median(one_shot),
@@ -549,6 +553,8 @@ def run_raycast(ctx, api, torch, scene, opts, cpu: bool, steps: int = 3):
         res["cpu_ms"] = 1000 * (time.perf_counter() - t0)
         res["cpu_threads"] = min(64, os.cpu_count() or 1)
         res["identical_to_oracle"] = bool(np.array_equal(img, want))
+        if not res["identical_to_oracle"]:
+            res["max_byte_difference"] = int(np.max(np.abs(img.astype(int) - want.astype(int))))
     return res
 
 
@@ -691,9 +697,11 @@ def run_b200(args):
                           "bvh_on_device": ctx.bvh_on_device(sid),
                           "upload_phases": {k: 1000 * v for k, v in ctx.upload_seconds(sid).items()}}
         ctx.release(sid)
-    raycast = None
+    raycast = raycast_pbr = None
     if args.raycast:
         raycast = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline)
+        raycast_pbr = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline,
+                                  pbr=True)
     mixed = None
     if args.mixed > 0:
         mixed = run_mixed(ctx, api, torch, args.mixed, 2026 + rank)
@@ -723,6 +731,7 @@ def run_b200(args):
             "e2e": e2e,
             "batched_mixed": mixed,
             "raycast": raycast,
+            "raycast_pbr": raycast_pbr,
             "served": served,
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),

@@ -406,6 +406,10 @@ typedef struct pt_raycast_options {
   float exposure;
   uint32_t max_ray_depth;  /* capped at 16 */
   float near_plane, far_plane;
+  /* PT_SHADE_PBR only: */
+  float ambient;                     /* uniform environment radiance (>= 0) */
+  uint32_t shadows;                  /* ray-traced hard shadows for every light */
+  float reflection_roughness_cutoff; /* in [0, 1]; 0 = no mirror rays */
 } pt_raycast_options;
 
 /* The Whitted ray tracer behind RenderBackend::Raycast (src/raycast.rs:145-560)
@@ -415,10 +419,16 @@ typedef struct pt_raycast_options {
  * Whitted's shadow, mirror and refraction rays up to max_ray_depth,
  * Wireframe, NormalDebug, DepthDebug), then the scanline backend's frame
  * resolve (src/scanline.rs:124-221): SSAA box filter, premultiplied
- * averages, exposure + tone map + sRGB for RGBA8. Writes the scene-linear
- * HDR image (width*height*4 floats) and/or the RGBA8 image
- * (width*height*4 bytes); either pointer may be NULL. PT_SHADE_PBR is not
- * built: PT_ERR_INVALID_ARG. */
+ * averages, exposure + tone map + sRGB for RGBA8. PT_SHADE_PBR evaluates the
+ * glTF metallic-roughness model at every hit (src/raycast.rs:518-740):
+ * ambient, emissive and direct light from every scene light (hard shadow
+ * rays when `shadows` is set, passing MASK cut-outs, BLEND and transmissive
+ * occluders), a mirror ray below reflection_roughness_cutoff, refraction
+ * through thin walls and KHR_materials_volume bodies with Beer-Lambert
+ * absorption, BLEND composited per ray, texture LOD from ray differentials
+ * at camera hits and ray cones after a bounce. Writes the scene-linear HDR
+ * image (width*height*4 floats) and/or the RGBA8 image (width*height*4
+ * bytes); either pointer may be NULL. */
 PT_API pt_status pt_raycast_render(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                                    const pt_raycast_options *opts, float *out_hdr, size_t hdr_floats,
                                    uint8_t *out_rgba, size_t rgba_bytes);

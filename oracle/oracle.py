@@ -292,8 +292,8 @@ def texture_sample(pixels: np.ndarray, sampler, u: float, v: float, lod: float, 
 
 
 def raycast(scene, opts):
-    """RenderBackend::Raycast render of a PreparedScene (legacy shading
-    modes): (HDR (h, w, 4) f32, RGBA8 (h, w, 4) u8)."""
+    """RenderBackend::Raycast render of a PreparedScene (every shading
+    mode): (HDR (h, w, 4) f32, RGBA8 (h, w, 4) u8)."""
     from oxideav_render_b200.scene import Camera
     w, h, aa = max(opts.width, 1), max(opts.height, 1), int(opts.aa)
     cam = Camera.resolve(scene, opts, w * aa, h * aa)
@@ -305,8 +305,29 @@ def raycast(scene, opts):
     st = lib().oracle_raycast(C.addressof(desc.desc), C.addressof(c), C.addressof(o),
                               hdr.ctypes.data_as(C.POINTER(C.c_float)), rgba.ctypes.data_as(C.POINTER(C.c_uint8)))
     if st != 0:
-        raise ValueError("the oracle's raycast covers the legacy shading modes only")
+        raise ValueError("options outside the raycast backend's range")
     return hdr, rgba
+
+
+def gltf_brdf(base, metallic: float, roughness: float, f0_dielectric: float, n, v, l):
+    """src/brdf.rs: (BrdfParams (c_diff, f0, alpha), eval(n, v, l))."""
+    f3 = C.c_float * 3
+    params, out = (C.c_float * 7)(), f3()
+    lib().oracle_gltf_brdf(f3(*base), C.c_float(metallic), C.c_float(roughness), C.c_float(f0_dielectric),
+                           f3(*n), f3(*v), f3(*l), params, out)
+    return (tuple(params[0:3]), tuple(params[3:6]), params[6]), tuple(out)
+
+
+def gltf_d_ggx(n_dot_h: float, alpha: float) -> float:
+    lib().oracle_gltf_d_ggx.restype = C.c_float
+    return lib().oracle_gltf_d_ggx(C.c_float(n_dot_h), C.c_float(alpha))
+
+
+def gltf_schlick(f0, v_dot_h: float):
+    f3 = C.c_float * 3
+    out = f3()
+    lib().oracle_gltf_schlick(f3(*f0), C.c_float(v_dot_h), out)
+    return tuple(out)
 
 
 def texture_mips(pixels: np.ndarray, srgb: bool) -> np.ndarray:

@@ -598,6 +598,362 @@ struct Raycaster {
     return out;
   }
 
+  // ---- Pbr: Ctx::radiance / miss / secondary / shade (src/raycast.rs:518-740)
+  // with TraceScene::shadow_transmittance, direct_light and
+  // barycentric_differentials (src/trace.rs:947-1082) and the glTF
+  // metallic-roughness BRDF (src/brdf.rs:24-148).
+  float ambient = 0.0f, cutoff = 0.0f, spread = 0.0f;
+  bool shadows = false;
+  float bg[4] = {0, 0, 0, 0};
+  static constexpr uint32_t kMaxLayers = 64;  // MAX_LAYERS, src/raycast.rs:126
+  static constexpr float kPi = 3.14159265358979323846f;
+
+  struct RayState {
+    uint32_t depth = 0, layers = 0;
+    bool camera = true;
+    bool inside = false;  // Some(sigma)
+    V3 sigma = {0, 0, 0};
+    bool has_skip = false;
+    uint32_t skip = 0;
+  };
+  struct Footprint {
+    bool diff = true;
+    V3 dxo, dxd, dyo, dyd;        // Diff: neighbouring camera rays
+    float width = 0.0f, spr = 0.0f;  // Cone
+  };
+  struct BrdfParams {
+    V3 c_diff, f0;
+    float alpha;
+  };
+  // BrdfParams::metallic_roughness, src/brdf.rs:96-123.
+  static BrdfParams metallic_roughness(V3 base, float metallic, float roughness, float f0d) {
+    float m = clampr(metallic, 0.0f, 1.0f), r = clampr(roughness, 0.0f, 1.0f);
+    return {{base.x * (1.0f - m), base.y * (1.0f - m), base.z * (1.0f - m)},
+            {f0d + (base.x - f0d) * m, f0d + (base.y - f0d) * m, f0d + (base.z - f0d) * m},
+            fmaxr(r * r, 1.0e-3f)};
+  }
+  // d_ggx / v_smith_ggx_correlated / f_schlick / eval, src/brdf.rs:31-148.
+  static float gltf_d_ggx(float n_dot_h, float alpha) {
+    float a2 = alpha * alpha;
+    float d = n_dot_h * n_dot_h * (a2 - 1.0f) + 1.0f;
+    return a2 / fmaxr(kPi * d * d, 1.0e-12f);
+  }
+  static float v_smith(float n_dot_l, float n_dot_v, float alpha) {
+    float a2 = alpha * alpha;
+    float gv = n_dot_l * std::sqrt(n_dot_v * n_dot_v * (1.0f - a2) + a2);
+    float gl = n_dot_v * std::sqrt(n_dot_l * n_dot_l * (1.0f - a2) + a2);
+    float s = gv + gl;
+    return s > 0.0f ? 0.5f / s : 0.0f;
+  }
+  static V3 f_schlick3(V3 f0, float v_dot_h) {
+    float k = powi5(1.0f - clampr(v_dot_h, 0.0f, 1.0f));
+    return {f0.x + (1.0f - f0.x) * k, f0.y + (1.0f - f0.y) * k, f0.z + (1.0f - f0.z) * k};
+  }
+  static V3 brdf_eval(const BrdfParams &p, V3 n, V3 v, V3 l) {
+    float n_dot_l = dot(n, l);
+    if (n_dot_l <= 0.0f) return {0.0f, 0.0f, 0.0f};
+    float n_dot_v = fmaxr(dot(n, v), 1.0e-4f);
+    V3 h = {l.x + v.x, l.y + v.y, l.z + v.z};
+    float hl = std::sqrt(dot(h, h));
+    h = hl > 0.0f ? V3{h.x / hl, h.y / hl, h.z / hl} : n;
+    float n_dot_h = fmaxr(dot(n, h), 0.0f), v_dot_h = fmaxr(dot(v, h), 0.0f);
+    V3 f = f_schlick3(p.f0, v_dot_h);
+    float spec = gltf_d_ggx(n_dot_h, p.alpha) * v_smith(n_dot_l, n_dot_v, p.alpha);
+    return {((1.0f - f.x) * p.c_diff.x / kPi + f.x * spec) * n_dot_l,
+            ((1.0f - f.y) * p.c_diff.y / kPi + f.y * spec) * n_dot_l,
+            ((1.0f - f.z) * p.c_diff.z / kPi + f.z * spec) * n_dot_l};
+  }
+  bool masked_out(const Hit &h) const {
+    const pt_material &mat = ts->material_of(h);
+    return mat.alpha_mode == PT_ALPHA_MASK && ts->alpha(h) < mat.alpha_cutoff;
+  }
+  // TraceScene::shadow_transmittance, src/trace.rs:947-1005. The product
+  // runs in f64 and is rounded once, so it does not depend on the order in
+  // which the BVH reports the partial occluders.
+  V3 shadow_transmittance(V3 origin, V3 dir, float t_max, const RayState &st) const {
+    double tr[3] = {1.0, 1.0, 1.0};
+    const double eps = (double)1.0e-4f;
+    bool blocked = ts->occluded_filtered(origin, dir, 0.0f, t_max, [&](const Hit &h) {
+      if (st.has_skip && h.global == st.skip) return false;
+      const pt_material &mat = ts->material_of(h);
+      float pass[3] = {0.0f, 0.0f, 0.0f};
+      if (mat.alpha_mode == PT_ALPHA_MASK) {
+        if (ts->alpha(h) < mat.alpha_cutoff) return false;
+      } else if (mat.alpha_mode == PT_ALPHA_BLEND) {
+        float a = 1.0f - clampr(ts->alpha(h), 0.0f, 1.0f);
+        pass[0] = pass[1] = pass[2] = a;
+      }
+      bool has_tr = (mat.ext_flags & PT_EXT_TRANSMISSION) && std::isfinite(mat.transmission_factor) &&
+                    mat.transmission_factor > 0.0f;
+      if (has_tr) {
+        Surface surf = ts->surface(h);
+        MaterialSample m = ts->material_oriented(h, surf, TexLod{}, false);
+        if (m.transmission > 0.0f) {
+          if (m.thickness > 0.0f && !h.front) return false;
+          float kt = m.transmission * (1.0f - m.metallic);
+          float a = mat.alpha_mode == PT_ALPHA_BLEND ? pass[0] : 0.0f;
+          for (int k = 0; k < 3; ++k) pass[k] = a + (1.0f - a) * kt * m.base_color[k];
+        }
+      }
+      for (int k = 0; k < 3; ++k) tr[k] *= (double)clampr(pass[k], 0.0f, 1.0f);
+      return tr[0] <= eps && tr[1] <= eps && tr[2] <= eps;
+    });
+    if (blocked) return {0.0f, 0.0f, 0.0f};
+    return {(float)tr[0], (float)tr[1], (float)tr[2]};
+  }
+  // TraceScene::direct_light, src/trace.rs:1007-1048.
+  V3 direct_light(V3 p, V3 n, V3 ng, V3 v, const BrdfParams &bp, const RayState &skip) const {
+    float out[3] = {0.0f, 0.0f, 0.0f};
+    for (const pt_light &L : ts->lights) {
+      LightSample s;
+      if (!light_sample(L, p, s)) continue;
+      V3 f = brdf_eval(bp, n, v, s.l);
+      if (f.x == 0.0f && f.y == 0.0f && f.z == 0.0f) continue;
+      V3 vis = {1.0f, 1.0f, 1.0f};
+      if (shadows) {
+        float side = dot(ng, s.l) >= 0.0f ? 1.0f : -1.0f;
+        V3 o = Integrator::offset_ray_origin(p, {ng.x * side, ng.y * side, ng.z * side});
+        float t_max = std::isfinite(s.distance) ? s.distance * (1.0f - 1.0e-4f) : INF;
+        vis = shadow_transmittance(o, s.l, t_max, skip);
+      }
+      out[0] += f.x * s.radiance.x * vis.x;
+      out[1] += f.y * s.radiance.y * vis.y;
+      out[2] += f.z * s.radiance.z * vis.z;
+    }
+    return {out[0], out[1], out[2]};
+  }
+  // barycentric_of, src/trace.rs:1120-1133.
+  static bool barycentric_of(V3 q, V3 p0, V3 p1, V3 p2, float out[3]) {
+    V3 e1 = sub(p1, p0), e2 = sub(p2, p0), r = sub(q, p0);
+    float d11 = dot(e1, e1), d12 = dot(e1, e2), d22 = dot(e2, e2);
+    float r1 = dot(r, e1), r2 = dot(r, e2);
+    float det = d11 * d22 - d12 * d12;
+    if (!std::isfinite(det) || std::fabs(det) <= FLT_MIN) return false;
+    float u = (d22 * r1 - d12 * r2) / det;
+    float v = (d11 * r2 - d12 * r1) / det;
+    out[0] = 1.0f - u - v;
+    out[1] = u;
+    out[2] = v;
+    return true;
+  }
+  // TraceScene::barycentric_differentials, src/trace.rs:1050-1082.
+  bool barycentric_differentials(const Hit &hit, const Footprint &fp, TexLod &lod, float &width) const {
+    V3 p0, p1, p2;
+    ts->triangle_positions(hit.global, p0, p1, p2);
+    V3 ng = cross(sub(p1, p0), sub(p2, p0));
+    const float *b = hit.bary;
+    V3 p = {p0.x * b[0] + p1.x * b[1] + p2.x * b[2], p0.y * b[0] + p1.y * b[1] + p2.y * b[2],
+            p0.z * b[0] + p1.z * b[1] + p2.z * b[2]};
+    auto on_plane = [&](V3 o, V3 d, float g[3], float &w) {
+      float denom = dot(ng, d);
+      if (std::fabs(denom) <= FLT_MIN) return false;
+      float t = dot(ng, sub(p0, o)) / denom;
+      V3 q = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+      float bq[3];
+      if (!barycentric_of(q, p0, p1, p2, bq)) return false;
+      V3 wv = sub(q, p);
+      float wl = std::sqrt(dot(wv, wv));
+      if (!std::isfinite(wl)) return false;
+      for (int k = 0; k < 3; ++k) g[k] = bq[k] - b[k];
+      w = wl;
+      return true;
+    };
+    float wx, wy;
+    if (!on_plane(fp.dxo, fp.dxd, lod.gx, wx)) return false;
+    if (!on_plane(fp.dyo, fp.dyd, lod.gy, wy)) return false;
+    lod.kind = TexLodKind::Grad;
+    width = fmaxr(wx, wy);
+    return true;
+  }
+  // Straight-alpha Porter-Duff over, src/raycast.rs:754-768.
+  static V4 over(V4 src, V4 dst) {
+    float a = clampr(src[3], 0.0f, 1.0f), ad = clampr(dst[3], 0.0f, 1.0f);
+    float ao = a + ad * (1.0f - a);
+    if (ao <= 0.0f) return V4{{0.0f, 0.0f, 0.0f, 0.0f}};
+    V4 c;
+    for (int k = 0; k < 3; ++k) c[k] = (src[k] * a + dst[k] * ad * (1.0f - a)) / ao;
+    c[3] = ao;
+    return c;
+  }
+  // attenuation_sigma, src/raycast.rs:744-751.
+  static V3 attenuation_sigma(V3 c, float distance) {
+    if (!(std::isfinite(distance) && distance > 0.0f)) return {0.0f, 0.0f, 0.0f};
+    return {-std::log(clampr(c.x, 1.0e-6f, 1.0f)) / distance, -std::log(clampr(c.y, 1.0e-6f, 1.0f)) / distance,
+            -std::log(clampr(c.z, 1.0e-6f, 1.0f)) / distance};
+  }
+  V4 miss(const RayState &st) const {
+    if (st.camera) return V4{{bg[0], bg[1], bg[2], bg[3]}};
+    return V4{{ambient, ambient, ambient, 1.0f}};
+  }
+  bool radiance(V3 o, V3 d, const Footprint &fp, const RayState &st, V4 &c) const {
+    const bool cull = !st.inside;
+    Hit hit;
+    auto filter = [&](const Hit &h) {
+      if (st.has_skip && h.global == st.skip) return false;
+      if (cull && !h.front && !ts->material_of(h).double_sided) return false;
+      return !masked_out(h);
+    };
+    if (!ts->closest_hit_filtered(o, d, 0.0f, INF, filter, hit)) return false;
+    c = shade(d, hit, fp, st);
+    if (st.inside) {
+      c[0] *= std::exp(-st.sigma.x * hit.t);
+      c[1] *= std::exp(-st.sigma.y * hit.t);
+      c[2] *= std::exp(-st.sigma.z * hit.t);
+    }
+    return true;
+  }
+  V3 secondary(V3 o, V3 d, const Footprint &fp, const RayState &st) const {
+    V4 c;
+    if (!radiance(o, d, fp, st, c)) c = miss(st);
+    return {c[0], c[1], c[2]};
+  }
+  V4 shade(V3 d, const Hit &hit, const Footprint &fp, const RayState &st) const {
+    Surface surf = ts->surface(hit);
+    TexLod lod;
+    float width = 0.0f;
+    if (fp.diff) {
+      if (!barycentric_differentials(hit, fp, lod, width)) {
+        lod = TexLod{};
+        width = 0.0f;
+      }
+    } else {
+      float w = fmaxr(fp.width + fp.spr * hit.t, 0.0f);
+      lod.kind = TexLodKind::Cone;
+      lod.width = w;
+      lod.dir = d;
+      width = w;
+    }
+    const pt_material &pm = ts->material_of(hit);
+    MaterialSample m = ts->material_oriented(hit, surf, lod, !hit.front);
+    V3 p = surf.position;
+    V3 ng = hit.front ? surf.geometric_normal : scale(surf.geometric_normal, -1.0f);
+    V3 n = m.normal;
+    V3 v = scale(d, -1.0f);
+    RayState skip_st;
+    skip_st.has_skip = true;
+    skip_st.skip = hit.global;
+    Footprint bounce;
+    bounce.diff = false;
+    bounce.width = width;
+    bounce.spr = spread;
+    const bool can_bounce = st.depth < max_depth;
+    float r0 = (m.ior - 1.0f) / (m.ior + 1.0f);
+    const float f0_d = r0 * r0;
+    auto next = [&](bool inside, V3 sigma) {
+      RayState s;
+      s.depth = st.depth + 1;
+      s.layers = st.layers;
+      s.camera = false;
+      s.inside = inside;
+      s.sigma = sigma;
+      s.has_skip = true;
+      s.skip = hit.global;
+      return s;
+    };
+    const V3 neg_ng = scale(ng, -1.0f);
+
+    if (st.inside && !hit.front && m.transmission > 0.0f && m.thickness > 0.0f) {
+      if (!can_bounce) {
+        V4 e = miss(next(false, {0, 0, 0}));
+        return V4{{e[0], e[1], e[2], 1.0f}};
+      }
+      float cos_i = clampr(dot(v, n), 0.0f, 1.0f);
+      V3 t;
+      if (refract(d, n, m.ior, t)) {
+        float sin2_t = m.ior * m.ior * (1.0f - cos_i * cos_i);
+        float f = schlick(f0_d, std::sqrt(fmaxr(1.0f - sin2_t, 0.0f)));
+        V3 out = secondary(Integrator::offset_ray_origin(p, neg_ng), t, bounce, next(false, {0, 0, 0}));
+        V3 inn = secondary(Integrator::offset_ray_origin(p, ng), reflect(d, n), bounce, next(true, st.sigma));
+        return V4{{f * inn.x + (1.0f - f) * out.x, f * inn.y + (1.0f - f) * out.y, f * inn.z + (1.0f - f) * out.z,
+                   1.0f}};
+      }
+      V3 inn = secondary(Integrator::offset_ray_origin(p, ng), reflect(d, n), bounce, next(true, st.sigma));
+      return V4{{inn.x, inn.y, inn.z, 1.0f}};
+    }
+
+    const float *col = m.base_color;
+    const float alpha = pm.alpha_mode == PT_ALPHA_BLEND ? clampr(col[3], 0.0f, 1.0f) : 1.0f;
+    float out[3] = {0.0f, 0.0f, 0.0f};
+    if (m.unlit) {
+      out[0] = col[0];
+      out[1] = col[1];
+      out[2] = col[2];
+    } else {
+      BrdfParams params = metallic_roughness({col[0], col[1], col[2]}, m.metallic, m.roughness, f0_d);
+      float kt = (can_bounce && m.transmission > 0.0f) ? m.transmission : 0.0f;
+      params.c_diff = scale(params.c_diff, 1.0f - kt);
+      float g = 0.0f;
+      if (can_bounce && m.roughness < cutoff) {
+        float x = 1.0f - m.roughness / cutoff;
+        g = x * x;
+      }
+      const float cd[3] = {params.c_diff.x, params.c_diff.y, params.c_diff.z};
+      const float f0[3] = {params.f0.x, params.f0.y, params.f0.z};
+      const float em[3] = {m.emissive.x, m.emissive.y, m.emissive.z};
+      for (int k = 0; k < 3; ++k) out[k] = em[k] + ambient * m.occlusion * (cd[k] + (1.0f - g) * f0[k]);
+      V3 direct = direct_light(p, n, ng, v, params, skip_st);
+      out[0] += direct.x;
+      out[1] += direct.y;
+      out[2] += direct.z;
+      if (g > 0.0f) {
+        float n_dot_v = clampr(dot(n, v), 0.0f, 1.0f);
+        V3 f = f_schlick3(params.f0, n_dot_v);
+        V3 r = reflect(d, n);
+        if (dot(r, ng) <= 0.0f) r = reflect(d, ng);
+        V3 l = secondary(Integrator::offset_ray_origin(p, ng), r, bounce, next(st.inside, st.sigma));
+        out[0] += g * f.x * l.x;
+        out[1] += g * f.y * l.y;
+        out[2] += g * f.z * l.z;
+      }
+      if (kt > 0.0f) {
+        float share = kt * (1.0f - m.metallic);
+        float cos_i = clampr(dot(v, n), 0.0f, 1.0f);
+        V3 through = Integrator::offset_ray_origin(p, neg_ng);
+        float f;
+        V3 l;
+        if (m.thickness > 0.0f && hit.front) {
+          V3 sigma = attenuation_sigma(m.attenuation_color, m.attenuation_distance);
+          V3 t;
+          if (refract(d, n, 1.0f / m.ior, t)) {
+            f = schlick(f0_d, cos_i);
+            l = secondary(through, t, bounce, next(true, sigma));
+          } else {
+            f = 1.0f;
+            l = {0.0f, 0.0f, 0.0f};
+          }
+        } else {
+          RayState st2 = next(st.inside, st.sigma);
+          st2.layers = st.layers + 1;
+          f = schlick(f0_d, cos_i);
+          l = secondary(through, d, fp, st2);
+        }
+        out[0] += share * (1.0f - f) * col[0] * l.x;
+        out[1] += share * (1.0f - f) * col[1] * l.y;
+        out[2] += share * (1.0f - f) * col[2] * l.z;
+      }
+    }
+    if (alpha >= 1.0f) return V4{{out[0], out[1], out[2], 1.0f}};
+    V4 dst;
+    if (st.layers < kMaxLayers) {
+      RayState st2 = st;
+      st2.layers = st.layers + 1;
+      st2.has_skip = true;
+      st2.skip = hit.global;
+      if (!radiance(Integrator::offset_ray_origin(p, neg_ng), d, fp, st2, dst)) dst = miss(st);
+    } else {
+      dst = miss(st);
+    }
+    return over(V4{{out[0], out[1], out[2], alpha}}, dst);
+  }
+  bool pbr_pixel(float px, float py, V4 &c) const {
+    V3 o, d;
+    primary_ray(px, py, o, d);
+    Footprint fp;
+    primary_ray(px + 1.0f, py, fp.dxo, fp.dxd);
+    primary_ray(px, py + 1.0f, fp.dyo, fp.dyd);
+    return radiance(o, d, fp, RayState{}, c);
+  }
+
   bool legacy(V3 o, V3 d, V4 &c) const {
     Hit hit;
     if (!ts->closest_hit_filtered(o, d, 0.0f, INF, [](const Hit &) { return true; }, hit)) return false;
@@ -652,7 +1008,7 @@ extern "C" {
 // RGBA8 (w*h*4 bytes); returns 0, or -1 for options it does not cover.
 int oracle_raycast(const pt_scene_desc *desc, const pt_camera *cam, const pt_raycast_options *o, float *hdr,
                    uint8_t *rgba) {
-  if (o->shading >= PT_SHADE_PBR || o->aa < 1 || o->aa > 8) return -1;
+  if (o->shading > PT_SHADE_PBR || o->aa < 1 || o->aa > 8) return -1;
   Scene sc(*desc);
   Raycaster rc;
   rc.ts = &sc;
@@ -671,6 +1027,13 @@ int oracle_raycast(const pt_scene_desc *desc, const pt_camera *cam, const pt_ray
   rc.near_p = o->near_plane;
   rc.far_p = o->far_plane;
   for (int i = 0; i < 256; ++i) rc.lut[i] = srgb_to_linear_f((float)i / 255.0f);
+  rc.ambient = std::isfinite(o->ambient) ? fmaxr(o->ambient, 0.0f) : 0.0f;
+  rc.cutoff = std::isfinite(o->reflection_roughness_cutoff) ? clampr(o->reflection_roughness_cutoff, 0.0f, 1.0f) : 0.0f;
+  rc.shadows = o->shadows != 0;
+  // trace::pixel_spread, src/trace.rs:1139-1146.
+  rc.spread = cam->projection == PT_PERSPECTIVE ? std::atan(2.0f * cam->half_h / (float)std::max(rc.rh, 1u)) : 0.0f;
+  for (int k = 0; k < 3; ++k) rc.bg[k] = rc.lut[o->background[k]];
+  rc.bg[3] = (float)o->background[3] / 255.0f;
   const size_t ns = (size_t)rc.rw * rc.rh;
   std::vector<V4> col(ns);
   std::vector<uint8_t> cov(ns, 0);
@@ -682,7 +1045,7 @@ int oracle_raycast(const pt_scene_desc *desc, const pt_camera *cam, const pt_ray
         V3 ro, rd;
         rc.primary_ray((float)x + 0.5f, (float)y + 0.5f, ro, rd);
         V4 c{{0, 0, 0, 0}};
-        bool hit = rc.legacy(ro, rd, c);
+        bool hit = o->shading == PT_SHADE_PBR ? rc.pbr_pixel((float)x + 0.5f, (float)y + 0.5f, c) : rc.legacy(ro, rd, c);
         col[y * rc.rw + x] = hit ? c : V4{{0, 0, 0, 0}};
         cov[y * rc.rw + x] = hit ? 1 : 0;
       }
@@ -748,6 +1111,27 @@ int oracle_raycast(const pt_scene_desc *desc, const pt_camera *cam, const pt_ray
       }
     }
   return 0;
+}
+
+// The glTF metallic-roughness BRDF of src/brdf.rs: `params` = c_diff[3],
+// f0[3], alpha of BrdfParams::metallic_roughness; `out` = eval(n, v, l).
+void oracle_gltf_brdf(const float base[3], float metallic, float roughness, float f0_dielectric, const float n[3],
+                      const float v[3], const float l[3], float params[7], float out[3]) {
+  Raycaster::BrdfParams p =
+      Raycaster::metallic_roughness({base[0], base[1], base[2]}, metallic, roughness, f0_dielectric);
+  V3 e = Raycaster::brdf_eval(p, {n[0], n[1], n[2]}, {v[0], v[1], v[2]}, {l[0], l[1], l[2]});
+  const float pv[7] = {p.c_diff.x, p.c_diff.y, p.c_diff.z, p.f0.x, p.f0.y, p.f0.z, p.alpha};
+  for (int k = 0; k < 7; ++k) params[k] = pv[k];
+  out[0] = e.x;
+  out[1] = e.y;
+  out[2] = e.z;
+}
+float oracle_gltf_d_ggx(float n_dot_h, float alpha) { return Raycaster::gltf_d_ggx(n_dot_h, alpha); }
+void oracle_gltf_schlick(const float f0[3], float v_dot_h, float out[3]) {
+  V3 f = Raycaster::f_schlick3({f0[0], f0[1], f0[2]}, v_dot_h);
+  out[0] = f.x;
+  out[1] = f.y;
+  out[2] = f.z;
 }
 
 void *oracle_scene_create(const pt_scene_desc *desc) {

@@ -515,6 +515,31 @@ static bool lod_of(const Scene &sc, const Item &item, const pt_texture_binding &
 bool Scene::sample_binding(const Item &item, const pt_texture_binding &bd, size_t base, const float bary[3],
                            const TexLod &lod, bool srgb, V4 &out) const {
   if (bd.texture < 0) return false;
+  if (lod.kind == TexLodKind::Grad) {
+    // TraceScene::sample_grad (src/trace.rs:596-620) + Texture::sample_grad
+    // (src/texture.rs:456-474): move the barycentrics by one pixel,
+    // difference the transformed UVs, LOD = log2 of the longer texel step.
+    const Texture *tex = texture(bd);
+    if (!tex) return false;
+    const auto *uvs = item.uv_set(bd.uv_set);
+    if (!uvs || uvs->size() != item.positions.size()) return false;
+    const auto &u = *uvs;
+    std::array<float, 2> uv = interp2(u, base, bary);
+    std::array<float, 2> tuv = transform_uv(bd, uv);
+    auto duv = [&](const float d[3]) {
+      std::array<float, 2> moved = {uv[0] + u[base][0] * d[0] + u[base + 1][0] * d[1] + u[base + 2][0] * d[2],
+                                    uv[1] + u[base][1] * d[0] + u[base + 1][1] * d[1] + u[base + 2][1] * d[2]};
+      std::array<float, 2> m = transform_uv(bd, moved);
+      return std::array<float, 2>{m[0] - tuv[0], m[1] - tuv[1]};
+    };
+    std::array<float, 2> gx = duv(lod.gx), gy = duv(lod.gy);
+    float w = (float)tex->img_w, h = (float)tex->img_h;
+    float lx = hypot_f32(gx[0] * w, gx[1] * h), ly = hypot_f32(gy[0] * w, gy[1] * h);
+    float rho = fmaxr(lx, ly);
+    float l = (std::isfinite(rho) && rho > 0.0f) ? std::log2(rho) : 0.0f;
+    out = tex->sample_lod(tuv[0], tuv[1], l, srgb);
+    return true;
+  }
   float l = 0.0f;
   if (!lod_of(*this, item, bd, base, lod, l)) l = 0.0f;
   const Texture *tex = texture(bd);

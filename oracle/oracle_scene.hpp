@@ -78,12 +78,22 @@ PreparedRay prepare_ray(V3 o, V3 d);
 // triangle's corners 0, 1, 2 (the reference's [w, u, v]).
 bool intersect_watertight(const PreparedRay &r, V3 v0, V3 v1, V3 v2, float &t, float bary[3], bool &front);
 
-enum class TexLodKind { Base, Cone };
+// TexLod, src/trace.rs:171-195: level 0, a ray cone, or ray differentials
+// (barycentric change per pixel along x and y).
+enum class TexLodKind { Base, Cone, Grad };
 struct TexLod {
   TexLodKind kind = TexLodKind::Base;
   float width = 0.0f;
   V3 dir = {0, 0, 0};
+  float gx[3] = {0, 0, 0}, gy[3] = {0, 0, 0};
 };
+
+// f32::hypot as glibc's hypotf computes it: the f64 root of the f64 sum of
+// squares (exact squares), rounded once.
+inline float hypot_f32(float a, float b) {
+  double x = (double)a, y = (double)b;
+  return (float)std::sqrt(x * x + y * y);
+}
 
 struct LightSample {
   V3 l;

@@ -239,6 +239,9 @@ class pt_raycast_options(C.Structure):
         ("max_ray_depth", C.c_uint32),
         ("near_plane", C.c_float),
         ("far_plane", C.c_float),
+        ("ambient", C.c_float),
+        ("shadows", C.c_uint32),
+        ("reflection_roughness_cutoff", C.c_float),
     ]
 
 

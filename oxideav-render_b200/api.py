@@ -390,9 +390,10 @@ class RaycastCudaRenderer:
     every call prepares and uploads the scene (as the reference's
     `render` builds its PreparedScene and TraceScene per call), resolves the
     camera at the SSAA resolution, traces one ray per sample and resolves the
-    frame. The legacy shading modes are built (Flat, Gouraud, Phong with
+    frame. Every shading mode: the legacy ones (Flat, Gouraud, Phong with
     Whitted's shadow / mirror / refraction rays, Wireframe, NormalDebug,
-    DepthDebug); `ShadingMode.Pbr` raises RenderError."""
+    DepthDebug) and Pbr (glTF metallic-roughness at every hit with hard
+    shadows, mirror reflection, refraction, see-through BLEND)."""
 
     def __init__(self, ctx: Optional[Context] = None):
         self.ctx = ctx or default_context()

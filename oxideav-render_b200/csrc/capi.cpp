@@ -991,8 +991,6 @@ pt_status pt_raycast_render(pt_context *ctx, uint32_t scene_id, const pt_camera 
   if (o.width == 0 || o.height == 0) return fail(ctx, PT_ERR_INVALID_ARG, "width and height must be positive");
   if (o.aa < 1 || o.aa > 8) return fail(ctx, PT_ERR_INVALID_ARG, "aa must be in 1..=8");
   if (o.shading > PT_SHADE_PBR) return fail(ctx, PT_ERR_INVALID_ARG, "unknown shading mode");
-  if (o.shading == PT_SHADE_PBR)
-    return fail(ctx, PT_ERR_INVALID_ARG, "Pbr shading on the raycast backend is not built (legacy modes are)");
   if (o.tone_map > PT_TONE_ACES) return fail(ctx, PT_ERR_INVALID_ARG, "unknown tone map");
   const uint64_t rw = (uint64_t)o.width * o.aa, rh = (uint64_t)o.height * o.aa;
   if (rw * rh > (1ull << 30)) return fail(ctx, PT_ERR_INVALID_ARG, "render resolution too large");
@@ -1015,20 +1013,40 @@ pt_status pt_raycast_render(pt_context *ctx, uint32_t scene_id, const pt_camera 
     float4 bg = make_float4(decode[o.background[0]], decode[o.background[1]], decode[o.background[2]],
                             (float)o.background[3] / 255.0f);
     const uint64_t ns = rw * rh;
-    // One stream-ordered allocation: samples, coverage, error word, outputs.
+    const bool pbr = o.shading == PT_SHADE_PBR;
+    // Samples the Pbr kernel re-traces with deep frame stacks: this many at
+    // a time.
+    const uint32_t deep_slots = 2048;
+    // One stream-ordered allocation: samples, coverage, error word and
+    // overflow count, outputs; for Pbr the overflow list and deep stacks.
     auto al = [](uint64_t x) { return (x + 255) & ~uint64_t(255); };
     const uint64_t off_cov = al(ns * sizeof(float4)), off_err = off_cov + al(ns);
     const uint64_t off_hdr = off_err + 256, off_rgba = off_hdr + al(npx * sizeof(float4));
-    const uint64_t total = off_rgba + al(npx * 4);
+    const uint64_t off_ovf = off_rgba + al(npx * 4);
+    const uint64_t off_deep = off_ovf + (pbr ? al(ns * sizeof(uint32_t)) : 0);
+    const uint64_t total = off_deep + (pbr ? al((uint64_t)deep_slots * raycast_pbr_frame_bytes()) : 0);
     void *buf = nullptr;
     CK(ctx, cudaMallocAsync(&buf, total, ctx->stream));
     std::unique_ptr<void, std::function<void(void *)>> hold(buf, [ctx](void *q) { cudaFreeAsync(q, ctx->stream); });
     uint8_t *b = static_cast<uint8_t *>(buf);
     uint32_t *d_err = reinterpret_cast<uint32_t *>(b + off_err);
-    CK(ctx, cudaMemsetAsync(d_err, 0, sizeof(uint32_t), ctx->stream));
-    CK(ctx, launch_raycast(sc->dev, *camera, (uint32_t)rw, (uint32_t)rh, o.shading, o.max_ray_depth, light,
-                           o.light_intensity, o.near_plane, o.far_plane, decode, reinterpret_cast<float4 *>(b),
-                           b + off_cov, d_err, ctx->num_sms, ctx->stream));
+    CK(ctx, cudaMemsetAsync(d_err, 0, 2 * sizeof(uint32_t), ctx->stream));
+    if (pbr) {
+      const float ambient = std::isfinite(o.ambient) ? std::max(o.ambient, 0.0f) : 0.0f;
+      const float cutoff = std::isfinite(o.reflection_roughness_cutoff)
+                               ? std::min(std::max(o.reflection_roughness_cutoff, 0.0f), 1.0f)
+                               : 0.0f;
+      // trace::pixel_spread, src/trace.rs:1139-1146.
+      const float spread = camera->projection == PT_PERSPECTIVE ? std::atan(2.0f * camera->half_h / (float)rh) : 0.0f;
+      CK(ctx, launch_raycast_pbr(sc->dev, *camera, (uint32_t)rw, (uint32_t)rh, o.max_ray_depth, o.shadows != 0,
+                                 ambient, cutoff, spread, bg, reinterpret_cast<float4 *>(b), b + off_cov, d_err,
+                                 reinterpret_cast<uint32_t *>(b + off_ovf), d_err + 1, b + off_deep, deep_slots,
+                                 ctx->num_sms, ctx->stream));
+    } else {
+      CK(ctx, launch_raycast(sc->dev, *camera, (uint32_t)rw, (uint32_t)rh, o.shading, o.max_ray_depth, light,
+                             o.light_intensity, o.near_plane, o.far_plane, decode, reinterpret_cast<float4 *>(b),
+                             b + off_cov, d_err, ctx->num_sms, ctx->stream));
+    }
     float4 *d_hdr = out_hdr ? reinterpret_cast<float4 *>(b + off_hdr) : nullptr;
     uchar4 *d_rgba = out_rgba ? reinterpret_cast<uchar4 *>(b + off_rgba) : nullptr;
     CK(ctx, launch_raycast_resolve(reinterpret_cast<float4 *>(b), b + off_cov, o.width, o.height, o.aa, bg,

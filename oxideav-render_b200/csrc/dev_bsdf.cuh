@@ -23,6 +23,7 @@ struct MaterialSample {
   float base_color[4];
   float metallic, roughness;
   V3 normal;
+  float occlusion;  // set by material_oriented<true> only
   V3 emissive;
   uint32_t unlit, double_sided;
   float ior, specular;

@@ -371,7 +371,27 @@ struct TexLod {
   bool cone;
   float width;
   V3 dir;
+  static constexpr bool kGrad = false;
 };
+
+// TexLod of the raycast backend (src/trace.rs:171-195): level 0, a ray cone,
+// or ray differentials — the barycentric change per output pixel along x
+// (gx) and y (gy).
+struct RayTexLod {
+  bool cone;
+  float width;
+  V3 dir;
+  bool grad;
+  float gx[3], gy[3];
+  static constexpr bool kGrad = true;
+};
+
+// f32::hypot as glibc's hypotf computes it: the f64 root of the f64 sum of
+// the (exact) f64 squares, rounded once to f32.
+PT_DEV float hypot_f32(float a, float b) {
+  const double x = (double)a, y = (double)b;
+  return (float)sqrt(x * x + y * y);
+}
 
 PT_DEV void transform_uv(const pt_texture_binding &b, float uv[2]) {
   if (!b.has_transform) return;
@@ -380,15 +400,43 @@ PT_DEV void transform_uv(const pt_texture_binding &b, float uv[2]) {
   uv[1] = b.transform[3] * u + b.transform[4] * v + b.transform[5];
 }
 
-// TraceScene::lod (src/trace.rs:518-554) + ::sample / ::sample_at.
+// TraceScene::lod (src/trace.rs:518-554) + ::sample / ::sample_at, and for
+// ray differentials ::sample_grad (:596-620) with Texture::sample_grad
+// (src/texture.rs:456-474).
+template <class Lod>
 PT_DEV bool sample_binding(const DevScene &s, const pt_texture_binding &bd, uint32_t g, uint32_t flags, float b0,
-                           float b1, float b2, const TexLod &lod, bool srgb, float4 &out) {
+                           float b1, float b2, const Lod &lod, bool srgb, float4 &out) {
   int ti = bd.texture;
   if (ti < 0 || (uint32_t)ti >= s.texture_count) return false;
   uint32_t set = bd.uv_set;
   if (set >= PT_MAX_UV_SETS || !(flags & (TRI_UV0 << set))) return false;
   const DevTexture &tex = s.textures[ti];
   const float *uvs = s.uv[set];
+  if constexpr (Lod::kGrad) {
+    if (lod.grad) {
+      // Move the barycentrics by one pixel, difference the transformed UVs.
+      const float *q = uvs + 6u * g;
+      const float u0 = __ldg(q), v0 = __ldg(q + 1), u1 = __ldg(q + 2), v1 = __ldg(q + 3), u2 = __ldg(q + 4),
+                  v2 = __ldg(q + 5);
+      float uv[2];
+      interp2(uvs, g, b0, b1, b2, uv);
+      float tuv[2] = {uv[0], uv[1]};
+      transform_uv(bd, tuv);
+      float dx[2] = {uv[0] + u0 * lod.gx[0] + u1 * lod.gx[1] + u2 * lod.gx[2],
+                     uv[1] + v0 * lod.gx[0] + v1 * lod.gx[1] + v2 * lod.gx[2]};
+      float dy[2] = {uv[0] + u0 * lod.gy[0] + u1 * lod.gy[1] + u2 * lod.gy[2],
+                     uv[1] + v0 * lod.gy[0] + v1 * lod.gy[1] + v2 * lod.gy[2]};
+      transform_uv(bd, dx);
+      transform_uv(bd, dy);
+      const float w = (float)tex.img_w, h = (float)tex.img_h;
+      const float lx = hypot_f32((dx[0] - tuv[0]) * w, (dx[1] - tuv[1]) * h);
+      const float ly = hypot_f32((dy[0] - tuv[0]) * w, (dy[1] - tuv[1]) * h);
+      const float rho = fmaxf(lx, ly);
+      const float l = (isfinite(rho) && rho > 0.0f) ? log2f(rho) : 0.0f;
+      out = sample_lod(s, tex, tuv[0], tuv[1], l, srgb);
+      return true;
+    }
+  }
   float l = 0.0f;
   if (lod.cone) {
     const float *q = uvs + 6u * g;
@@ -453,9 +501,11 @@ PT_DEV V3 perturb(const DevScene &s, uint32_t g, uint32_t flags, float b0, float
 PT_DEV float fin(float v, float d) { return isfinite(v) ? v : d; }
 
 // TraceScene::material_oriented, src/trace.rs:700-923 (the occlusion
-// input is not evaluated: the path tracer never reads it).
+// input is evaluated only when kOcclusion is set: the path tracer never
+// reads it).
+template <bool kOcclusion = false, class Lod>
 PT_DEV void material_oriented(const DevScene &s, const DevMaterial &dm, uint32_t g, uint32_t flags, float b0, float b1,
-                              float b2, V3 shading_normal, const TexLod &lod, bool flip, MaterialSample &m) {
+                              float b2, V3 shading_normal, const Lod &lod, bool flip, MaterialSample &m) {
   const pt_material &mat = dm.m;
   V3 sn = flip ? vneg(shading_normal) : shading_normal;
   float4 t;
@@ -481,6 +531,12 @@ PT_DEV void material_oriented(const DevScene &s, const DevMaterial &dm, uint32_t
   V3 normal = sn;
   if (sample_binding(s, mat.normal_texture, g, flags, b0, b1, b2, lod, false, t))
     normal = perturb(s, g, flags, b0, b1, b2, normal, t, mat.normal_scale);
+  if constexpr (kOcclusion) {
+    float occlusion = 1.0f;
+    if (sample_binding(s, mat.occlusion_texture, g, flags, b0, b1, b2, lod, false, t))
+      occlusion = 1.0f + mat.occlusion_strength * (t.x - 1.0f);
+    m.occlusion = clampr(occlusion, 0.0f, 1.0f);
+  }
   V3 emissive = {mat.emissive[0], mat.emissive[1], mat.emissive[2]};
   if (sample_binding(s, mat.emissive_texture, g, flags, b0, b1, b2, lod, true, t)) {
     emissive.x *= t.x;

@@ -151,6 +151,7 @@ PT_DEV uint8_t srgb_byte(float c) {
 }  // namespace ptd
 
 #include "raycast.cuh"
+#include "raycast_pbr.cuh"
 
 namespace ptd {
 
@@ -432,6 +433,39 @@ cudaError_t launch_raycast(const DevScene &s, const pt_camera &cam, uint32_t rw,
   const uint64_t n = (uint64_t)rw * rh;
   const uint64_t blocks = std::min<uint64_t>((n + 127) / 128, (uint64_t)num_sms * 16);
   k_raycast<<<(unsigned)std::max<uint64_t>(blocks, 1), 128, 0, st>>>(p);
+  return cudaGetLastError();
+}
+
+size_t raycast_pbr_frame_bytes() { return sizeof(PbrFrame) * (size_t)kPbrDeepFrames; }
+
+cudaError_t launch_raycast_pbr(const DevScene &s, const pt_camera &cam, uint32_t rw, uint32_t rh, uint32_t max_depth,
+                               bool shadows, float ambient, float cutoff, float spread, float4 bg, float4 *samples,
+                               uint8_t *covered, uint32_t *err, uint32_t *ovf_list, uint32_t *ovf_count, void *deep,
+                               uint32_t deep_slots, int num_sms, cudaStream_t st) {
+  PbrParams p;
+  p.s = s;
+  p.cam = cam;
+  p.rw = rw;
+  p.rh = rh;
+  p.max_depth = max_depth < kRayDepthCap ? max_depth : kRayDepthCap;
+  p.shadows = shadows ? 1u : 0u;
+  p.ambient = ambient;
+  p.cutoff = cutoff;
+  p.spread = spread;
+  p.bg = bg;
+  p.samples = samples;
+  p.covered = covered;
+  p.err = err;
+  p.ovf_list = ovf_list;
+  p.ovf_count = ovf_count;
+  p.deep = static_cast<PbrFrame *>(deep);
+  p.deep_slots = deep_slots;
+  const uint64_t n = (uint64_t)rw * rh;
+  const uint64_t blocks = std::min<uint64_t>((n + 127) / 128, (uint64_t)num_sms * 16);
+  k_raycast_pbr<<<(unsigned)std::max<uint64_t>(blocks, 1), 128, 0, st>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_raycast_pbr_deep<<<(deep_slots + 63) / 64, 64, 0, st>>>(p);
   return cudaGetLastError();
 }
 

@@ -47,6 +47,14 @@ cudaError_t launch_raycast(const DevScene &s, const pt_camera &cam, uint32_t rw,
                            uint32_t max_depth, const float light_dir[3], float light_intensity, float near_plane,
                            float far_plane, const float decode[256], float4 *samples, uint8_t *covered,
                            uint32_t *err, int num_sms, cudaStream_t st);
+// ShadingMode::Pbr (raycast_pbr.cuh): every sample with a short frame stack,
+// then the samples listed in ovf_list again with deep stacks (`deep` holds
+// deep_slots * raycast_pbr_frame_bytes()).
+size_t raycast_pbr_frame_bytes();
+cudaError_t launch_raycast_pbr(const DevScene &s, const pt_camera &cam, uint32_t rw, uint32_t rh, uint32_t max_depth,
+                               bool shadows, float ambient, float cutoff, float spread, float4 bg, float4 *samples,
+                               uint8_t *covered, uint32_t *err, uint32_t *ovf_list, uint32_t *ovf_count, void *deep,
+                               uint32_t deep_slots, int num_sms, cudaStream_t st);
 cudaError_t launch_raycast_resolve(const float4 *samples, const uint8_t *covered, uint32_t out_w, uint32_t out_h,
                                    uint32_t aa, float4 bg, uint32_t tone, float exposure, float4 *hdr, uchar4 *rgba,
                                    cudaStream_t st);

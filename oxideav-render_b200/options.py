@@ -172,6 +172,9 @@ class RenderOptions:
         o.max_ray_depth = int(self.max_ray_depth)
         o.near_plane = float(near_plane)
         o.far_plane = float(far_plane)
+        o.ambient = float(self.ambient)
+        o.shadows = 1 if self.shadows else 0
+        o.reflection_roughness_cutoff = float(self.reflection_roughness_cutoff)
         return o
 
     def validate(self) -> None:

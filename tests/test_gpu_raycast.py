@@ -4,6 +4,8 @@ for every legacy shading mode, with and without SSAA, on perspective and
 orthographic cameras, scene cameras, textured / metallic / transmissive /
 alpha-mode / large (device-BVH) scenes, deep Whitted recursion between two
 mirrors, and the display transform's tone maps and exposure."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -91,8 +93,11 @@ def test_backend_arm_and_errors(ctx):
     r = api.make_renderer(RenderBackend.Raycast, ctx)
     img = r.render(ts.lambert_plane(0.5), RenderOptions(width=8, height=6, background=BackgroundColor((1, 2, 3, 4))))
     assert img.shape == (6, 8, 4)
-    with pytest.raises(api.RenderError) as ei:
-        r.render(ts.lambert_plane(0.5), RenderOptions(width=8, height=8, shading=ShadingMode.Pbr))
-    assert ei.value.status == abi.PT_ERR_INVALID_ARG
+    pbr = r.render(ts.lambert_plane(0.5), RenderOptions(width=8, height=8, shading=ShadingMode.Pbr))
+    assert pbr.shape == (8, 8, 4)
+    bad = RenderOptions(width=8, height=8).to_raycast_c(0.01, 100.0)
+    bad.aa = 9
+    cam = abi.pt_camera()
+    assert ctx.lib.pt_raycast_render(ctx.ptr, 0, C.byref(cam), C.byref(bad), None, 0, None, 0) == abi.PT_ERR_INVALID_ARG
     empty = r.render(PreparedScene(), RenderOptions(width=5, height=3, background=BackgroundColor((42, 7, 99, 255))))
     assert np.all(empty == np.array([42, 7, 99, 255], np.uint8))

@@ -1,4 +1,4 @@
-"""The oracle's RenderBackend::Raycast (legacy shading modes), pinned to the
+"""The oracle's RenderBackend::Raycast legacy shading modes, pinned to the
 reference's own tests of src/raycast.rs (:823-1250): every mode paints the
 triangle, an empty scene is pure background, output size with SSAA,
 wireframe sparser than flat, Phong never brighter than the base colour on a
@@ -152,8 +152,3 @@ def test_unlit_and_emissive_materials(oracle):
     e.add_primitive(Primitive(np.array([[-0.5, -0.5, 0], [0.5, -0.5, 0], [0, 0.5, 0]], np.float32),
                               np.array([0, 1, 2], np.uint32), material=e.add_material(em)))
     assert oracle.raycast(e, o)[0][8, 8, 1] >= 0.5 - 1e-6
-
-
-def test_pbr_mode_is_outside_the_oracle(oracle):
-    with pytest.raises(ValueError):
-        oracle.raycast(unit_triangle(), RenderOptions(width=8, height=8, shading=ShadingMode.Pbr))
