@@ -578,6 +578,21 @@ def run_uploads(args):
     ctx.close()
 
 
+def run_raycasts(args):
+    """Profiling case: `--raycast-only` frames of the workload's scene on the
+    raycast backend, Phong then Pbr, on a resident scene, and the timings."""
+    import torch
+    entry.load_package()
+    from oxideav_render_b200 import api
+    scene, opts, env, wname = workload(args.config)
+    ctx = api.Context(torch.cuda.current_device())
+    out = {"workload": wname,
+           "phong": run_raycast(ctx, api, torch, scene, opts, cpu=False, steps=args.raycast_only),
+           "pbr": run_raycast(ctx, api, torch, scene, opts, cpu=False, steps=args.raycast_only, pbr=True)}
+    print(json.dumps(out))
+    ctx.close()
+
+
 def run_b200(args):
     import torch
     ws, rank, local = dist_setup()
@@ -774,12 +789,16 @@ def main():
                     help="skip the RenderBackend::Raycast measurement")
     ap.add_argument("--upload-only", type=int, default=0,
                     help="profiling case: upload the scene this many times (device BVH, device mips) and exit")
+    ap.add_argument("--raycast-only", type=int, default=0,
+                    help="profiling case: this many raycast frames (Phong, then Pbr) of the scene and exit")
     args = ap.parse_args()
     args.serve_rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
     if args.warmup < 3:
         args.warmup = 3
     if args.upload_only > 0:
         run_uploads(args)
+    elif args.raycast_only > 0:
+        run_raycasts(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
