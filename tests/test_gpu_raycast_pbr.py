@@ -14,7 +14,7 @@ import pytest
 import raycast_pbr_scenes as P
 from oxideav_render_b200 import abi, api, testscenes as ts
 from oxideav_render_b200.options import BackgroundColor, CameraSpec, Projection, ToneMap
-from oxideav_render_b200.scene import Material, MaterialExt, Transmission
+from oxideav_render_b200.scene import Material, MaterialExt, Transmission, spot_light
 
 pytestmark = pytest.mark.gpu
 
@@ -70,6 +70,10 @@ def exact_case(name):
         m = P.unlit((1.0, 1.0, 1.0))
         m.double_sided = True
         return P.single_quad(m, P.rotate_y(3.0)), P.opts(24, 24)
+    if name == "spot":
+        s = ts.shadow_box()
+        s.add_light(spot_light((1.0, 0.9, 0.8), 30.0, 8.0, 0.15, 0.45), [1.5, 3.0, 1.0], [-0.4, -1.0, -0.3])
+        return s, P.opts(64, 48, shadows=True)
     if name == "soup":
         s = ts.random_soup(40000, seed=5)
         s.add_light(ts.point_light((1.0, 0.9, 0.8), 4.0), [0.5, 1.5, 0.5], [0.0, -1.0, 0.0])
@@ -99,7 +103,7 @@ def render(ctx, scene, o):
 @pytest.mark.parametrize("name", ["cornell", "cornell_shadows_aa", "shadow_box", "alpha_planes", "mask_occluder",
                                   "blend_occluder", "tinted_pane_shadow", "mirror", "rough_mirror", "dielectric",
                                   "clear_ball", "thin_ball", "mirrors16", "blend_stack70", "spheres", "ortho",
-                                  "backface", "soup"])
+                                  "backface", "spot", "soup"])
 def test_pbr_equals_the_oracle(ctx, oracle, name):
     scene, o = exact_case(name)
     want_hdr, want_img = oracle.raycast(scene, o)
