@@ -59,7 +59,9 @@ def exact_case(name):
         s.add_light(ts.point_light((1.0, 1.0, 1.0), 3.0), [0.5, 1.5, 0.0], [0.0, -1.0, 0.0])
         return s, P.opts(32, 32, max_ray_depth=16, shadows=True)
     if name == "blend_stack70":
-        return P.blend_stack(70), P.opts(24, 24, shadows=True)
+        # About 3400 samples cross all 70 layers: more than the deep pass's
+        # 2048 slots, so its threads take several samples each.
+        return P.blend_stack(70), P.opts(64, 64, shadows=True)
     if name == "spheres":
         return ts.sphere_grid(3, 3, 24, 12), P.opts(64, 64, shadows=True, aa=2)
     if name == "ortho":
