@@ -45,6 +45,9 @@ PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n)
  * (three small kernels per bounce; on by default). Images are identical
  * either way. */
 PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
+/* Occupancy of the wavefront shade kernel: 3 (default) or 4 blocks of 128
+ * threads per SM. Images are identical either way. */
+PT_API pt_status pt_set_shade_blocks(pt_context *ctx, uint32_t blocks_per_sm);
 /* Wavefront waves replayed from CUDA graphs (one capture per bounce count
  * and sort setting; on by default, bypassed while stage timing is on). */
 PT_API pt_status pt_set_wave_graphs(pt_context *ctx, int on);
@@ -66,9 +69,11 @@ typedef struct pt_tune_choice {
   uint32_t material_sort;        /* 0 / 1 */
   uint32_t wave_slots;
   float samples_per_s;           /* calibration throughput */
+  uint32_t shade_blocks_per_sm;  /* 3 or 4: the shade kernel's occupancy */
 } pt_tune_choice;
 /* Times every candidate (megakernel; wavefront x node widths x material sort
- * x wave size) on a calibration refine of `samples` spp (0: one full wave of
+ * x wave size; then the winner with the shade kernel at 4 instead of 3
+ * blocks per SM) on a calibration refine of `samples` spp (0: one full wave of
  * 4,194,304 paths, capped at 4096 spp) of the tracer's
  * scene, camera and options (a scratch accumulator: the tracer's own is
  * untouched) and records the fastest as the configuration of the scene's

@@ -363,20 +363,23 @@ pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_trac
 // restores the context's own afterwards.
 struct KnobScope {
   pt_context *ctx;
-  uint32_t schedule, wave_slots;
+  uint32_t schedule, wave_slots, shade_blocks;
   bool sort;
   KnobScope(pt_context *c, const TuneChoice *tc)
-      : ctx(c), schedule(c->schedule), wave_slots(c->wave_slots), sort(c->material_sort) {
+      : ctx(c), schedule(c->schedule), wave_slots(c->wave_slots), shade_blocks(c->shade_blocks),
+        sort(c->material_sort) {
     if (tc) {
       c->schedule = tc->schedule;
       c->wave_slots = tc->wave_slots;
       c->material_sort = tc->material_sort != 0;
+      c->shade_blocks = tc->shade_blocks;
     }
   }
   ~KnobScope() {
     ctx->schedule = schedule;
     ctx->wave_slots = wave_slots;
     ctx->material_sort = sort;
+    ctx->shade_blocks = shade_blocks;
   }
 };
 
@@ -436,11 +439,12 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
   const double paths = (double)s.w * s.h * samples;
   best = cands[0];
   float best_ms = -1.0f;
-  for (TuneChoice &c : cands) {
+  auto time_choice = [&](TuneChoice &c, float &ms) -> pt_status {
     ctx->schedule = c.schedule;
     ctx->wave_slots = c.wave_slots;
     ctx->material_sort = c.material_sort != 0;
-    float ms = -1.0f;
+    ctx->shade_blocks = c.shade_blocks;
+    ms = -1.0f;
     for (int rep = 0; rep < 2; ++rep) {
       s.samples = 0;
       std::vector<pt_tracer *> tr{&s};
@@ -451,7 +455,25 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
       if (ms < 0.0f || ctx->last_batch_ms < ms) ms = ctx->last_batch_ms;
     }
     c.samples_per_s = ms > 0.0f ? (float)(paths / (ms * 1e-3)) : 0.0f;
+    return PT_OK;
+  };
+  for (TuneChoice &c : cands) {
+    float ms;
+    pt_status st = time_choice(c, ms);
+    if (st != PT_OK) return st;
     if (best_ms < 0.0f || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  if (best.schedule == PT_SCHEDULE_WAVEFRONT) {
+    // The shade kernel's occupancy on the winning configuration.
+    TuneChoice c = best;
+    c.shade_blocks = 4;
+    float ms;
+    pt_status st = time_choice(c, ms);
+    if (st != PT_OK) return st;
+    if (ms < best_ms) {
       best_ms = ms;
       best = c;
     }
@@ -603,15 +625,16 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
     WaveBuffers w = ctx->wf;
     w.iterations = iters;
     w.sort_materials = ctx->material_sort ? 1u : 0u;
+    w.shade_blocks = ctx->shade_blocks == 4 ? 4u : 3u;
     // Pageable source: the copy is staged before the call returns and lands
     // in stream order, after the previous wave has read its descriptor.
     WaveDesc wd{d_reqs, d_segs, nseg, total, max_pix, 0};
     CK(ctx, cudaMemcpyAsync(w.desc, &wd, sizeof wd, cudaMemcpyHostToDevice, ctx->stream));
     const bool timed = timer && timer->events;
     if (ctx->use_graphs && !timed) {
-      // One captured graph per (bounce count, material sort) replays the
-      // whole wave: one launch instead of ~6 per bounce.
-      const uint32_t key = iters << 1 | w.sort_materials;
+      // One captured graph per (bounce count, shade variant, material sort)
+      // replays the whole wave: one launch instead of ~6 per bounce.
+      const uint32_t key = iters << 2 | (w.shade_blocks == 4 ? 2u : 0u) | w.sort_materials;
       auto it = ctx->graphs.find(key);
       if (it == ctx->graphs.end()) {
         cudaGraphExec_t ge = nullptr;
@@ -1085,6 +1108,7 @@ pt_tune_choice to_c(const TuneChoice &c) {
   o.node_width_extension = (c.wide_nodes & WIDE_EXTENSION) ? 4u : 2u;
   o.node_width_shadow = (c.wide_nodes & WIDE_SHADOW) ? 4u : 2u;
   o.material_sort = c.material_sort;
+  o.shade_blocks_per_sm = c.shade_blocks;
   o.wave_slots = c.wave_slots;
   o.samples_per_s = c.samples_per_s;
   return o;
@@ -1132,6 +1156,13 @@ pt_status pt_tune_reset(pt_context *ctx) {
 pt_status pt_set_wave_graphs(pt_context *ctx, int on) {
   if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
   ctx->use_graphs = on != 0;
+  return PT_OK;
+}
+
+pt_status pt_set_shade_blocks(pt_context *ctx, uint32_t blocks_per_sm) {
+  if (!ctx || (blocks_per_sm != 3 && blocks_per_sm != 4))
+    return fail(ctx, PT_ERR_INVALID_ARG, "shade blocks per SM must be 3 or 4");
+  ctx->shade_blocks = blocks_per_sm;
   return PT_OK;
 }
 

@@ -19,6 +19,7 @@ namespace ptd {
 struct TuneChoice {
   uint32_t schedule, wide_nodes, material_sort, wave_slots;
   float samples_per_s;
+  uint32_t shade_blocks = 3;  // k_wf_shade blocks per SM (3 or 4)
 };
 }  // namespace ptd
 
@@ -34,6 +35,7 @@ struct pt_context {
   // (default: both kinds).
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   bool material_sort = true;  // bucket each shade queue by material
+  uint32_t shade_blocks = 3;   // k_wf_shade instantiation: blocks per SM (3 or 4)
   int bvh_builder = ptd::BVH_BUILD_AUTO;  // where pt_scene_upload builds the BVH (ptd::BvhBuilder)
   ptd::HostStaging staging;  // pinned host image buffer of pt_scene_upload
   std::map<uint32_t, ptd::TuneChoice> tuned;  // by scene class (ptd::scene_class)

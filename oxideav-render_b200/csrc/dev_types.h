@@ -156,6 +156,7 @@ struct WaveBuffers {
   uint32_t *sort_counts;       // [iterations][2][kSortBuckets]: bucket sizes, then cursors
   struct WaveDesc *desc;       // this wave's requests and segments (written before each wave)
   uint32_t capacity, shadow_slots, iterations, sort_materials;
+  uint32_t shade_blocks;       // 3 or 4: the k_wf_shade instantiation (blocks per SM)
 };
 
 // What changes from one wave to the next, read by the kernels from device

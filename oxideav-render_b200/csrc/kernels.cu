@@ -328,7 +328,8 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
   if (e != cudaSuccess) return e;
   int per_sm_ext, per_sm_sh;
   persistent_blocks(per_sm_ext, per_sm_sh);
-  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext), g_shade = (uint32_t)num_sms * 6,
+  const bool shade4 = w.shade_blocks == 4;
+  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext), g_shade = (uint32_t)num_sms * (shade4 ? 8 : 6),
                  g_sh = (uint32_t)(num_sms * per_sm_sh), g_wide = (uint32_t)num_sms * 16;
   tm.mark(STAGE_RAYGEN, st);
   k_wf_raygen<<<g_wide, 256, 0, st>>>(w);
@@ -342,7 +343,10 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
       k_wf_sort_scatter<<<g_shade, 256, 0, st>>>(w, it);
     }
     tm.mark(STAGE_SHADE, st);
-    k_wf_shade<<<g_shade, 128, 0, st>>>(w, it);
+    if (shade4)
+      k_wf_shade<4><<<g_shade, 128, 0, st>>>(w, it);
+    else
+      k_wf_shade<3><<<g_shade, 128, 0, st>>>(w, it);
     tm.mark(STAGE_SHADOW, st);
     k_wf_shadow<<<g_sh, 256, 0, st>>>(w, it, ctr);
   }

@@ -297,9 +297,13 @@ __global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t
   }
 }
 
-// Three 128-thread blocks per SM (168 registers): measured faster than the
-// unconstrained 234-register build despite a few spills.
-__global__ void __launch_bounds__(128, 3) k_wf_shade(WaveBuffers w, uint32_t iter) {
+// kBlocks 128-thread blocks per SM. Three (168 registers) measured faster
+// than the unconstrained 234-register build despite a few spills, and than
+// four on scenes with light shading (C1); four (128 registers, more
+// spills) is faster where shading is heavy (C2's f64 area-light sampling).
+// The tuner picks per scene class.
+template <int kBlocks>
+__global__ void __launch_bounds__(128, kBlocks) k_wf_shade(WaveBuffers w, uint32_t iter) {
   const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.sort_materials ? w.q_sorted : w.q[iter & 1u];

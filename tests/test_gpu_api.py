@@ -105,9 +105,14 @@ def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
             d, rd, _ = _accum_with(ctx, 1, scene, opts, env)
             assert np.array_equal(a, d), sort
             assert rd == ra
+        # The shade kernel at 4 blocks per SM (fewer registers): same image.
+        ctx.set_shade_blocks(4)
+        e, re_, _ = _accum_with(ctx, 1, scene, opts, env)
+        assert np.array_equal(a, e) and re_ == ra
     finally:
         ctx.set_node_width(4, 4)
         ctx.set_material_sort(True)
+        ctx.set_shade_blocks(3)
         ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
 
 
