@@ -45,6 +45,12 @@ PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n)
  * (three small kernels per bounce; on by default). Images are identical
  * either way. */
 PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
+/* Overlapped waves (default on): a refine of two or more waves traces
+ * consecutive waves in two path-state arenas on two streams, so one wave's
+ * last bounces (few paths, most of the GPU idle) run beside the next wave's
+ * first; the accumulates stay in wave order. Images are identical either
+ * way; off: one wave at a time. */
+PT_API pt_status pt_set_wave_overlap(pt_context *ctx, int on);
 /* Occupancy of the wavefront shade kernel: 3 (default) or 4 blocks of 128
  * threads per SM. Images are identical either way. */
 PT_API pt_status pt_set_shade_blocks(pt_context *ctx, uint32_t blocks_per_sm);

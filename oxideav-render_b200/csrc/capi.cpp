@@ -186,18 +186,23 @@ SceneHost *find_scene(pt_context *ctx, uint32_t id) {
   return it == ctx->scenes.end() ? nullptr : it->second.get();
 }
 
-// (Re)allocates the wavefront arena for `capacity` slots with `shadow_slots`
-// queued shadow rays each and `iterations` bounce rounds.
-pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_slots, uint32_t iterations) {
-  WaveBuffers &w = ctx->wf;
-  if (ctx->wf_arena && w.capacity >= capacity && w.shadow_slots >= shadow_slots) {
+// (Re)allocates wavefront arena `which` (0 or 1) for `capacity` slots with
+// `shadow_slots` queued shadow rays each and `iterations` bounce rounds.
+pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_slots, uint32_t iterations,
+                           int which = 0) {
+  WaveBuffers &w = which ? ctx->wf2 : ctx->wf;
+  void *&arena = which ? ctx->wf_arena2 : ctx->wf_arena;
+  size_t &arena_bytes = which ? ctx->wf_bytes2 : ctx->wf_bytes;
+  if (arena && w.capacity >= capacity && w.shadow_slots >= shadow_slots) {
     if (w.iterations >= iterations) return PT_OK;
   }
-  if (ctx->wf_arena) {
+  if (arena) {
+    // Every wave of earlier calls has finished: refines synchronise
+    // ctx->stream, whose accumulates wait for the waves traced elsewhere.
     CK(ctx, cudaStreamSynchronize(ctx->stream));
-    cudaFree(ctx->wf_arena);
-    ctx->wf_arena = nullptr;
-    ctx->wf_bytes = 0;
+    cudaFree(arena);
+    arena = nullptr;
+    arena_bytes = 0;
   }
   // Captured waves point into the old arena.
   for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
@@ -219,9 +224,9 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
     off[i] = total;
     total += sizes[i];
   }
-  CK(ctx, cudaMalloc(&ctx->wf_arena, total));
-  ctx->wf_bytes = total;
-  char *b = static_cast<char *>(ctx->wf_arena);
+  CK(ctx, cudaMalloc(&arena, total));
+  arena_bytes = total;
+  char *b = static_cast<char *>(arena);
   int k = 0;
   w.o = (float4 *)(b + off[k++]);
   w.d = (float4 *)(b + off[k++]);
@@ -289,7 +294,11 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
     }
     max_slots = std::max(max_slots, slots);
   }
-  pt_status st = engine_reserve(ctx, max_slots, max_shadow, max_iter);
+  // Overlapped waves need the wavefront, two or more waves, and no per-stage
+  // timing (whose events sit on one stream).
+  const bool overlap = ctx->overlap_waves && ctx->schedule == PT_SCHEDULE_WAVEFRONT && waves.size() >= 2 &&
+                       !ctx->stage_timing;
+  pt_status st = engine_reserve(ctx, max_slots, max_shadow, max_iter, overlap);
   if (st != PT_OK) return st;
   if ((st = ensure(ctx, ctx->d_segs, ctx->seg_cap, flat.size())) != PT_OK) return st;
   if ((st = ensure(ctx, ctx->d_reqs, ctx->req_cap, jobs.size())) != PT_OK) return st;
@@ -312,10 +321,12 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
     timer.capacity = ctx->stage_events.size();
   }
   CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  if (overlap && (st = engine_overlap_begin(ctx)) != PT_OK) return st;
   for (size_t i = 0; i < waves.size(); ++i) {
     uint32_t iters = 1;
     for (const WaveSegment &s : waves[i]) iters = std::max(iters, jobs[s.request].iterations);
-    st = launch_wave(ctx, ctx->d_reqs, ctx->d_segs + first_seg[i], waves[i], iters, &timer);
+    st = launch_wave(ctx, ctx->d_reqs, ctx->d_segs + first_seg[i], waves[i], iters, &timer,
+                     overlap ? (int)(i & 1) : -1);
     if (st != PT_OK) return st;
   }
   timer.mark(STAGE_END, ctx->stream);
@@ -608,13 +619,32 @@ pt_status autotune(pt_context *ctx, const pt_tracer *t, SceneHost &sc, const Env
   return autotune_scene(ctx, t, &sc, env, samples, best);
 }
 
-pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations) {
-  if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) return ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations);
+pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations,
+                         bool both_arenas) {
+  if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
+    pt_status st = ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations, 0);
+    if (st == PT_OK && both_arenas) st = ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations, 1);
+    return st;
+  }
   return ensure(ctx, ctx->d_out, ctx->out_cap, slots);
 }
 
+pt_status engine_overlap_begin(pt_context *ctx) {
+  if (!ctx->ev_ready) {
+    for (int k = 0; k < 2; ++k) {
+      CK(ctx, cudaStreamCreateWithFlags(&ctx->wave_streams[k], cudaStreamNonBlocking));
+      CK(ctx, cudaEventCreateWithFlags(&ctx->ev_traced[k], cudaEventDisableTiming));
+      CK(ctx, cudaEventCreateWithFlags(&ctx->ev_accumulated[k], cudaEventDisableTiming));
+    }
+    CK(ctx, cudaEventCreateWithFlags(&ctx->ev_ready, cudaEventDisableTiming));
+  }
+  CK(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
+  for (int k = 0; k < 2; ++k) CK(ctx, cudaStreamWaitEvent(ctx->wave_streams[k], ctx->ev_ready, 0));
+  return PT_OK;
+}
+
 pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
-                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer) {
+                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena) {
   uint32_t nseg = (uint32_t)segs.size(), total = 0, max_pix = 0;
   for (const WaveSegment &s : segs) {
     total += s.pixel_count * s.spp;
@@ -622,28 +652,42 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
   }
   if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
     if (total == 0) return PT_OK;
-    WaveBuffers w = ctx->wf;
+    const bool own_stream = arena >= 0;
+    WaveBuffers w = arena == 1 ? ctx->wf2 : ctx->wf;
     w.iterations = iters;
     w.sort_materials = ctx->material_sort ? 1u : 0u;
     w.shade_blocks = ctx->shade_blocks == 4 ? 4u : 3u;
+    cudaStream_t ws = own_stream ? ctx->wave_streams[arena] : ctx->stream;
+    // The arena's previous wave must be accumulated before this one
+    // overwrites its descriptor, queues and per-slot radiance.
+    if (own_stream) CK(ctx, cudaStreamWaitEvent(ws, ctx->ev_accumulated[arena], 0));
     // Pageable source: the copy is staged before the call returns and lands
     // in stream order, after the previous wave has read its descriptor.
     WaveDesc wd{d_reqs, d_segs, nseg, total, max_pix, 0};
-    CK(ctx, cudaMemcpyAsync(w.desc, &wd, sizeof wd, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(w.desc, &wd, sizeof wd, cudaMemcpyHostToDevice, ws));
     const bool timed = timer && timer->events;
     if (ctx->use_graphs && !timed) {
-      // One captured graph per (bounce count, shade variant, material sort)
-      // replays the whole wave: one launch instead of ~6 per bounce.
-      const uint32_t key = iters << 2 | (w.shade_blocks == 4 ? 2u : 0u) | w.sort_materials;
+      // One captured graph per (bounce count, arena / whole wave, shade
+      // variant, material sort) replays the wave: one launch instead of ~6
+      // per bounce.
+      const uint32_t key = iters << 4 | (own_stream ? 8u + 4u * (uint32_t)arena : 0u) |
+                           (w.shade_blocks == 4 ? 2u : 0u) | w.sort_materials;
       auto it = ctx->graphs.find(key);
       if (it == ctx->graphs.end()) {
         cudaGraphExec_t ge = nullptr;
-        CK(ctx, capture_wavefront(w, ctx->d_ctr, ctx->num_sms, &ge));
+        CK(ctx, capture_wavefront(w, ctx->d_ctr, ctx->num_sms, &ge, !own_stream));
         it = ctx->graphs.emplace(key, ge).first;
       }
-      CK(ctx, cudaGraphLaunch(it->second, ctx->stream));
+      CK(ctx, cudaGraphLaunch(it->second, ws));
     } else {
-      CK(ctx, launch_wavefront(w, ctx->d_ctr, ctx->num_sms, ctx->stream, timer));
+      CK(ctx, launch_wavefront(w, ctx->d_ctr, ctx->num_sms, ws, timer, !own_stream));
+    }
+    if (own_stream) {
+      // Accumulate in wave order on ctx->stream once the trace is done.
+      CK(ctx, cudaEventRecord(ctx->ev_traced[arena], ws));
+      CK(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_traced[arena], 0));
+      CK(ctx, launch_wave_accumulate(w, ctx->num_sms, ctx->stream));
+      CK(ctx, cudaEventRecord(ctx->ev_accumulated[arena], ctx->stream));
     }
   } else {
     if (timer) timer->mark(STAGE_MEGAKERNEL, ctx->stream);
@@ -696,12 +740,21 @@ void pt_destroy(pt_context *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (cudaStream_t s : ctx->wave_streams)
+    if (s) cudaStreamSynchronize(s);
   for (auto &kv : ctx->scenes) release_scene(*kv.second);
   ctx->scenes.clear();
   if (ctx->d_out) cudaFree(ctx->d_out);
   for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
   if (ctx->wf_arena) cudaFree(ctx->wf_arena);
+  if (ctx->wf_arena2) cudaFree(ctx->wf_arena2);
+  for (int k = 0; k < 2; ++k) {
+    if (ctx->wave_streams[k]) cudaStreamDestroy(ctx->wave_streams[k]);
+    if (ctx->ev_traced[k]) cudaEventDestroy(ctx->ev_traced[k]);
+    if (ctx->ev_accumulated[k]) cudaEventDestroy(ctx->ev_accumulated[k]);
+  }
+  if (ctx->ev_ready) cudaEventDestroy(ctx->ev_ready);
   if (ctx->d_segs) cudaFree(ctx->d_segs);
   if (ctx->d_reqs) cudaFree(ctx->d_reqs);
   if (ctx->d_ctr) cudaFree(ctx->d_ctr);
@@ -1156,6 +1209,12 @@ pt_status pt_tune_reset(pt_context *ctx) {
 pt_status pt_set_wave_graphs(pt_context *ctx, int on) {
   if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
   ctx->use_graphs = on != 0;
+  return PT_OK;
+}
+
+pt_status pt_set_wave_overlap(pt_context *ctx, int on) {
+  if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
+  ctx->overlap_waves = on != 0;
   return PT_OK;
 }
 

@@ -56,10 +56,20 @@ struct pt_context {
   int num_sms = 148;
   bool stage_timing = false;
   std::vector<cudaEvent_t> stage_events;
-  // Wavefront schedule: one arena holding the SoA path state and queues.
+  // Wavefront schedule: an arena holding the SoA path state and queues, and a
+  // second one so that consecutive waves of a refine overlap (one wave's
+  // last bounces, which leave most of the GPU idle, with the next wave's
+  // first), each traced on its own stream while the accumulates stay in
+  // order on `stream`.
   ptd::WaveBuffers wf{};
   void *wf_arena = nullptr;
   size_t wf_bytes = 0;
+  ptd::WaveBuffers wf2{};
+  void *wf_arena2 = nullptr;
+  size_t wf_bytes2 = 0;
+  bool overlap_waves = true;
+  cudaStream_t wave_streams[2] = {nullptr, nullptr};
+  cudaEvent_t ev_ready = nullptr, ev_traced[2] = {nullptr, nullptr}, ev_accumulated[2] = {nullptr, nullptr};
 };
 
 // The object behind pt_tracer: one progressive accumulation (the
@@ -119,12 +129,20 @@ std::vector<WaveSegment> pack_wave(std::vector<Job> &jobs, const std::vector<uin
 
 // Sizes the context's wave buffers for waves of `slots` paths with up to
 // `shadow_slots` shadow rays per path and `iterations` bounce rounds.
-pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations);
-// Enqueues one wave on ctx->stream: path kernels + ordered accumulate.
-// `d_reqs` / `d_segs` are device copies of the wave's request table and
-// `segs`; `iters` is the largest bounce-round count among the wave's jobs.
+pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, uint32_t iterations,
+                         bool both_arenas = false);
+// Enqueues one wave: path kernels + ordered accumulate. `d_reqs` / `d_segs`
+// are device copies of the wave's request table and `segs`; `iters` is the
+// largest bounce-round count among the wave's jobs. With `arena` -1 the whole
+// wave runs on ctx->stream in the first arena; with 0 or 1 the wave is traced
+// in that arena on its own stream (after the arena's previous accumulate)
+// and accumulated on ctx->stream after the trace (engine_reserve must have
+// been asked for both arenas, and engine_overlap_begin called).
 pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
-                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer);
+                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena = -1);
+// Makes both wave streams wait for the work enqueued on ctx->stream so far
+// (request / segment uploads, counter reset) before overlapped waves.
+pt_status engine_overlap_begin(pt_context *ctx);
 // A new context's engine state on `device` (stream, tables, counters).
 pt_status engine_create(int device, pt_context **out);
 // The background colour in linear light (PathTracer::bg_linear,

@@ -319,7 +319,7 @@ void persistent_blocks(int &per_sm_ext, int &per_sm_sh) {
 }
 
 cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
-                             StageTimer *timer) {
+                             StageTimer *timer, bool accumulate) {
   StageTimer none;
   StageTimer &tm = timer ? *timer : none;
   cudaError_t e = cudaMemsetAsync(w.counters, 0, sizeof(uint32_t) * kWfCounterStride * (w.iterations + 1), st);
@@ -350,12 +350,20 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
     tm.mark(STAGE_SHADOW, st);
     k_wf_shadow<<<g_sh, 256, 0, st>>>(w, it, ctr);
   }
-  tm.mark(STAGE_ACCUMULATE, st);
-  k_wf_accumulate<<<g_wide, 256, 0, st>>>(w);
+  if (accumulate) {
+    tm.mark(STAGE_ACCUMULATE, st);
+    k_wf_accumulate<<<g_wide, 256, 0, st>>>(w);
+  }
   return LAUNCH_CHECK();
 }
 
-cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out) {
+cudaError_t launch_wave_accumulate(const WaveBuffers &w, int num_sms, cudaStream_t st) {
+  k_wf_accumulate<<<(unsigned)num_sms * 16, 256, 0, st>>>(w);
+  return LAUNCH_CHECK();
+}
+
+cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out,
+                              bool accumulate) {
   *out = nullptr;
   int a, b;
   persistent_blocks(a, b);
@@ -365,7 +373,7 @@ cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sm
   cudaGraph_t g = nullptr;
   e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    cudaError_t le = launch_wavefront(w, ctr, num_sms, cs, nullptr);
+    cudaError_t le = launch_wavefront(w, ctr, num_sms, cs, nullptr, accumulate);
     e = cudaStreamEndCapture(cs, &g);
     if (e == cudaSuccess) e = le;
   }

@@ -27,13 +27,17 @@ cudaError_t set_tables(const float *sheen_lut, const float *srgb_thresh);
 cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t total,
                               float4 *out, DevCounters *ctr, cudaStream_t st);
 // One wave of the wavefront schedule (counter reset, ray generation,
-// `w.iterations` bounces, accumulate), driven by the wave descriptor `w.desc`
-// that the caller has written on `st` beforehand.
+// `w.iterations` bounces, and unless `accumulate` is false the in-order
+// accumulate), driven by the wave descriptor `w.desc` that the caller has
+// written on `st` beforehand.
 cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
-                             StageTimer *timer = nullptr);
+                             StageTimer *timer = nullptr, bool accumulate = true);
+// The in-order accumulate of a traced wave on its own (k_wf_accumulate).
+cudaError_t launch_wave_accumulate(const WaveBuffers &w, int num_sms, cudaStream_t st);
 // The same launch sequence captured once as an executable CUDA graph; it
 // stays valid while `w`'s buffers, `ctr` and the bounce count are unchanged.
-cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out);
+cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out,
+                              bool accumulate = true);
 cudaError_t launch_accumulate(const DevRequest *reqs, const WaveSegment *segs, uint32_t nseg, uint32_t max_pixels,
                               const float4 *out, cudaStream_t st);
 cudaError_t launch_resolve_hdr(const double *accum, uint32_t n, uint32_t samples, float4 bg, float4 *out,

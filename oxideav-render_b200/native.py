@@ -95,6 +95,7 @@ SIGNATURES = {
     "pt_set_node_width": (i32, [vp, u32, u32]),
     "pt_set_material_sort": (i32, [vp, i32]),
     "pt_set_shade_blocks": (i32, [vp, u32]),
+    "pt_set_wave_overlap": (i32, [vp, i32]),
     "pt_set_wave_graphs": (i32, [vp, i32]),
     "pt_debug_prepare_scene": (i32, [C.POINTER(abi.pt_scene_desc), dp, u64p]),
     "pt_autotune": (i32, [vp, vp, u32, C.POINTER(abi.pt_tune_choice)]),

@@ -48,6 +48,46 @@ def test_refinement_is_additive_across_waves(ctx):
         ctx.set_wave_slots(1 << 22)
 
 
+@pytest.mark.parametrize("slots", [1024, 20000])
+def test_overlapped_waves_are_bit_identical(ctx, slots):
+    # Many small waves (traced two at a time in two arenas on two streams,
+    # accumulated in wave order) against one wave at a time and the
+    # megakernel: the same accumulators and ray counts, single tracers and a
+    # batch of tracers of different scenes, sizes and bounce limits.
+    cases = [ts.cornell_c0(), ts.sphere_grid_c1(48, 6)]
+    cases[0] = (cases[0][0], cases[0][1].replace(width=40, height=30,
+                                                 path_trace=PathTraceOptions(samples_per_pixel=12, max_bounces=6)))
+    cases.append((ts.alpha_planes(), ts.pt_opts(24, 8, 3)))
+
+    def run(schedule, overlap):
+        ctx.set_schedule(schedule)
+        ctx.set_wave_overlap(overlap)
+        ctx.set_wave_slots(slots)
+        try:
+            ts_ = []
+            for scene, o in cases:
+                t = api.PathTracer(ctx)
+                t.sync(scene, o)
+                ts_.append(t)
+            ts_[0].refine(5)
+            api.refine_many(ctx, ts_, [7, 6, 8])
+            out = [(t.accum(), t.ray_counts()) for t in ts_]
+            for t in ts_:
+                t.close()
+            return out
+        finally:
+            ctx.set_wave_overlap(True)
+            ctx.set_wave_slots(1 << 22)
+            ctx.set_schedule(0)
+
+    mk = run(0, False)
+    seq = run(1, False)
+    ovl = run(1, True)
+    for (a, ra), (b, rb), (c, rc) in zip(mk, seq, ovl):
+        assert np.array_equal(a, b) and np.array_equal(a, c)
+        assert ra == rb == rc
+
+
 def _accum_with(ctx, schedule, scene, opts, env=None):
     ctx.set_schedule(schedule)
     try:
