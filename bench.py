@@ -235,7 +235,8 @@ def run_served(ctx, api, torch, args):
     t0 = time.perf_counter()
     scenes = serving_scenes(args.serve_scenes, 2026)
     gen_s = time.perf_counter() - t0
-    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), autotune=args.autotune)
+    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), autotune=args.autotune,
+                       wave_overlap=args.wave_overlap)
     t0 = time.perf_counter()
     keys = [srv.register(s, o, api.EnvironmentMap(e) if e is not None else None) for s, o, e in scenes]
     register_s = time.perf_counter() - t0
@@ -303,8 +304,9 @@ def run_served(ctx, api, torch, args):
     st = srv.stats()
     srv.close()
 
-    # Plain per-request path on the saturated run's requests (new ones, in
-    # arrival order) within a time budget: one-shot render (scene prepared
+    # Plain per-request path on the saturated run's first --plain-requests new
+    # requests (in arrival order; --plain-seconds caps the time): one-shot
+    # render (scene prepared
     # and uploaded per request, PathTraceRenderer::render_hdr semantics),
     # once with this library's default preparation (device BVH for large
     # scenes) and once with the BVH built on the host as the reference's
@@ -319,7 +321,7 @@ def run_served(ctx, api, torch, args):
     for i, sp in enumerate(spec):
         if sp[0] != "new":
             continue
-        if time.perf_counter() > budget_end:
+        if len(plain_t) >= args.plain_requests or time.perf_counter() > budget_end:
             break
         s, _, e = scenes[sp[1]]
         o = sp[2]
@@ -786,7 +788,8 @@ def main():
     ap.add_argument("--serve-scenes", type=int, default=32, help="resident scenes of the served runs")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
-    ap.add_argument("--plain-seconds", type=float, default=15.0, help="time budget of the plain-path sample")
+    ap.add_argument("--plain-requests", type=int, default=24, help="requests in the plain-path sample")
+    ap.add_argument("--plain-seconds", type=float, default=60.0, help="time cap of the plain-path sample")
     ap.add_argument("--no-raycast", dest="raycast", action="store_false",
                     help="skip the RenderBackend::Raycast measurement")
     ap.add_argument("--upload-only", type=int, default=0,

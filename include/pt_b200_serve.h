@@ -55,6 +55,8 @@ typedef struct pt_server_config {
                                     (pt_autotune on the request's camera and options; the node
                                     layouts of the class's requests follow the result) */
   uint32_t material_sort_off;    /* nonzero: shade without material sort */
+  uint32_t wave_overlap_off;     /* nonzero: trace one wave at a time (default: consecutive waves
+                                    overlap in two path-state arenas on two streams) */
 } pt_server_config;
 
 typedef struct pt_server_request {

@@ -257,6 +257,7 @@ class pt_server_config(C.Structure):
         ("node_width_shadow", C.c_uint32),
         ("autotune", C.c_uint32),
         ("material_sort_off", C.c_uint32),
+        ("wave_overlap_off", C.c_uint32),
     ]
 
 

@@ -178,6 +178,15 @@ struct pt_server {
   bool autotune = false;
   bool tune_pending = false;  // a request waits for an idle stream to tune its class
   uint64_t rays_base = 0;     // rays counted before the device counters were last cleared
+  // Overlapped waves (wavefront engine): consecutive waves are traced in the
+  // engine's two arenas on its two wave streams; the accumulates, resolves
+  // and accumulator allocations stay on the engine stream. Scene and
+  // environment uploads then run on `upload` (the host waits for each, so a
+  // trace never waits on the engine stream), and an eviction's frees wait
+  // on the engine stream's position first (every trace already launched).
+  bool overlap = false;
+  cudaStream_t upload = nullptr;
+  cudaEvent_t ev_free = nullptr;
 };
 
 namespace {
@@ -189,6 +198,12 @@ uint64_t env_bytes_estimate(const pt_environment &e) {
 
 void evict(pt_server *s, SceneEntry &e) {
   if (!e.dev) return;
+  if (s->overlap) {
+    // The arenas are freed on the upload stream: after the engine stream's
+    // accumulates, which wait for their waves' traces.
+    cudaEventRecord(s->ev_free, s->eng->stream);
+    cudaStreamWaitEvent(s->upload, s->ev_free, 0);
+  }
   release_scene(*e.dev);  // stream-ordered free: after every wave already queued
   e.dev.reset();
   if (e.env_dev) {
@@ -234,7 +249,7 @@ Admit make_resident(pt_server *s, const std::shared_ptr<SceneEntry> &e, std::uni
       evict(s, *victim);
     }
   }
-  cudaStream_t stream = s->eng->stream;
+  cudaStream_t stream = s->overlap ? s->upload : s->eng->stream;
   e->pins++;  // keeps it from eviction / unregistration while unlocked
   lk.unlock();
   auto dev = std::make_unique<SceneHost>();
@@ -246,6 +261,16 @@ Admit make_resident(pt_server *s, const std::shared_ptr<SceneEntry> &e, std::uni
     msg = upload_env(e->env, *env_dev, oom, stream);
     if (!msg.empty()) {
       release_scene(*dev);
+      env_dev.reset();
+    }
+  }
+  if (msg.empty() && s->overlap) {
+    // Resident before any wave that reads it is launched, on any stream.
+    cudaError_t se = cudaStreamSynchronize(stream);
+    if (se != cudaSuccess) {
+      msg = std::string("scene upload failed: ") + cudaGetErrorString(se);
+      release_scene(*dev);
+      if (env_dev) release_env(*env_dev);
       env_dev.reset();
     }
   }
@@ -314,6 +339,9 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
     // The calibration refines used the engine's counters: restart them.
     s->rays_base = s->st.rays;
     cudaMemsetAsync(s->eng->d_ctr, 0, sizeof(DevCounters), s->eng->stream);
+    // No wave is in flight while a class tunes: the wave streams may wait
+    // for the engine stream here without serialising anything.
+    if (s->overlap) engine_overlap_begin(s->eng);
     if (tst != PT_OK) {
       fail_admission(s, r, tst, "autotune: " + s->eng->err);
       return Admit::Failed;
@@ -423,7 +451,7 @@ void launch_next_wave(pt_server *s) {
     total += (uint64_t)sg.pixel_count * sg.spp;
     sg.request = (uint32_t)remap[sg.request];
   }
-  pt_status pst = engine_reserve(s->eng, s->wave_slots, shadow, iters);
+  pt_status pst = engine_reserve(s->eng, s->wave_slots, shadow, iters, s->overlap);
   if (pst != PT_OK) {
     break_server(s, "wave buffers: " + s->eng->err);
     return;
@@ -439,15 +467,21 @@ void launch_next_wave(pt_server *s) {
   }
   std::memcpy(f.h_reqs, table.data(), table.size() * sizeof(DevRequest));
   std::memcpy(f.h_segs, segs.data(), segs.size() * sizeof(WaveSegment));
-  e = cudaMemcpyAsync(f.d_reqs, f.h_reqs, table.size() * sizeof(DevRequest), cudaMemcpyHostToDevice, stream);
+  // Overlapped: the tables go up on the wave's own stream, so its trace
+  // waits for nothing queued on the engine stream.
+  const int arena = s->overlap ? (int)(s->wave_no & 1) : -1;
+  cudaStream_t up = arena >= 0 ? s->eng->wave_streams[arena] : stream;
+  if (arena >= 0) e = cudaStreamWaitEvent(up, s->eng->ev_accumulated[arena], 0);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(f.d_segs, f.h_segs, segs.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice, stream);
-  if (e == cudaSuccess) e = cudaEventRecord(f.ev_start, stream);
+    e = cudaMemcpyAsync(f.d_reqs, f.h_reqs, table.size() * sizeof(DevRequest), cudaMemcpyHostToDevice, up);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(f.d_segs, f.h_segs, segs.size() * sizeof(WaveSegment), cudaMemcpyHostToDevice, up);
+  if (e == cudaSuccess) e = cudaEventRecord(f.ev_start, up);
   if (e != cudaSuccess) {
     break_server(s, std::string("wave upload: ") + cudaGetErrorString(e));
     return;
   }
-  pst = launch_wave(s->eng, f.d_reqs, f.d_segs, segs, iters, nullptr);
+  pst = launch_wave(s->eng, f.d_reqs, f.d_segs, segs, iters, nullptr, arena);
   if (pst != PT_OK) {
     break_server(s, "wave launch: " + s->eng->err);
     return;
@@ -614,6 +648,7 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
     s->eng->wide_nodes = (c.node_width_extension == 2 ? 0u : WIDE_EXTENSION) |
                          (c.node_width_shadow == 2 ? 0u : WIDE_SHADOW);
     s->eng->material_sort = c.material_sort_off == 0;
+    s->eng->overlap_waves = c.wave_overlap_off == 0;
     s->autotune = c.autotune != 0;
     s->flights.resize(s->depth + 1);
     cudaError_t e = cudaSuccess;
@@ -624,6 +659,12 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(s->eng->d_ctr, 0, sizeof(DevCounters), s->eng->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->eng->stream);
+    s->overlap = e == cudaSuccess && s->eng->schedule == PT_SCHEDULE_WAVEFRONT && s->eng->overlap_waves;
+    if (s->overlap) {
+      e = cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_free, cudaEventDisableTiming);
+      if (e == cudaSuccess && engine_overlap_begin(s->eng) != PT_OK) e = cudaErrorUnknown;
+    }
     if (e != cudaSuccess) {
       pt_server_destroy(s.release());
       return sfail(PT_ERR_DEVICE, std::string("server setup failed: ") + cudaGetErrorString(e));
@@ -657,6 +698,11 @@ void pt_server_destroy(pt_server *s) {
     }
     if (s->d_resolve) cudaFreeAsync(s->d_resolve, s->eng->stream);
     cudaStreamSynchronize(s->eng->stream);
+    if (s->upload) {
+      cudaStreamSynchronize(s->upload);
+      cudaStreamDestroy(s->upload);
+    }
+    if (s->ev_free) cudaEventDestroy(s->ev_free);
     for (Flight &f : s->flights) {
       if (f.ev_start) cudaEventDestroy(f.ev_start);
       if (f.ev_end) cudaEventDestroy(f.ev_end);

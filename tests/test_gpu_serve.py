@@ -65,10 +65,14 @@ def register_all(srv, scenes):
     return [srv.register(s, o, e) for s, o, e in scenes]
 
 
-@pytest.mark.parametrize("megakernel", [False, True])
-def test_served_images_match_plain(ctx, workload, megakernel):
+@pytest.mark.parametrize("megakernel,overlap,slots", [(False, True, 0), (False, True, 20000), (False, False, 20000),
+                                                      (True, False, 6000)])
+def test_served_images_match_plain(ctx, workload, megakernel, overlap, slots):
+    # Wavefront waves overlapped in two arenas (the default) or one at a
+    # time, large or small waves, and the megakernel: images equal the
+    # plain path's.
     scenes, reqs, ref = workload
-    srv = RenderServer(ctx, wave_slots=6000 if megakernel else 0, megakernel=megakernel)
+    srv = RenderServer(ctx, wave_slots=slots, megakernel=megakernel, wave_overlap=overlap)
     try:
         keys = register_all(srv, scenes)
         tickets = [srv.submit(keys[k], o) for k, o in reqs]
