@@ -610,6 +610,8 @@ def run_b200(args):
     ctx = api.Context(local if ws > 1 else torch.cuda.current_device())
     if not args.wave_overlap:
         ctx.set_wave_overlap(False)
+    elif args.wave_arenas:
+        ctx.set_wave_overlap(args.wave_arenas)
     ctx.set_schedule({"megakernel": 0, "wavefront": 1}[args.schedule])
     if args.seed_per_rank and ws > 1:
         opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__, "seed": rank}))
@@ -796,6 +798,8 @@ def main():
                     help="profiling case: upload the scene this many times (device BVH, device mips) and exit")
     ap.add_argument("--no-wave-overlap", dest="wave_overlap", action="store_false",
                     help="trace one wave at a time instead of overlapping consecutive waves")
+    ap.add_argument("--wave-arenas", type=int, default=0,
+                    help="waves in flight at once (2 or 3; 0: the library's default)")
     ap.add_argument("--raycast-only", type=int, default=0,
                     help="profiling case: this many raycast frames (Phong, then Pbr) of the scene and exit")
     args = ap.parse_args()

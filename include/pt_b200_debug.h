@@ -46,10 +46,11 @@ PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n)
  * either way. */
 PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
 /* Overlapped waves (default on): a refine of two or more waves traces
- * consecutive waves in two path-state arenas on two streams, so one wave's
- * last bounces (few paths, most of the GPU idle) run beside the next wave's
- * first; the accumulates stay in wave order. Images are identical either
- * way; off: one wave at a time. */
+ * consecutive waves in several path-state arenas on as many streams, so one
+ * wave's last bounces (few paths, most of the GPU idle) run beside the next
+ * wave's first; the accumulates stay in wave order. `on`: 0 one wave at a
+ * time, 1 the default (two arenas), 2 or 3 that many arenas. Images are
+ * identical whatever the setting. */
 PT_API pt_status pt_set_wave_overlap(pt_context *ctx, int on);
 /* Occupancy of the wavefront shade kernel: 3 (default) or 4 blocks of 128
  * threads per SM. Images are identical either way. */

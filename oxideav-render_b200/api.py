@@ -137,9 +137,10 @@ class Context:
     def set_material_sort(self, on: bool) -> None:
         self.check(self.lib.pt_set_material_sort(self.ptr, 1 if on else 0))
 
-    def set_wave_overlap(self, on: bool) -> None:
-        """Overlapped waves (two path-state arenas on two streams; default on)."""
-        self.check(self.lib.pt_set_wave_overlap(self.ptr, 1 if on else 0))
+    def set_wave_overlap(self, on) -> None:
+        """Overlapped waves: False / 0 one wave at a time, True / 1 the default
+        (two path-state arenas on two streams), 2 or 3 that many arenas."""
+        self.check(self.lib.pt_set_wave_overlap(self.ptr, int(on)))
 
     def set_shade_blocks(self, blocks_per_sm: int) -> None:
         """Occupancy of the wavefront shade kernel (3 or 4 blocks per SM)."""

@@ -190,9 +190,9 @@ SceneHost *find_scene(pt_context *ctx, uint32_t id) {
 // `shadow_slots` queued shadow rays each and `iterations` bounce rounds.
 pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_slots, uint32_t iterations,
                            int which = 0) {
-  WaveBuffers &w = which ? ctx->wf2 : ctx->wf;
-  void *&arena = which ? ctx->wf_arena2 : ctx->wf_arena;
-  size_t &arena_bytes = which ? ctx->wf_bytes2 : ctx->wf_bytes;
+  WaveBuffers &w = which ? ctx->wf_more[which - 1] : ctx->wf;
+  void *&arena = which ? ctx->wf_arena_more[which - 1] : ctx->wf_arena;
+  size_t &arena_bytes = which ? ctx->wf_bytes_more[which - 1] : ctx->wf_bytes;
   if (arena && w.capacity >= capacity && w.shadow_slots >= shadow_slots) {
     if (w.iterations >= iterations) return PT_OK;
   }
@@ -326,7 +326,7 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
     uint32_t iters = 1;
     for (const WaveSegment &s : waves[i]) iters = std::max(iters, jobs[s.request].iterations);
     st = launch_wave(ctx, ctx->d_reqs, ctx->d_segs + first_seg[i], waves[i], iters, &timer,
-                     overlap ? (int)(i & 1) : -1);
+                     overlap ? (int)(i % ctx->overlap_arenas) : -1);
     if (st != PT_OK) return st;
   }
   timer.mark(STAGE_END, ctx->stream);
@@ -623,7 +623,8 @@ pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, u
                          bool both_arenas) {
   if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
     pt_status st = ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations, 0);
-    if (st == PT_OK && both_arenas) st = ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations, 1);
+    const int n = both_arenas ? (int)ctx->overlap_arenas : 1;
+    for (int k = 1; k < n && st == PT_OK; ++k) st = ensure_wavefront(ctx, (uint32_t)slots, shadow_slots, iterations, k);
     return st;
   }
   return ensure(ctx, ctx->d_out, ctx->out_cap, slots);
@@ -631,7 +632,7 @@ pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, u
 
 pt_status engine_overlap_begin(pt_context *ctx) {
   if (!ctx->ev_ready) {
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < pt_context::kMaxArenas; ++k) {
       CK(ctx, cudaStreamCreateWithFlags(&ctx->wave_streams[k], cudaStreamNonBlocking));
       CK(ctx, cudaEventCreateWithFlags(&ctx->ev_traced[k], cudaEventDisableTiming));
       CK(ctx, cudaEventCreateWithFlags(&ctx->ev_accumulated[k], cudaEventDisableTiming));
@@ -639,7 +640,7 @@ pt_status engine_overlap_begin(pt_context *ctx) {
     CK(ctx, cudaEventCreateWithFlags(&ctx->ev_ready, cudaEventDisableTiming));
   }
   CK(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
-  for (int k = 0; k < 2; ++k) CK(ctx, cudaStreamWaitEvent(ctx->wave_streams[k], ctx->ev_ready, 0));
+  for (int k = 0; k < pt_context::kMaxArenas; ++k) CK(ctx, cudaStreamWaitEvent(ctx->wave_streams[k], ctx->ev_ready, 0));
   return PT_OK;
 }
 
@@ -653,7 +654,7 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
   if (ctx->schedule == PT_SCHEDULE_WAVEFRONT) {
     if (total == 0) return PT_OK;
     const bool own_stream = arena >= 0;
-    WaveBuffers w = arena == 1 ? ctx->wf2 : ctx->wf;
+    WaveBuffers w = arena > 0 ? ctx->wf_more[arena - 1] : ctx->wf;
     w.iterations = iters;
     w.sort_materials = ctx->material_sort ? 1u : 0u;
     w.shade_blocks = ctx->shade_blocks == 4 ? 4u : 3u;
@@ -670,7 +671,7 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
       // One captured graph per (bounce count, arena / whole wave, shade
       // variant, material sort) replays the wave: one launch instead of ~6
       // per bounce.
-      const uint32_t key = iters << 4 | (own_stream ? 8u + 4u * (uint32_t)arena : 0u) |
+      const uint32_t key = iters << 5 | (own_stream ? 4u * (1u + (uint32_t)arena) : 0u) |
                            (w.shade_blocks == 4 ? 2u : 0u) | w.sort_materials;
       auto it = ctx->graphs.find(key);
       if (it == ctx->graphs.end()) {
@@ -748,8 +749,9 @@ void pt_destroy(pt_context *ctx) {
   for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
   ctx->graphs.clear();
   if (ctx->wf_arena) cudaFree(ctx->wf_arena);
-  if (ctx->wf_arena2) cudaFree(ctx->wf_arena2);
-  for (int k = 0; k < 2; ++k) {
+  for (void *a : ctx->wf_arena_more)
+    if (a) cudaFree(a);
+  for (int k = 0; k < pt_context::kMaxArenas; ++k) {
     if (ctx->wave_streams[k]) cudaStreamDestroy(ctx->wave_streams[k]);
     if (ctx->ev_traced[k]) cudaEventDestroy(ctx->ev_traced[k]);
     if (ctx->ev_accumulated[k]) cudaEventDestroy(ctx->ev_accumulated[k]);
@@ -1214,7 +1216,9 @@ pt_status pt_set_wave_graphs(pt_context *ctx, int on) {
 
 pt_status pt_set_wave_overlap(pt_context *ctx, int on) {
   if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
-  ctx->overlap_waves = on != 0;
+  if (on < 0 || on > pt_context::kMaxArenas) return fail(ctx, PT_ERR_INVALID_ARG, "overlap must be 0..3");
+  ctx->overlap_arenas = on == 0 ? 0u : (on == 1 ? 2u : (uint32_t)on);
+  ctx->overlap_waves = ctx->overlap_arenas >= 2;
   return PT_OK;
 }
 

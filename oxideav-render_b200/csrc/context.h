@@ -61,15 +61,17 @@ struct pt_context {
   // last bounces, which leave most of the GPU idle, with the next wave's
   // first), each traced on its own stream while the accumulates stay in
   // order on `stream`.
-  ptd::WaveBuffers wf{};
+  static constexpr int kMaxArenas = 3;
+  ptd::WaveBuffers wf{};  // the first arena (the only one without overlap)
   void *wf_arena = nullptr;
   size_t wf_bytes = 0;
-  ptd::WaveBuffers wf2{};
-  void *wf_arena2 = nullptr;
-  size_t wf_bytes2 = 0;
-  bool overlap_waves = true;
-  cudaStream_t wave_streams[2] = {nullptr, nullptr};
-  cudaEvent_t ev_ready = nullptr, ev_traced[2] = {nullptr, nullptr}, ev_accumulated[2] = {nullptr, nullptr};
+  ptd::WaveBuffers wf_more[kMaxArenas - 1] = {};  // the others
+  void *wf_arena_more[kMaxArenas - 1] = {};
+  size_t wf_bytes_more[kMaxArenas - 1] = {};
+  uint32_t overlap_arenas = 2;  // waves in flight at once; 0: one wave at a time
+  bool overlap_waves = true;    // overlap_arenas >= 2
+  cudaStream_t wave_streams[kMaxArenas] = {};
+  cudaEvent_t ev_ready = nullptr, ev_traced[kMaxArenas] = {}, ev_accumulated[kMaxArenas] = {};
 };
 
 // The object behind pt_tracer: one progressive accumulation (the

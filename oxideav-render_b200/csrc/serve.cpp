@@ -469,7 +469,7 @@ void launch_next_wave(pt_server *s) {
   std::memcpy(f.h_segs, segs.data(), segs.size() * sizeof(WaveSegment));
   // Overlapped: the tables go up on the wave's own stream, so its trace
   // waits for nothing queued on the engine stream.
-  const int arena = s->overlap ? (int)(s->wave_no & 1) : -1;
+  const int arena = s->overlap ? (int)(s->wave_no % s->eng->overlap_arenas) : -1;
   cudaStream_t up = arena >= 0 ? s->eng->wave_streams[arena] : stream;
   if (arena >= 0) e = cudaStreamWaitEvent(up, s->eng->ev_accumulated[arena], 0);
   if (e == cudaSuccess)
@@ -648,7 +648,10 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
     s->eng->wide_nodes = (c.node_width_extension == 2 ? 0u : WIDE_EXTENSION) |
                          (c.node_width_shadow == 2 ? 0u : WIDE_SHADOW);
     s->eng->material_sort = c.material_sort_off == 0;
-    s->eng->overlap_waves = c.wave_overlap_off == 0;
+    if (c.wave_overlap_off) {
+      s->eng->overlap_waves = false;
+      s->eng->overlap_arenas = 0;
+    }
     s->autotune = c.autotune != 0;
     s->flights.resize(s->depth + 1);
     cudaError_t e = cudaSuccess;

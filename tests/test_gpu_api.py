@@ -83,9 +83,10 @@ def test_overlapped_waves_are_bit_identical(ctx, slots):
     mk = run(0, False)
     seq = run(1, False)
     ovl = run(1, True)
-    for (a, ra), (b, rb), (c, rc) in zip(mk, seq, ovl):
-        assert np.array_equal(a, b) and np.array_equal(a, c)
-        assert ra == rb == rc
+    ovl3 = run(1, 3)
+    for (a, ra), (b, rb), (c, rc), (d, rd) in zip(mk, seq, ovl, ovl3):
+        assert np.array_equal(a, b) and np.array_equal(a, c) and np.array_equal(a, d)
+        assert ra == rb == rc == rd
 
 
 def _accum_with(ctx, schedule, scene, opts, env=None):
