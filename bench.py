@@ -689,13 +689,14 @@ def run_b200(args):
     renderer = api.PathTraceCudaRenderer(ctx)
     if env is not None:
         renderer.tracer_mut().set_environment(api.EnvironmentMap(env))
-    e2e_s = []
+    e2e_s, e2e_calls = [], []
     h2d = d2h = 0
     for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         img = renderer.render(scene, opts)
         dt = time.perf_counter() - t0
+        e2e_calls.append({"wall_ms": 1000 * dt, "refine_device_ms": renderer.tracer.last_kernel_ms()})
         if i > 0:
             e2e_s.append(dt)
         h2d = ctx.scene_bytes(renderer.tracer.scene_id)
@@ -706,7 +707,8 @@ def run_b200(args):
         e2e = {"value": samples_per_step * ws / e2e_t, "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_t,
                "call": "PathTraceCudaRenderer.render (scene preparation and upload incl. the BVH build, "
-                       "refine, sRGB image readback)"}
+                       "refine, sRGB image readback)",
+               "calls": e2e_calls}
         # Where the host part of that time goes (one extra, separately timed upload).
         t0 = time.perf_counter()
         desc = scene.to_desc(opts)

@@ -77,10 +77,12 @@ typedef struct pt_tune_choice {
   uint32_t wave_slots;
   float samples_per_s;           /* calibration throughput */
   uint32_t shade_blocks_per_sm;  /* 3 or 4: the shade kernel's occupancy */
+  uint32_t wave_arenas;          /* 2 or 3: overlapped waves in flight (pt_set_wave_overlap) */
 } pt_tune_choice;
 /* Times every candidate (megakernel; wavefront x node widths x material sort
  * x wave size; then the winner with the shade kernel at 4 instead of 3
- * blocks per SM) on a calibration refine of `samples` spp (0: one full wave of
+ * blocks per SM, and with 2 or 3 waves in flight over four waves) on a
+ * calibration refine of `samples` spp (0: one full wave of
  * 4,194,304 paths, capped at 4096 spp) of the tracer's
  * scene, camera and options (a scratch accumulator: the tracer's own is
  * untouched) and records the fastest as the configuration of the scene's

@@ -313,6 +313,7 @@ class pt_tune_choice(C.Structure):
         ("wave_slots", C.c_uint32),
         ("samples_per_s", C.c_float),
         ("shade_blocks_per_sm", C.c_uint32),
+        ("wave_arenas", C.c_uint32),
     ]
 
 

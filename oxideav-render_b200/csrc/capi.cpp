@@ -374,16 +374,19 @@ pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_trac
 // restores the context's own afterwards.
 struct KnobScope {
   pt_context *ctx;
-  uint32_t schedule, wave_slots, shade_blocks;
+  uint32_t schedule, wave_slots, shade_blocks, arenas;
   bool sort;
   KnobScope(pt_context *c, const TuneChoice *tc)
       : ctx(c), schedule(c->schedule), wave_slots(c->wave_slots), shade_blocks(c->shade_blocks),
-        sort(c->material_sort) {
+        arenas(c->overlap_arenas), sort(c->material_sort) {
     if (tc) {
       c->schedule = tc->schedule;
       c->wave_slots = tc->wave_slots;
       c->material_sort = tc->material_sort != 0;
       c->shade_blocks = tc->shade_blocks;
+      // The tuned number of waves in flight, unless overlap is switched off
+      // or its count was set explicitly.
+      if (c->overlap_waves && !c->overlap_fixed) c->overlap_arenas = tc->arenas;
     }
   }
   ~KnobScope() {
@@ -391,6 +394,7 @@ struct KnobScope {
     ctx->wave_slots = wave_slots;
     ctx->material_sort = sort;
     ctx->shade_blocks = shade_blocks;
+    ctx->overlap_arenas = arenas;
   }
 };
 
@@ -447,30 +451,30 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
     for (uint32_t sort : {1u, 0u})
       for (uint32_t slots : {1u << 22, 1u << 20}) cands.push_back({PT_SCHEDULE_WAVEFRONT, wide, sort, slots, 0.0f});
   KnobScope restore(ctx, nullptr);
-  const double paths = (double)s.w * s.h * samples;
   best = cands[0];
   float best_ms = -1.0f;
-  auto time_choice = [&](TuneChoice &c, float &ms) -> pt_status {
+  auto time_choice = [&](TuneChoice &c, float &ms, uint32_t spp) -> pt_status {
     ctx->schedule = c.schedule;
     ctx->wave_slots = c.wave_slots;
     ctx->material_sort = c.material_sort != 0;
     ctx->shade_blocks = c.shade_blocks;
+    if (ctx->overlap_waves) ctx->overlap_arenas = c.arenas;
     ms = -1.0f;
     for (int rep = 0; rep < 2; ++rep) {
       s.samples = 0;
       std::vector<pt_tracer *> tr{&s};
-      std::vector<Job> jobs{make_job(s, *sc, env, samples)};
+      std::vector<Job> jobs{make_job(s, *sc, env, spp)};
       jobs[0].req.wide_nodes = c.wide_nodes;
       pt_status st = run_jobs(ctx, tr, jobs, nullptr);
       if (st != PT_OK) return st;
       if (ms < 0.0f || ctx->last_batch_ms < ms) ms = ctx->last_batch_ms;
     }
-    c.samples_per_s = ms > 0.0f ? (float)(paths / (ms * 1e-3)) : 0.0f;
+    c.samples_per_s = ms > 0.0f ? (float)((double)s.w * s.h * spp / (ms * 1e-3)) : 0.0f;
     return PT_OK;
   };
   for (TuneChoice &c : cands) {
     float ms;
-    pt_status st = time_choice(c, ms);
+    pt_status st = time_choice(c, ms, samples);
     if (st != PT_OK) return st;
     if (best_ms < 0.0f || ms < best_ms) {
       best_ms = ms;
@@ -482,11 +486,23 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
     TuneChoice c = best;
     c.shade_blocks = 4;
     float ms;
-    pt_status st = time_choice(c, ms);
+    pt_status st = time_choice(c, ms, samples);
     if (st != PT_OK) return st;
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
+    }
+    if (ctx->overlap_waves) {
+      // Waves in flight: measured on eight waves (one cannot overlap, and
+      // the third arena pays off only over several).
+      const uint32_t spp4 = std::min<uint32_t>(samples * 8, 32768);
+      TuneChoice c2 = best, c3 = best;
+      c2.arenas = 2;
+      c3.arenas = 3;
+      float ms2, ms3;
+      if ((st = time_choice(c2, ms2, spp4)) != PT_OK) return st;
+      if ((st = time_choice(c3, ms3, spp4)) != PT_OK) return st;
+      best.arenas = ms3 < ms2 ? 3u : 2u;
     }
   }
   ctx->tuned[cls] = best;
@@ -1164,6 +1180,7 @@ pt_tune_choice to_c(const TuneChoice &c) {
   o.node_width_shadow = (c.wide_nodes & WIDE_SHADOW) ? 4u : 2u;
   o.material_sort = c.material_sort;
   o.shade_blocks_per_sm = c.shade_blocks;
+  o.wave_arenas = c.arenas;
   o.wave_slots = c.wave_slots;
   o.samples_per_s = c.samples_per_s;
   return o;
@@ -1219,6 +1236,7 @@ pt_status pt_set_wave_overlap(pt_context *ctx, int on) {
   if (on < 0 || on > pt_context::kMaxArenas) return fail(ctx, PT_ERR_INVALID_ARG, "overlap must be 0..3");
   ctx->overlap_arenas = on == 0 ? 0u : (on == 1 ? 2u : (uint32_t)on);
   ctx->overlap_waves = ctx->overlap_arenas >= 2;
+  ctx->overlap_fixed = on >= 2;
   return PT_OK;
 }
 

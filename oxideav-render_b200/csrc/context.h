@@ -20,6 +20,7 @@ struct TuneChoice {
   uint32_t schedule, wide_nodes, material_sort, wave_slots;
   float samples_per_s;
   uint32_t shade_blocks = 3;  // k_wf_shade blocks per SM (3 or 4)
+  uint32_t arenas = 2;        // overlapped waves in flight (2 or 3)
 };
 }  // namespace ptd
 
@@ -70,6 +71,7 @@ struct pt_context {
   size_t wf_bytes_more[kMaxArenas - 1] = {};
   uint32_t overlap_arenas = 2;  // waves in flight at once; 0: one wave at a time
   bool overlap_waves = true;    // overlap_arenas >= 2
+  bool overlap_fixed = false;   // the count was set explicitly: tuned choices keep it
   cudaStream_t wave_streams[kMaxArenas] = {};
   cudaEvent_t ev_ready = nullptr, ev_traced[kMaxArenas] = {}, ev_accumulated[kMaxArenas] = {};
 };

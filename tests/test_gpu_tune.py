@@ -27,7 +27,7 @@ def test_autotune_records_a_class_choice_and_keeps_images(ctx):
     assert choice["schedule"] in (0, 1)
     assert choice["node_width_extension"] in (2, 4) and choice["node_width_shadow"] in (2, 4)
     assert choice["material_sort"] in (0, 1) and choice["wave_slots"] > 0
-    assert choice["shade_blocks_per_sm"] in (3, 4)
+    assert choice["shade_blocks_per_sm"] in (3, 4) and choice["wave_arenas"] in (2, 3)
     assert choice["samples_per_s"] > 0
     assert ctx.tune_lookup(t) == choice
     # The tracer's own accumulator was not touched; tuned refines continue it.
