@@ -612,6 +612,8 @@ def run_b200(args):
         ctx.set_wave_overlap(False)
     elif args.wave_arenas:
         ctx.set_wave_overlap(args.wave_arenas)
+    if args.wave_slots:
+        ctx.set_wave_slots(args.wave_slots)
     ctx.set_schedule({"megakernel": 0, "wavefront": 1}[args.schedule])
     if args.seed_per_rank and ws > 1:
         opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__, "seed": rank}))
@@ -677,7 +679,10 @@ def run_b200(args):
     achieved = stage_bytes[dom] / (stage[dom] / 1000.0) / 1e9
     kernel_names = {"extend": "k_wf_extend", "shade": "k_wf_shade", "shadow": "k_wf_shadow",
                     "megakernel": "k_megakernel", "accumulate": "k_accumulate"}
-    waves = max(math.ceil(samples_per_step / (1 << 22)), 1)
+    # Waves of the refine: the tuned wave size, else the one set or the
+    # library's default (8,388,608 path slots).
+    wave_slots = (tuned or {}).get("wave_slots") or args.wave_slots or (1 << 23)
+    waves = max(math.ceil(samples_per_step / wave_slots), 1)
     iters = opts.path_trace.max_bounces + 1
     per_wave = (2 + 3 * iters) if args.schedule == "wavefront" else 2
     launches = args.steps * waves * per_wave
@@ -800,6 +805,8 @@ def main():
                     help="profiling case: upload the scene this many times (device BVH, device mips) and exit")
     ap.add_argument("--no-wave-overlap", dest="wave_overlap", action="store_false",
                     help="trace one wave at a time instead of overlapping consecutive waves")
+    ap.add_argument("--wave-slots", type=int, default=0,
+                    help="path slots per wave (0: the library's default; autotune may override)")
     ap.add_argument("--wave-arenas", type=int, default=0,
                     help="waves in flight at once (2 or 3; 0: the library's default)")
     ap.add_argument("--raycast-only", type=int, default=0,

@@ -83,7 +83,7 @@ typedef struct pt_tune_choice {
  * x wave size; then the winner with the shade kernel at 4 instead of 3
  * blocks per SM, and with 2 or 3 waves in flight over four waves) on a
  * calibration refine of `samples` spp (0: one full wave of
- * 4,194,304 paths, capped at 4096 spp) of the tracer's
+ * 8,388,608 paths, capped at 4096 spp) of the tracer's
  * scene, camera and options (a scratch accumulator: the tracer's own is
  * untouched) and records the fastest as the configuration of the scene's
  * class: later refines of tracers in that class use it. Every candidate

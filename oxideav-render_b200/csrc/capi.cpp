@@ -422,10 +422,10 @@ pt_status refine_impl(pt_tracer *t, uint32_t n) {
 pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, const EnvHost *env, uint32_t samples,
                          TuneChoice &best) {
   if (samples == 0) {
-    // One full wave (4,194,304 paths): the size real refines run at, where
+    // One full wave (8,388,608 paths): the size real refines run at, where
     // per-launch costs weigh as they will in use.
     const uint64_t npix = (uint64_t)std::max(t->w, 1u) * std::max(t->h, 1u);
-    samples = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((1ull << 22) / npix, 1), 4096);
+    samples = (uint32_t)std::min<uint64_t>(std::max<uint64_t>((1ull << 23) / npix, 1), 4096);
   }
   CK(ctx, cudaSetDevice(ctx->device));
   pt_tracer s;
@@ -449,7 +449,7 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
   cands.push_back({PT_SCHEDULE_MEGAKERNEL, WIDE_EXTENSION | WIDE_SHADOW, 0, 1u << 22, 0.0f});
   for (uint32_t wide : {WIDE_EXTENSION | WIDE_SHADOW, (uint32_t)WIDE_SHADOW, 0u, (uint32_t)WIDE_EXTENSION})
     for (uint32_t sort : {1u, 0u})
-      for (uint32_t slots : {1u << 22, 1u << 20}) cands.push_back({PT_SCHEDULE_WAVEFRONT, wide, sort, slots, 0.0f});
+      for (uint32_t slots : {1u << 23, 1u << 20}) cands.push_back({PT_SCHEDULE_WAVEFRONT, wide, sort, slots, 0.0f});
   KnobScope restore(ctx, nullptr);
   best = cands[0];
   float best_ms = -1.0f;
