@@ -236,7 +236,7 @@ def run_served(ctx, api, torch, args):
     scenes = serving_scenes(args.serve_scenes, 2026)
     gen_s = time.perf_counter() - t0
     srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), autotune=args.autotune,
-                       wave_overlap=args.wave_overlap)
+                       wave_overlap=args.wave_overlap, wave_slots=args.serve_wave_slots)
     t0 = time.perf_counter()
     keys = [srv.register(s, o, api.EnvironmentMap(e) if e is not None else None) for s, o, e in scenes]
     register_s = time.perf_counter() - t0
@@ -797,6 +797,7 @@ def main():
     ap.add_argument("--serve-scenes", type=int, default=32, help="resident scenes of the served runs")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
+    ap.add_argument("--serve-wave-slots", type=int, default=0, help="path slots per served wave (0: the server's default)")
     ap.add_argument("--plain-requests", type=int, default=24, help="requests in the plain-path sample")
     ap.add_argument("--plain-seconds", type=float, default=60.0, help="time cap of the plain-path sample")
     ap.add_argument("--no-raycast", dest="raycast", action="store_false",
