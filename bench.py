@@ -397,17 +397,21 @@ def algorithmic_bytes(ext_rays, shadow_rays, nodes, tris, samples):
             + 32 * samples)
 
 
-def profiled_traffic(kernel: str, config: str):
+def profiled_traffic(kernel: str, config: str, wave_paths: int):
     """DRAM bytes per launch of `kernel` from the committed ncu summary
     (profiles/<kernel>_*.md, line `traffic_bytes_per_launch | N`), scaled to
-    this workload's launch size when the capture ran a smaller case."""
+    this workload's launch size when the capture ran a smaller wave (line
+    `profiled_wave_paths | M`): a launch's traffic grows with the paths it
+    processes."""
     import glob
     import re
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
         text = open(path).read()
         m = re.search(r"traffic_bytes_per_launch \| (\d+)", text)
         if m and f"config={config}" in text:
-            return int(m.group(1))
+            w = re.search(r"profiled_wave_paths \| (\d+)", text)
+            scale = wave_paths / int(w.group(1)) if w else 1.0
+            return int(int(m.group(1)) * scale)
     return None
 
 
@@ -688,7 +692,7 @@ def run_b200(args):
     launches = args.steps * waves * per_wave
     launches_of_dom = args.steps * waves * (iters if args.schedule == "wavefront" and dom in
                                             ("extend", "shade", "shadow") else 1)
-    traffic = profiled_traffic(kernel_names[dom], args.config)
+    traffic = profiled_traffic(kernel_names[dom], args.config, min(wave_slots, samples_per_step))
 
     # End to end: the reference-facing one-shot call (re-prepare + render + image).
     renderer = api.PathTraceCudaRenderer(ctx)
