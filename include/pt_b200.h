@@ -365,14 +365,21 @@ PT_API pt_status pt_render_hdr(pt_context *ctx, uint32_t scene_id, const pt_came
  * width*height*4 doubles (sum r, g, b, covered count per pixel) that this
  * call adds `samples` samples to, starting at sample index `first_sample`
  * (so consecutive calls continue the sequence exactly like
- * pt_tracer_refine). The per-wave path samples live in a fixed scratch array
- * compiled into the library (1,048,576 path slots, 16 MiB, held by every GPU
- * that loads the library until the process exits); images above 1,048,576
+ * pt_tracer_refine). `d_accum` must be 16-byte aligned, on the context's
+ * device, and lie inside one device allocation with room for the whole
+ * image; anything else is rejected with PT_ERR_INVALID_ARG before any
+ * launch. The per-wave path samples live in a fixed scratch array compiled
+ * into the library (1,048,576 path slots, 16 MiB, held by every GPU that
+ * loads the library until the process exits); images above 1,048,576
  * pixels are rejected with PT_ERR_INVALID_ARG. No environment map (the sky is
- * `ambient`). The first call on a device looks up the scratch address for
- * that device; make that first call before any stream capture. Every call
- * reuses the same scratch, so calls that overlap on the GPU race: serialise
- * them. */
+ * `ambient`). The samples are traced by the megakernel schedule whatever
+ * the context's schedule and tuned choices say: the image equals
+ * pt_tracer_refine's, the speed is the megakernel's. The call waits for its
+ * work (it synchronises the context's stream) before returning. The first
+ * call on a device looks up the scratch address for that device and keeps
+ * it for the life of the process (a cudaDeviceReset makes it stale); make
+ * that first call before any stream capture. Every call reuses the same
+ * scratch, so calls that overlap on the GPU race: serialise them. */
 PT_API pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
                                    const pt_render_options *opts, uint32_t first_sample, uint32_t samples,
                                    double *d_accum);

@@ -49,8 +49,8 @@ PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
  * consecutive waves in several path-state arenas on as many streams, so one
  * wave's last bounces (few paths, most of the GPU idle) run beside the next
  * wave's first; the accumulates stay in wave order. `on`: 0 one wave at a
- * time, 1 the default (two arenas), 2 or 3 that many arenas. Images are
- * identical whatever the setting. */
+ * time, 1 the default (three arenas, or the scene class's tuned count), 2
+ * or 3 that many arenas. Images are identical whatever the setting. */
 PT_API pt_status pt_set_wave_overlap(pt_context *ctx, int on);
 /* Occupancy of the wavefront shade kernel: 3 (default) or 4 blocks of 128
  * threads per SM. Images are identical either way. */
@@ -129,8 +129,8 @@ PT_API pt_status pt_debug_scene_texels(pt_context *ctx, uint32_t scene_id, float
                                        uint64_t *total);
 
 /* Schedule of the hot loop: one path per thread (megakernel), or the
- * wavefront (extend / shade / shadow kernels over compacted queues). Both
- * produce bit-identical accumulators. */
+ * wavefront (extend / shade / shadow kernels over compacted queues; the
+ * default of a new context). Both produce bit-identical accumulators. */
 typedef enum pt_schedule { PT_SCHEDULE_MEGAKERNEL = 0, PT_SCHEDULE_WAVEFRONT = 1 } pt_schedule;
 PT_API pt_status pt_set_schedule(pt_context *ctx, uint32_t schedule);
 /* Maximum path slots per wave (device sample buffer 16 B per slot). */

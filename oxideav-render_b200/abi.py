@@ -47,6 +47,10 @@ PT_PERSPECTIVE, PT_ORTHOGRAPHIC = 0, 1
 PT_MIS, PT_LIGHT_ONLY, PT_BSDF_ONLY = 0, 1, 2
 PT_TONE_CLAMP, PT_TONE_REINHARD, PT_TONE_ACES = 0, 1, 2
 PT_BVH_BUILD_AUTO, PT_BVH_BUILD_HOST, PT_BVH_BUILD_DEVICE, PT_BVH_BUILD_DEVICE_PLOC = 0, 1, 2, 3
+# pt_schedule (include/pt_b200_debug.h); a new context runs the wavefront.
+PT_SCHEDULE_MEGAKERNEL, PT_SCHEDULE_WAVEFRONT = 0, 1
+# A new context's path slots per wave.
+PT_DEFAULT_WAVE_SLOTS = 1 << 23
 
 f3 = C.c_float * 3
 f4 = C.c_float * 4

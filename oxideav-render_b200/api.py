@@ -139,7 +139,8 @@ class Context:
 
     def set_wave_overlap(self, on) -> None:
         """Overlapped waves: False / 0 one wave at a time, True / 1 the default
-        (two path-state arenas on two streams), 2 or 3 that many arenas."""
+        (three path-state arenas on three streams, or the scene class's tuned
+        count), 2 or 3 that many arenas."""
         self.check(self.lib.pt_set_wave_overlap(self.ptr, int(on)))
 
     def set_shade_blocks(self, blocks_per_sm: int) -> None:

@@ -1234,7 +1234,7 @@ pt_status pt_set_wave_graphs(pt_context *ctx, int on) {
 pt_status pt_set_wave_overlap(pt_context *ctx, int on) {
   if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
   if (on < 0 || on > pt_context::kMaxArenas) return fail(ctx, PT_ERR_INVALID_ARG, "overlap must be 0..3");
-  ctx->overlap_arenas = on == 0 ? 0u : (on == 1 ? 2u : (uint32_t)on);
+  ctx->overlap_arenas = on == 0 ? 0u : (on == 1 ? 3u : (uint32_t)on);
   ctx->overlap_waves = ctx->overlap_arenas >= 2;
   ctx->overlap_fixed = on >= 2;
   return PT_OK;

@@ -16,8 +16,18 @@
 // process exits. Each call overwrites it; calls that overlap on the GPU
 // (two contexts, or two threads, on the same device at the same time) race
 // on it and must be serialised by the caller.
+//
+// The samples are traced by the one-launch megakernel schedule: the
+// wavefront's path-state arenas are far larger than a fixed scratch can
+// hold. Images are identical to pt_tracer_refine's (whose default is the
+// wavefront), but the speed is the megakernel's, and the context's schedule
+// and tuned per-class knobs are not consulted here.
+#include <cudaTypedefs.h>
+
 #include <cmath>
+#include <cstdint>
 #include <mutex>
+#include <new>
 #include <string>
 
 #include "context.h"
@@ -56,6 +66,43 @@ cudaError_t scratch_address(int device, NoAllocScratch **out) {
   return cudaSuccess;
 }
 
+// The caller's accumulator must be device (or managed) memory of this
+// context's device, 16-byte aligned (the accumulate kernel reads and writes
+// it as double4), and lie wholly inside one allocation of at least `bytes`
+// from `p`: a kernel given anything else would fault on a shared GPU.
+// The allocation range comes from the driver (cuMemGetAddressRange, fetched
+// through the runtime's entry-point query, so no libcuda link is needed).
+std::string check_accumulator(int device, const void *p, uint64_t bytes) {
+  if (reinterpret_cast<uintptr_t>(p) % 16 != 0) return "d_accum must be 16-byte aligned";
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return "d_accum is not a pointer the CUDA runtime knows";
+  }
+  if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+    return "d_accum must point to device (or managed) memory";
+  if (a.type == cudaMemoryTypeDevice && a.device != device)
+    return "d_accum belongs to device " + std::to_string(a.device) + ", the context to device " +
+           std::to_string(device);
+  static PFN_cuMemGetAddressRange_v3020 range_fn = [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      fn = nullptr;
+    return reinterpret_cast<PFN_cuMemGetAddressRange_v3020>(fn);
+  }();
+  if (!range_fn) return "the driver does not report allocation ranges; d_accum cannot be checked";
+  CUdeviceptr_v2 base = 0;
+  size_t size = 0;
+  const CUdeviceptr_v2 at = static_cast<CUdeviceptr_v2>(reinterpret_cast<uintptr_t>(p));
+  if (range_fn(&base, &size, at) != CUDA_SUCCESS) return "d_accum is not inside a device allocation";
+  if (at + bytes > base + size)
+    return "d_accum holds " + std::to_string((base + size - at) / 32) + " pixels, the image needs " +
+           std::to_string(bytes / 32);
+  return std::string();
+}
+
 #define NA_CHECK(call)                                                                                     \
   do {                                                                                                     \
     cudaError_t e_ = (call);                                                                               \
@@ -63,12 +110,9 @@ cudaError_t scratch_address(int device, NoAllocScratch **out) {
       return ptd::ctx_fail(ctx, PT_ERR_DEVICE, std::string(#call) + ": " + cudaGetErrorString(e_));       \
   } while (0)
 
-}  // namespace
-
-extern "C" pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
-                                       const pt_render_options *opts, uint32_t first_sample, uint32_t samples,
-                                       double *d_accum) {
-  if (!ctx) return PT_ERR_INVALID_ARG;
+pt_status refine_noalloc_impl(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+                              const pt_render_options *opts, uint32_t first_sample, uint32_t samples,
+                              double *d_accum) {
   if (!camera || !opts || !d_accum) return ptd::ctx_fail(ctx, PT_ERR_INVALID_ARG, "camera / options / accum is NULL");
   if (opts->path_trace.max_bounces > 1024)
     return ptd::ctx_fail(ctx, PT_ERR_INVALID_ARG, "path_trace.max_bounces must be <= 1024");
@@ -87,6 +131,8 @@ extern "C" pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const
   if (!sc) return ptd::ctx_fail(ctx, PT_ERR_NOT_FOUND, "unknown scene " + std::to_string(scene_id));
   if (samples == 0) return PT_OK;
   NA_CHECK(cudaSetDevice(ctx->device));
+  const std::string bad = check_accumulator(ctx->device, d_accum, npix * 4 * sizeof(double));
+  if (!bad.empty()) return ptd::ctx_fail(ctx, PT_ERR_INVALID_ARG, "pt_refine_noalloc: " + bad);
   NoAllocScratch *scratch = nullptr;
   NA_CHECK(scratch_address(ctx->device, &scratch));
 
@@ -127,4 +173,20 @@ extern "C" pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const
   if (counters.error_flags & ptd::ERR_STACK_OVERFLOW)
     return ptd::ctx_fail(ctx, PT_ERR_DEVICE, "BVH traversal stack overflow");
   return PT_OK;
+}
+}  // namespace
+
+extern "C" pt_status pt_refine_noalloc(pt_context *ctx, uint32_t scene_id, const pt_camera *camera,
+                                       const pt_render_options *opts, uint32_t first_sample, uint32_t samples,
+                                       double *d_accum) {
+  if (!ctx) return PT_ERR_INVALID_ARG;
+  // No exception crosses the C ABI.
+  try {
+    return refine_noalloc_impl(ctx, scene_id, camera, opts, first_sample, samples, d_accum);
+  } catch (const std::bad_alloc &) {
+    ctx->err = "host allocation failed";
+    return PT_ERR_OOM;
+  } catch (...) {
+    return PT_ERR_DEVICE;
+  }
 }

@@ -45,7 +45,7 @@ def test_refinement_is_additive_across_waves(ctx):
         t2.refine(7)
         assert np.array_equal(t2.accum(), ref)
     finally:
-        ctx.set_wave_slots(1 << 22)
+        ctx.set_wave_slots(abi.PT_DEFAULT_WAVE_SLOTS)
 
 
 @pytest.mark.parametrize("slots", [1024, 20000])
@@ -77,8 +77,8 @@ def test_overlapped_waves_are_bit_identical(ctx, slots):
             return out
         finally:
             ctx.set_wave_overlap(True)
-            ctx.set_wave_slots(1 << 22)
-            ctx.set_schedule(0)
+            ctx.set_wave_slots(abi.PT_DEFAULT_WAVE_SLOTS)
+            ctx.set_schedule(abi.PT_SCHEDULE_WAVEFRONT)
 
     mk = run(0, False)
     seq = run(1, False)
@@ -101,7 +101,7 @@ def _accum_with(ctx, schedule, scene, opts, env=None):
         t.close()
         return out
     finally:
-        ctx.set_schedule(0)
+        ctx.set_schedule(abi.PT_SCHEDULE_WAVEFRONT)
 
 
 @pytest.mark.parametrize("case", ["cornell", "spheres", "materials", "env", "alpha", "dispersion"])
@@ -229,3 +229,32 @@ def test_scene_release_and_counts(ctx):
     ctx.release(sid)
     with pytest.raises(api.RenderError):
         ctx.release(sid)
+
+
+def test_a_fresh_context_runs_the_wavefront_by_default():
+    # The drop-in path (make_renderer / pt_create with nothing set) must run
+    # the wavefront schedule, and its accumulator must equal the megakernel's.
+    scene, opts = ts.sphere_grid_c1(64, 4)
+    fresh = api.Context(0)
+    try:
+        fresh.set_stage_timing(True)  # only records per-stage device times
+        t = api.PathTracer(fresh)
+        t.sync(scene, opts)
+        t.refine(4)
+        stages = t.stage_ms()
+        assert stages["extend"] > 0.0 and stages["shade"] > 0.0 and stages["shadow"] > 0.0, stages
+        assert stages["megakernel"] == 0.0, stages
+        wf = t.accum()
+        t.close()
+    finally:
+        fresh.close()
+    mk = api.Context(0)
+    try:
+        mk.set_schedule(abi.PT_SCHEDULE_MEGAKERNEL)
+        t = api.PathTracer(mk)
+        t.sync(scene, opts)
+        t.refine(4)
+        assert np.array_equal(t.accum(), wf)
+        t.close()
+    finally:
+        mk.close()

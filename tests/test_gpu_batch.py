@@ -4,7 +4,7 @@ limits, environment maps; both schedules; waves that split images)."""
 import numpy as np
 import pytest
 
-from oxideav_render_b200 import api, testscenes as ts
+from oxideav_render_b200 import abi, api, testscenes as ts
 from oxideav_render_b200.options import PathTraceOptions
 
 pytestmark = pytest.mark.gpu
@@ -61,8 +61,8 @@ def test_batched_refine_is_bit_identical_to_separate_refines(ctx, schedule, slot
         for t in tracers:
             t.close()
     finally:
-        ctx.set_schedule(0)
-        ctx.set_wave_slots(1 << 22)
+        ctx.set_schedule(abi.PT_SCHEDULE_WAVEFRONT)
+        ctx.set_wave_slots(abi.PT_DEFAULT_WAVE_SLOTS)
 
 
 def test_batch_rejects_duplicate_tracers(ctx):

@@ -60,7 +60,7 @@ def render(ctx, builder, scene, opts, env, schedule):
         return out
     finally:
         ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
-        ctx.set_schedule(0)
+        ctx.set_schedule(abi.PT_SCHEDULE_WAVEFRONT)
 
 
 @pytest.mark.parametrize("name", ["spheres", "soup", "materials", "env", "alpha", "dispersion"])
