@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define PT_ABI_VERSION 1u
+#define PT_ABI_VERSION 2u
 
 #if defined(__GNUC__)
 #define PT_API __attribute__((visibility("default")))

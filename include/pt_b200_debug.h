@@ -128,6 +128,12 @@ PT_API pt_status pt_scene_upload_seconds(pt_context *ctx, uint32_t scene_id, dou
 PT_API pt_status pt_debug_scene_texels(pt_context *ctx, uint32_t scene_id, float *out, uint64_t capacity,
                                        uint64_t *total);
 
+/* Fault injection on the host (tests): the next `count` device allocations
+ * the context makes (accumulators, wave arenas and tables, scene uploads)
+ * fail with PT_ERR_OOM as if cudaMalloc had run out of memory, without
+ * calling CUDA. The context stays usable. 0 disarms it. */
+PT_API pt_status pt_debug_fail_allocations(pt_context *ctx, uint32_t count);
+
 /* Schedule of the hot loop: one path per thread (megakernel), or the
  * wavefront (extend / shade / shadow kernels over compacted queues; the
  * default of a new context). Both produce bit-identical accumulators. */

@@ -19,9 +19,14 @@
  *     the accumulator of an earlier request (PathTracer::refine on a live
  *     tracer) and returns the refined image.
  *   - A worker thread admits requests as accumulator slots and scene memory
- *     allow and runs waves of path slots drawn from every admitted request
- *     (shortest remaining work first), so requests that arrive while others
- *     are on the GPU share the next waves.
+ *     allow and runs waves of path slots drawn from every admitted request,
+ *     so requests that arrive while others are on the GPU share the next
+ *     waves. Waves are packed earliest expected finish first: a request's
+ *     key is its submit time plus its remaining samples at the measured
+ *     throughput, which favours short requests without starving long ones.
+ *   - A request can be cancelled (pt_server_cancel) or given a deadline
+ *     (pt_server_request.deadline_ms) after which it fails with
+ *     PT_ERR_TIMEOUT; pt_server_poll asks without blocking.
  *
  * Determinism: every sample is a pure function of (request seed, pixel,
  * sample index) and each pixel's samples are accumulated in index order, so
@@ -65,6 +70,8 @@ typedef struct pt_server_request {
   uint64_t continues;         /* 0: a new accumulation; else the ticket whose accumulator gains `samples` */
   pt_camera camera;           /* Camera::resolve output (ignored for continuations) */
   pt_render_options options;  /* as for pt_tracer_sync (ignored for continuations) */
+  uint32_t deadline_ms;       /* 0: none; else the request fails with PT_ERR_TIMEOUT when it has not
+                                 finished this many ms after its submit (checked between waves) */
 } pt_server_request;
 
 typedef struct pt_request_stats {
@@ -86,6 +93,8 @@ typedef struct pt_server_stats {
   uint64_t resident_bytes, peak_resident_bytes;
   uint32_t resident_scenes, active, pending, accumulators;
   uint64_t tuned_classes;   /* scene classes tuned by the server (config.autotune) */
+  uint64_t cancelled;       /* requests ended by pt_server_cancel (also counted in `failed`) */
+  uint64_t timed_out;       /* requests ended by their deadline (also counted in `failed`) */
 } pt_server_stats;
 
 /* A server on `ctx`'s device. `cfg` may be NULL (defaults). The server does
@@ -114,14 +123,35 @@ PT_API pt_status pt_server_submit(pt_server *server, const pt_server_request *re
 /* Waits up to `timeout_ms` (< 0: no limit) for `ticket`. PT_OK: the request
  * finished; its HDR image (width * height * 4 floats, row-major RGBA) is
  * copied to `hdr` when non-NULL (`hdr_floats` is its capacity) and `stats`
- * is filled when non-NULL. PT_ERR_NOT_READY: still running at the timeout.
- * Any other status is the request's own failure. */
+ * is filled when non-NULL. PT_ERR_TIMEOUT: still running when `timeout_ms`
+ * ran out (the request goes on; wait again or cancel it). Any other status
+ * is the request's own failure (PT_ERR_CANCELLED, PT_ERR_TIMEOUT from its
+ * deadline, PT_ERR_OOM, ...). */
 PT_API pt_status pt_server_wait(pt_server *server, uint64_t ticket, int32_t timeout_ms, float *hdr,
                                 size_t hdr_floats, pt_request_stats *stats);
+/* pt_server_wait without blocking: PT_ERR_NOT_READY while the request is
+ * queued or running, else what pt_server_wait returns. */
+PT_API pt_status pt_server_poll(pt_server *server, uint64_t ticket, float *hdr, size_t hdr_floats,
+                                pt_request_stats *stats);
+/* Cancels `ticket`. A queued request leaves the queue; a running one gets no
+ * further waves (waves already on the GPU finish, their samples are
+ * discarded with the accumulation). Either way it ends with
+ * PT_ERR_CANCELLED, and continuations of a cancelled request fail. A request
+ * whose last wave is already on the GPU ends cancelled when that wave
+ * completes; its accumulation stays usable. PT_ERR_INVALID_ARG when the
+ * request has already finished, PT_ERR_NOT_FOUND for an unknown ticket.
+ * The ticket must still be released. */
+PT_API pt_status pt_server_cancel(pt_server *server, uint64_t ticket);
 /* Drops a finished request's image; the accumulator goes once no ticket on
  * it is left. A released ticket cannot be continued. */
 PT_API pt_status pt_server_release(pt_server *server, uint64_t ticket);
 PT_API pt_status pt_server_stats_get(pt_server *server, pt_server_stats *out);
+/* Fault injection on the host (tests): the next `count` device allocations
+ * the server makes for requests and scenes (accumulators, scene and
+ * environment images) fail as if the device were out of memory, without
+ * calling CUDA. The request that needed one fails with PT_ERR_OOM; the
+ * server goes on serving. 0 disarms it. */
+PT_API pt_status pt_server_debug_fail_allocations(pt_server *server, uint32_t count);
 
 #ifdef __cplusplus
 }

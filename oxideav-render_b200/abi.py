@@ -272,6 +272,7 @@ class pt_server_request(C.Structure):
         ("continues", C.c_uint64),
         ("camera", pt_camera),
         ("options", pt_render_options),
+        ("deadline_ms", C.c_uint32),
     ]
 
 
@@ -304,6 +305,8 @@ class pt_server_stats(C.Structure):
         ("pending", C.c_uint32),
         ("accumulators", C.c_uint32),
         ("tuned_classes", C.c_uint64),
+        ("cancelled", C.c_uint64),
+        ("timed_out", C.c_uint64),
     ]
 
 

@@ -151,6 +151,11 @@ class Context:
         """BVH node layout (2 or 4 children) of extension and shadow rays."""
         self.check(self.lib.pt_set_node_width(self.ptr, extension, shadow))
 
+    def fail_allocations(self, count: int) -> None:
+        """pt_debug_fail_allocations: the next `count` device allocations of
+        the context fail with PT_ERR_OOM (host-side injection, no CUDA call)."""
+        self.check(self.lib.pt_debug_fail_allocations(self.ptr, int(count)))
+
     def set_stage_timing(self, on: bool) -> None:
         self.check(self.lib.pt_set_stage_timing(self.ptr, 1 if on else 0))
 

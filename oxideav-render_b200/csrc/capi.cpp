@@ -43,6 +43,22 @@ pt_status fail(pt_context *ctx, pt_status st, const std::string &msg) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                           \
   } while (0)
 
+// Consumes one injected allocation failure of `ctx`, if armed.
+bool injected_oom(pt_context *ctx) {
+  if (!ctx) return false;
+  uint32_t n = ctx->fail_allocs.load();
+  while (n > 0)
+    if (ctx->fail_allocs.compare_exchange_weak(n, n - 1)) return true;
+  return false;
+}
+
+// cudaMalloc, or the injected out-of-memory failure.
+template <class T>
+cudaError_t dev_malloc(pt_context *ctx, T **p, size_t bytes) {
+  if (injected_oom(ctx)) return cudaErrorMemoryAllocation;
+  return cudaMalloc(p, bytes);
+}
+
 template <class F>
 pt_status guard(pt_context *ctx, F &&f) {
   try {
@@ -62,7 +78,7 @@ pt_status ensure(pt_context *ctx, T *&p, size_t &cap, size_t need) {
   if (p) cudaFree(p);
   p = nullptr;
   cap = 0;
-  CK(ctx, cudaMalloc(&p, std::max<size_t>(need, 1) * sizeof(T)));
+  CK(ctx, dev_malloc(ctx, &p, std::max<size_t>(need, 1) * sizeof(T)));
   cap = need;
   return PT_OK;
 }
@@ -224,7 +240,7 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
     off[i] = total;
     total += sizes[i];
   }
-  CK(ctx, cudaMalloc(&arena, total));
+  CK(ctx, dev_malloc(ctx, &arena, total));
   arena_bytes = total;
   char *b = static_cast<char *>(arena);
   int k = 0;
@@ -585,7 +601,7 @@ pt_status read_impl(pt_tracer *t, void *out, size_t count, bool image) {
     if (t->d_resolve) cudaFree(t->d_resolve);
     t->d_resolve = nullptr;
     t->resolve_cap = 0;
-    CK(ctx, cudaMalloc(&t->d_resolve, n * elem));
+    CK(ctx, dev_malloc(ctx, &t->d_resolve, n * elem));
     t->resolve_cap = n * elem;
   }
   if (image) {
@@ -792,6 +808,7 @@ pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *
   return guard(ctx, [&]() -> pt_status {
     CK(ctx, cudaSetDevice(ctx->device));
     auto sc = std::make_unique<SceneHost>();
+    if (injected_oom(ctx)) return fail(ctx, PT_ERR_OOM, "scene upload: device allocation failed (injected)");
     bool oom = false;
     std::string err = upload_scene(*desc, *sc, oom, ctx->bvh_builder, ctx->stream, &ctx->staging);
     if (!err.empty()) return fail(ctx, oom ? PT_ERR_OOM : PT_ERR_INVALID_ARG, err);
@@ -889,7 +906,7 @@ pt_status pt_tracer_create(pt_context *ctx, pt_tracer **out) {
     auto t = std::make_unique<pt_tracer>();
     t->ctx = ctx;
     CK(ctx, cudaSetDevice(ctx->device));
-    CK(ctx, cudaMalloc(&t->d_req, sizeof(DevRequest)));
+    CK(ctx, dev_malloc(ctx, &t->d_req, sizeof(DevRequest)));
     *out = t.release();
     return PT_OK;
   });
@@ -1222,6 +1239,12 @@ pt_status pt_tune_lookup(pt_context *ctx, const pt_tracer *t, pt_tune_choice *ou
 pt_status pt_tune_reset(pt_context *ctx) {
   if (!ctx) return fail(ctx, PT_ERR_INVALID_ARG, "context is NULL");
   ctx->tuned.clear();
+  return PT_OK;
+}
+
+pt_status pt_debug_fail_allocations(pt_context *ctx, uint32_t count) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  ctx->fail_allocs.store(count);
   return PT_OK;
 }
 

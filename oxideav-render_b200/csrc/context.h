@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <map>
 #include <memory>
 #include <string>
@@ -80,6 +81,9 @@ struct pt_context {
   bool overlap_fixed = false;   // the count was set explicitly: tuned choices keep it
   cudaStream_t wave_streams[kMaxArenas] = {};
   cudaEvent_t ev_ready = nullptr, ev_traced[kMaxArenas] = {}, ev_accumulated[kMaxArenas] = {};
+  // Host-side fault injection (pt_debug_fail_allocations): this many of the
+  // next device allocations fail as out of memory without calling CUDA.
+  std::atomic<uint32_t> fail_allocs{0};
 };
 
 // The object behind pt_tracer: one progressive accumulation (the

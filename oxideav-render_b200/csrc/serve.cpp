@@ -7,8 +7,10 @@
 //      request's scene resident (evicting least-recently-used scenes that no
 //      admitted request needs, within the HBM budget), allocate and clear its
 //      accumulator, build its refine job;
-//   2. pack one wave from every admitted request, shortest remaining work
-//      first (ptd::pack_wave), upload the wave's request table and segments
+//   2. pack one wave from every admitted request, earliest expected finish
+//      first (submit time + remaining samples at the measured throughput:
+//      short requests overtake long ones only by about their own length, so
+//      nothing starves), upload the wave's request table and segments
 //      from pinned staging, launch it; requests whose last samples are in the
 //      wave get a resolve kernel + a copy of the HDR image into pinned host
 //      memory behind it, on the same stream;
@@ -18,6 +20,7 @@
 // request, first sample, sample count), and waves keep every pixel's samples
 // in index order, so images do not depend on the mix.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -98,6 +101,12 @@ struct Request {
   uint32_t w = 0, h = 0;
   float *hdr = nullptr;               // pinned host image, w * h * 4 floats
   size_t hdr_bytes = 0;
+  bool has_deadline = false;
+  Clock::time_point deadline;
+  // Cancelled (or timed out) while its last wave was on the GPU: it ends
+  // with this status when that wave completes.
+  pt_status end_status = PT_OK;
+  std::string end_msg;
 };
 
 // Pinned host buffers, recycled by power-of-two size class.
@@ -187,6 +196,10 @@ struct pt_server {
   bool overlap = false;
   cudaStream_t upload = nullptr;
   cudaEvent_t ev_free = nullptr;
+  // Packing key: expected samples per ms of the served waves (measured; the
+  // first waves use a nominal 100 M samples/s).
+  double samples_per_ms = 1e5;
+  std::atomic<uint32_t> fail_allocs{0};  // host-side allocation-failure injection
 };
 
 namespace {
@@ -216,6 +229,14 @@ void evict(pt_server *s, SceneEntry &e) {
 }
 
 enum class Admit { Yes, Wait, Failed };
+
+// Consumes one injected allocation failure, if armed.
+bool injected_oom(pt_server *s) {
+  uint32_t n = s->fail_allocs.load();
+  while (n > 0)
+    if (s->fail_allocs.compare_exchange_weak(n, n - 1)) return true;
+  return false;
+}
 
 void fail_request(pt_server *s, const std::shared_ptr<Request> &r, pt_status st, const std::string &msg) {
   r->state = RState::Failed;
@@ -248,6 +269,10 @@ Admit make_resident(pt_server *s, const std::shared_ptr<SceneEntry> &e, std::uni
       }
       evict(s, *victim);
     }
+  }
+  if (injected_oom(s)) {
+    err = "scene " + std::to_string(e->key) + ": device allocation failed (injected)";
+    return Admit::Failed;
   }
   cudaStream_t stream = s->overlap ? s->upload : s->eng->stream;
   e->pins++;  // keeps it from eviction / unregistration while unlocked
@@ -317,6 +342,8 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
   }
   std::string err;
   Admit a = make_resident(s, sc, lk, err);
+  // Cancelled or timed out while the lock was dropped: already ended.
+  if (r->state != RState::Pending) return Admit::Failed;
   if (a == Admit::Wait) return a;
   if (a == Admit::Failed) {
     fail_admission(s, r, PT_ERR_OOM, err);
@@ -342,6 +369,11 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
     // No wave is in flight while a class tunes: the wave streams may wait
     // for the engine stream here without serialising anything.
     if (s->overlap) engine_overlap_begin(s->eng);
+    if (r->state != RState::Pending) {
+      // Ended while tuning; the class is tuned all the same.
+      if (tst == PT_OK) s->st.tuned_classes++;
+      return Admit::Failed;
+    }
     if (tst != PT_OK) {
       fail_admission(s, r, tst, "autotune: " + s->eng->err);
       return Admit::Failed;
@@ -352,7 +384,7 @@ Admit try_admit(pt_server *s, const std::shared_ptr<Request> &r, std::unique_loc
   pt_tracer &t = acc.t;
   if (!t.d_accum) {
     size_t bytes = (size_t)t.w * t.h * 4 * sizeof(double);
-    cudaError_t e = cudaMallocAsync((void **)&t.d_accum, bytes, stream);
+    cudaError_t e = injected_oom(s) ? cudaErrorMemoryAllocation : cudaMallocAsync((void **)&t.d_accum, bytes, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(t.d_accum, 0, bytes, stream);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -388,10 +420,14 @@ void admit(pt_server *s, std::unique_lock<std::mutex> &lk) {
   for (size_t i = 0; i < s->pending.size() && s->active.size() < s->max_active;) {
     std::shared_ptr<Request> r = s->pending[i];
     Admit a = try_admit(s, r, lk);
-    if (a == Admit::Wait)
-      ++i;
-    else
-      s->pending.erase(s->pending.begin() + (ptrdiff_t)i);
+    // try_admit may drop the lock: a cancel can have changed the queue.
+    auto it = std::find(s->pending.begin(), s->pending.end(), r);
+    if (a == Admit::Wait) {
+      i = it == s->pending.end() ? i : (size_t)(it - s->pending.begin()) + 1;
+    } else if (it != s->pending.end()) {
+      i = (size_t)(it - s->pending.begin());
+      s->pending.erase(it);
+    }
   }
 }
 
@@ -428,11 +464,17 @@ void launch_next_wave(pt_server *s) {
   for (size_t i = 0; i < n; ++i) jobs[i] = s->active[i]->job;
   std::vector<uint32_t> order(n);
   std::iota(order.begin(), order.end(), 0u);
-  auto remaining = [&](uint32_t i) {
+  // Earliest expected finish first: submit time (ms since the oldest active
+  // request's) + remaining samples / measured throughput.
+  Clock::time_point t0 = s->active[0]->t_submit;
+  for (size_t i = 1; i < n; ++i) t0 = std::min(t0, s->active[i]->t_submit);
+  std::vector<double> key(n);
+  for (size_t i = 0; i < n; ++i) {
     const Job &j = jobs[i];
-    return (uint64_t)j.npix * (j.target - j.done) - j.pix_done;
-  };
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return remaining(a) < remaining(b); });
+    const double remaining = (double)j.npix * (j.target - j.done) - j.pix_done;
+    key[i] = ms_between(t0, s->active[i]->t_submit) + remaining / s->samples_per_ms;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
   std::vector<WaveSegment> segs = pack_wave(jobs, order, s->wave_slots);
   // Compact request table: only the jobs this wave carries.
   std::vector<int> remap(n, -1);
@@ -553,6 +595,10 @@ void complete_flight(pt_server *s, size_t fi, cudaError_t e) {
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, f.ev_start, f.ev_end);
   s->st.gpu_ms += ms;
+  if (ms > 0.0f && f.samples >= (1u << 20)) {
+    // Throughput of full-ish waves steers the packing key (smoothed).
+    s->samples_per_ms = 0.8 * s->samples_per_ms + 0.2 * ((double)f.samples / ms);
+  }
   s->st.waves++;
   s->st.samples += f.samples;
   s->st.rays = s->rays_base + f.h_ctr->ext_rays + f.h_ctr->shadow_rays;
@@ -561,6 +607,10 @@ void complete_flight(pt_server *s, size_t fi, cudaError_t e) {
   for (auto &r : f.finishing) {
     if (overflow) {
       fail_request(s, r, PT_ERR_DEVICE, "BVH traversal stack overflow");
+      continue;
+    }
+    if (r->end_status != PT_OK) {
+      fail_request(s, r, r->end_status, r->end_msg);
       continue;
     }
     r->state = RState::Done;
@@ -584,11 +634,70 @@ void free_dead(pt_server *s) {
   s->dead_scenes.clear();
 }
 
+// Ends request `r` with `st` (PT_ERR_CANCELLED or PT_ERR_TIMEOUT). Called
+// with the lock held. A queued request leaves the queue. An admitted one
+// gets no further waves: its waves on the GPU still add to its accumulator,
+// which is left inconsistent, so the accumulation fails for continuations;
+// stream-ordered frees keep its memory alive until those waves are done. A
+// request whose last wave was launched ends when that wave completes.
+pt_status end_request(pt_server *s, const std::shared_ptr<Request> &r, pt_status st, const std::string &msg) {
+  if (r->state == RState::Done || r->state == RState::Failed)
+    return sfail(PT_ERR_INVALID_ARG, "request " + std::to_string(r->ticket) + " has already finished");
+  (st == PT_ERR_CANCELLED ? s->st.cancelled : s->st.timed_out)++;
+  if (r->state == RState::Pending) {
+    auto it = std::find(s->pending.begin(), s->pending.end(), r);
+    if (it != s->pending.end()) s->pending.erase(it);
+    if (!r->in.continues) {
+      fail_admission(s, r, st, msg);
+    } else {
+      fail_request(s, r, st, msg);
+    }
+  } else {
+    auto it = std::find(s->active.begin(), s->active.end(), r);
+    if (it != s->active.end()) {
+      s->active.erase(it);
+      Accum &acc = *r->acc;
+      acc.busy = false;
+      acc.failed = true;
+      acc.fail_status = st;
+      acc.fail_msg = msg + " with samples still to add";
+      acc.scene->pins--;
+      fail_request(s, r, st, msg);
+    } else {
+      r->end_status = st;  // its last wave is on the GPU
+      r->end_msg = msg;
+    }
+  }
+  s->cv_work.notify_all();
+  return PT_OK;
+}
+
+// Ends every queued or admitted request whose deadline has passed, and
+// returns the nearest deadline still ahead (or `far`).
+Clock::time_point expire_deadlines(pt_server *s, Clock::time_point far) {
+  const Clock::time_point now = Clock::now();
+  Clock::time_point next = far;
+  std::vector<std::shared_ptr<Request>> due;
+  auto check = [&](const std::shared_ptr<Request> &r) {
+    if (!r->has_deadline || r->end_status != PT_OK) return;
+    if (r->deadline <= now)
+      due.push_back(r);
+    else
+      next = std::min(next, r->deadline);
+  };
+  for (auto &r : s->pending) check(r);
+  for (auto &r : s->active) check(r);
+  for (auto &r : due) end_request(s, r, PT_ERR_TIMEOUT, "deadline of " + std::to_string(r->in.deadline_ms) + " ms passed");
+  return next;
+}
+
 void worker_main(pt_server *s) {
   cudaSetDevice(s->eng->device);
   std::unique_lock<std::mutex> lk(s->mu);
+  const Clock::time_point far = Clock::time_point::max();
   for (;;) {
     free_dead(s);
+    const Clock::time_point next_deadline = expire_deadlines(s, far);
     if (!s->stop && !s->broken) admit(s, lk);
     if (!s->stop && !s->broken && !s->tune_pending && !s->active.empty() && s->inflight.size() < s->depth) {
       launch_next_wave(s);
@@ -604,7 +713,10 @@ void worker_main(pt_server *s) {
       continue;
     }
     if (s->stop) break;
-    s->cv_work.wait(lk);
+    if (next_deadline == far)
+      s->cv_work.wait(lk);
+    else
+      s->cv_work.wait_until(lk, next_deadline);
   }
   for (auto &r : s->active) fail_request(s, r, PT_ERR_CANCELLED, "server stopped");
   s->active.clear();
@@ -818,6 +930,10 @@ pt_status pt_server_submit(pt_server *s, const pt_server_request *in, uint64_t *
     r->h = r->acc->t.h;
     r->ticket = s->next_ticket++;
     r->t_submit = Clock::now();
+    if (in->deadline_ms) {
+      r->has_deadline = true;
+      r->deadline = r->t_submit + std::chrono::milliseconds(in->deadline_ms);
+    }
     s->reqs[r->ticket] = r;
     s->pending.push_back(r);
     s->st.submitted++;
@@ -838,7 +954,8 @@ pt_status pt_server_wait(pt_server *s, uint64_t ticket, int32_t timeout_ms, floa
   if (timeout_ms < 0)
     s->cv_done.wait(lk, ready);
   else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
-    return sfail(PT_ERR_NOT_READY, "request still running");
+    return sfail(timeout_ms == 0 ? PT_ERR_NOT_READY : PT_ERR_TIMEOUT,
+                 "request " + std::to_string(ticket) + " still running");
   if (r->state == RState::Failed) return sfail(r->status, r->error);
   const size_t nf = (size_t)r->w * r->h * 4;
   if (hdr) {
@@ -853,6 +970,26 @@ pt_status pt_server_wait(pt_server *s, uint64_t ticket, int32_t timeout_ms, floa
     stats->samples = r->samples_after;
     stats->waves = r->waves;
   }
+  return PT_OK;
+}
+
+pt_status pt_server_poll(pt_server *s, uint64_t ticket, float *hdr, size_t hdr_floats, pt_request_stats *stats) {
+  return pt_server_wait(s, ticket, 0, hdr, hdr_floats, stats);
+}
+
+pt_status pt_server_cancel(pt_server *s, uint64_t ticket) {
+  if (!s) return sfail(PT_ERR_INVALID_ARG, "server is NULL");
+  return sguard([&]() -> pt_status {
+    std::lock_guard<std::mutex> g(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return sfail(PT_ERR_NOT_FOUND, "ticket " + std::to_string(ticket) + " is unknown");
+    return end_request(s, it->second, PT_ERR_CANCELLED, "request " + std::to_string(ticket) + " was cancelled");
+  });
+}
+
+pt_status pt_server_debug_fail_allocations(pt_server *s, uint32_t count) {
+  if (!s) return sfail(PT_ERR_INVALID_ARG, "server is NULL");
+  s->fail_allocs.store(count);
   return PT_OK;
 }
 

@@ -74,6 +74,9 @@ SIGNATURES = {
     "pt_server_scene_info": (i32, [vp, u32, u64p, C.POINTER(C.c_int)]),
     "pt_server_submit": (i32, [vp, C.POINTER(abi.pt_server_request), u64p]),
     "pt_server_wait": (i32, [vp, u64, i32, fp, C.c_size_t, C.POINTER(abi.pt_request_stats)]),
+    "pt_server_poll": (i32, [vp, u64, fp, C.c_size_t, C.POINTER(abi.pt_request_stats)]),
+    "pt_server_cancel": (i32, [vp, u64]),
+    "pt_server_debug_fail_allocations": (i32, [vp, u32]),
     "pt_server_release": (i32, [vp, u64]),
     "pt_server_stats_get": (i32, [vp, C.POINTER(abi.pt_server_stats)]),
     # include/pt_b200_debug.h
@@ -97,6 +100,7 @@ SIGNATURES = {
     "pt_set_shade_blocks": (i32, [vp, u32]),
     "pt_set_wave_overlap": (i32, [vp, i32]),
     "pt_set_wave_graphs": (i32, [vp, i32]),
+    "pt_debug_fail_allocations": (i32, [vp, u32]),
     "pt_debug_prepare_scene": (i32, [C.POINTER(abi.pt_scene_desc), dp, u64p]),
     "pt_autotune": (i32, [vp, vp, u32, C.POINTER(abi.pt_tune_choice)]),
     "pt_tune_lookup": (i32, [vp, vp, C.POINTER(abi.pt_tune_choice)]),

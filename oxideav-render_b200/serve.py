@@ -73,41 +73,75 @@ class RenderServer:
         self._check(self.lib.pt_server_scene_info(self.ptr, key, C.byref(b), C.byref(r)))
         return {"device_bytes": b.value, "resident": bool(r.value)}
 
-    def submit(self, key: int, opts: RenderOptions, samples: Optional[int] = None) -> int:
-        """A new accumulation of `samples` (default: opts' samples_per_pixel)."""
+    def submit(self, key: int, opts: RenderOptions, samples: Optional[int] = None, deadline_ms: int = 0) -> int:
+        """A new accumulation of `samples` (default: opts' samples_per_pixel).
+        With `deadline_ms` > 0 the request fails with PT_ERR_TIMEOUT when it
+        has not finished that many ms after this call."""
         scene = self._scenes[key]
         w, h = max(opts.width, 1), max(opts.height, 1)
         cam = Camera.resolve(scene, opts, w, h)
         n = opts.path_trace.samples_per_pixel if samples is None else samples
-        req = abi.pt_server_request(key, int(n), 0, cam.to_c(), opts.to_c())
+        req = abi.pt_server_request(key, int(n), 0, cam.to_c(), opts.to_c(), int(deadline_ms))
         t = C.c_uint64()
         self._check(self.lib.pt_server_submit(self.ptr, C.byref(req), C.byref(t)))
         self._tickets[t.value] = (h, w)
         return t.value
 
-    def submit_continuation(self, ticket: int, samples: int) -> int:
+    def submit_continuation(self, ticket: int, samples: int, deadline_ms: int = 0) -> int:
         """`samples` more on the accumulator of `ticket` (PathTracer::refine)."""
         req = abi.pt_server_request()
         req.samples = int(samples)
         req.continues = int(ticket)
+        req.deadline_ms = int(deadline_ms)
         t = C.c_uint64()
         self._check(self.lib.pt_server_submit(self.ptr, C.byref(req), C.byref(t)))
         self._tickets[t.value] = self._tickets[ticket]
         return t.value
 
+    @staticmethod
+    def _stats(st: abi.pt_request_stats) -> dict:
+        return {"queue_ms": st.queue_ms, "latency_ms": st.latency_ms, "width": st.width, "height": st.height,
+                "samples": st.samples, "waves": st.waves}
+
     def wait(self, ticket: int, timeout_ms: int = -1):
         """(hdr (h, w, 4) float32, stats dict) once the request finished;
-        None when it is still running at the timeout."""
+        None when it is still running when `timeout_ms` (>= 0) runs out.
+        Raises RenderError with the request's own failure (cancelled, its
+        deadline passed, out of memory, ...)."""
         h, w = self._tickets[ticket]
         out = np.empty((h, w, 4), np.float32)
         st = abi.pt_request_stats()
         rc = self.lib.pt_server_wait(self.ptr, ticket, int(timeout_ms), out.ctypes.data_as(native.fp), out.size,
                                      C.byref(st))
+        if rc == abi.PT_ERR_NOT_READY or (rc == abi.PT_ERR_TIMEOUT and timeout_ms >= 0 and self.poll_status(ticket)
+                                          == abi.PT_ERR_NOT_READY):
+            return None
+        self._check(rc)
+        return out, self._stats(st)
+
+    def poll_status(self, ticket: int) -> int:
+        """pt_server_poll's status: PT_ERR_NOT_READY while queued or running."""
+        return self.lib.pt_server_poll(self.ptr, ticket, None, 0, None)
+
+    def poll(self, ticket: int):
+        """wait() without blocking: None while the request is queued or running."""
+        h, w = self._tickets[ticket]
+        out = np.empty((h, w, 4), np.float32)
+        st = abi.pt_request_stats()
+        rc = self.lib.pt_server_poll(self.ptr, ticket, out.ctypes.data_as(native.fp), out.size, C.byref(st))
         if rc == abi.PT_ERR_NOT_READY:
             return None
         self._check(rc)
-        return out, {"queue_ms": st.queue_ms, "latency_ms": st.latency_ms, "width": st.width, "height": st.height,
-                     "samples": st.samples, "waves": st.waves}
+        return out, self._stats(st)
+
+    def cancel(self, ticket: int) -> None:
+        """pt_server_cancel: the request ends with PT_ERR_CANCELLED."""
+        self._check(self.lib.pt_server_cancel(self.ptr, ticket))
+
+    def fail_allocations(self, count: int) -> None:
+        """pt_server_debug_fail_allocations: the next `count` device
+        allocations of the server fail as out of memory (host-side injection)."""
+        self._check(self.lib.pt_server_debug_fail_allocations(self.ptr, int(count)))
 
     def release(self, ticket: int) -> None:
         self._check(self.lib.pt_server_release(self.ptr, ticket))

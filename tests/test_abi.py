@@ -52,7 +52,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), n
         assert n in native.SIGNATURES, f"{n} has no ctypes signature"
-    assert lib.pt_abi_version() == 1
+    assert lib.pt_abi_version() == 2
 
 
 def test_create_without_a_device_fails_cleanly():

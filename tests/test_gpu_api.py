@@ -258,3 +258,38 @@ def test_a_fresh_context_runs_the_wavefront_by_default():
         t.close()
     finally:
         mk.close()
+
+
+def test_injected_allocation_failure_leaves_the_context_usable():
+    # pt_debug_fail_allocations: host-side, no CUDA call fails. The sync
+    # that needed an accumulator returns PT_ERR_OOM; the next one works and
+    # renders what a fresh context renders.
+    scene, opts = ts.cornell_c0()
+    o = opts.replace(width=40, height=24, path_trace=PathTraceOptions(samples_per_pixel=4, max_bounces=4))
+    c = api.Context(0)
+    try:
+        t = api.PathTracer(c)
+        c.fail_allocations(1)
+        with pytest.raises(api.RenderError) as ei:
+            t.sync(scene, o)
+        assert ei.value.status == abi.PT_ERR_OOM
+        t.invalidate_scene()
+        t.sync(scene, o)
+        t.refine(4)
+        got = t.accum()
+        t.close()
+        c.fail_allocations(1)  # a scene upload
+        with pytest.raises(api.RenderError) as ei:
+            c.upload(scene.to_desc(o))
+        assert ei.value.status == abi.PT_ERR_OOM
+    finally:
+        c.close()
+    fresh = api.Context(0)
+    try:
+        want = api.PathTracer(fresh)
+        want.sync(scene, o)
+        want.refine(4)
+        assert np.array_equal(got, want.accum())
+        want.close()
+    finally:
+        fresh.close()

@@ -209,3 +209,141 @@ def test_destroy_with_queued_requests(ctx):
     for _ in range(4):
         srv.submit(key, opts)
     srv.close()
+
+
+def _plain_hdr(ctx, scene, opts, spp=None):
+    t = api.PathTracer(ctx)
+    t.sync(scene, opts)
+    t.refine(opts.path_trace.samples_per_pixel if spp is None else spp)
+    out = t.hdr()
+    t.close()
+    return out
+
+
+def _status_of(srv, ticket):
+    with pytest.raises(api.RenderError) as ei:
+        srv.wait(ticket)
+    return ei.value.status
+
+
+def test_cancel_a_queued_request(ctx):
+    # One request at a time: the second one waits in the queue behind a long
+    # first one and is cancelled there; its continuation fails with it; the
+    # long one and a later request still equal the plain path.
+    soup = ts.random_soup(20000, seed=3)
+    big = ts.pt_opts(256, 64, 4)
+    small = ts.pt_opts(32, 2, 3)
+    srv = RenderServer(ctx, max_active=1, wave_slots=1 << 16)
+    try:
+        k = srv.register(soup, big)
+        a = srv.submit(k, big)
+        b = srv.submit(k, small)
+        c = srv.submit_continuation(b, 2)
+        srv.cancel(b)
+        assert _status_of(srv, b) == abi.PT_ERR_CANCELLED
+        assert _status_of(srv, c) in (abi.PT_ERR_CANCELLED, abi.PT_ERR_INVALID_ARG)
+        img, _ = srv.wait(a)
+        assert np.array_equal(img, _plain_hdr(ctx, soup, big))
+        d = srv.submit(k, small)
+        assert np.array_equal(srv.wait(d)[0], _plain_hdr(ctx, soup, small))
+        s = srv.stats()
+        assert s["cancelled"] == 1 and s["failed"] >= 2 and s["completed"] == 2
+        for t in (a, b, c, d):
+            srv.release(t)
+        with pytest.raises(api.RenderError) as ei:
+            srv.cancel(a)
+        assert ei.value.status == abi.PT_ERR_NOT_FOUND
+    finally:
+        srv.close()
+
+
+def test_cancel_a_running_request(ctx):
+    # Small waves make the request span hundreds of waves; it is cancelled
+    # while they run. Its accumulation can no longer be continued; the
+    # server goes on serving.
+    soup = ts.random_soup(20000, seed=3)
+    big = ts.pt_opts(256, 256, 4)
+    small = ts.pt_opts(32, 2, 3)
+    srv = RenderServer(ctx, wave_slots=1 << 14)
+    try:
+        k = srv.register(soup, big)
+        a = srv.submit(k, big)
+        for _ in range(2000):
+            if srv.stats()["waves"] >= 2:
+                break
+            time.sleep(0.001)
+        assert srv.poll(a) is None  # still running
+        srv.cancel(a)
+        assert _status_of(srv, a) == abi.PT_ERR_CANCELLED
+        with pytest.raises(api.RenderError):
+            srv.submit_continuation(a, 1)
+        with pytest.raises(api.RenderError) as ei:
+            srv.cancel(a)
+        assert ei.value.status == abi.PT_ERR_INVALID_ARG  # already finished
+        e = srv.submit(k, small)
+        assert np.array_equal(srv.wait(e)[0], _plain_hdr(ctx, soup, small))
+        srv.release(a)
+        srv.release(e)
+        assert srv.stats()["cancelled"] == 1
+    finally:
+        srv.close()
+
+
+def test_poll_bounded_wait_and_deadline(ctx):
+    soup = ts.random_soup(20000, seed=3)
+    big = ts.pt_opts(256, 64, 4)
+    small = ts.pt_opts(32, 2, 3)
+    srv = RenderServer(ctx, max_active=1, wave_slots=1 << 16)
+    try:
+        k = srv.register(soup, big)
+        a = srv.submit(k, big)
+        assert srv.poll(a) is None
+        assert srv.poll_status(a) == abi.PT_ERR_NOT_READY
+        assert srv.wait(a, timeout_ms=1) is None  # PT_ERR_TIMEOUT from the bounded wait
+        rc = srv.lib.pt_server_wait(srv.ptr, a, 1, None, 0, None)
+        assert rc in (abi.PT_ERR_TIMEOUT, abi.PT_OK)
+        # Queued behind `a` with a 1 ms deadline: it times out.
+        b = srv.submit(k, small, deadline_ms=1)
+        assert _status_of(srv, b) == abi.PT_ERR_TIMEOUT
+        img, _ = srv.wait(a)
+        assert np.array_equal(img, _plain_hdr(ctx, soup, big))
+        got = srv.poll(a)
+        assert got is not None and np.array_equal(got[0], img)
+        # A generous deadline does not fire.
+        c = srv.submit(k, small, deadline_ms=600000)
+        assert np.array_equal(srv.wait(c)[0], _plain_hdr(ctx, soup, small))
+        s = srv.stats()
+        assert s["timed_out"] == 1 and s["completed"] == 2
+        for t in (a, b, c):
+            srv.release(t)
+    finally:
+        srv.close()
+
+
+def test_injected_allocation_failures_surface_as_oom(ctx):
+    # Host-side injection: no CUDA call fails, the server's allocation
+    # points report out of memory. The failed requests end with PT_ERR_OOM
+    # and the server keeps serving.
+    scene, opts = ts.cornell_c0()
+    small = opts.replace(width=24, height=16, path_trace=PathTraceOptions(samples_per_pixel=3, max_bounces=4))
+    want = _plain_hdr(ctx, scene, small)
+    srv = RenderServer(ctx)
+    try:
+        k = srv.register(scene, small)
+        srv.fail_allocations(1)  # the scene's first device commit
+        a = srv.submit(k, small)
+        assert _status_of(srv, a) == abi.PT_ERR_OOM
+        assert not srv.scene_info(k)["resident"]
+        b = srv.submit(k, small)
+        assert np.array_equal(srv.wait(b)[0], want)
+        srv.fail_allocations(1)  # the next request's accumulator
+        c = srv.submit(k, small)
+        assert _status_of(srv, c) == abi.PT_ERR_OOM
+        d = srv.submit(k, small)
+        assert np.array_equal(srv.wait(d)[0], want)
+        s = srv.stats()
+        assert s["failed"] == 2 and s["completed"] == 2
+        for t in (a, b, c, d):
+            srv.release(t)
+    finally:
+        srv.close()
