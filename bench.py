@@ -1,23 +1,34 @@
-"""Benchmark: samples/s of the path-tracing hot path on one B200 (or N, weak scaling).
+"""Benchmark of the path-tracing hot path on one B200 (or N, weak scaling):
+the served / batched form against the plain per-request GPU path.
 
-Workload (default): the metallic x roughness sphere grid — 7x7 UV spheres of
-64x32 segments (200,706 triangles with the floor), a 512^2 sRGB checker floor
-texture with trilinear mips, one directional and one point light, sky 0.3;
-512x512 pixels, 256 samples per pixel, 8 bounces. One step = one frame:
-`PathTracer.refine(256)` on the resident scene (67,108,864 camera paths).
+Headline workload (config 3): a mix of 64 render requests, each drawing its
+scene uniformly from {Cornell box C0, sphere grid C1, the ~4.1M-triangle
+stress scene C2 with environment map and emitters, 8 random soups of
+10k-500k triangles}, its resolution from {128^2, 256^2, 512^2, 1024x768},
+its spp from {1, 4, 16, 64} and its bounce limit from {2, 4, 8}. One step =
+every request's samples (about 310 M camera paths).
 
 Reported (one JSON line from rank 0):
-  value      samples/s over all ranks, device time (CUDA events on the
-             library's stream around the path-tracing kernels), max over ranks;
-  e2e        the same metric through `PathTraceCudaRenderer.render` (scene
-             upload with the host BVH build, refine, image readback), wall time;
-  roofline   the path kernel's algorithmic bytes (per-ray / per-vertex byte
-             model of the design notes, from device counters) / kernel time,
-             against the measured HBM copy bandwidth;
-  cpu_baseline  the CPU restatement of the reference (oracle) on this host's
-             cores on a bounded sample of the same frame.
-`--impl reference` times that CPU restatement alone (the Rust reference has no
-toolchain here) on the same workload and prints the same metric.
+  value       samples/s of the batched form: pt_tracer_refine_many over one
+              tracer per request, scenes resident, device time of the waves
+              (CUDA events on the library's stream), max over ranks;
+  e2e         the same requests through the serving C ABI (pt_server_submit
+              / pt_server_wait on a warm server), host request descriptors in,
+              HDR images back to host memory, wall clock;
+  vs_plain    the plain per-request GPU path on the SAME requests:
+              PathTraceCudaRenderer.render_hdr per request (scene prepared and
+              uploaded per call) and refine + hdr on an uploaded scene, with
+              p50 / p99 latencies and the speed-ups;
+  served_poisson  config 4: Poisson arrivals (5 and 200 requests/s over a 60 s
+              window, 20 % +16 spp continuations) against 32 resident scenes
+              under a 60 GB budget; p50 / p99 latency, samples/s, and the plain
+              path on the same requests replayed under the same arrivals;
+  roofline    the dominant kernel's algorithmic bytes (byte model from device
+              counters) / its device time, against the measured HBM bandwidth;
+  plain_frame the single C1 frame (512^2, 256 spp) as a secondary figure;
+  cpu_baseline  the oracle (CPU restatement of the reference) on this host's
+              cores over one row of every request of the mix.
+`--impl reference` times that CPU restatement alone on the same request mix.
 """
 from __future__ import annotations
 
@@ -146,11 +157,12 @@ def mixed_scene(k: int, stress_grid: int = 1024, stress_spheres: int = 500):
     return v
 
 
-def mixed_requests(n: int, seed: int):
+def mixed_requests(n: int, seed: int, seed_base: int = 0):
     """The batched workload: `n` requests, each drawing its scene uniformly
     from {Cornell box, sphere grid, stress scene, 8 random soups of
     10k-500k triangles}, its resolution from {128^2, 256^2, 512^2, 1024x768},
-    its spp from {1, 4, 16, 64} and its bounce limit from {2, 4, 8}."""
+    its spp from {1, 4, 16, 64} and its bounce limit from {2, 4, 8}.
+    Request i renders with sample seed `seed_base + i`."""
     from oxideav_render_b200.options import PathTraceOptions
     rng = np.random.default_rng(seed)
     res = [(128, 128), (256, 256), (512, 512), (1024, 768)]
@@ -162,16 +174,24 @@ def mixed_requests(n: int, seed: int):
         b = [2, 4, 8][int(rng.integers(0, 3))]
         s, o, env = mixed_scene(k)
         opts = o.replace(width=w, height=h, path_trace=PathTraceOptions(samples_per_pixel=spp, max_bounces=b,
-                                                                        seed=i))
+                                                                        seed=seed_base + i))
         out.append((k, s, opts, env))
     return out
 
 
-def run_mixed(ctx, api, torch, n_requests: int, seed: int, check: int = 8):
-    """Plain per-request GPU path (each request synced, refined and read back
-    alone, one after another) against the batched path (all requests in one
-    pt_tracer_refine_many call, then read back). Returns the comparison."""
-    reqs = mixed_requests(n_requests, seed)
+def request_samples(o) -> int:
+    return o.width * o.height * o.path_trace.samples_per_pixel
+
+
+def percentiles(lat_ms):
+    return {"p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+            "max_ms": float(np.max(lat_ms))}
+
+
+def run_batched(ctx, api, torch, reqs, args, ws, flush):
+    """Headline: the request mix refined in shared waves (pt_tracer_refine_many
+    over one tracer per request, scenes resident). One step = every request's
+    samples; device time of the waves (CUDA events on the library's stream)."""
     tracers = []
     for k, s, o, env in reqs:
         t = api.PathTracer(ctx)
@@ -179,36 +199,127 @@ def run_mixed(ctx, api, torch, n_requests: int, seed: int, check: int = 8):
             t.set_environment(api.EnvironmentMap(env))
         t.sync(s, o)
         tracers.append(t)
-    total = sum(o.width * o.height * o.path_trace.samples_per_pixel for _, _, o, _ in reqs)
-    # Warm-up (loads modules, allocates wave buffers).
-    api.refine_many(ctx, tracers[:4], [1] * 4)
-    for t in tracers[:4]:
+    spp = [o.path_trace.samples_per_pixel for _, _, o, _ in reqs]
+    total = sum(request_samples(o) for _, _, o, _ in reqs)
+
+    def step():
+        for t in tracers:
+            t.reset()
+        flush.zero_()
+        torch.cuda.synchronize()
+        api.refine_many(ctx, tracers, spp)
+
+    for _ in range(args.warmup):
+        step()
+    barrier(ws)
+    ms, rays, waves = [], 0, 0
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for _ in range(args.steps):
+            step()
+            st = api.batch_stats(ctx)
+            ms.append(st["ms"])
+            rays += st["rays"]
+            waves += st["waves"]
+    barrier(ws)
+    # One more (untimed) batch with CUDA events between the stages: the
+    # stage split and the counters the roofline uses. Stage events need
+    # direct launches on one stream, so this batch runs without overlap.
+    ctx.set_stage_timing(True)
+    step()
+    bc = api.batch_counters(ctx)
+    stage_batch_ms = api.batch_stats(ctx)["ms"]
+    ctx.set_stage_timing(False)
+    return tracers, {"ms": ms, "rays": rays, "waves": waves, "total": total, "counters": bc,
+                     "stage_batch_ms": stage_batch_ms, "clocks": clocks.summary()}
+
+
+def register_scenes(srv, api, scenes):
+    """Registers (scene, opts, env) triples and makes each resident with one
+    tiny request, as a warm server holds them. Returns the keys."""
+    from oxideav_render_b200.options import PathTraceOptions
+    keys = [srv.register(s, o, api.EnvironmentMap(e) if e is not None else None) for s, o, e in scenes]
+    warm = [srv.submit(k, o.replace(width=16, height=16, path_trace=PathTraceOptions(samples_per_pixel=1)))
+            for k, (_, o, _) in zip(keys, scenes)]
+    for t in warm:
+        srv.wait(t)
+        srv.release(t)
+    return keys
+
+
+def run_served_batch(ctx, api, torch, reqs, args, tracers):
+    """End to end through the serving C ABI: the same requests submitted to a
+    warm RenderServer (their 11 scenes resident) all at once, each HDR image
+    copied back to host memory; wall time from the first submit to the last
+    image. Request descriptors go host -> device, HDR images device -> host."""
+    import ctypes as C
+    from oxideav_render_b200 import abi
+    from oxideav_render_b200.serve import RenderServer
+    srv = RenderServer(ctx, wave_overlap=args.wave_overlap, wave_slots=args.serve_wave_slots)
+    try:
+        kinds = sorted({k for k, _, _, _ in reqs})
+        scenes = [mixed_scene(k) for k in kinds]
+        keys = dict(zip(kinds, register_scenes(srv, api, scenes)))
+        total = sum(request_samples(o) for _, _, o, _ in reqs)
+        h2d = len(reqs) * C.sizeof(abi.pt_server_request)
+        d2h = sum(o.width * o.height * 16 for _, _, o, _ in reqs)
+        runs, identical = [], []
+        for rep in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tickets = [srv.submit(keys[k], o) for k, _, o, _ in reqs]
+            lat = []
+            for i, t in enumerate(tickets):
+                img, st = srv.wait(t)
+                lat.append(st["latency_ms"])
+                if rep == 0 and i < args.serve_check:
+                    identical.append(bool(np.array_equal(img, tracers[i].hdr())))
+                srv.release(t)
+            wall = time.perf_counter() - t0
+            if rep > 0:  # the first pass is a warm-up
+                runs.append({"wall_s": wall, **percentiles(lat)})
+        st = srv.stats()
+    finally:
+        srv.close()
+    wall = sum(r["wall_s"] for r in runs) / len(runs)
+    return {"value": total / wall, "unit": "samples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": 1000 * wall, "p50_ms": statistics.mean(r["p50_ms"] for r in runs),
+            "p99_ms": statistics.mean(r["p99_ms"] for r in runs),
+            "call": "pt_server_submit of every request at once to a warm server (scenes resident), "
+                    "pt_server_wait copies each HDR image to host memory; wall clock first submit -> last image",
+            "steps": len(runs), "server_gpu_mrays_per_s": st["rays"] / (st["gpu_ms"] / 1000.0) / 1e6
+            if st["gpu_ms"] > 0 else None,
+            "bit_identical_checked": len(identical), "bit_identical": all(identical) if identical else None}
+
+
+def run_plain_requests(ctx, api, torch, reqs, tracers):
+    """The plain per-request GPU path on the same requests, one after
+    another in request order: PathTraceCudaRenderer.render_hdr per request
+    (PathTraceRenderer::render_hdr: the scene prepared and uploaded per call,
+    refine, HDR read back), and refine + hdr on the request's tracer whose
+    scene is already uploaded. Latencies assume every request arrived at
+    once (first come, first served)."""
+    renderer = api.PathTraceCudaRenderer(ctx)
+    one, res = [], []
+    for (k, s, o, env), t in zip(reqs, tracers):
+        renderer.tracer_mut().set_environment(api.EnvironmentMap(env) if env is not None else None)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        renderer.render_hdr(s, o)
+        one.append(time.perf_counter() - t0)
         t.reset()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for t, (_, _, o, _) in zip(tracers, reqs):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         t.refine(o.path_trace.samples_per_pixel)
         t.hdr()
-    plain_s = time.perf_counter() - t0
-    plain_acc = [tracers[i].accum() for i in range(min(check, len(tracers)))]
-    for t in tracers:
-        t.reset()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    api.refine_many(ctx, tracers, [o.path_trace.samples_per_pixel for _, _, o, _ in reqs])
-    for t in tracers:
-        t.hdr()
-    batched_s = time.perf_counter() - t0
-    st = api.batch_stats(ctx)
-    identical = all(np.array_equal(tracers[i].accum(), plain_acc[i]) for i in range(len(plain_acc)))
-    for t in tracers:
-        t.close()
-    return {"requests": n_requests, "samples": int(total), "plain_s": plain_s, "batched_s": batched_s,
-            "plain_samples_per_s": total / plain_s, "batched_samples_per_s": total / batched_s,
-            "speedup": plain_s / batched_s, "batched_waves": st["waves"],
-            "batched_mrays_per_s": st["rays"] / (st["ms"] / 1000.0) / 1e6 if st["ms"] > 0 else None,
-            "bit_identical_checked": len(plain_acc), "bit_identical": identical,
-            "timing": "wall clock, host submit to HDR readback of every request"}
+        res.append(time.perf_counter() - t0)
+    renderer.tracer.close()
+    total = sum(request_samples(o) for _, _, o, _ in reqs)
+    return {"one_shot": {"samples_per_s": total / sum(one), "wall_s": sum(one),
+                         **percentiles(1000 * np.cumsum(one)),
+                         "call": "PathTraceCudaRenderer.render_hdr per request (scene prepared + uploaded per call)"},
+            "resident": {"samples_per_s": total / sum(res), "wall_s": sum(res),
+                         **percentiles(1000 * np.cumsum(res)),
+                         "call": "PathTracer.refine + hdr per request, its scene already on the device"}}
 
 
 def serving_scenes(n: int, seed: int):
@@ -225,166 +336,134 @@ def serving_scenes(n: int, seed: int):
     return out
 
 
-def run_served(ctx, api, torch, args):
-    """Poisson arrivals of mixed requests against the render server, per
-    arrival rate: p50/p99 latency (submit -> HDR in host memory) and the
-    delivered samples/s; beside it the plain per-request path on a bounded
-    sample of the same requests, timed back to back."""
+def served_spec(n: int, scenes, seed: int):
+    """Config 4's requests: drawn like the batched mix over the resident
+    scenes; 20 % are +16 spp continuations of an earlier request."""
     from oxideav_render_b200.options import PathTraceOptions
+    rng = np.random.default_rng(seed)
+    res = [(128, 128), (256, 256), (512, 512), (1024, 768)]
+    spec = []
+    for i in range(n):
+        if i > 0 and rng.random() < 0.2:
+            j = int(rng.integers(0, i))
+            while spec[j][0] == "cont":
+                j = spec[j][1]
+            spec.append(("cont", j, 16))
+        else:
+            k = int(rng.integers(0, len(scenes)))
+            w, h = res[int(rng.integers(0, 4))]
+            spp = [1, 4, 16, 64][int(rng.integers(0, 4))]
+            b = [2, 4, 8][int(rng.integers(0, 3))]
+            o = scenes[k][1].replace(width=w, height=h,
+                                     path_trace=PathTraceOptions(samples_per_pixel=spp, max_bounces=b, seed=i))
+            spec.append(("new", k, o))
+    samples = []
+    for sp in spec:
+        o = sp[2] if sp[0] == "new" else spec[sp[1]][2]
+        samples.append(o.width * o.height * (o.path_trace.samples_per_pixel if sp[0] == "new" else sp[2]))
+    return spec, samples
+
+
+def run_poisson(ctx, api, torch, args):
+    """Config 4: Poisson arrivals of `served_spec` requests against a warm
+    server holding 32 scenes under the HBM budget, per arrival rate (the
+    requests of a rate arrive over --serve-seconds, at most --serve-max);
+    p50/p99 latency (submit -> HDR in host memory) and delivered samples/s.
+    The plain per-request path runs the SAME requests, continuations
+    included: a new request is one PathTraceCudaRenderer.render_hdr (scene
+    prepared + uploaded), a continuation refine(16) + hdr on its base
+    request's renderer (PathTracer::refine on a live tracer). Its latencies
+    under each rate's arrivals follow from the measured service times, one
+    request at a time in arrival order (Lindley's recursion)."""
     from oxideav_render_b200.serve import RenderServer
     t0 = time.perf_counter()
     scenes = serving_scenes(args.serve_scenes, 2026)
     gen_s = time.perf_counter() - t0
-    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), autotune=args.autotune,
-                       wave_overlap=args.wave_overlap, wave_slots=args.serve_wave_slots)
+    n = max(8, min(int(max(args.serve_rates) * args.serve_seconds), args.serve_max))
+    spec, samples = served_spec(n, scenes, 4242)
+    srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), wave_overlap=args.wave_overlap,
+                       wave_slots=args.serve_wave_slots)
     t0 = time.perf_counter()
-    keys = [srv.register(s, o, api.EnvironmentMap(e) if e is not None else None) for s, o, e in scenes]
+    keys = register_scenes(srv, api, scenes)
     register_s = time.perf_counter() - t0
-    # Make every scene resident (one tiny request each), as a warm server is.
-    t0 = time.perf_counter()
-    warm = [srv.submit(k, o.replace(width=16, height=16, path_trace=PathTraceOptions(samples_per_pixel=1)))
-            for k, (_, o, _) in zip(keys, scenes)]
-    for t in warm:
-        srv.wait(t)
-        srv.release(t)
-    admit_s = time.perf_counter() - t0
-    res = [(128, 128), (256, 256), (512, 512), (1024, 768)]
-    runs = []
-    sample_reqs = None
+    runs, images = [], {}
     for rate in args.serve_rates:
-        rng = np.random.default_rng(int(rate * 1000) + 17)
-        n = max(8, min(int(rate * args.serve_seconds), args.serve_max))
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
-        spec = []
-        for i in range(n):
-            if i > 0 and rng.random() < 0.2:
-                spec.append(("cont", int(rng.integers(0, i)), 16))
-            else:
-                k = int(rng.integers(0, len(scenes)))
-                w, h = res[int(rng.integers(0, 4))]
-                spp = [1, 4, 16, 64][int(rng.integers(0, 4))]
-                b = [2, 4, 8][int(rng.integers(0, 3))]
-                o = scenes[k][1].replace(width=w, height=h,
-                                         path_trace=PathTraceOptions(samples_per_pixel=spp, max_bounces=b, seed=i))
-                spec.append(("new", k, o))
-        tickets, submit_t, samples = [None] * n, [0.0] * n, [0] * n
+        m = max(8, min(int(rate * args.serve_seconds), n))
+        arrivals = np.cumsum(np.random.default_rng(int(rate * 1000) + 17).exponential(1.0 / rate, m))
+        tickets, lat = [None] * m, [0.0] * m
         start = time.perf_counter()
-        for i, sp in enumerate(spec):
+        for i in range(m):
             delay = start + arrivals[i] - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            submit_t[i] = time.perf_counter()
-            if sp[0] == "new":
-                tickets[i] = srv.submit(keys[sp[1]], sp[2])
-                samples[i] = sp[2].width * sp[2].height * sp[2].path_trace.samples_per_pixel
-            else:
-                base = sp[1]
-                while spec[base][0] == "cont":
-                    base = spec[base][1]
-                o = spec[base][2]
-                tickets[i] = srv.submit_continuation(tickets[sp[1]], sp[2])
-                samples[i] = o.width * o.height * sp[2]
-        lat, done_t, images = [], [], {}
-        for i, t in enumerate(tickets):
-            img, st = srv.wait(t)
-            lat.append(st["latency_ms"])
-            done_t.append(submit_t[i] + st["latency_ms"] / 1000.0)
-            if spec[i][0] == "new" and len(images) < args.serve_check:
+            sp = spec[i]
+            tickets[i] = (srv.submit(keys[sp[1]], sp[2]) if sp[0] == "new"
+                          else srv.submit_continuation(tickets[sp[1]], sp[2]))
+        done = []
+        for i in range(m):
+            img, st = srv.wait(tickets[i])
+            lat[i] = st["latency_ms"]
+            done.append(start + arrivals[i] + st["latency_ms"] / 1000.0)
+            if rate == args.serve_rates[0] and len(images) < args.serve_check:
                 images[i] = img
-        makespan = max(done_t) - submit_t[0]
-        stats = srv.stats()
+        makespan = max(done) - (start + arrivals[0])
         for t in tickets:
             srv.release(t)
-        runs.append({"rate_per_s": rate, "requests": n, "continuations": sum(1 for s in spec if s[0] == "cont"),
-                     "samples": int(sum(samples)), "makespan_s": makespan,
-                     "samples_per_s": sum(samples) / makespan,
-                     "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                     "max_ms": float(max(lat))})
-        sample_reqs = (spec, arrivals, images)
+        runs.append({"rate_per_s": rate, "requests": m, "continuations": sum(1 for s in spec[:m] if s[0] == "cont"),
+                     "arrival_window_s": float(arrivals[-1]), "samples": int(sum(samples[:m])),
+                     "makespan_s": makespan, "samples_per_s": sum(samples[:m]) / makespan, **percentiles(lat),
+                     "_arrivals": arrivals})
     st = srv.stats()
     srv.close()
-
-    # Plain per-request path on the saturated run's first --plain-requests new
-    # requests (in arrival order; --plain-seconds caps the time): one-shot
-    # render (scene prepared
-    # and uploaded per request, PathTraceRenderer::render_hdr semantics),
-    # once with this library's default preparation (device BVH for large
-    # scenes) and once with the BVH built on the host as the reference's
-    # TraceScene::new does; and refine + hdr on a tracer whose scene is
-    # already uploaded.
-    from oxideav_render_b200 import abi
-    spec, arrivals, images = sample_reqs
-    renderer = api.PathTraceCudaRenderer(ctx)
-    plain_t, plain_n, resident_t, identical, arr = [], [], [], [], []
-    host_t = []
-    budget_end = time.perf_counter() + args.plain_seconds
-    for i, sp in enumerate(spec):
-        if sp[0] != "new":
-            continue
-        if len(plain_t) >= args.plain_requests or time.perf_counter() > budget_end:
-            break
-        s, _, e = scenes[sp[1]]
-        o = sp[2]
-        renderer.tracer_mut().set_environment(api.EnvironmentMap(e) if e is not None else None)
+    # The plain path: measured service time of every request, in order.
+    m_all = max(r["requests"] for r in runs)
+    need = {sp[1] for sp in spec[:m_all] if sp[0] == "cont"}
+    renderers, service, identical = {}, [], []
+    shared = api.PathTraceCudaRenderer(ctx)
+    for i in range(m_all):
+        sp = spec[i]
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        img = renderer.render_hdr(s, o)
-        plain_t.append(time.perf_counter() - t0)
-        plain_n.append(o.width * o.height * o.path_trace.samples_per_pixel)
-        arr.append(arrivals[i])
+        if sp[0] == "new":
+            s, _, e = scenes[sp[1]]
+            # A request that a continuation will extend keeps its own
+            # renderer (its accumulator); the others share one.
+            r = api.PathTraceCudaRenderer(ctx) if i in need else shared
+            r.tracer_mut().set_environment(api.EnvironmentMap(e) if e is not None else None)
+            t0 = time.perf_counter()
+            img = r.render_hdr(s, sp[2])
+            service.append(time.perf_counter() - t0)
+            if i in need:
+                renderers[i] = r
+        else:
+            r = renderers[sp[1]]
+            t0 = time.perf_counter()
+            r.tracer.refine(sp[2])
+            img = r.tracer.hdr()
+            service.append(time.perf_counter() - t0)
         if i in images:
             identical.append(bool(np.array_equal(img, images[i])))
-        tr = renderer.tracer
-        tr.reset()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        tr.refine(o.path_trace.samples_per_pixel)
-        tr.hdr()
-        resident_t.append(time.perf_counter() - t0)
-        ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST)
-        try:
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            renderer.render_hdr(s, o)
-            host_t.append(time.perf_counter() - t0)
-        finally:
-            ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
-    renderer.tracer.close()
-    # Latency of the plain path under the same arrivals: one request at a
-    # time, first come first served (Lindley recursion on measured times).
-    def fcfs_latency(times):
-        free_at, lat = 0.0, []
-        for a, s_ in zip(arr, times):
-            begin = max(a, free_at)
-            free_at = begin + s_
-            lat.append(1000.0 * (free_at - a))
-        return lat
-
-    plain_lat, host_lat = fcfs_latency(plain_t), fcfs_latency(host_t)
-    sat = max(runs, key=lambda r: r["rate_per_s"])
-    plain_sps = sum(plain_n) / sum(plain_t)
-    host_sps = sum(plain_n) / sum(host_t)
-    resident_sps = sum(plain_n) / sum(resident_t)
-    return {
-        "scenes": len(scenes), "budget_gb": args.serve_budget_gb, "scene_gen_s": gen_s, "register_s": register_s,
-        "first_admission_s": admit_s, "scene_uploads": st["scene_uploads"], "scene_evictions": st["scene_evictions"],
-        "peak_resident_gb": st["peak_resident_bytes"] / (1 << 30), "waves": st["waves"],
-        "gpu_mrays_per_s": st["rays"] / (st["gpu_ms"] / 1000.0) / 1e6 if st["gpu_ms"] > 0 else None,
-        "runs": runs,
-        "plain_render": {"requests": len(plain_t), "samples_per_s": plain_sps,
-                         "p50_ms": float(np.percentile(plain_lat, 50)), "p99_ms": float(np.percentile(plain_lat, 99)),
-                         "call": "PathTraceCudaRenderer.render_hdr per request (scene prepared + uploaded per call)"},
-        "plain_render_host_bvh": {"requests": len(host_t), "samples_per_s": host_sps,
-                                  "p50_ms": float(np.percentile(host_lat, 50)),
-                                  "p99_ms": float(np.percentile(host_lat, 99)),
-                                  "call": "the same one-shot render with the BVH built on the host per call"},
-        "plain_resident": {"requests": len(resident_t), "samples_per_s": resident_sps,
-                           "call": "PathTracer.refine + hdr per request, scene already on the device"},
-        "speedup_vs_plain_render": sat["samples_per_s"] / plain_sps,
-        "speedup_vs_plain_render_host_bvh": sat["samples_per_s"] / host_sps,
-        "speedup_vs_plain_resident": sat["samples_per_s"] / resident_sps,
-        "bit_identical_checked": len(identical), "bit_identical": all(identical) if identical else None,
-    }
+    for r in list(renderers.values()) + [shared]:
+        r.tracer.close()
+    for run in runs:
+        arr = run.pop("_arrivals")
+        m = run["requests"]
+        free_at, plat, end = 0.0, [], 0.0
+        for a, s_ in zip(arr, service[:m]):
+            free_at = max(a, free_at) + s_
+            plat.append(1000.0 * (free_at - a))
+        plain_sps = sum(samples[:m]) / (free_at - arr[0])
+        run["plain"] = {"samples_per_s": plain_sps, **percentiles(plat)}
+        run["speedup_vs_plain"] = run["samples_per_s"] / plain_sps
+    plain_busy = sum(samples[:m_all]) / sum(service)
+    return {"scenes": len(scenes), "budget_gb": args.serve_budget_gb, "scene_gen_s": gen_s,
+            "register_s": register_s, "scene_uploads": st["scene_uploads"], "scene_evictions": st["scene_evictions"],
+            "peak_resident_gb": st["peak_resident_bytes"] / (1 << 30), "waves": st["waves"],
+            "gpu_mrays_per_s": st["rays"] / (st["gpu_ms"] / 1000.0) / 1e6 if st["gpu_ms"] > 0 else None,
+            "runs": runs,
+            "plain_service_samples_per_s": plain_busy,
+            "plain_call": "new: PathTraceCudaRenderer.render_hdr (scene prepared + uploaded per call); "
+                          "continuation: refine(16) + hdr on its base request's renderer",
+            "bit_identical_checked": len(identical), "bit_identical": all(identical) if identical else None}
 
 
 def algorithmic_bytes(ext_rays, shadow_rays, nodes, tris, samples):
@@ -442,6 +521,51 @@ def cpu_baseline(scene, opts, env, budget_s: float):
             "mrays_per_s": (rc[0] + rc[1]) / dt / 1e6}
 
 
+def oracle_mixed(reqs, passes: int = 0, budget_s: float = 0.0, first_pass: int = 0, stride: int = 256):
+    """The oracle (CPU restatement of the reference) over the request mix on
+    all host cores. Pass p renders, of every request r, the rows
+    y = (17 r + p) mod `stride` + k * `stride` at the request's full spp: each
+    pass is about 1/`stride` of the whole mix, in the mix's own proportions
+    of scenes, sizes, spp and bounces. Rows run in parallel, one host thread
+    each. Runs `passes` passes, or as many as fit in `budget_s`. Returns
+    (camera paths, seconds per pass, rays, cores)."""
+    import concurrent.futures as cf
+    orc = entry.load_oracle()
+    from oxideav_render_b200.scene import Camera
+    cores = os.cpu_count() or 1
+    built = {}
+    jobs = []
+    for k, s, o, env in reqs:
+        if k not in built:
+            desc = s.to_desc(o)
+            built[k] = (desc, orc.OracleScene(desc), orc.OracleEnv(env) if env is not None else None)
+        _, sc, oenv = built[k]
+        jobs.append((sc, Camera.resolve(s, o, o.width, o.height), o, oenv))
+
+    def one(job, row):
+        sc, cam, o, oenv = job
+        _, rc = orc.refine_rows(sc, cam, o, oenv, row, 1, 1, 0, o.path_trace.samples_per_pixel, 1)
+        return o.width * o.path_trace.samples_per_pixel, rc[0] + rc[1]
+
+    times, paths, rays = [], 0, 0
+    with cf.ThreadPoolExecutor(cores) as ex:
+        p = first_pass
+        t_start = time.perf_counter()
+        while (passes and len(times) < passes) or (not passes and time.perf_counter() - t_start < budget_s):
+            t0 = time.perf_counter()
+            work = [(job, y) for r, job in enumerate(jobs)
+                    for y in range((17 * r + p) % stride, job[2].height, stride)]
+            # Largest rows first: the pool ends each pass with small ones.
+            work.sort(key=lambda jy: -jy[0][2].width * jy[0][2].path_trace.samples_per_pixel)
+            for f in [ex.submit(one, job, y) for job, y in work]:
+                n, r = f.result()
+                paths += n
+                rays += r
+            times.append(time.perf_counter() - t0)
+            p += 1
+    return paths, times, rays, cores
+
+
 def dist_setup():
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -472,36 +596,26 @@ def barrier(ws: int):
 
 
 def run_reference(args):
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference arm: the oracle (the CPU restatement of the reference's
+    PathTracer; the Rust crate cannot be built here) on the host cores, on
+    the headline's request mix. One step = one pass: every 256th row of
+    every request at its full spp (a bounded sample of the mix, in its
+    proportions)."""
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pkg = entry.load_package()
-    scene, opts, env, wname = workload(args.config)
-    orc = entry.load_oracle()
-    from oxideav_render_b200.scene import Camera
-    desc = scene.to_desc(opts)
-    sc = orc.OracleScene(desc)
-    cam = Camera.resolve(scene, opts, opts.width, opts.height)
-    oenv = orc.OracleEnv(env) if env is not None else None
-    cores = os.cpu_count() or 1
-    rows, spp = min(args.ref_rows, opts.height), args.ref_spp
-    stride = max(opts.height // rows, 1)
-    times, rays = [], 0
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        _, rc = orc.refine_rows(sc, cam, opts, oenv, stride // 2, stride, rows, i * spp, spp, cores)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            times.append(dt)
-            rays += rc[0] + rc[1]
-    n = opts.width * rows * spp
-    value = n * len(times) / sum(times)
-    sample = f"every {stride}th row ({rows} of {opts.height}) x {spp} spp per step ({n} camera paths)"
+    entry.load_package()
+    reqs = mixed_requests(args.mixed, 2026)
+    oracle_mixed(reqs, passes=args.warmup)  # warm-up passes (also builds the oracle scenes)
+    paths, times, rays, cores = oracle_mixed(reqs, passes=args.steps, first_pass=args.warmup)
+    value = paths / sum(times)
+    sample = (f"every 256th row of each of the {len(reqs)} requests per step (offset by request and step) at the "
+              f"request's full spp, about 1/256 of the mix; {paths // max(len(times), 1)} camera paths per step")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": wname, "parallelism": "host threads"},
+        "data": "synthetic", "config": {"workload": MIX_WORKLOAD, "parallelism": "host threads"},
         "mrays_per_s": rays / sum(times) / 1e6,
         "cpu_baseline": {"value": value, "unit": "samples/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -599,11 +713,39 @@ def run_raycasts(args):
     ctx.close()
 
 
-def run_b200(args):
-    import torch
-    ws, rank, local = dist_setup()
-    pkg = entry.load_package()
-    from oxideav_render_b200 import api
+MIX_WORKLOAD = ("config 3 request mix: 64 requests (seed 2026), scene uniform over {Cornell box C0, sphere grid C1, "
+                "stress scene C2 (~4.1M tris, env + 8 emitters), 8 random soups of 10k-500k tris}, resolution "
+                "{128^2, 256^2, 512^2, 1024x768}, spp {1, 4, 16, 64}, bounces {2, 4, 8}")
+
+
+def stage_roofline(bc, peak, peak_kind, config_tag, wave_paths):
+    """Roofline of the dominant wavefront stage from a stage-timed refine:
+    its algorithmic bytes (the byte model) / its device time."""
+    ext, shadow = bc["ext_rays"], bc["shadow_rays"]
+    stage = bc["stage_ms"]
+    stage_bytes = {
+        "extend": 48 * ext + 64 * bc["ext_nodes"] + 48 * bc["ext_tris"],
+        "shadow": 48 * shadow + 64 * bc["sh_nodes"] + 48 * bc["sh_tris"],
+        "shade": ext * (16 + 128 + 32) + 32 * shadow,
+        "megakernel": algorithmic_bytes(ext, shadow, bc["ext_nodes"] + bc["sh_nodes"],
+                                        bc["ext_tris"] + bc["sh_tris"], 0),
+        "accumulate": 32 * bc["samples"],
+    }
+    names = {"extend": "k_wf_extend", "shade": "k_wf_shade", "shadow": "k_wf_shadow", "megakernel": "k_megakernel",
+             "accumulate": "k_accumulate"}
+    dom = max((k for k in stage_bytes if stage.get(k, 0) > 0), key=lambda k: stage[k])
+    launches = bc["rounds"] if dom in ("extend", "shade", "shadow") else bc["waves"]
+    achieved = stage_bytes[dom] / (stage[dom] / 1000.0) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": profiled_traffic(names[dom], config_tag, wave_paths), "peak_kind": peak_kind,
+            "kernel": names[dom], "bytes_per_launch": stage_bytes[dom] / max(launches, 1),
+            "ms_per_launch": stage[dom] / max(launches, 1), "launches": int(launches)}
+
+
+def run_frame(ctx, api, torch, args, ws, rank, flush):
+    """Secondary: one plain frame of --config (default: the C1 sphere grid,
+    512^2, 256 spp) refined by one tracer on a resident scene, K steps, plus
+    its end-to-end one-shot render and raycast frames of the same scene."""
     scene, opts, env, wname = workload(args.config)
     if args.spp:
         opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__,
@@ -611,14 +753,6 @@ def run_b200(args):
         wname += f" (override: {args.spp} spp)"
     spp = opts.path_trace.samples_per_pixel
     samples_per_step = opts.width * opts.height * spp
-    ctx = api.Context(local if ws > 1 else torch.cuda.current_device())
-    if not args.wave_overlap:
-        ctx.set_wave_overlap(False)
-    elif args.wave_arenas:
-        ctx.set_wave_overlap(args.wave_arenas)
-    if args.wave_slots:
-        ctx.set_wave_slots(args.wave_slots)
-    ctx.set_schedule({"megakernel": 0, "wavefront": 1}[args.schedule])
     if args.seed_per_rank and ws > 1:
         opts = opts.replace(path_trace=opts.path_trace.__class__(**{**opts.path_trace.__dict__, "seed": rank}))
     tracer = api.PathTracer(ctx)
@@ -627,150 +761,155 @@ def run_b200(args):
     tracer.sync(scene, opts)
     tuned = None
     if args.autotune:
-        # pt_autotune: calibration refines on a scratch accumulator pick this
-        # scene class's configuration (images are identical under every one).
         t0 = time.perf_counter()
         tuned = ctx.autotune(tracer, 0)
         tuned["seconds"] = time.perf_counter() - t0
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     for _ in range(args.warmup):
         tracer.refine(spp)
     barrier(ws)
-    kernel_ms, wall_ms = [], []
-    ext = shadow = 0
-    split = {"ext_nodes": 0, "ext_tris": 0, "sh_nodes": 0, "sh_tris": 0}
-    stage = {k: 0.0 for k in api.PathTracer.STAGES}
-    with ClockSampler(local if ws > 1 else torch.cuda.current_device()) as clocks:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            tracer.refine(spp)
-            wall_ms.append(1000 * (time.perf_counter() - t0))
-            kernel_ms.append(tracer.last_kernel_ms())
-            e, s = tracer.ray_counts()
-            ext, shadow = ext + e, shadow + s
-            for k, v in tracer.traversal_split().items():
-                split[k] += v
+    kernel_ms, ext, shadow = [], 0, 0
+    for _ in range(args.frame_steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        tracer.refine(spp)
+        kernel_ms.append(tracer.last_kernel_ms())
+        e, s = tracer.ray_counts()
+        ext, shadow = ext + e, shadow + s
     barrier(ws)
-    # Stage split: one more (untimed) frame with CUDA events between the
-    # stages. Events need direct launches; the timed frames replay each wave
-    # as one CUDA graph.
     ctx.set_stage_timing(True)
     flush.zero_()
     torch.cuda.synchronize()
     tracer.refine(spp)
-    stage = {k: v * args.steps for k, v in tracer.stage_ms().items()}
-    stage_frame_ms = tracer.last_kernel_ms()
+    bc = api.batch_counters(ctx)
     ctx.set_stage_timing(False)
     dev_s = max_over_ranks(sum(kernel_ms) / 1000.0, ws)
-    value = samples_per_step * args.steps * ws / dev_s
-    ms_per_step = 1000 * dev_s / args.steps
-    rays = ext + shadow
-    mrays = max(rays / (sum(kernel_ms) / 1000.0) / 1e6, 0.0)
-    # Roofline of the dominant kernel: its algorithmic bytes / its device time.
     peak, peak_kind = load_peaks()
-    n_samples = samples_per_step * args.steps
-    stage_bytes = {
-        "extend": 48 * ext + 64 * split["ext_nodes"] + 48 * split["ext_tris"],
-        "shadow": 48 * shadow + 64 * split["sh_nodes"] + 48 * split["sh_tris"],
-        "shade": ext * (16 + 128 + 32) + 32 * shadow,
-        "megakernel": algorithmic_bytes(ext, shadow, split["ext_nodes"] + split["sh_nodes"],
-                                        split["ext_tris"] + split["sh_tris"], 0),
-        "accumulate": 32 * n_samples,
-    }
-    dom = max((k for k in stage_bytes if stage[k] > 0), key=lambda k: stage[k])
-    achieved = stage_bytes[dom] / (stage[dom] / 1000.0) / 1e9
-    kernel_names = {"extend": "k_wf_extend", "shade": "k_wf_shade", "shadow": "k_wf_shadow",
-                    "megakernel": "k_megakernel", "accumulate": "k_accumulate"}
-    # Waves of the refine: the tuned wave size, else the one set or the
-    # library's default (8,388,608 path slots).
     wave_slots = (tuned or {}).get("wave_slots") or args.wave_slots or (1 << 23)
-    waves = max(math.ceil(samples_per_step / wave_slots), 1)
-    iters = opts.path_trace.max_bounces + 1
-    per_wave = (2 + 3 * iters) if args.schedule == "wavefront" else 2
-    launches = args.steps * waves * per_wave
-    launches_of_dom = args.steps * waves * (iters if args.schedule == "wavefront" and dom in
-                                            ("extend", "shade", "shadow") else 1)
-    traffic = profiled_traffic(kernel_names[dom], args.config, min(wave_slots, samples_per_step))
-
-    # End to end: the reference-facing one-shot call (re-prepare + render + image).
+    out = {"workload": wname, "samples_per_step": samples_per_step, "steps": args.frame_steps,
+           "value": samples_per_step * args.frame_steps * ws / dev_s, "unit": "samples/s",
+           "ms_per_step": 1000 * dev_s / args.frame_steps,
+           "mrays_per_s": (ext + shadow) / (sum(kernel_ms) / 1000.0) / 1e6,
+           "stage_ms_per_frame": {k: v for k, v in bc["stage_ms"].items() if v > 0},
+           "roofline": stage_roofline(bc, peak, peak_kind, args.config, min(wave_slots, samples_per_step)),
+           "autotuned": tuned,
+           "l2": "flushed (256 MB write) before every timed step"}
     renderer = api.PathTraceCudaRenderer(ctx)
     if env is not None:
         renderer.tracer_mut().set_environment(api.EnvironmentMap(env))
-    e2e_s, e2e_calls = [], []
-    h2d = d2h = 0
-    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+    e2e_s = []
+    for i in range(3):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         img = renderer.render(scene, opts)
-        dt = time.perf_counter() - t0
-        e2e_calls.append({"wall_ms": 1000 * dt, "refine_device_ms": renderer.tracer.last_kernel_ms()})
         if i > 0:
-            e2e_s.append(dt)
-        h2d = ctx.scene_bytes(renderer.tracer.scene_id)
-        d2h = img.nbytes
-    e2e = None
-    if e2e_s:
-        e2e_t = max_over_ranks(sum(e2e_s) / len(e2e_s), ws)
-        e2e = {"value": samples_per_step * ws / e2e_t, "unit": "samples/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1000 * e2e_t,
-               "call": "PathTraceCudaRenderer.render (scene preparation and upload incl. the BVH build, "
-                       "refine, sRGB image readback)",
-               "calls": e2e_calls}
-        # Where the host part of that time goes (one extra, separately timed upload).
-        t0 = time.perf_counter()
-        desc = scene.to_desc(opts)
-        t1 = time.perf_counter()
-        sid = ctx.upload(desc)
-        t2 = time.perf_counter()
-        e2e["host_ms"] = {"flatten": 1000 * (t1 - t0), "prepare_and_upload": 1000 * (t2 - t1),
-                          "bvh_build": 1000 * ctx.bvh_stats(sid)["build_seconds"],
-                          "bvh_on_device": ctx.bvh_on_device(sid),
-                          "upload_phases": {k: 1000 * v for k, v in ctx.upload_seconds(sid).items()}}
-        ctx.release(sid)
-    raycast = raycast_pbr = None
+            e2e_s.append(time.perf_counter() - t0)
+    e2e_t = max_over_ranks(sum(e2e_s) / len(e2e_s), ws)
+    out["e2e"] = {"value": samples_per_step * ws / e2e_t, "unit": "samples/s", "ms_per_step": 1000 * e2e_t,
+                  "h2d_bytes_per_step": int(ctx.scene_bytes(renderer.tracer.scene_id)),
+                  "d2h_bytes_per_step": int(img.nbytes),
+                  "call": "PathTraceCudaRenderer.render (scene preparation and upload incl. the BVH build, "
+                          "refine, sRGB image readback)"}
+    renderer.tracer.close()
     if args.raycast:
-        raycast = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline)
-        raycast_pbr = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline,
-                                  pbr=True)
-    mixed = None
-    if args.mixed > 0:
-        mixed = run_mixed(ctx, api, torch, args.mixed, 2026 + rank)
-    served = None
-    if args.serve_rates:
-        served = run_served(ctx, api, torch, args)
+        out["raycast"] = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline)
+        out["raycast_pbr"] = run_raycast(ctx, api, torch, scene, opts, cpu=rank == 0 and not args.no_cpu_baseline,
+                                         pbr=True)
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(scene, opts, env, args.cpu_seconds / 2)
+    tracer.close()
+    return out
+
+
+def run_b200(args):
+    import torch
+    ws, rank, local = dist_setup()
+    entry.load_package()
+    from oxideav_render_b200 import api
+    ctx = api.Context(local if ws > 1 else torch.cuda.current_device())
+    if not args.wave_overlap:
+        ctx.set_wave_overlap(False)
+    elif args.wave_arenas:
+        ctx.set_wave_overlap(args.wave_arenas)
+    if args.wave_slots:
+        ctx.set_wave_slots(args.wave_slots)
+    if args.schedule == "megakernel":
+        ctx.set_schedule(0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    # Headline: the config-3 request mix in shared waves (one tracer per
+    # request, scenes resident). With N ranks the mix holds 64 N requests
+    # (seed 2026; request i renders with sample seed i) and rank r serves
+    # requests r, r + N, ... with its own scene cache: 64 requests per GPU
+    # (weak scaling), no exchange. N = 1 is exactly the 64-request mix.
+    from oxideav_render_b200 import shard
+    reqs = shard.shard(mixed_requests(args.mixed * ws, 2026), rank, ws)
+    tracers, b = run_batched(ctx, api, torch, reqs, args, ws, flush)
+    dev_s = max_over_ranks(sum(b["ms"]) / 1000.0, ws)
+    value = b["total"] * args.steps * ws / dev_s
+    peak, peak_kind = load_peaks()
+    bc = b["counters"]
+    roofline = stage_roofline(bc, peak, peak_kind, "mixed", min(args.wave_slots or (1 << 23), b["total"]))
+    launches = args.steps * (2 * bc["waves"] + 6 * bc["rounds"])
+
+    # End to end on the same requests through the serving C ABI (host I/O).
+    e2e = run_served_batch(ctx, api, torch, reqs, args, tracers)
+    e2e_wall = max_over_ranks(e2e["ms_per_step"] / 1000.0, ws)
+    e2e["value"] = b["total"] * ws / e2e_wall
+    e2e["ms_per_step"] = 1000 * e2e_wall
+    # The plain per-request path on the same requests.
+    plain = run_plain_requests(ctx, api, torch, reqs, tracers)
+    for t in tracers:
+        t.close()
+    vs_plain = {
+        "same_requests": True,
+        "plain_one_shot_samples_per_s": plain["one_shot"]["samples_per_s"],
+        "plain_resident_samples_per_s": plain["resident"]["samples_per_s"],
+        "served_e2e_samples_per_s": e2e["value"] / ws,
+        "batched_device_samples_per_s": value / ws,
+        "speedup_served_vs_plain_one_shot": (e2e["value"] / ws) / plain["one_shot"]["samples_per_s"],
+        "speedup_served_vs_plain_resident": (e2e["value"] / ws) / plain["resident"]["samples_per_s"],
+        "speedup_batched_vs_plain_resident": (value / ws) / plain["resident"]["samples_per_s"],
+        "latency_ms": {"served": {"p50": e2e["p50_ms"], "p99": e2e["p99_ms"]},
+                       "plain_one_shot": {"p50": plain["one_shot"]["p50_ms"], "p99": plain["one_shot"]["p99_ms"]},
+                       "plain_resident": {"p50": plain["resident"]["p50_ms"], "p99": plain["resident"]["p99_ms"]}},
+        "latency_note": "all requests submitted at once; plain latencies are cumulative, in request order",
+        "per_rank": ws > 1,
+    }
+
+    frame = run_frame(ctx, api, torch, args, ws, rank, flush) if args.frame else None
+    poisson = run_poisson(ctx, api, torch, args) if (args.serve_rates and ws == 1) else None
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(scene, opts, env, args.cpu_seconds)
+        paths, times, rays, cores = oracle_mixed(reqs, budget_s=args.cpu_seconds)
+        cpu = {"value": paths / sum(times), "unit": "samples/s", "cores": cores, "kind": "port",
+               "sample": f"{len(times)} passes over every 256th row of each of the {len(reqs)} requests at "
+                         f"its full spp ({paths} camera paths, {sum(times):.1f} s)",
+               "mrays_per_s": rays / sum(times) / 1e6}
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wname, "samples_per_step": samples_per_step, "global_batch": samples_per_step * ws,
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "flushed (256 MB write) before every timed step", "schedule": args.schedule,
-                       "autotuned": tuned},
-            "mrays_per_s": mrays, "rays_per_step": rays / args.steps, "wall_ms_per_step": statistics.mean(wall_ms),
-            "stage_ms_per_step": {k: v / args.steps for k, v in stage.items() if v > 0},
-            "stage_frame_ms": stage_frame_ms,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": kernel_names[dom],
-                         "bytes_per_launch": stage_bytes[dom] / max(launches_of_dom, 1),
-                         "ms_per_launch": stage[dom] / max(launches_of_dom, 1)},
+            "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": MIX_WORKLOAD, "requests_per_step": len(reqs), "samples_per_step": b["total"],
+                       "global_batch": b["total"] * ws,
+                       "parallelism": f"request mix per rank x{ws}" if ws > 1 else "single GPU",
+                       "path": "pt_tracer_refine_many: every request's paths in shared wavefront waves",
+                       "l2": "flushed (256 MB write) before every timed step; resident scenes 2+ GB",
+                       "schedule": args.schedule},
+            "mrays_per_s": b["rays"] / (sum(b["ms"]) / 1000.0) / 1e6,
+            "waves_per_step": b["waves"] / args.steps,
+            "stage_ms_per_step": {k: v for k, v in bc["stage_ms"].items() if v > 0},
+            "stage_note": "stage split from one extra batch timed stage by stage (sequential waves)",
+            "roofline": roofline,
             "e2e": e2e,
-            "batched_mixed": mixed,
-            "raycast": raycast,
-            "raycast_pbr": raycast_pbr,
-            "served": served,
+            "vs_plain": vs_plain,
+            "served_poisson": poisson,
+            "plain_frame": frame,
             "cpu_baseline": cpu,
-            "clocks": clocks.summary(),
-            "gpu_launches": launches,
+            "clocks": b["clocks"],
+            "gpu_launches": int(launches),
         }
         print(json.dumps(out))
-    tracer.close()
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -782,28 +921,27 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "soup"])
+    ap.add_argument("--mixed", type=int, default=64, help="requests of the headline request mix")
+    ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "soup"],
+                    help="scene of the secondary single-frame measurement")
+    ap.add_argument("--no-frame", dest="frame", action="store_false", help="skip the single-frame measurement")
+    ap.add_argument("--frame-steps", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed-per-rank", action="store_true")
-    ap.add_argument("--ref-rows", type=int, default=32)
-    ap.add_argument("--ref-spp", type=int, default=8)
-    ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling cases)")
+    ap.add_argument("--spp", type=int, default=0, help="override the frame's samples per pixel (profiling cases)")
     ap.add_argument("--schedule", default="wavefront", choices=["megakernel", "wavefront"])
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
-                    help="keep the default configuration instead of pt_autotune's per-class choice")
-    ap.add_argument("--mixed", type=int, default=64, help="requests in the batched-vs-plain comparison (0: skip)")
-    ap.add_argument("--serve-rates", default="5,20,200",
-                    help="Poisson arrival rates (requests/s) of the served runs, comma-separated ('' : skip)")
-    ap.add_argument("--serve-seconds", type=float, default=8.0, help="arrival window per served run")
-    ap.add_argument("--serve-max", type=int, default=96, help="requests per served run at most")
-    ap.add_argument("--serve-scenes", type=int, default=32, help="resident scenes of the served runs")
+                    help="keep the default configuration instead of pt_autotune's per-class choice (frame only)")
+    ap.add_argument("--serve-rates", default="5,200",
+                    help="Poisson arrival rates (requests/s) of the config-4 runs, comma-separated ('' : skip)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="arrival window per config-4 run")
+    ap.add_argument("--serve-max", type=int, default=300, help="requests per config-4 run at most")
+    ap.add_argument("--serve-scenes", type=int, default=32, help="resident scenes of the config-4 runs")
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
     ap.add_argument("--serve-wave-slots", type=int, default=0, help="path slots per served wave (0: the server's default)")
-    ap.add_argument("--plain-requests", type=int, default=24, help="requests in the plain-path sample")
-    ap.add_argument("--plain-seconds", type=float, default=60.0, help="time cap of the plain-path sample")
     ap.add_argument("--no-raycast", dest="raycast", action="store_false",
                     help="skip the RenderBackend::Raycast measurement")
     ap.add_argument("--upload-only", type=int, default=0,

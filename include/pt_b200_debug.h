@@ -40,6 +40,14 @@ PT_API pt_status pt_tracer_traversal_split(const pt_tracer *tr, uint64_t out[4])
  * material sort. */
 PT_API pt_status pt_set_stage_timing(pt_context *ctx, int on);
 PT_API pt_status pt_tracer_stage_ms(const pt_tracer *tr, float *out, uint32_t n);
+/* The same figures for the last refine or batch of the context as a whole
+ * (pt_tracer_refine_many included): out = {closest-hit rays, any-hit rays,
+ * closest-hit nodes, closest-hit triangles, any-hit nodes, any-hit
+ * triangles, samples, waves, bounce rounds summed over the waves (each
+ * round is one extension, shade and shadow launch in the wavefront)}, and
+ * per-stage device ms (stage timing on). */
+PT_API pt_status pt_batch_counters(const pt_context *ctx, uint64_t out[9]);
+PT_API pt_status pt_batch_stage_ms(const pt_context *ctx, float *out, uint32_t n);
 /* Wavefront shade order: nonzero buckets the active queue by (scene,
  * material) before each shade launch so warps shade one material at a time
  * (three small kernels per bounce; on by default). Images are identical

@@ -371,6 +371,19 @@ def refine_many(ctx: Context, tracers, samples) -> None:
     ctx.check(ctx.lib.pt_tracer_refine_many(ctx.ptr, arr, sp, n))
 
 
+def batch_counters(ctx: Context) -> dict:
+    """pt_batch_counters + pt_batch_stage_ms: the last refine / batch as a whole."""
+    v = np.zeros(9, np.uint64)
+    ctx.check(ctx.lib.pt_batch_counters(ctx.ptr, v.ctypes.data_as(native.u64p)))
+    st = np.zeros(len(PathTracer.STAGES), np.float32)
+    ctx.check(ctx.lib.pt_batch_stage_ms(ctx.ptr, st.ctypes.data_as(native.fp), len(PathTracer.STAGES)))
+    names = ("ext_rays", "shadow_rays", "ext_nodes", "ext_tris", "sh_nodes", "sh_tris", "samples", "waves",
+             "rounds")
+    out = {k: int(x) for k, x in zip(names, v)}
+    out["stage_ms"] = dict(zip(PathTracer.STAGES, (float(x) for x in st)))
+    return out
+
+
 def batch_stats(ctx: Context) -> dict:
     ms, waves, rays = C.c_float(), C.c_uint32(), C.c_uint64()
     ctx.check(ctx.lib.pt_batch_stats(ctx.ptr, C.byref(ms), C.byref(waves), C.byref(rays)))

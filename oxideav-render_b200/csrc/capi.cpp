@@ -354,6 +354,24 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
   CK(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   ctx->last_batch_ms = ms;
   ctx->last_batch_waves = (uint32_t)waves.size();
+  {
+    uint64_t samples = 0, rounds = 0;
+    for (const Job &jb : jobs) samples += (uint64_t)jb.npix * jb.target;
+    for (const auto &wv : waves) {
+      uint32_t iters = 1;
+      for (const WaveSegment &s : wv) iters = std::max(iters, jobs[s.request].iterations);
+      rounds += iters;
+    }
+    const uint64_t v[9] = {c.ext_rays, c.shadow_rays, c.ext_nodes, c.ext_tris, c.sh_nodes, c.sh_tris, samples,
+                           (uint64_t)waves.size(), rounds};
+    std::memcpy(ctx->last_batch_counts, v, sizeof v);
+    for (int k = 0; k < STAGE_COUNT; ++k) ctx->last_batch_stage_ms[k] = 0.0f;
+    for (size_t i = 0; i + 1 < timer.count(); ++i) {
+      float sm = 0.0f;
+      CK(ctx, cudaEventElapsedTime(&sm, ctx->stage_events[i], ctx->stage_events[i + 1]));
+      ctx->last_batch_stage_ms[timer.kinds[i]] += sm;
+    }
+  }
   if (stats_to) {
     pt_tracer *t = stats_to;
     t->last_ms = ms;
@@ -946,6 +964,18 @@ pt_status pt_batch_stats(const pt_context *ctx, float *ms, uint32_t *waves, uint
   if (ms) *ms = ctx->last_batch_ms;
   if (waves) *waves = ctx->last_batch_waves;
   if (rays) *rays = ctx->last_batch_rays;
+  return PT_OK;
+}
+
+pt_status pt_batch_counters(const pt_context *ctx, uint64_t out[9]) {
+  if (!ctx || !out) return fail(nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  std::memcpy(out, ctx->last_batch_counts, sizeof ctx->last_batch_counts);
+  return PT_OK;
+}
+
+pt_status pt_batch_stage_ms(const pt_context *ctx, float *out, uint32_t n) {
+  if (!ctx || !out) return fail(nullptr, PT_ERR_INVALID_ARG, "NULL argument");
+  for (uint32_t k = 0; k < n && k < (uint32_t)STAGE_COUNT; ++k) out[k] = ctx->last_batch_stage_ms[k];
   return PT_OK;
 }
 

@@ -57,6 +57,10 @@ struct pt_context {
   float last_batch_ms = 0.0f;
   uint32_t last_batch_waves = 0;
   uint64_t last_batch_rays = 0;
+  // Counters of the last batch: extension / shadow rays, their nodes and
+  // triangles, samples, waves (pt_batch_counters); per-stage ms.
+  uint64_t last_batch_counts[9] = {};
+  float last_batch_stage_ms[ptd::STAGE_COUNT] = {};
   ptd::DevCounters *d_ctr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 148;

@@ -92,6 +92,8 @@ SIGNATURES = {
     "pt_tracer_traversal_split": (i32, [vp, u64p]),
     "pt_set_stage_timing": (i32, [vp, i32]),
     "pt_tracer_stage_ms": (i32, [vp, fp, u32]),
+    "pt_batch_counters": (i32, [vp, u64p]),
+    "pt_batch_stage_ms": (i32, [vp, fp, u32]),
     "pt_scene_bvh_stats": (i32, [vp, u32, u32p, u32p, u32p, dp, dp]),
     "pt_set_schedule": (i32, [vp, u32]),
     "pt_set_wave_slots": (i32, [vp, u32]),
