@@ -188,16 +188,38 @@ def percentiles(lat_ms):
             "max_ms": float(np.max(lat_ms))}
 
 
+def upload_resident(ctx, api, reqs, spatial: bool):
+    """Uploads each distinct scene of the request mix once, as resident
+    scenes: with the spatial-split tree (PT_BVH_BUILD_HOST_SPATIAL) when
+    `spatial`, since a resident scene amortises the slower build."""
+    from oxideav_render_b200 import abi
+    ids, descs = {}, []
+    ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST_SPATIAL if spatial else abi.PT_BVH_BUILD_AUTO)
+    try:
+        for k, s, o, _ in reqs:
+            if k not in ids:
+                d = s.to_desc(o)
+                descs.append(d)
+                ids[k] = ctx.upload(d)
+    finally:
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
+    return ids, descs
+
+
 def run_batched(ctx, api, torch, reqs, args, ws, flush):
     """Headline: the request mix refined in shared waves (pt_tracer_refine_many
-    over one tracer per request, scenes resident). One step = every request's
-    samples; device time of the waves (CUDA events on the library's stream)."""
+    over one tracer per request, each scene uploaded once and resident).
+    One step = every request's samples; device time of the waves (CUDA
+    events on the library's stream)."""
+    t0 = time.perf_counter()
+    scene_ids, descs = upload_resident(ctx, api, reqs, args.spatial_bvh)
+    upload_s = time.perf_counter() - t0
     tracers = []
     for k, s, o, env in reqs:
         t = api.PathTracer(ctx)
         if env is not None:
             t.set_environment(api.EnvironmentMap(env))
-        t.sync(s, o)
+        t.sync_resident(scene_ids[k], s, o)
         tracers.append(t)
     spp = [o.path_trace.samples_per_pixel for _, _, o, _ in reqs]
     total = sum(request_samples(o) for _, _, o, _ in reqs)
@@ -230,7 +252,8 @@ def run_batched(ctx, api, torch, reqs, args, ws, flush):
     stage_batch_ms = api.batch_stats(ctx)["ms"]
     ctx.set_stage_timing(False)
     return tracers, {"ms": ms, "rays": rays, "waves": waves, "total": total, "counters": bc,
-                     "stage_batch_ms": stage_batch_ms, "clocks": clocks.summary()}
+                     "stage_batch_ms": stage_batch_ms, "clocks": clocks.summary(), "scene_ids": scene_ids,
+                     "descs": descs, "scene_upload_s": upload_s}
 
 
 def register_scenes(srv, api, scenes):
@@ -254,7 +277,8 @@ def run_served_batch(ctx, api, torch, reqs, args, tracers):
     import ctypes as C
     from oxideav_render_b200 import abi
     from oxideav_render_b200.serve import RenderServer
-    srv = RenderServer(ctx, wave_overlap=args.wave_overlap, wave_slots=args.serve_wave_slots)
+    srv = RenderServer(ctx, wave_overlap=args.wave_overlap, wave_slots=args.serve_wave_slots,
+                       spatial_bvh=args.spatial_bvh)
     try:
         kinds = sorted({k for k, _, _, _ in reqs})
         scenes = [mixed_scene(k) for k in kinds]
@@ -382,7 +406,7 @@ def run_poisson(ctx, api, torch, args):
     n = max(8, min(int(max(args.serve_rates) * args.serve_seconds), args.serve_max))
     spec, samples = served_spec(n, scenes, 4242)
     srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), wave_overlap=args.wave_overlap,
-                       wave_slots=args.serve_wave_slots)
+                       wave_slots=args.serve_wave_slots, spatial_bvh=args.spatial_bvh)
     t0 = time.perf_counter()
     keys = register_scenes(srv, api, scenes)
     register_s = time.perf_counter() - t0
@@ -835,6 +859,15 @@ def run_b200(args):
     if args.schedule == "megakernel":
         ctx.set_schedule(0)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    if args.mixed == 0:
+        # Profiling case: the single frame of --config alone.
+        frame = run_frame(ctx, api, torch, args, ws, rank, flush)
+        if rank == 0:
+            print(json.dumps(frame))
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     # Headline: the config-3 request mix in shared waves (one tracer per
     # request, scenes resident). With N ranks the mix holds 64 N requests
@@ -860,6 +893,8 @@ def run_b200(args):
     plain = run_plain_requests(ctx, api, torch, reqs, tracers)
     for t in tracers:
         t.close()
+    for sid in b["scene_ids"].values():
+        ctx.release(sid)
     vs_plain = {
         "same_requests": True,
         "plain_one_shot_samples_per_s": plain["one_shot"]["samples_per_s"],
@@ -894,6 +929,8 @@ def run_b200(args):
                        "global_batch": b["total"] * ws,
                        "parallelism": f"request mix per rank x{ws}" if ws > 1 else "single GPU",
                        "path": "pt_tracer_refine_many: every request's paths in shared wavefront waves",
+                       "resident_bvh": "spatial-split (host build once per scene)" if args.spatial_bvh
+                       else "binned SAH", "scene_upload_s": b["scene_upload_s"],
                        "l2": "flushed (256 MB write) before every timed step; resident scenes 2+ GB",
                        "schedule": args.schedule},
             "mrays_per_s": b["rays"] / (sum(b["ms"]) / 1000.0) / 1e6,
@@ -921,7 +958,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--mixed", type=int, default=64, help="requests of the headline request mix")
+    ap.add_argument("--mixed", type=int, default=64,
+                    help="requests of the headline request mix (0: only the single frame of --config, for profiling)")
     ap.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "soup"],
                     help="scene of the secondary single-frame measurement")
     ap.add_argument("--no-frame", dest="frame", action="store_false", help="skip the single-frame measurement")
@@ -942,6 +980,8 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
     ap.add_argument("--serve-wave-slots", type=int, default=0, help="path slots per served wave (0: the server's default)")
+    ap.add_argument("--binned-bvh", dest="spatial_bvh", action="store_false",
+                    help="resident and served scenes get the binned-SAH tree instead of the spatial-split one")
     ap.add_argument("--no-raycast", dest="raycast", action="store_false",
                     help="skip the RenderBackend::Raycast measurement")
     ap.add_argument("--upload-only", type=int, default=0,

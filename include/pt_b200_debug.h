@@ -119,9 +119,24 @@ typedef enum pt_bvh_builder {
   PT_BVH_BUILD_AUTO = 0,
   PT_BVH_BUILD_HOST = 1,
   PT_BVH_BUILD_DEVICE = 2,
-  PT_BVH_BUILD_DEVICE_PLOC = 3
+  PT_BVH_BUILD_DEVICE_PLOC = 3,
+  /* Spatial-split BVH on the host (Stich et al. 2009): triangles straddling
+   * a split plane are referenced from both sides with clipped bounds, up
+   * to 4x the triangle records. On scenes of many small overlapping
+   * triangles (the random soups) it cuts node visits by about 38 % and
+   * triangle tests by a third; well-shaped meshes barely change. The build
+   * takes seconds, so it suits scenes that stay resident. */
+  PT_BVH_BUILD_HOST_SPATIAL = 4
 } pt_bvh_builder;
 PT_API pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder);
+/* Host-only BVH build of a triangle soup (9 floats per triangle), for tests
+ * and tree-quality studies: `spatial` nonzero builds the spatial-split tree.
+ * stats = {two-child nodes, leaves, max depth, SAH cost, seconds, triangle
+ * records}. When `nodes` / `records` are non-NULL and their capacities
+ * (in 64-byte nodes / 48-byte records) suffice, the two-child nodes and the
+ * leaf-ordered records are copied out. */
+PT_API pt_status pt_debug_build_bvh(const float *positions, uint32_t triangles, uint32_t spatial, double stats[6],
+                                    void *nodes, uint64_t node_capacity, void *records, uint64_t record_capacity);
 /* 1 when the scene's current BVH was built on the device. */
 PT_API pt_status pt_scene_bvh_on_device(pt_context *ctx, uint32_t scene_id, int *on_device);
 /* Host wall time in seconds of the scene's pt_scene_upload: [0] the host

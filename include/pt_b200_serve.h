@@ -62,6 +62,9 @@ typedef struct pt_server_config {
   uint32_t material_sort_off;    /* nonzero: shade without material sort */
   uint32_t wave_overlap_off;     /* nonzero: trace one wave at a time (default: consecutive waves
                                     overlap in two path-state arenas on two streams) */
+  uint32_t bvh_binned;           /* nonzero: registered scenes get the binned-SAH tree; default: the
+                                    spatial-split tree (PT_BVH_BUILD_HOST_SPATIAL), built once at
+                                    registration since the scene stays resident */
 } pt_server_config;
 
 typedef struct pt_server_request {

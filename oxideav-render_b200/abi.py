@@ -47,6 +47,7 @@ PT_PERSPECTIVE, PT_ORTHOGRAPHIC = 0, 1
 PT_MIS, PT_LIGHT_ONLY, PT_BSDF_ONLY = 0, 1, 2
 PT_TONE_CLAMP, PT_TONE_REINHARD, PT_TONE_ACES = 0, 1, 2
 PT_BVH_BUILD_AUTO, PT_BVH_BUILD_HOST, PT_BVH_BUILD_DEVICE, PT_BVH_BUILD_DEVICE_PLOC = 0, 1, 2, 3
+PT_BVH_BUILD_HOST_SPATIAL = 4
 # pt_schedule (include/pt_b200_debug.h); a new context runs the wavefront.
 PT_SCHEDULE_MEGAKERNEL, PT_SCHEDULE_WAVEFRONT = 0, 1
 # A new context's path slots per wave.
@@ -262,6 +263,7 @@ class pt_server_config(C.Structure):
         ("autotune", C.c_uint32),
         ("material_sort_off", C.c_uint32),
         ("wave_overlap_off", C.c_uint32),
+        ("bvh_binned", C.c_uint32),
     ]
 
 

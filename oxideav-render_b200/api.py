@@ -266,6 +266,21 @@ class PathTracer:
         self.opts = opts
         return bool(reset.value)
 
+    def sync_resident(self, scene_id: int, scene: PreparedScene, opts: RenderOptions) -> bool:
+        """PathTracer::sync against a scene already uploaded to this context
+        (Context.upload), which several tracers may share; the tracer does
+        not own it (the caller releases it after the tracers are done).
+        Resets exactly when the scene or a radiance input changed."""
+        w, h = max(opts.width, 1), max(opts.height, 1)
+        self.camera = Camera.resolve(scene, opts, w, h)
+        cam = self.camera.to_c()
+        o = opts.to_c()
+        reset = C.c_int()
+        self.ctx.check(self.lib.pt_tracer_sync(self.ptr, int(scene_id), C.byref(cam), C.byref(o), C.byref(reset)))
+        self.opts = opts
+        self._scene = None
+        return bool(reset.value)
+
     def refine(self, samples: int) -> None:
         self.ctx.check(self.lib.pt_tracer_refine(self.ptr, int(samples)))
 

@@ -13,6 +13,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pt_b200.h"
@@ -881,7 +882,7 @@ pt_status pt_scene_bvh_stats(pt_context *ctx, uint32_t scene_id, uint32_t *nodes
 
 pt_status pt_set_bvh_builder(pt_context *ctx, uint32_t builder) {
   if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
-  if (builder > PT_BVH_BUILD_DEVICE_PLOC) return fail(ctx, PT_ERR_INVALID_ARG, "unknown BVH builder");
+  if (builder > PT_BVH_BUILD_HOST_SPATIAL) return fail(ctx, PT_ERR_INVALID_ARG, "unknown BVH builder");
   ctx->bvh_builder = (int)builder;
   return PT_OK;
 }
@@ -1242,6 +1243,31 @@ pt_status pt_debug_prepare_scene(const pt_scene_desc *desc, double seconds[4], u
     if (!err.empty()) return fail(nullptr, PT_ERR_INVALID_ARG, err);
     for (int k = 0; k < 4; ++k) seconds[k] = img.seconds[k];
     if (device_bytes) *device_bytes = img.device_bytes();
+    return PT_OK;
+  });
+}
+
+pt_status pt_debug_build_bvh(const float *positions, uint32_t triangles, uint32_t spatial, double stats[6],
+                             void *nodes, uint64_t node_capacity, void *records, uint64_t record_capacity) {
+  if (!positions || !stats) return fail(nullptr, PT_ERR_INVALID_ARG, "positions / stats is NULL");
+  return guard(nullptr, [&]() -> pt_status {
+    std::vector<BvhNode> n2;
+    std::vector<Bvh4Node> n4;
+    std::vector<float4> rec;
+    BvhBuildStats st;
+    const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (spatial)
+      build_bvh_spatial(positions, triangles, nullptr, n2, n4, rec, st, threads);
+    else
+      build_bvh(positions, triangles, nullptr, n2, n4, rec, st, threads);
+    stats[0] = (double)st.nodes;
+    stats[1] = (double)st.leaves;
+    stats[2] = (double)st.max_depth;
+    stats[3] = st.sah_cost;
+    stats[4] = st.seconds;
+    stats[5] = (double)(rec.size() / 3);
+    if (nodes && node_capacity >= n2.size()) std::memcpy(nodes, n2.data(), n2.size() * sizeof(BvhNode));
+    if (records && record_capacity >= rec.size() / 3) std::memcpy(records, rec.data(), rec.size() * sizeof(float4));
     return PT_OK;
   });
 }

@@ -439,6 +439,450 @@ void pad_box(const float lo[3], const float hi[3], float plo[3], float phi[3]) {
   }
 }
 
+// Spatial-split BVH (Stich, Friedrich & Dietrich, "Spatial Splits in
+// Bounding Volume Hierarchies", HPG 2009). At every node the binned object
+// split (Builder's rule: SAH over centroid bins) competes with a spatial
+// split, which cuts the node's box at a plane and every triangle reference
+// straddling it into two references bounding the clipped triangle. A
+// spatial split is tried only where the object split's two children
+// overlap by more than kAlpha of the root's surface area, and only while
+// the node's subtree stays within its share of the reference budget
+// (kMaxGrowth times the triangle count overall). A triangle may end
+// up in several leaves; its record is repeated. Traversal answers do not
+// change: the closest hit is the accepted candidate of smallest t (ties to
+// the lowest global id) wherever it is found, and every point of a triangle
+// lies in the box of some leaf that references it.
+struct SpatialBuilder {
+  struct Ref {
+    float lo[3], hi[3];
+    uint32_t g;
+  };
+  // A node to split: its references and the most references its subtree
+  // may end with (the root's is the whole budget; a split hands each child
+  // a share in proportion to its references, so the tree does not depend
+  // on thread timing).
+  struct Task {
+    uint32_t node, depth;
+    std::vector<Ref> refs;
+    uint64_t budget;
+  };
+  static constexpr int kObjBins = 16, kSpatialBins = 32;
+  static constexpr uint32_t kMaxLeaf = 8;
+  static constexpr uint32_t kLocalThreshold = 4096;
+  static constexpr uint32_t kParallelNode = 262144;  // nodes binned on three threads
+  static constexpr float kAlpha = 1e-5f;
+  static constexpr double kMaxGrowth = 4.0;
+
+  const float *pos = nullptr;
+  uint32_t n = 0;
+  std::vector<BNode> nodes;
+  std::atomic<uint32_t> node_count{1};
+  std::vector<uint32_t> order;
+  std::atomic<uint64_t> order_fill{0};
+  uint64_t max_refs = 0;
+  float min_overlap = 0.0f;
+  std::atomic<uint32_t> max_depth{0};
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Task> stack;
+  int active = 0;
+  bool done = false;
+
+  static void grow(float lo[3], float hi[3], const float p[3]) {
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], p[k]);
+      hi[k] = std::max(hi[k], p[k]);
+    }
+  }
+  static void grow_box(float lo[3], float hi[3], const float blo[3], const float bhi[3]) {
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], blo[k]);
+      hi[k] = std::max(hi[k], bhi[k]);
+    }
+  }
+  static bool valid(const float lo[3], const float hi[3]) {
+    return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2];
+  }
+  static void empty_box(float lo[3], float hi[3]) {
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = INFINITY;
+      hi[k] = -INFINITY;
+    }
+  }
+
+  // The parts of reference `r` (its triangle clipped to its box) on either
+  // side of `plane` on `axis`: bounds of the triangle's vertices and edge
+  // crossings on each side, cut at the plane and intersected with r's box.
+  void split_ref(const Ref &r, int axis, float plane, Ref &L, Ref &R) const {
+    const float *p = pos + 9 * (size_t)r.g;
+    empty_box(L.lo, L.hi);
+    empty_box(R.lo, R.hi);
+    for (int i = 0; i < 3; ++i) {
+      const float *v0 = p + 3 * i, *v1 = p + 3 * ((i + 1) % 3);
+      if (v0[axis] <= plane) grow(L.lo, L.hi, v0);
+      if (v0[axis] >= plane) grow(R.lo, R.hi, v0);
+      if ((v0[axis] < plane && v1[axis] > plane) || (v0[axis] > plane && v1[axis] < plane)) {
+        const float t = (plane - v0[axis]) / (v1[axis] - v0[axis]);
+        float q[3];
+        for (int k = 0; k < 3; ++k) q[k] = v0[k] + t * (v1[k] - v0[k]);
+        q[axis] = plane;
+        grow(L.lo, L.hi, q);
+        grow(R.lo, R.hi, q);
+      }
+    }
+    L.hi[axis] = std::min(L.hi[axis], plane);
+    R.lo[axis] = std::max(R.lo[axis], plane);
+    for (int k = 0; k < 3; ++k) {
+      L.lo[k] = std::max(L.lo[k], r.lo[k]);
+      L.hi[k] = std::min(L.hi[k], r.hi[k]);
+      R.lo[k] = std::max(R.lo[k], r.lo[k]);
+      R.hi[k] = std::min(R.hi[k], r.hi[k]);
+    }
+    L.g = R.g = r.g;
+  }
+
+  void make_leaf(BNode &nd, const std::vector<Ref> &refs) {
+    const uint64_t first = order_fill.fetch_add(refs.size());
+    for (size_t i = 0; i < refs.size(); ++i) order[first + i] = refs[i].g;
+    nd.first = (uint32_t)first;
+    nd.count = (uint32_t)refs.size();
+    nd.left = 0;
+  }
+
+  // Processes one node: a leaf, or two child tasks in `out`.
+  int split(Task &t, Task out[2]) {
+    BNode &nd = nodes[t.node];
+    std::vector<Ref> &refs = t.refs;
+    const uint32_t cnt = (uint32_t)refs.size();
+    float lo[3], hi[3], clo[3], chi[3];
+    empty_box(lo, hi);
+    empty_box(clo, chi);
+    for (const Ref &r : refs) {
+      grow_box(lo, hi, r.lo, r.hi);
+      float c[3] = {(r.lo[0] + r.hi[0]) * 0.5f, (r.lo[1] + r.hi[1]) * 0.5f, (r.lo[2] + r.hi[2]) * 0.5f};
+      grow(clo, chi, c);
+    }
+    for (int k = 0; k < 3; ++k) {
+      nd.lo[k] = lo[k];
+      nd.hi[k] = hi[k];
+    }
+    uint32_t d = max_depth.load(std::memory_order_relaxed);
+    while (t.depth > d && !max_depth.compare_exchange_weak(d, t.depth)) {
+    }
+    if (cnt <= 1) {
+      make_leaf(nd, refs);
+      return 0;
+    }
+    uint32_t need = 0;
+    for (uint32_t c = cnt; c > kMaxLeaf; c = (c + 1) / 2) ++need;
+    const bool median = t.depth + need >= 56;
+    const float parent = std::max(Builder::area(lo, hi), 1e-30f);
+    // Object split over centroid bins, and (where the object split's
+    // children overlap enough and the reference budget allows) a spatial
+    // split over bins of the node's box; each axis is an independent pass,
+    // run on its own thread for large nodes.
+    struct ObjAxis {
+      float cost = INFINITY, scale = 0.0f, lo_l[3], hi_l[3], lo_r[3], hi_r[3];
+      int bin = 0;
+    } oa[3];
+    struct SpAxis {
+      float cost = INFINITY, plane = 0.0f;
+    } sa[3];
+    auto object_axis = [&](int k) {
+      ObjAxis &res = oa[k];
+      const float span = chi[k] - clo[k];
+      if (!(span > 0.0f)) return;
+      const float sc = (float)kObjBins / span;
+      uint32_t bc[kObjBins] = {};
+      float bl[kObjBins][3], bh[kObjBins][3];
+      for (int b = 0; b < kObjBins; ++b) empty_box(bl[b], bh[b]);
+      for (const Ref &r : refs) {
+        const float c = (r.lo[k] + r.hi[k]) * 0.5f;
+        const int b = std::min(kObjBins - 1, std::max(0, (int)((c - clo[k]) * sc)));
+        bc[b]++;
+        grow_box(bl[b], bh[b], r.lo, r.hi);
+      }
+      float rl[kObjBins][3], rh[kObjBins][3];
+      uint32_t rc[kObjBins];
+      float al[3], ah[3];
+      empty_box(al, ah);
+      uint32_t acc = 0;
+      for (int b = kObjBins - 1; b >= 1; --b) {
+        acc += bc[b];
+        grow_box(al, ah, bl[b], bh[b]);
+        rc[b] = acc;
+        std::copy(al, al + 3, rl[b]);
+        std::copy(ah, ah + 3, rh[b]);
+      }
+      float ll[3], lh[3];
+      empty_box(ll, lh);
+      uint32_t lc = 0;
+      for (int sp = 1; sp < kObjBins; ++sp) {
+        lc += bc[sp - 1];
+        grow_box(ll, lh, bl[sp - 1], bh[sp - 1]);
+        if (lc == 0 || rc[sp] == 0) continue;
+        const float cost =
+            1.0f + (Builder::area(ll, lh) * (float)lc + Builder::area(rl[sp], rh[sp]) * (float)rc[sp]) / parent;
+        if (cost < res.cost) {
+          res.cost = cost;
+          res.bin = sp;
+          res.scale = sc;
+          std::copy(ll, ll + 3, res.lo_l);
+          std::copy(lh, lh + 3, res.hi_l);
+          std::copy(rl[sp], rl[sp] + 3, res.lo_r);
+          std::copy(rh[sp], rh[sp] + 3, res.hi_r);
+        }
+      }
+    };
+    auto spatial_axis = [&](int k) {
+      SpAxis &res = sa[k];
+      const float span = hi[k] - lo[k];
+      if (!(span > 0.0f)) return;
+      const float w = span / (float)kSpatialBins;
+      auto bin_of = [&](float x) { return std::min(kSpatialBins - 1, std::max(0, (int)((x - lo[k]) / w))); };
+      uint32_t entry[kSpatialBins] = {}, exit[kSpatialBins] = {};
+      float bl[kSpatialBins][3], bh[kSpatialBins][3];
+      for (int b = 0; b < kSpatialBins; ++b) empty_box(bl[b], bh[b]);
+      for (const Ref &r : refs) {
+        const int fb = bin_of(r.lo[k]), lb = std::max(fb, bin_of(r.hi[k]));
+        entry[fb]++;
+        exit[lb]++;
+        Ref cur = r;
+        for (int b = fb; b < lb; ++b) {
+          Ref L, R;
+          split_ref(cur, k, lo[k] + w * (float)(b + 1), L, R);
+          if (valid(L.lo, L.hi)) grow_box(bl[b], bh[b], L.lo, L.hi);
+          cur = R;
+          if (!valid(cur.lo, cur.hi)) break;
+        }
+        if (valid(cur.lo, cur.hi)) grow_box(bl[lb], bh[lb], cur.lo, cur.hi);
+      }
+      float rl[kSpatialBins][3], rh[kSpatialBins][3];
+      uint32_t rc[kSpatialBins];
+      float al[3], ah[3];
+      empty_box(al, ah);
+      uint32_t acc = 0;
+      for (int b = kSpatialBins - 1; b >= 1; --b) {
+        acc += exit[b];
+        grow_box(al, ah, bl[b], bh[b]);
+        rc[b] = acc;
+        std::copy(al, al + 3, rl[b]);
+        std::copy(ah, ah + 3, rh[b]);
+      }
+      float ll[3], lh[3];
+      empty_box(ll, lh);
+      uint32_t lc = 0;
+      for (int sp = 1; sp < kSpatialBins; ++sp) {
+        lc += entry[sp - 1];
+        grow_box(ll, lh, bl[sp - 1], bh[sp - 1]);
+        if (lc == 0 || rc[sp] == 0 || !valid(ll, lh) || !valid(rl[sp], rh[sp])) continue;
+        const float cost =
+            1.0f + (Builder::area(ll, lh) * (float)lc + Builder::area(rl[sp], rh[sp]) * (float)rc[sp]) / parent;
+        if (cost < res.cost) {
+          res.cost = cost;
+          res.plane = lo[k] + w * (float)sp;
+        }
+      }
+    };
+    const bool par = cnt >= kParallelNode;
+    auto each_axis = [&](auto &&fn) {
+      if (par) {
+        std::thread t1([&] { fn(1); }), t2([&] { fn(2); });
+        fn(0);
+        t1.join();
+        t2.join();
+      } else {
+        for (int k = 0; k < 3; ++k) fn(k);
+      }
+    };
+    int oaxis = -1, obin = 0;
+    float ocost = INFINITY, oscale = 0.0f;
+    if (!median) {
+      each_axis(object_axis);
+      for (int k = 0; k < 3; ++k)
+        if (oa[k].cost < ocost) {
+          ocost = oa[k].cost;
+          oaxis = k;
+          obin = oa[k].bin;
+          oscale = oa[k].scale;
+        }
+    }
+    int saxis = -1;
+    float scost = INFINITY, splane = 0.0f;
+    if (!median && oaxis >= 0 && t.budget > cnt) {
+      const ObjAxis &o = oa[oaxis];
+      float ilo[3], ihi[3];
+      for (int k = 0; k < 3; ++k) {
+        ilo[k] = std::max(o.lo_l[k], o.lo_r[k]);
+        ihi[k] = std::min(o.hi_l[k], o.hi_r[k]);
+      }
+      const float overlap = valid(ilo, ihi) ? Builder::area(ilo, ihi) : 0.0f;
+      if (overlap > min_overlap) {
+        each_axis(spatial_axis);
+        for (int k = 0; k < 3; ++k)
+          if (sa[k].cost < scost) {
+            scost = sa[k].cost;
+            saxis = k;
+            splane = sa[k].plane;
+          }
+      }
+    }
+    const float best = std::min(ocost, scost);
+    if (cnt <= kMaxLeaf && (oaxis < 0 || (float)cnt <= best)) {
+      make_leaf(nd, refs);
+      return 0;
+    }
+    std::vector<Ref> left, right;
+    if (saxis >= 0 && scost < ocost) {
+      uint64_t straddle = 0;
+      for (const Ref &r : refs)
+        if (r.lo[saxis] < splane && r.hi[saxis] > splane) ++straddle;
+      if (cnt + straddle <= t.budget) {
+        left.reserve(cnt);
+        right.reserve(cnt);
+        for (const Ref &r : refs) {
+          if (r.hi[saxis] <= splane) {
+            left.push_back(r);
+          } else if (r.lo[saxis] >= splane) {
+            right.push_back(r);
+          } else {
+            Ref L, R;
+            split_ref(r, saxis, splane, L, R);
+            const bool vl = valid(L.lo, L.hi), vr = valid(R.lo, R.hi);
+            if (vl) left.push_back(L);
+            if (vr) right.push_back(R);
+            if (!vl && !vr) right.push_back(r);  // degenerate clip: keep the reference whole
+          }
+        }
+        if (left.empty() || right.empty()) {
+          left.clear();
+          right.clear();
+        }
+      }
+    }
+    if (left.empty() && right.empty() && oaxis >= 0) {
+      for (const Ref &r : refs) {
+        const float c = (r.lo[oaxis] + r.hi[oaxis]) * 0.5f;
+        const int b = std::min(kObjBins - 1, std::max(0, (int)((c - clo[oaxis]) * oscale)));
+        (b < obin ? left : right).push_back(r);
+      }
+      if (left.empty() || right.empty()) {
+        left.clear();
+        right.clear();
+      }
+    }
+    if (left.empty() || right.empty()) {
+      // Object median along the widest centroid axis (or index halves).
+      left.clear();
+      right.clear();
+      int ax = 0;
+      float wd = chi[0] - clo[0];
+      for (int k = 1; k < 3; ++k)
+        if (chi[k] - clo[k] > wd) {
+          wd = chi[k] - clo[k];
+          ax = k;
+        }
+      const uint32_t mid = cnt / 2;
+      if (wd > 0.0f)
+        std::nth_element(refs.begin(), refs.begin() + mid, refs.end(), [&](const Ref &a, const Ref &b) {
+          return a.lo[ax] + a.hi[ax] < b.lo[ax] + b.hi[ax];
+        });
+      left.assign(refs.begin(), refs.begin() + mid);
+      right.assign(refs.begin() + mid, refs.end());
+    }
+    std::vector<Ref>().swap(refs);
+    const uint32_t c = node_count.fetch_add(2);
+    nd.left = c;
+    nd.count = 0;
+    const uint64_t nl = left.size(), nr = right.size();
+    const uint64_t bl = std::max<uint64_t>(nl, (uint64_t)((double)t.budget * (double)nl / (double)(nl + nr)));
+    out[0].node = c;
+    out[0].depth = t.depth + 1;
+    out[0].refs = std::move(left);
+    out[0].budget = bl;
+    out[1].node = c + 1;
+    out[1].depth = t.depth + 1;
+    out[1].refs = std::move(right);
+    out[1].budget = std::max<uint64_t>(nr, t.budget > bl ? t.budget - bl : 0);
+    return 2;
+  }
+
+  void local_build(Task t) {
+    std::vector<Task> st;
+    st.push_back(std::move(t));
+    while (!st.empty()) {
+      Task cur = std::move(st.back());
+      st.pop_back();
+      Task ch[2];
+      if (split(cur, ch) == 2) {
+        st.push_back(std::move(ch[1]));
+        st.push_back(std::move(ch[0]));
+      }
+    }
+  }
+
+  void worker() {
+    for (;;) {
+      Task t;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return done || !stack.empty(); });
+        if (stack.empty()) return;
+        t = std::move(stack.back());
+        stack.pop_back();
+        ++active;
+      }
+      if (t.refs.size() <= kLocalThreshold) {
+        local_build(std::move(t));
+      } else {
+        Task ch[2];
+        if (split(t, ch) == 2) {
+          std::lock_guard<std::mutex> lk(mu);
+          stack.push_back(std::move(ch[0]));
+          stack.push_back(std::move(ch[1]));
+          cv.notify_all();
+        }
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        --active;
+        if (active == 0 && stack.empty()) {
+          done = true;
+          cv.notify_all();
+        }
+      }
+    }
+  }
+
+  void run(std::vector<Ref> refs, int threads) {
+    max_refs = (uint64_t)std::ceil(kMaxGrowth * (double)n);
+    order.resize(max_refs);
+    nodes.resize(2 * max_refs + 2);
+    float lo[3], hi[3];
+    empty_box(lo, hi);
+    for (const Ref &r : refs) grow_box(lo, hi, r.lo, r.hi);
+    min_overlap = kAlpha * Builder::area(lo, hi);
+    Task root{0, 0, std::move(refs), max_refs};
+    if (threads <= 1 || root.refs.size() <= kLocalThreshold) {
+      local_build(std::move(root));
+    } else {
+      stack.push_back(std::move(root));
+      std::vector<std::thread> pool;
+      for (int i = 0; i < threads; ++i) pool.emplace_back([this] { worker(); });
+      for (auto &th : pool) th.join();
+    }
+    nodes.resize(node_count.load());
+    order.resize(order_fill.load());
+  }
+};
+
+// Lays out a built binary tree (`nodes`, leaves indexing `order`, the
+// global triangle id of each leaf slot) as two-child nodes, four-child nodes
+// and leaf-ordered triangle records.
+void emit_tree(const std::vector<BNode> &nodes, const std::vector<uint32_t> &order, uint32_t max_depth,
+               const float *pos, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
+               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats);
+
 }  // namespace
 
 void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
@@ -466,11 +910,69 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
   }
   b.wide = std::max(1, threads);
   b.run(std::max(1, threads));
+  std::vector<uint32_t> order(tri_count);
+  for (size_t i = 0; i < tri_count; ++i) order[i] = b.prims[i].g;
+  emit_tree(b.nodes, order, b.max_depth.load(), pos, rec_flags, out_nodes, out_nodes4, records, stats);
+  stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
+void build_bvh_spatial(const float *pos, uint32_t tri_count, const uint32_t *rec_flags,
+                       std::vector<BvhNode> &out_nodes, std::vector<Bvh4Node> &out_nodes4,
+                       std::vector<float4> &records, BvhBuildStats &stats, int threads) {
+  auto t0 = std::chrono::steady_clock::now();
+  out_nodes.clear();
+  out_nodes4.clear();
+  records.clear();
+  stats = BvhBuildStats{};
+  if (tri_count == 0) return;
+  SpatialBuilder b;
+  b.pos = pos;
+  b.n = tri_count;
+  std::vector<SpatialBuilder::Ref> refs(tri_count);
+  for (size_t g = 0; g < tri_count; ++g) {
+    const float *p = pos + 9 * g;
+    SpatialBuilder::Ref &r = refs[g];
+    r.g = (uint32_t)g;
+    for (int k = 0; k < 3; ++k) {
+      r.lo[k] = std::min({p[k], p[3 + k], p[6 + k]});
+      r.hi[k] = std::max({p[k], p[3 + k], p[6 + k]});
+    }
+  }
+  b.run(std::move(refs), std::max(1, threads));
+  emit_tree(b.nodes, b.order, b.max_depth.load(), pos, rec_flags, out_nodes, out_nodes4, records, stats);
+  stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+namespace {
+
+void emit_tree(const std::vector<BNode> &in_nodes, const std::vector<uint32_t> &in_order, uint32_t max_depth,
+               const float *pos, const uint32_t *rec_flags, std::vector<BvhNode> &out_nodes,
+               std::vector<Bvh4Node> &out_nodes4, std::vector<float4> &records, BvhBuildStats &stats) {
+  // Records in depth-first leaf order (left child first), whatever order
+  // the builder's threads filled `in_order` in: the layout is deterministic
+  // and a subtree's triangles are contiguous.
+  std::vector<BNode> nodes(in_nodes);
+  std::vector<uint32_t> order;
+  order.reserve(in_order.size());
+  {
+    std::vector<uint32_t> st{0};
+    while (!st.empty()) {
+      BNode &nd = nodes[st.back()];
+      st.pop_back();
+      if (nd.count > 0) {
+        const uint32_t first = (uint32_t)order.size();
+        order.insert(order.end(), in_order.begin() + nd.first, in_order.begin() + nd.first + nd.count);
+        nd.first = first;
+      } else {
+        st.push_back(nd.left + 1);
+        st.push_back(nd.left);
+      }
+    }
+  }
   // Depth-first two-child layout.
   auto leaf_ref = [](uint32_t first, uint32_t count) { return (int)~(first | (count << 27)); };
   std::vector<uint32_t> gstack;
-  const BNode &root = b.nodes[0];
+  const BNode &root = nodes[0];
   auto child_box = [&](const BNode &c, float lo[3], float hi[3]) { pad_box(c.lo, c.hi, lo, hi); };
   auto fill = [&](BvhNode &gn, const BNode &c0, const BNode &c1, int r0, int r1) {
     float l0[3], h0[3], l1[3], h1[3];
@@ -499,9 +1001,9 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
     while (!st.empty()) {
       Item it = st.back();
       st.pop_back();
-      const BNode &nd = b.nodes[it.bin];
-      const BNode &c0 = b.nodes[nd.left];
-      const BNode &c1 = b.nodes[nd.left + 1];
+      const BNode &nd = nodes[it.bin];
+      const BNode &c0 = nodes[nd.left];
+      const BNode &c1 = nodes[nd.left + 1];
       int r[2];
       const BNode *cs[2] = {&c0, &c1};
       for (int k = 0; k < 2; ++k) {
@@ -546,14 +1048,14 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
       while (!st.empty()) {
         Item it = st.back();
         st.pop_back();
-        const BNode &nd = b.nodes[it.bin];
+        const BNode &nd = nodes[it.bin];
         uint32_t ch[4] = {nd.left, nd.left + 1, 0, 0};
         int nch = 2;
         while (nch < 4) {
           int best = -1;
           float best_area = -1.0f;
           for (int i = 0; i < nch; ++i) {
-            const BNode &c = b.nodes[ch[i]];
+            const BNode &c = nodes[ch[i]];
             if (c.count > 0) continue;
             float a = Builder::area(c.lo, c.hi);
             if (a > best_area) {
@@ -564,8 +1066,8 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
           if (best < 0) break;
           uint32_t opened = ch[best];
           for (int i = nch; i > best + 1; --i) ch[i] = ch[i - 1];
-          ch[best] = b.nodes[opened].left;
-          ch[best + 1] = b.nodes[opened].left + 1;
+          ch[best] = nodes[opened].left;
+          ch[best + 1] = nodes[opened].left + 1;
           ++nch;
         }
         std::vector<Item> next;
@@ -574,7 +1076,7 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
             set_child(out_nodes4[it.gpu], k, nullptr, kEmptyChild);
             continue;
           }
-          const BNode &c = b.nodes[ch[k]];
+          const BNode &c = nodes[ch[k]];
           int ref;
           if (c.count > 0) {
             ref = leaf_ref(c.first, c.count);
@@ -590,9 +1092,9 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
       }
     }
   }
-  records.resize(3 * (size_t)tri_count);
-  for (size_t i = 0; i < tri_count; ++i) {
-    uint32_t g = b.prims[i].g;
+  records.resize(3 * order.size());
+  for (size_t i = 0; i < order.size(); ++i) {
+    uint32_t g = order[i];
     const float *p = pos + 9 * (size_t)g;
     float gid, fl;
     std::memcpy(&gid, &g, 4);
@@ -603,17 +1105,19 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
     records[3 * i + 2] = make_float4(p[6], p[7], p[8], 0.0f);
   }
   stats.nodes = (uint32_t)out_nodes.size();
-  stats.max_depth = b.max_depth.load();
+  stats.max_depth = max_depth;
+  stats.references = (uint64_t)order.size();
   // SAH cost of the tree (traversal 1, intersection 1, relative to the root box).
-  double root_area = Builder::area(b.nodes[0].lo, b.nodes[0].hi);
+  double root_area = Builder::area(nodes[0].lo, nodes[0].hi);
   double cost = 0.0;
-  for (const BNode &nd : b.nodes) {
+  for (const BNode &nd : nodes) {
     double a = Builder::area(nd.lo, nd.hi) / std::max(root_area, 1e-30);
     cost += nd.count > 0 ? a * nd.count : a;
   }
   stats.sah_cost = cost;
-  stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
+
+}  // namespace
 
 // ============================================================ arena
 void DeviceArena::release() {
@@ -747,7 +1251,8 @@ void HostStaging::release() {
   cap = 0;
 }
 
-std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh, HostStaging *staging) {
+std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh, HostStaging *staging,
+                              bool spatial) {
   using clk = std::chrono::steady_clock;
   const auto t_start = clk::now();
   auto since = [](clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); };
@@ -1047,7 +1552,10 @@ std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool w
   // BVH (host build) from the positions now in the blob.
   const auto t_bvh = clk::now();
   const float *pos = reinterpret_cast<const float *>(dst + plan.off[p_pos]);
-  if (with_bvh) build_bvh(pos, tc, rec_flags.data(), img.tree.nodes, img.tree.nodes4, img.tree.records, img.bvh, threads);
+  if (with_bvh && spatial)
+    build_bvh_spatial(pos, tc, rec_flags.data(), img.tree.nodes, img.tree.nodes4, img.tree.records, img.bvh, threads);
+  else if (with_bvh)
+    build_bvh(pos, tc, rec_flags.data(), img.tree.nodes, img.tree.nodes4, img.tree.records, img.bvh, threads);
   img.seconds[2] = since(t_bvh);
   img.textures = texs;
   img.tex_src_off = plan.off[p_src];
@@ -1248,7 +1756,7 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
   }
   SceneImage img;
   const auto t1 = clk::now();
-  std::string err = build_scene_image(desc, img);
+  std::string err = build_scene_image(desc, img, true, nullptr, builder == BVH_BUILD_HOST_SPATIAL);
   if (!err.empty()) return err;
   const auto t2 = clk::now();
   err = commit_scene(img, out, oom);

@@ -18,6 +18,7 @@ namespace ptd {
 struct BvhBuildStats {
   uint32_t nodes = 0, leaves = 0, max_depth = 0;
   double sah_cost = 0.0, seconds = 0.0;
+  uint64_t references = 0;  // triangle records (above the triangle count with spatial splits)
 };
 
 // Binned-SAH BVH over the soup (positions: 9 floats per triangle), laid out
@@ -26,6 +27,13 @@ struct BvhBuildStats {
 // `rec_flags[g]` goes into each record (REC_* bits).
 void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, std::vector<BvhNode> &nodes,
                std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads);
+// The same outputs from a spatial-split BVH: fewer overlapping leaves for
+// scenes of many small overlapping triangles, at a few times the build time
+// and up to 1.6x the triangle records (a triangle cut by split planes is
+// referenced from several leaves).
+void build_bvh_spatial(const float *pos, uint32_t tri_count, const uint32_t *rec_flags,
+                       std::vector<BvhNode> &nodes, std::vector<Bvh4Node> &nodes4, std::vector<float4> &records,
+                       BvhBuildStats &stats, int threads);
 
 // One device allocation holding a scene (or an environment) plus the
 // device copy of its descriptor. `stream` non-null: the allocation is
@@ -124,8 +132,9 @@ struct SceneHost {
 // Validates `desc` and builds its device image on the host. Returns an
 // empty string on success, else an error message. `with_bvh` false leaves
 // the BVH parts out (node counts 0) for a build on the device.
+// `spatial` builds the spatial-split tree (build_bvh_spatial) instead.
 std::string build_scene_image(const pt_scene_desc &desc, SceneImage &img, bool with_bvh = true,
-                              HostStaging *staging = nullptr);
+                              HostStaging *staging = nullptr, bool spatial = false);
 // Allocates the arena and copies `img` into it (stream-ordered when `stream`
 // is non-null). `oom` is set when the failure was a device allocation.
 std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaStream_t stream = nullptr);
@@ -137,7 +146,15 @@ constexpr uint32_t kMaxTreeDepth = 56;
 // on the device with the binned-SAH rule (the host builder's tree, in
 // milliseconds), smaller ones on the host. BVH_BUILD_DEVICE_PLOC clusters
 // on the device instead (faster to build, 3-12 % more node visits).
-enum BvhBuilder : int { BVH_BUILD_AUTO = 0, BVH_BUILD_HOST = 1, BVH_BUILD_DEVICE = 2, BVH_BUILD_DEVICE_PLOC = 3 };
+// BVH_BUILD_HOST_SPATIAL builds the spatial-split tree on the host (seconds
+// for large soups; for scenes that stay resident).
+enum BvhBuilder : int {
+  BVH_BUILD_AUTO = 0,
+  BVH_BUILD_HOST = 1,
+  BVH_BUILD_DEVICE = 2,
+  BVH_BUILD_DEVICE_PLOC = 3,
+  BVH_BUILD_HOST_SPATIAL = 4
+};
 constexpr uint64_t kAutoDeviceBuildTris = 16384;
 // build_scene_image + commit_scene, with the BVH built where `builder`
 // says (`stream`: the device build's stream). A device-built tree deeper

@@ -185,6 +185,7 @@ struct pt_server {
   uint64_t tick = 0;
   uint32_t accum_count = 0;
   bool autotune = false;
+  bool spatial_bvh = true;    // registered scenes get the spatial-split tree
   bool tune_pending = false;  // a request waits for an idle stream to tune its class
   uint64_t rays_base = 0;     // rays counted before the device counters were last cleared
   // Overlapped waves (wavefront engine): consecutive waves are traced in the
@@ -765,6 +766,7 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
       s->eng->overlap_arenas = 0;
     }
     s->autotune = c.autotune != 0;
+    s->spatial_bvh = c.bvh_binned == 0;
     s->flights.resize(s->depth + 1);
     cudaError_t e = cudaSuccess;
     for (Flight &f : s->flights) {
@@ -840,7 +842,7 @@ pt_status pt_server_scene_register(pt_server *s, const pt_scene_desc *desc, cons
   if (!s || !desc || !key) return sfail(PT_ERR_INVALID_ARG, "server / desc / scene_key is NULL");
   return sguard([&]() -> pt_status {
     auto e = std::make_shared<SceneEntry>();
-    std::string err = build_scene_image(*desc, e->img);
+    std::string err = build_scene_image(*desc, e->img, true, nullptr, s->spatial_bvh);
     if (!err.empty()) return sfail(PT_ERR_INVALID_ARG, err);
     e->est_bytes = e->img.device_bytes();
     if (env) {

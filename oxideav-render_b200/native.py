@@ -81,6 +81,7 @@ SIGNATURES = {
     "pt_server_stats_get": (i32, [vp, C.POINTER(abi.pt_server_stats)]),
     # include/pt_b200_debug.h
     "pt_set_bvh_builder": (i32, [vp, u32]),
+    "pt_debug_build_bvh": (i32, [fp, u32, u32, dp, vp, u64, vp, u64]),
     "pt_scene_bvh_on_device": (i32, [vp, u32, C.POINTER(C.c_int)]),
     "pt_scene_upload_seconds": (i32, [vp, u32, dp]),
     "pt_debug_scene_texels": (i32, [vp, u32, fp, u64, u64p]),

@@ -24,12 +24,12 @@ from .scene import Camera, PreparedScene
 class RenderServer:
     def __init__(self, ctx: Optional[Context] = None, hbm_budget_bytes: int = 0, wave_slots: int = 0,
                  max_active: int = 0, megakernel: bool = False, pipeline_depth: int = 0, autotune: bool = False,
-                 material_sort: bool = True, wave_overlap: bool = True):
+                 material_sort: bool = True, wave_overlap: bool = True, spatial_bvh: bool = True):
         self.ctx = ctx or default_context()
         self.lib = native.load()
         cfg = abi.pt_server_config(int(hbm_budget_bytes), int(wave_slots), int(max_active), 1 if megakernel else 0,
                                    int(pipeline_depth), 0, 0, 1 if autotune else 0, 0 if material_sort else 1,
-                                   0 if wave_overlap else 1)
+                                   0 if wave_overlap else 1, 0 if spatial_bvh else 1)
         p = C.c_void_p()
         st = self.lib.pt_server_create(self.ctx.ptr, C.byref(cfg), C.byref(p))
         if st != abi.PT_OK:

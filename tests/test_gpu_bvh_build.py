@@ -157,3 +157,21 @@ def test_hostile_geometry_on_every_builder(ctx):
         assert on_device and st["max_depth"] <= 56
         assert np.array_equal(a, b), builder
         assert rb == ra
+
+
+@pytest.mark.parametrize("name", ["spheres", "soup", "env", "alpha"])
+def test_spatial_split_tree_renders_identically(ctx, name):
+    # The spatial-split tree (a triangle referenced from several leaves, with
+    # clipped leaf bounds) gives the host tree's accumulator bit for bit, on
+    # both schedules; on the soup it holds more records than triangles.
+    scene, opts, env = case(name)
+    a, ra, sa, _ = render(ctx, abi.PT_BVH_BUILD_HOST, scene, opts, env, 1)
+    for schedule in (0, 1):
+        b, rb, sb, db = render(ctx, abi.PT_BVH_BUILD_HOST_SPATIAL, scene, opts, env, schedule)
+        assert not db
+        assert np.array_equal(a, b), (name, schedule)
+        assert ra == rb
+        assert 0 < sb["max_depth"] <= 56
+    if name == "soup":
+        assert sb["nodes"] > sa["nodes"]
+        assert sb["sah_cost"] < sa["sah_cost"]
