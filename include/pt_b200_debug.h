@@ -53,6 +53,12 @@ PT_API pt_status pt_batch_stage_ms(const pt_context *ctx, float *out, uint32_t n
  * (three small kernels per bounce; on by default). Images are identical
  * either way. */
 PT_API pt_status pt_set_material_sort(pt_context *ctx, int on);
+/* Traversal kernels (closest hit and shadow rays): `threads` per block (128
+ * or 256; 1,024 threads per SM either way) and `claim_chunk` queue entries
+ * a lane claims per refill (1, 2 or 4: fewer atomics, coarser load
+ * balance). Defaults 256 and 1. Images are identical whatever the setting;
+ * pt_autotune tries both knobs on its winning configuration. */
+PT_API pt_status pt_set_traversal(pt_context *ctx, uint32_t threads, uint32_t claim_chunk);
 /* Overlapped waves (default on): a refine of two or more waves traces
  * consecutive waves in several path-state arenas on as many streams, so one
  * wave's last bounces (few paths, most of the GPU idle) run beside the next
@@ -86,10 +92,13 @@ typedef struct pt_tune_choice {
   float samples_per_s;           /* calibration throughput */
   uint32_t shade_blocks_per_sm;  /* 3 or 4: the shade kernel's occupancy */
   uint32_t wave_arenas;          /* 2 or 3: overlapped waves in flight (pt_set_wave_overlap) */
+  uint32_t traversal_threads;    /* 128 or 256: block size of the traversal kernels (pt_set_traversal) */
+  uint32_t claim_chunk;          /* 1, 2 or 4: queue entries a traversal lane claims per refill */
 } pt_tune_choice;
 /* Times every candidate (megakernel; wavefront x node widths x material sort
  * x wave size; then the winner with the shade kernel at 4 instead of 3
- * blocks per SM, and with 2 or 3 waves in flight over four waves) on a
+ * blocks per SM, with 128-thread traversal blocks or 2 / 4 queue entries per
+ * lane refill, and with 2 or 3 waves in flight over eight waves) on a
  * calibration refine of `samples` spp (0: one full wave of
  * 8,388,608 paths, capped at 4096 spp) of the tracer's
  * scene, camera and options (a scratch accumulator: the tracer's own is

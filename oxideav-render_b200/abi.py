@@ -323,6 +323,8 @@ class pt_tune_choice(C.Structure):
         ("samples_per_s", C.c_float),
         ("shade_blocks_per_sm", C.c_uint32),
         ("wave_arenas", C.c_uint32),
+        ("traversal_threads", C.c_uint32),
+        ("claim_chunk", C.c_uint32),
     ]
 
 

@@ -147,6 +147,11 @@ class Context:
         """Occupancy of the wavefront shade kernel (3 or 4 blocks per SM)."""
         self.check(self.lib.pt_set_shade_blocks(self.ptr, int(blocks_per_sm)))
 
+    def set_traversal(self, threads: int = 256, claim_chunk: int = 1) -> None:
+        """pt_set_traversal: traversal kernels' block size (128 / 256) and
+        queue entries per lane refill (1 / 2 / 4)."""
+        self.check(self.lib.pt_set_traversal(self.ptr, int(threads), int(claim_chunk)))
+
     def set_node_width(self, extension: int, shadow: int) -> None:
         """BVH node layout (2 or 4 children) of extension and shadow rays."""
         self.check(self.lib.pt_set_node_width(self.ptr, extension, shadow))

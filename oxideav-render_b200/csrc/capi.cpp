@@ -409,16 +409,19 @@ pt_status add_job(pt_context *ctx, pt_tracer *t, uint32_t n, std::vector<pt_trac
 // restores the context's own afterwards.
 struct KnobScope {
   pt_context *ctx;
-  uint32_t schedule, wave_slots, shade_blocks, arenas;
+  uint32_t schedule, wave_slots, shade_blocks, arenas, trav_threads, claim_chunk;
   bool sort;
   KnobScope(pt_context *c, const TuneChoice *tc)
       : ctx(c), schedule(c->schedule), wave_slots(c->wave_slots), shade_blocks(c->shade_blocks),
-        arenas(c->overlap_arenas), sort(c->material_sort) {
+        arenas(c->overlap_arenas), trav_threads(c->trav_threads), claim_chunk(c->claim_chunk),
+        sort(c->material_sort) {
     if (tc) {
       c->schedule = tc->schedule;
       c->wave_slots = tc->wave_slots;
       c->material_sort = tc->material_sort != 0;
       c->shade_blocks = tc->shade_blocks;
+      c->trav_threads = tc->trav_threads;
+      c->claim_chunk = tc->claim_chunk;
       // The tuned number of waves in flight, unless overlap is switched off
       // or its count was set explicitly.
       if (c->overlap_waves && !c->overlap_fixed) c->overlap_arenas = tc->arenas;
@@ -430,6 +433,8 @@ struct KnobScope {
     ctx->material_sort = sort;
     ctx->shade_blocks = shade_blocks;
     ctx->overlap_arenas = arenas;
+    ctx->trav_threads = trav_threads;
+    ctx->claim_chunk = claim_chunk;
   }
 };
 
@@ -493,6 +498,8 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
     ctx->wave_slots = c.wave_slots;
     ctx->material_sort = c.material_sort != 0;
     ctx->shade_blocks = c.shade_blocks;
+    ctx->trav_threads = c.trav_threads;
+    ctx->claim_chunk = c.claim_chunk;
     if (ctx->overlap_waves) ctx->overlap_arenas = c.arenas;
     ms = -1.0f;
     for (int rep = 0; rep < 2; ++rep) {
@@ -526,6 +533,17 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
     if (ms < best_ms) {
       best_ms = ms;
       best = c;
+    }
+    // The traversal kernels' block size and refill chunk on the winner.
+    for (auto tc2 : {std::make_pair(128u, 1u), std::make_pair(256u, 2u), std::make_pair(256u, 4u)}) {
+      TuneChoice t = best;
+      t.trav_threads = tc2.first;
+      t.claim_chunk = tc2.second;
+      if ((st = time_choice(t, ms, samples)) != PT_OK) return st;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = t;
+      }
     }
     if (ctx->overlap_waves) {
       // Waves in flight: measured on eight waves (one cannot overlap, and
@@ -709,6 +727,8 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
     w.iterations = iters;
     w.sort_materials = ctx->material_sort ? 1u : 0u;
     w.shade_blocks = ctx->shade_blocks == 4 ? 4u : 3u;
+    w.trav_threads = ctx->trav_threads == 128 ? 128u : 256u;
+    w.claim_chunk = ctx->claim_chunk == 2 || ctx->claim_chunk == 4 ? ctx->claim_chunk : 1u;
     cudaStream_t ws = own_stream ? ctx->wave_streams[arena] : ctx->stream;
     // The arena's previous wave must be accumulated before this one
     // overwrites its descriptor, queues and per-slot radiance.
@@ -722,8 +742,9 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
       // One captured graph per (bounce count, arena / whole wave, shade
       // variant, material sort) replays the wave: one launch instead of ~6
       // per bounce.
-      const uint32_t key = iters << 5 | (own_stream ? 4u * (1u + (uint32_t)arena) : 0u) |
-                           (w.shade_blocks == 4 ? 2u : 0u) | w.sort_materials;
+      const uint32_t key = iters << 10 | w.claim_chunk << 7 | (w.trav_threads == 128 ? 64u : 0u) |
+                           (own_stream ? 4u * (1u + (uint32_t)arena) : 0u) | (w.shade_blocks == 4 ? 2u : 0u) |
+                           w.sort_materials;
       auto it = ctx->graphs.find(key);
       if (it == ctx->graphs.end()) {
         cudaGraphExec_t ge = nullptr;
@@ -1231,6 +1252,8 @@ pt_tune_choice to_c(const TuneChoice &c) {
   o.wave_arenas = c.arenas;
   o.wave_slots = c.wave_slots;
   o.samples_per_s = c.samples_per_s;
+  o.traversal_threads = c.trav_threads;
+  o.claim_chunk = c.claim_chunk;
   return o;
 }
 }  // namespace
@@ -1323,6 +1346,14 @@ pt_status pt_set_shade_blocks(pt_context *ctx, uint32_t blocks_per_sm) {
   if (!ctx || (blocks_per_sm != 3 && blocks_per_sm != 4))
     return fail(ctx, PT_ERR_INVALID_ARG, "shade blocks per SM must be 3 or 4");
   ctx->shade_blocks = blocks_per_sm;
+  return PT_OK;
+}
+
+pt_status pt_set_traversal(pt_context *ctx, uint32_t threads, uint32_t claim_chunk) {
+  if (!ctx || (threads != 128 && threads != 256) || (claim_chunk != 1 && claim_chunk != 2 && claim_chunk != 4))
+    return fail(ctx, PT_ERR_INVALID_ARG, "traversal threads must be 128 or 256 and the claim chunk 1, 2 or 4");
+  ctx->trav_threads = threads;
+  ctx->claim_chunk = claim_chunk;
   return PT_OK;
 }
 

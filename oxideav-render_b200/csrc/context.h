@@ -22,6 +22,8 @@ struct TuneChoice {
   float samples_per_s;
   uint32_t shade_blocks = 3;  // k_wf_shade blocks per SM (3 or 4)
   uint32_t arenas = 2;        // overlapped waves in flight (2 or 3)
+  uint32_t trav_threads = 256;  // traversal kernels' block size (128 or 256)
+  uint32_t claim_chunk = 1;     // queue entries per traversal refill (1, 2, 4)
 };
 }  // namespace ptd
 
@@ -42,6 +44,8 @@ struct pt_context {
   uint32_t wide_nodes = ptd::WIDE_EXTENSION | ptd::WIDE_SHADOW;
   bool material_sort = true;  // bucket each shade queue by material
   uint32_t shade_blocks = 3;   // k_wf_shade instantiation: blocks per SM (3 or 4)
+  uint32_t trav_threads = 256;  // traversal kernels' block size (128 or 256; 1,024 threads per SM)
+  uint32_t claim_chunk = 1;     // queue entries a traversal lane claims per refill (1, 2 or 4)
   int bvh_builder = ptd::BVH_BUILD_AUTO;  // where pt_scene_upload builds the BVH (ptd::BvhBuilder)
   ptd::HostStaging staging;  // pinned host image buffer of pt_scene_upload
   std::map<uint32_t, ptd::TuneChoice> tuned;  // by scene class (ptd::scene_class)

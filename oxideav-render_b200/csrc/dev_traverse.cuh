@@ -281,20 +281,40 @@ struct ShadowTrav {
   PT_DEV bool done() const { return occluded || core.finished(); }
 };
 
-// Warp-aggregated claim of queue entries for the lanes with `need`; returns
-// this lane's entry index (meaningful when `need`). `exhausted` turns true
-// (warp-uniformly) once the claims pass `n`, after which no atomics are
-// issued.
-PT_DEV uint32_t warp_claim(uint32_t *counter, bool need, uint32_t n, bool &exhausted) {
+// Warp-aggregated claim of `chunk` consecutive queue entries for each lane
+// with `need`; returns this lane's first entry index (meaningful when
+// `need`). `exhausted` turns true (warp-uniformly) once the claims pass `n`,
+// after which no atomics are issued.
+PT_DEV uint32_t warp_claim(uint32_t *counter, bool need, uint32_t n, bool &exhausted, uint32_t chunk = 1) {
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t mask = __ballot_sync(0xffffffffu, need);
   if (mask == 0 || exhausted) return 0xffffffffu;
   uint32_t leader = __ffs(mask) - 1;
   uint32_t base = 0;
-  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask) * chunk);
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (base + (uint32_t)__popc(mask) >= n) exhausted = true;
-  return base + __popc(mask & ((1u << lane) - 1u));
+  if (base + (uint32_t)__popc(mask) * chunk >= n) exhausted = true;
+  return base + (uint32_t)__popc(mask & ((1u << lane) - 1u)) * chunk;
 }
+
+// A lane's claimed queue entries not yet started: entries [next, next + left).
+struct ClaimedRun {
+  uint32_t next = 0, left = 0;
+  // Refills the run (warp-collective: every lane calls it) for lanes with
+  // no ray and no entries left, then hands out this lane's next entry in
+  // `idx` when it has no ray. Returns whether a new entry was taken.
+  PT_DEV bool take(uint32_t *counter, bool has, uint32_t n, bool &exhausted, uint32_t chunk, uint32_t &idx) {
+    const bool need = !has && left == 0;
+    const uint32_t first = warp_claim(counter, need, n, exhausted, chunk);
+    if (need && first < n) {
+      next = first;
+      left = min(chunk, n - first);
+    }
+    if (has || left == 0) return false;
+    idx = next++;
+    --left;
+    return true;
+  }
+};
 
 }  // namespace ptd

@@ -157,6 +157,8 @@ struct WaveBuffers {
   struct WaveDesc *desc;       // this wave's requests and segments (written before each wave)
   uint32_t capacity, shadow_slots, iterations, sort_materials;
   uint32_t shade_blocks;       // 3 or 4: the k_wf_shade instantiation (blocks per SM)
+  uint32_t trav_threads;       // 128 or 256: block size of the traversal kernels (1,024 threads per SM)
+  uint32_t claim_chunk;        // 1, 2 or 4: queue entries a traversal lane claims per refill
 };
 
 // What changes from one wave to the next, read by the kernels from device

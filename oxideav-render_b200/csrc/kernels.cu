@@ -308,14 +308,22 @@ cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, u
 // extend / shade / shadow over device-side queue counters (no host sync).
 // The traversal kernels are persistent: exactly the blocks that fit at once
 // (occupancy queried once, outside any stream capture).
-void persistent_blocks(int &per_sm_ext, int &per_sm_sh) {
-  static int ext = 0, sh = 0;
-  if (ext == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ext, k_wf_extend, 256, 0) != cudaSuccess || ext < 1) ext = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sh, k_wf_shadow, 256, 0) != cudaSuccess || sh < 1) sh = 1;
+// Index 0: the 256-thread instantiations, 1: the 128-thread ones.
+void persistent_blocks(int per_sm_ext[2], int per_sm_sh[2]) {
+  static int ext[2] = {0, 0}, sh[2] = {0, 0};
+  if (ext[0] == 0) {
+    auto q = [](int &v, const void *fn, int threads) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, fn, threads, 0) != cudaSuccess || v < 1) v = 1;
+    };
+    q(ext[0], (const void *)k_wf_extend<256>, 256);
+    q(sh[0], (const void *)k_wf_shadow<256>, 256);
+    q(ext[1], (const void *)k_wf_extend<128>, 128);
+    q(sh[1], (const void *)k_wf_shadow<128>, 128);
   }
-  per_sm_ext = ext;
-  per_sm_sh = sh;
+  for (int k = 0; k < 2; ++k) {
+    per_sm_ext[k] = ext[k];
+    per_sm_sh[k] = sh[k];
+  }
 }
 
 cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
@@ -326,16 +334,21 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
   if (e == cudaSuccess && w.sort_materials)
     e = cudaMemsetAsync(w.sort_counts, 0, sizeof(uint32_t) * 2 * kSortBuckets * (w.iterations + 1), st);
   if (e != cudaSuccess) return e;
-  int per_sm_ext, per_sm_sh;
+  int per_sm_ext[2], per_sm_sh[2];
   persistent_blocks(per_sm_ext, per_sm_sh);
   const bool shade4 = w.shade_blocks == 4;
-  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext), g_shade = (uint32_t)num_sms * (shade4 ? 8 : 6),
-                 g_sh = (uint32_t)(num_sms * per_sm_sh), g_wide = (uint32_t)num_sms * 16;
+  const bool t128 = w.trav_threads == 128;
+  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext[t128 ? 1 : 0]),
+                 g_shade = (uint32_t)num_sms * (shade4 ? 8 : 6),
+                 g_sh = (uint32_t)(num_sms * per_sm_sh[t128 ? 1 : 0]), g_wide = (uint32_t)num_sms * 16;
   tm.mark(STAGE_RAYGEN, st);
   k_wf_raygen<<<g_wide, 256, 0, st>>>(w);
   for (uint32_t it = 0; it < w.iterations; ++it) {
     tm.mark(STAGE_EXTEND, st);
-    k_wf_extend<<<g_ext, 256, 0, st>>>(w, it, ctr);
+    if (t128)
+      k_wf_extend<128><<<g_ext, 128, 0, st>>>(w, it, ctr);
+    else
+      k_wf_extend<256><<<g_ext, 256, 0, st>>>(w, it, ctr);
     if (w.sort_materials) {
       tm.mark(STAGE_SORT, st);
       k_wf_sort_count<<<g_shade, 256, 0, st>>>(w, it);
@@ -348,7 +361,10 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
     else
       k_wf_shade<3><<<g_shade, 128, 0, st>>>(w, it);
     tm.mark(STAGE_SHADOW, st);
-    k_wf_shadow<<<g_sh, 256, 0, st>>>(w, it, ctr);
+    if (t128)
+      k_wf_shadow<128><<<g_sh, 128, 0, st>>>(w, it, ctr);
+    else
+      k_wf_shadow<256><<<g_sh, 256, 0, st>>>(w, it, ctr);
   }
   if (accumulate) {
     tm.mark(STAGE_ACCUMULATE, st);
@@ -365,7 +381,7 @@ cudaError_t launch_wave_accumulate(const WaveBuffers &w, int num_sms, cudaStream
 cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out,
                               bool accumulate) {
   *out = nullptr;
-  int a, b;
+  int a[2], b[2];
   persistent_blocks(a, b);
   cudaStream_t cs = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);

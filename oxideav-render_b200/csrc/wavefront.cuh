@@ -166,11 +166,13 @@ PT_DEV uint32_t sort_key(const DevScene *s, bool found, uint32_t g) {
 }
 
 // Closest hit of every queued path: persistent lanes, one ray each, refilled
-// from the queue as rays finish (dev_traverse.cuh).
-__global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t iter,
-                                                   DevCounters *ctr) {
+// from the queue as rays finish (dev_traverse.cuh), in runs of
+// w.claim_chunk entries. kThreads per block, 1,024 threads per SM.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_extend(WaveBuffers w, uint32_t iter,
+                                                                       DevCounters *ctr) {
   const DevRequest *reqs = w.desc->reqs;
-  __shared__ int s_stack[kShortStack * 256];
+  __shared__ int s_stack[kShortStack * kThreads];
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.q[iter & 1u];
   uint32_t *claim = w.counters + iter * kWfCounterStride + 2;
@@ -183,9 +185,10 @@ __global__ void __launch_bounds__(256, 4) k_wf_extend(WaveBuffers w, uint32_t it
   const DevRequest *rq = nullptr;
   Sampler smp;
   ClosestRay cr;
+  ClaimedRun run;
   for (;;) {
-    uint32_t idx = warp_claim(claim, !has, n, exhausted);
-    if (!has && idx < n) {
+    uint32_t idx = 0;
+    if (run.take(claim, has, n, exhausted, w.claim_chunk, idx)) {
       qpos = idx;
       slot = q[idx];
       float4 o = w.o[slot], d = w.d[slot];
@@ -339,11 +342,13 @@ __global__ void __launch_bounds__(128, kBlocks) k_wf_shade(WaveBuffers w, uint32
 // Shadow rays of every queued path, each path's rays in generation order
 // (a visible ray adds its contribution to the path radiance, so the float
 // sum rounds as in the megakernel). Persistent lanes own one path at a time
-// and are refilled from the queue when its last ray finishes.
-__global__ void __launch_bounds__(256, 4) k_wf_shadow(WaveBuffers w, uint32_t iter,
-                                                   DevCounters *ctr) {
+// and are refilled from the queue when its last ray finishes (runs of
+// w.claim_chunk entries). kThreads per block, 1,024 threads per SM.
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_shadow(WaveBuffers w, uint32_t iter,
+                                                                       DevCounters *ctr) {
   const DevRequest *reqs = w.desc->reqs;
-  __shared__ int s_stack[kShortStack * 256];
+  __shared__ int s_stack[kShortStack * kThreads];
   const uint32_t n = w.counters[iter * kWfCounterStride + 1];
   uint32_t *claim = w.counters + iter * kWfCounterStride + 3;
   TravStack stk;
@@ -366,9 +371,10 @@ __global__ void __launch_bounds__(256, 4) k_wf_shadow(WaveBuffers w, uint32_t it
     skip = __float_as_uint(sc.w);
     ts.shadow_rays++;
   };
+  ClaimedRun run;
   for (;;) {
-    uint32_t idx = warp_claim(claim, !has, n, exhausted);
-    if (!has && idx < n) {
+    uint32_t idx = 0;
+    if (run.take(claim, has, n, exhausted, w.claim_chunk, idx)) {
       slot = w.q_shadow[idx];
       uint4 sd = w.seed[slot];
       rq = reqs + sd.w;

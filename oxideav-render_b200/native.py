@@ -100,6 +100,7 @@ SIGNATURES = {
     "pt_set_wave_slots": (i32, [vp, u32]),
     "pt_set_node_width": (i32, [vp, u32, u32]),
     "pt_set_material_sort": (i32, [vp, i32]),
+    "pt_set_traversal": (i32, [vp, u32, u32]),
     "pt_set_shade_blocks": (i32, [vp, u32]),
     "pt_set_wave_overlap": (i32, [vp, i32]),
     "pt_set_wave_graphs": (i32, [vp, i32]),
