@@ -278,7 +278,7 @@ def run_served_batch(ctx, api, torch, reqs, args, tracers):
     from oxideav_render_b200 import abi
     from oxideav_render_b200.serve import RenderServer
     srv = RenderServer(ctx, wave_overlap=args.wave_overlap, wave_slots=args.serve_wave_slots,
-                       spatial_bvh=args.spatial_bvh)
+                       spatial_bvh=args.spatial_bvh, pipeline_depth=args.serve_depth)
     try:
         kinds = sorted({k for k, _, _, _ in reqs})
         scenes = [mixed_scene(k) for k in kinds]
@@ -406,7 +406,7 @@ def run_poisson(ctx, api, torch, args):
     n = max(8, min(int(max(args.serve_rates) * args.serve_seconds), args.serve_max))
     spec, samples = served_spec(n, scenes, 4242)
     srv = RenderServer(ctx, hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), wave_overlap=args.wave_overlap,
-                       wave_slots=args.serve_wave_slots, spatial_bvh=args.spatial_bvh)
+                       wave_slots=args.serve_wave_slots, spatial_bvh=args.spatial_bvh, pipeline_depth=args.serve_depth)
     t0 = time.perf_counter()
     keys = register_scenes(srv, api, scenes)
     register_s = time.perf_counter() - t0
@@ -858,6 +858,8 @@ def run_b200(args):
         ctx.set_wave_slots(args.wave_slots)
     if args.schedule == "megakernel":
         ctx.set_schedule(0)
+    if args.trav_threads or args.claim_chunk:
+        ctx.set_traversal(args.trav_threads or 256, args.claim_chunk or 1)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
     if args.mixed == 0:
         # Profiling case: the single frame of --config alone.
@@ -980,6 +982,7 @@ def main():
     ap.add_argument("--serve-budget-gb", type=float, default=60.0, help="HBM budget of the resident scenes")
     ap.add_argument("--serve-check", type=int, default=8, help="served images compared with the plain path")
     ap.add_argument("--serve-wave-slots", type=int, default=0, help="path slots per served wave (0: the server's default)")
+    ap.add_argument("--serve-depth", type=int, default=0, help="served waves in flight (0: the server's default)")
     ap.add_argument("--binned-bvh", dest="spatial_bvh", action="store_false",
                     help="resident and served scenes get the binned-SAH tree instead of the spatial-split one")
     ap.add_argument("--no-raycast", dest="raycast", action="store_false",
@@ -992,6 +995,8 @@ def main():
                     help="path slots per wave (0: the library's default; autotune may override)")
     ap.add_argument("--wave-arenas", type=int, default=0,
                     help="waves in flight at once (2 or 3; 0: the library's default)")
+    ap.add_argument("--trav-threads", type=int, default=0, help="traversal block size 128 / 256 (0: default)")
+    ap.add_argument("--claim-chunk", type=int, default=0, help="queue entries per traversal refill 1 / 2 / 4 (0: default)")
     ap.add_argument("--raycast-only", type=int, default=0,
                     help="profiling case: this many raycast frames (Phong, then Pbr) of the scene and exit")
     args = ap.parse_args()

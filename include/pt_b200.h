@@ -303,6 +303,17 @@ PT_API uint32_t pt_abi_version(void);
  * evicts it). */
 PT_API pt_status pt_scene_upload(pt_context *ctx, const pt_scene_desc *desc, uint32_t *scene_id);
 PT_API pt_status pt_scene_release(pt_context *ctx, uint32_t scene_id);
+/* An animated frame of resident scene `scene_id` (no counterpart in the
+ * reference, which re-prepares the scene every frame:
+ * PreparedScene::build, src/prepare.rs:1110-1119, then TraceScene::new):
+ * `desc` is the scene at another time with the same draw items and triangle
+ * counts. Its streams and tables replace the old ones; the BVH keeps its
+ * structure and is refitted on the device (records rewritten, node bounds
+ * recomputed bottom up) instead of rebuilt. Images equal those of a fresh
+ * pt_scene_upload of `desc` bit for bit (closest hits do not depend on the
+ * tree); tracers on the scene must sync again (their accumulation resets).
+ * PT_ERR_INVALID_ARG when the topology differs. */
+PT_API pt_status pt_scene_refit(pt_context *ctx, uint32_t scene_id, const pt_scene_desc *desc);
 /* Device bytes held by a resident scene. */
 PT_API pt_status pt_scene_device_bytes(pt_context *ctx, uint32_t scene_id, uint64_t *bytes);
 PT_API pt_status pt_scene_triangle_count(pt_context *ctx, uint32_t scene_id, uint64_t *count);

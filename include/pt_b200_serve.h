@@ -53,7 +53,7 @@ typedef struct pt_server_config {
   uint32_t wave_slots;       /* path slots per wave; 0 = 4194304 */
   uint32_t max_active;       /* requests admitted to the GPU at once; 0 = 256 */
   uint32_t megakernel;       /* nonzero: one-kernel-per-path schedule instead of the wavefront */
-  uint32_t pipeline_depth;   /* waves in flight on the stream; 0 = 2 */
+  uint32_t pipeline_depth;   /* waves in flight; 0 = 3 (one per path-state arena) */
   uint32_t node_width_extension; /* BVH node layout of extension rays: 2 or 4; 0 = 4 */
   uint32_t node_width_shadow;    /* BVH node layout of shadow rays: 2 or 4; 0 = 4 */
   uint32_t autotune;             /* nonzero: tune each new scene class before its first request runs

@@ -66,6 +66,11 @@ class Context:
     def release(self, scene_id: int) -> None:
         self.check(self.lib.pt_scene_release(self.ptr, scene_id))
 
+    def refit(self, scene_id: int, desc: SceneDesc) -> None:
+        """pt_scene_refit: resident scene `scene_id` becomes `desc` (same draw
+        items and triangle counts), its BVH refitted on the device."""
+        self.check(self.lib.pt_scene_refit(self.ptr, scene_id, C.byref(desc.desc)))
+
     def scene_bytes(self, scene_id: int) -> int:
         b = C.c_uint64()
         self.check(self.lib.pt_scene_device_bytes(self.ptr, scene_id, C.byref(b)))
@@ -246,11 +251,24 @@ class PathTracer:
         # PrepareOptions::from_render_options (src/prepare.rs:137-146).
         return (o.time, o.animation, o.material_variant, o.use_scene_lights, o.light)
 
-    def sync(self, scene: PreparedScene, opts: RenderOptions) -> bool:
+    def sync(self, scene: PreparedScene, opts: RenderOptions, refit: bool = False) -> bool:
         """PathTracer::sync: re-uploads the scene when invalidated or when a
-        preparation input changed; resets exactly when radiance inputs change."""
+        preparation input changed; resets exactly when radiance inputs change.
+        With `refit` (animated frames), a scene with the same draw items and
+        triangle counts as the uploaded one replaces it in place and its BVH
+        is refitted instead of rebuilt (same images, cheaper per frame)."""
         key = (id(scene), self._prep_key(opts))
         need_prepare = self._dirty or self._scene is not scene or self._scene_key != key
+        if need_prepare and refit and self._scene_id is not None:
+            desc = scene.to_desc(opts)
+            st = self.lib.pt_scene_refit(self.ctx.ptr, self._scene_id, C.byref(desc.desc))
+            if st == abi.PT_OK:
+                self._desc, self._scene, self._scene_key = desc, scene, key
+                self._dirty = False
+                self.lib.pt_tracer_invalidate_scene(self.ptr)
+                need_prepare = False
+            elif st != abi.PT_ERR_INVALID_ARG:
+                self.ctx.check(st)
         if need_prepare:
             desc = scene.to_desc(opts)
             # The old scene goes first: its device memory and any background
@@ -345,7 +363,7 @@ class PathTracer:
         self.ctx.check(self.lib.pt_tracer_traversal_counts(self.ptr, C.byref(n), C.byref(t)))
         return n.value, t.value
 
-    STAGES = ("raygen", "extend", "shade", "shadow", "accumulate", "megakernel", "sort")
+    STAGES = ("raygen", "extend", "shade", "shadow", "accumulate", "megakernel", "sort", "nee")
 
     def stage_ms(self) -> dict:
         """Device ms per stage of the last refine (with stage timing on)."""
@@ -431,6 +449,15 @@ class PathTraceCudaRenderer:
     def render_hdr(self, scene: PreparedScene, opts: RenderOptions) -> np.ndarray:
         self._run(scene, opts)
         return self.tracer.hdr()
+
+    def render_frame(self, scene: PreparedScene, opts: RenderOptions) -> np.ndarray:
+        """`render` for consecutive frames of an animation: a frame with the
+        same draw items and triangle counts as the previous one refits the
+        resident scene's BVH instead of rebuilding it (the image is the one
+        `render` gives)."""
+        self.tracer.sync(scene, opts, refit=True)
+        self.tracer.refine(max(opts.path_trace.samples_per_pixel, 1))
+        return self.tracer.image()
 
 
 class RaycastCudaRenderer:

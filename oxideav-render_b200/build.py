@@ -25,7 +25,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
                      "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden",
                      "-I", INCLUDE]
-SOURCES = ["kernels.cu", "host_scene.cpp", "capi.cpp", "noalloc.cu", "serve.cpp", "bvh_build.cu", "mip_build.cu"]
+SOURCES = ["kernels.cu", "host_scene.cpp", "capi.cpp", "noalloc.cu", "serve.cpp", "bvh_build.cu", "mip_build.cu",
+           "bvh_refit.cu"]
 
 
 def _nvcc() -> str:

@@ -1497,6 +1497,7 @@ std::string device_build_bvh_sah(SceneHost &sc, cudaStream_t st, uint32_t max_de
   sc.bvh_arena = arena;
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   sc.bvh = BvhBuildStats{};
+  sc.bvh.references = n;
   sc.bvh.nodes = n2;
   sc.bvh.leaves = n2 + 1;  // a binary tree: one leaf more than interior nodes
   sc.bvh.max_depth = depth;
@@ -1663,6 +1664,7 @@ std::string device_build_bvh(SceneHost &sc, cudaStream_t st, uint32_t max_depth_
   arena.base = nullptr;  // owned by the scene now
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   sc.bvh = BvhBuildStats{};
+  sc.bvh.references = n;
   sc.bvh.nodes = n2;
   sc.bvh.leaves = cnt[1];
   sc.bvh.max_depth = cnt[0];

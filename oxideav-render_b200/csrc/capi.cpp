@@ -234,7 +234,8 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
                     4 * P, 4 * P, 4 * P,                                     // q0 q1 q_shadow
                     4 * (size_t)kWfCounterStride * (iterations + 1),
                     4 * P, 4 * 2 * (size_t)kSortBuckets * (iterations + 1),   // q_sorted sort_counts
-                    sizeof(WaveDesc), 4 * P};                                  // desc sort_keys
+                    sizeof(WaveDesc), 4 * P,                                   // desc sort_keys
+                    3 * 16 * P};                                               // nee
   size_t off[sizeof(sizes) / sizeof(sizes[0])], total = 0;
   for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); ++i) {
     total = (total + 255) & ~(size_t)255;
@@ -266,6 +267,7 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   w.sort_counts = (uint32_t *)(b + off[k++]);
   w.desc = (WaveDesc *)(b + off[k++]);
   w.sort_keys = (uint32_t *)(b + off[k++]);
+  w.nee = (float4 *)(b + off[k++]);
   w.capacity = capacity;
   w.shadow_slots = shadow_slots;
   w.iterations = iterations;
@@ -868,6 +870,23 @@ pt_status pt_scene_release(pt_context *ctx, uint32_t scene_id) {
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     release_scene(*it->second);
     ctx->scenes.erase(it);
+    return PT_OK;
+  });
+}
+
+pt_status pt_scene_refit(pt_context *ctx, uint32_t scene_id, const pt_scene_desc *desc) {
+  if (!ctx) return fail(nullptr, PT_ERR_INVALID_ARG, "context is NULL");
+  if (!desc) return fail(ctx, PT_ERR_INVALID_ARG, "desc is NULL");
+  return guard(ctx, [&]() -> pt_status {
+    SceneHost *sc = find_scene(ctx, scene_id);
+    if (!sc) return fail(ctx, PT_ERR_NOT_FOUND, "unknown scene " + std::to_string(scene_id));
+    CK(ctx, cudaSetDevice(ctx->device));
+    // Waves already queued read the old arena: let them finish first.
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (injected_oom(ctx)) return fail(ctx, PT_ERR_OOM, "scene refit: device allocation failed (injected)");
+    bool oom = false;
+    std::string err = refit_scene(*desc, *sc, oom, ctx->stream, &ctx->staging);
+    if (!err.empty()) return fail(ctx, oom ? PT_ERR_OOM : PT_ERR_INVALID_ARG, err);
     return PT_OK;
   });
 }

@@ -201,12 +201,126 @@ PT_DEV float tri_pdf(const DevRequest &rq, uint32_t li, uint32_t g, V3 p, V3 q) 
   return tri_pdf_omega(rq, li, a, b, c, triangle_solid_angle(p, a, b, c), p, q);
 }
 
+// Integrator::tri_pdf of the emissive triangle g hit at q from prev_pos
+// (the light-sampling pdf of the emission MIS weight); 0 when g is not in
+// the emissive table.
+PT_DEV float emission_light_pdf(const DevRequest &rq, const DevScene &s, uint32_t g, V3 prev_pos, V3 q) {
+  const uint32_t li = __ldg(s.em_lookup + g);
+  return li != 0xffffffffu ? tri_pdf(rq, li, g, prev_pos, q) : 0.0f;
+}
+
+// Whether the request samples area lights (environment or emissive
+// triangles) in its next-event estimation.
+PT_DEV bool area_nee(const DevRequest &rq, const DevScene &s) {
+  return rq.strategy != PT_BSDF_ONLY && (rq.env || s.em_count > 0);
+}
+
+// The area-set light sample of next-event estimation at p
+// (Integrator::sample, src/pathtrace.rs:2171-2290, its environment /
+// emissive-triangle branch): direction, radiance, pdf, shadow-ray extent and
+// skipped triangle; `go` false when no sample.
+struct AreaSample {
+  V3 l, le;
+  float pl, tmax;
+  uint32_t skip;
+  bool go;
+};
+PT_DEV AreaSample sample_area_light(const DevRequest &rq, const DevScene &s, V3 p, const float pl_u[4]) {
+  AreaSample out;
+  out.l = vzero();
+  out.le = vzero();
+  out.pl = 0.0f;
+  out.tmax = inf();
+  out.skip = 0xffffffffu;
+  out.go = false;
+  const float pe = rq.p_env;
+  if (pl_u[2] < pe) {
+    float epdf;
+    if (rq.env && env_sample(*rq.env, pl_u[0], pl_u[1], out.l, out.le, epdf)) {
+      out.pl = pe * epdf;
+      out.go = true;
+    }
+  } else if (s.em_count > 0) {
+    float us = pe > 0.0f ? clampr((pl_u[2] - pe) / (1.0f - pe), 0.0f, 0.999999f) : pl_u[2];
+    uint32_t li = min(upper_bound(s.em_cdf, s.em_count, us), s.em_count - 1);
+    uint32_t g = __ldg(s.em_tris + li);
+    V3 a, b, cc;
+    tri_positions(s, g, a, b, cc);
+    bool have_target = false;
+    V3 q = vzero();
+    // The solid angle picks the sampling method and is the pdf's
+    // denominator (one evaluation serves both).
+    const float omega = triangle_solid_angle(p, a, b, cc);
+    if (omega >= 1.0e-4f) {
+      V3 ld;
+      if (sample_spherical_triangle(p, a, b, cc, pl_u[0], pl_u[1], ld)) {
+        V3 n = vcross(vsub(b, a), vsub(cc, a));
+        float dn = vdot(ld, n);
+        if (dn != 0.0f) {
+          float t = vdot(vsub(a, p), n) / dn;
+          if (t > 0.0f && isfinite(t)) {
+            q = vadd(p, vscale(ld, t));
+            have_target = true;
+          }
+        }
+      }
+    } else {
+      float su = sqrtf(pl_u[0]);
+      float w0 = 1.0f - su, w1 = su * (1.0f - pl_u[1]), w2 = su * pl_u[1];
+      q = {a.x * w0 + b.x * w1 + cc.x * w2, a.y * w0 + b.y * w1 + cc.y * w2, a.z * w0 + b.z * w1 + cc.z * w2};
+      have_target = true;
+    }
+    if (have_target) {
+      // barycentric_of, src/trace.rs:1120-1133.
+      V3 e1 = vsub(b, a), e2 = vsub(cc, a), r = vsub(q, a);
+      float d11 = vdot(e1, e1), d12 = vdot(e1, e2), d22 = vdot(e2, e2);
+      float r1 = vdot(r, e1), r2 = vdot(r, e2);
+      float det = d11 * d22 - d12 * d12;
+      if (isfinite(det) && fabsf(det) > F32_MIN_POSITIVE) {
+        float u = (d22 * r1 - d12 * r2) / det;
+        float vv = (d11 * r2 - d12 * r1) / det;
+        float lb0 = clampr(1.0f - u - vv, 0.0f, 1.0f), lb1 = clampr(u, 0.0f, 1.0f), lb2 = clampr(vv, 0.0f, 1.0f);
+        V3 to = vsub(q, p);
+        float dist2 = vdot(to, to);
+        uint2 linfo = __ldg(s.tri_info + g);
+        const DevMaterial &lmat = s.materials[linfo.x];
+        Surface lsurf = surface(s, g, lb0, lb1, lb2, linfo.y);
+        if (dist2 > 1.0e-12f) {
+          float dist = sqrtf(dist2);
+          out.l = vscale(to, 1.0f / dist);
+          float cos_l = -vdot(lsurf.ng, out.l);
+          out.pl = tri_pdf_omega(rq, li, a, b, cc, omega, p, q);
+          if ((cos_l > 0.0f || (lmat.m.double_sided && cos_l < 0.0f)) && out.pl > 0.0f && isfinite(out.pl)) {
+            out.le = emission(s, lmat, g, linfo.y, lb0, lb1, lb2);
+            out.tmax = fmaxf(dist * (1.0f - 1.0e-4f), 0.0f);
+            out.skip = g;
+            out.go = true;
+          }
+        }
+      }
+    }
+  }
+  return out;
+}
+
+// What the wavefront's NEE kernel computed for a vertex ahead of shade:
+// the area-light sample and the emission MIS pdf. The megakernel computes
+// both inline; the values are the same either way.
+struct NeeInput {
+  AreaSample area;
+  float pl_emit;
+};
+
 // Shade vertex k of the path whose extension ray produced (found, hit).
 // Shadow rays go to `sink.emit(ray)` in the reference's order. Returns false
 // when the path terminated (the sink may still hold shadow rays of this
-// vertex that contribute).
-template <class Sink>
-PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hit, Sink &sink) {
+// vertex that contribute). With kPre, the area-light sample and the
+// emission MIS pdf come from `pre` instead of being computed here, which
+// keeps the f64 spherical-triangle and environment sampling code out of
+// this (large) function's instruction footprint.
+template <class Sink, bool kPre = false>
+PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hit, Sink &sink,
+                  const NeeInput *pre = nullptr) {
   const DevScene &s = *rq.scene;
   const uint32_t k = ps.k;
   const uint32_t ray_id = k << 16;
@@ -249,9 +363,11 @@ PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hi
       if (k == 0) {
         ps.radiance = vadd(ps.radiance, vmul(ps.beta, le));
       } else {
-        float pl = 0.0f;
-        uint32_t li = __ldg(s.em_lookup + hit.g);
-        if (li != 0xffffffffu) pl = tri_pdf(rq, li, hit.g, ps.prev_pos, surf.position);
+        float pl;
+        if constexpr (kPre)
+          pl = pre->pl_emit;
+        else
+          pl = emission_light_pdf(rq, s, hit.g, ps.prev_pos, surf.position);
         float w;
         if (pl <= 0.0f)
           w = 1.0f;
@@ -313,11 +429,10 @@ PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hi
   // (punctual lights, then the area sample) and every value is computed as
   // in Integrator::sample (src/pathtrace.rs:2171-2290); only the code path
   // to eval is shared, which keeps the kernel's instruction footprint small.
-  float pl_u[4], pb_u[4];
-  ps.smp.pattern(2 + 2 * k, pl_u);
+  float pb_u[4];
   ps.smp.pattern(1 + 2 * k, pb_u);
   const uint32_t nl = s.light_count;
-  const bool area_nee = strategy != PT_BSDF_ONLY && (rq.env || s.em_count > 0);
+  const bool area = area_nee(rq, s);
   const uint32_t shadow_id = ray_id | 0xffffu;
   V3 l, f;
   float pdf;
@@ -336,73 +451,22 @@ PT_DEV bool shade(const DevRequest &rq, PathState &ps, bool found, const Hit &hi
         go = true;
       }
     } else if (c == nl) {
-      if (!area_nee) continue;
-      const float pe = rq.p_env;
-      if (pl_u[2] < pe) {
-        float epdf;
-        if (rq.env && env_sample(*rq.env, pl_u[0], pl_u[1], l, le, epdf)) {
-          pl = pe * epdf;
-          go = true;
-        }
-      } else if (s.em_count > 0) {
-        float us = pe > 0.0f ? clampr((pl_u[2] - pe) / (1.0f - pe), 0.0f, 0.999999f) : pl_u[2];
-        uint32_t li = min(upper_bound(s.em_cdf, s.em_count, us), s.em_count - 1);
-        uint32_t g = __ldg(s.em_tris + li);
-        V3 a, b, cc;
-        tri_positions(s, g, a, b, cc);
-        bool have_target = false;
-        V3 q = vzero();
-        // The solid angle picks the sampling method and is the pdf's
-        // denominator (one evaluation serves both).
-        const float omega = triangle_solid_angle(p, a, b, cc);
-        if (omega >= 1.0e-4f) {
-          V3 ld;
-          if (sample_spherical_triangle(p, a, b, cc, pl_u[0], pl_u[1], ld)) {
-            V3 n = vcross(vsub(b, a), vsub(cc, a));
-            float dn = vdot(ld, n);
-            if (dn != 0.0f) {
-              float t = vdot(vsub(a, p), n) / dn;
-              if (t > 0.0f && isfinite(t)) {
-                q = vadd(p, vscale(ld, t));
-                have_target = true;
-              }
-            }
-          }
-        } else {
-          float su = sqrtf(pl_u[0]);
-          float w0 = 1.0f - su, w1 = su * (1.0f - pl_u[1]), w2 = su * pl_u[1];
-          q = {a.x * w0 + b.x * w1 + cc.x * w2, a.y * w0 + b.y * w1 + cc.y * w2, a.z * w0 + b.z * w1 + cc.z * w2};
-          have_target = true;
-        }
-        if (have_target) {
-          // barycentric_of, src/trace.rs:1120-1133.
-          V3 e1 = vsub(b, a), e2 = vsub(cc, a), r = vsub(q, a);
-          float d11 = vdot(e1, e1), d12 = vdot(e1, e2), d22 = vdot(e2, e2);
-          float r1 = vdot(r, e1), r2 = vdot(r, e2);
-          float det = d11 * d22 - d12 * d12;
-          if (isfinite(det) && fabsf(det) > F32_MIN_POSITIVE) {
-            float u = (d22 * r1 - d12 * r2) / det;
-            float vv = (d11 * r2 - d12 * r1) / det;
-            float lb0 = clampr(1.0f - u - vv, 0.0f, 1.0f), lb1 = clampr(u, 0.0f, 1.0f), lb2 = clampr(vv, 0.0f, 1.0f);
-            V3 to = vsub(q, p);
-            float dist2 = vdot(to, to);
-            uint2 linfo = __ldg(s.tri_info + g);
-            const DevMaterial &lmat = s.materials[linfo.x];
-            Surface lsurf = surface(s, g, lb0, lb1, lb2, linfo.y);
-            if (dist2 > 1.0e-12f) {
-              float dist = sqrtf(dist2);
-              l = vscale(to, 1.0f / dist);
-              float cos_l = -vdot(lsurf.ng, l);
-              pl = tri_pdf_omega(rq, li, a, b, cc, omega, p, q);
-              if ((cos_l > 0.0f || (lmat.m.double_sided && cos_l < 0.0f)) && pl > 0.0f && isfinite(pl)) {
-                le = emission(s, lmat, g, linfo.y, lb0, lb1, lb2);
-                tmax = fmaxf(dist * (1.0f - 1.0e-4f), 0.0f);
-                skip = g;
-                go = true;
-              }
-            }
-          }
-        }
+      if (!area) continue;
+      AreaSample as;
+      if constexpr (kPre) {
+        as = pre->area;
+      } else {
+        float pl_u[4];
+        ps.smp.pattern(2 + 2 * k, pl_u);
+        as = sample_area_light(rq, s, p, pl_u);
+      }
+      if (as.go) {
+        l = as.l;
+        le = as.le;
+        pl = as.pl;
+        tmax = as.tmax;
+        skip = as.skip;
+        go = true;
       }
     } else {
       if (!bsdf.sample_dir(pb_u, l)) return false;

@@ -154,6 +154,7 @@ struct WaveBuffers {
   uint32_t *q_sorted;          // the active queue bucketed by material (material sort on)
   uint32_t *sort_keys;         // material-sort key of each active-queue position (set by extend)
   uint32_t *sort_counts;       // [iterations][2][kSortBuckets]: bucket sizes, then cursors
+  float4 *nee;                 // [3][capacity]: the NEE kernel's area sample and emission pdf per slot
   struct WaveDesc *desc;       // this wave's requests and segments (written before each wave)
   uint32_t capacity, shadow_slots, iterations, sort_materials;
   uint32_t shade_blocks;       // 3 or 4: the k_wf_shade instantiation (blocks per SM)
@@ -181,7 +182,7 @@ struct DevCounters {
 
 // Stages timed by the optional per-stage CUDA events.
 enum Stage : int { STAGE_RAYGEN = 0, STAGE_EXTEND, STAGE_SHADE, STAGE_SHADOW, STAGE_ACCUMULATE, STAGE_MEGAKERNEL,
-                   STAGE_SORT, STAGE_END, STAGE_COUNT = STAGE_END };
+                   STAGE_SORT, STAGE_NEE, STAGE_END, STAGE_COUNT = STAGE_END };
 enum ErrorFlags : uint32_t { ERR_STACK_OVERFLOW = 1u };
 
 }  // namespace ptd

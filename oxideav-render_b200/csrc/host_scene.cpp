@@ -1724,6 +1724,8 @@ std::string commit_scene(const SceneImage &img, SceneHost &out, bool &oom, cudaS
 std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder, cudaStream_t stream,
                          HostStaging *staging) {
   oom = false;
+  out.item_tris.clear();
+  for (uint32_t i = 0; desc.items && i < desc.item_count; ++i) out.item_tris.push_back(desc.items[i].triangle_count);
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
   auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
@@ -1766,6 +1768,57 @@ std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, i
   out.upload_seconds[2] = 0.0;
   out.upload_seconds[3] = secs(t0, t3);
   return err;
+}
+
+std::string refit_scene(const pt_scene_desc &desc, SceneHost &sc, bool &oom, cudaStream_t stream,
+                        HostStaging *staging) {
+  oom = false;
+  using clk = std::chrono::steady_clock;
+  auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+  const auto t0 = clk::now();
+  std::vector<uint32_t> tris;
+  for (uint32_t i = 0; desc.items && i < desc.item_count; ++i) tris.push_back(desc.items[i].triangle_count);
+  if (tris != sc.item_tris)
+    return "refit needs the same draw items with the same triangle counts (upload the scene instead)";
+  SceneImage img;
+  std::string err = build_scene_image(desc, img, false, staging);
+  if (!err.empty()) return err;
+  const auto t1 = clk::now();
+  SceneHost fresh;
+  err = commit_scene(img, fresh, oom, stream);
+  if (!err.empty()) return err;
+  const auto t2 = clk::now();
+  // The old tree, refitted to the new positions, goes with the new arena.
+  fresh.bvh_arena = sc.bvh_arena;
+  fresh.dev.nodes = sc.dev.nodes;
+  fresh.dev.nodes4 = sc.dev.nodes4;
+  fresh.dev.tris = sc.dev.tris;
+  fresh.dev.node_count = sc.dev.node_count;
+  fresh.dev.node4_count = sc.dev.node4_count;
+  fresh.dev.max_depth = sc.dev.max_depth;
+  fresh.bvh = sc.bvh;
+  fresh.device_bvh = sc.device_bvh;
+  fresh.item_tris = sc.item_tris;
+  err = device_refit_bvh(fresh, sc.bvh.references, stream);
+  cudaError_t e = cudaSuccess;
+  if (err.empty()) e = cudaMemcpyAsync(fresh.d_desc, &fresh.dev, sizeof(DevScene), cudaMemcpyHostToDevice, stream);
+  if (err.empty() && e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (err.empty() && e != cudaSuccess) err = std::string("refit: ") + cudaGetErrorString(e);
+  if (!err.empty()) {
+    // The tree stays with the old scene, which is still whole.
+    fresh.bvh_arena = DeviceArena{};
+    fresh.arena.release();
+    return err;
+  }
+  sc.arena.release();
+  sc.bvh_arena = DeviceArena{};
+  const auto t3 = clk::now();
+  fresh.upload_seconds[0] = secs(t0, t1);
+  fresh.upload_seconds[1] = secs(t1, t2);
+  fresh.upload_seconds[2] = secs(t2, t3);
+  fresh.upload_seconds[3] = secs(t0, t3);
+  sc = std::move(fresh);
+  return "";
 }
 
 void release_scene(SceneHost &s) {

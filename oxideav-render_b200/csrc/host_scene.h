@@ -29,7 +29,7 @@ void build_bvh(const float *pos, uint32_t tri_count, const uint32_t *rec_flags, 
                std::vector<Bvh4Node> &nodes4, std::vector<float4> &records, BvhBuildStats &stats, int threads);
 // The same outputs from a spatial-split BVH: fewer overlapping leaves for
 // scenes of many small overlapping triangles, at a few times the build time
-// and up to 1.6x the triangle records (a triangle cut by split planes is
+// and up to 4x the triangle records (a triangle cut by split planes is
 // referenced from several leaves).
 void build_bvh_spatial(const float *pos, uint32_t tri_count, const uint32_t *rec_flags,
                        std::vector<BvhNode> &nodes, std::vector<Bvh4Node> &nodes4, std::vector<float4> &records,
@@ -126,6 +126,8 @@ struct SceneHost {
   // Host wall time of upload_scene: host image, arena allocation + copy,
   // device BVH build, total.
   double upload_seconds[4] = {0.0, 0.0, 0.0, 0.0};
+  // Triangle count of every draw item, in order: a refit needs the same.
+  std::vector<uint32_t> item_tris;
   uint64_t device_bytes() const { return arena.bytes + bvh_arena.bytes; }
 };
 
@@ -162,6 +164,16 @@ constexpr uint64_t kAutoDeviceBuildTris = 16384;
 std::string upload_scene(const pt_scene_desc &desc, SceneHost &out, bool &oom, int builder = BVH_BUILD_HOST,
                          cudaStream_t stream = nullptr, HostStaging *staging = nullptr);
 void release_scene(SceneHost &s);
+// An animated frame of a resident scene with the same draw items and
+// triangle counts: the new host image (no BVH) replaces the scene arena, the
+// tree keeps its structure and is refitted on the device
+// (device_refit_bvh). upload_seconds then holds: host image, arena copy,
+// refit, total.
+std::string refit_scene(const pt_scene_desc &desc, SceneHost &sc, bool &oom, cudaStream_t stream,
+                        HostStaging *staging);
+// Records rewritten from the scene's positions and both node layouts'
+// bounds recomputed bottom up (bvh_refit.cu); `records` triangle records.
+std::string device_refit_bvh(SceneHost &sc, uint64_t records, cudaStream_t stream);
 struct EnvHost {
   DevEnv dev{};
   DevEnv *d_desc = nullptr;

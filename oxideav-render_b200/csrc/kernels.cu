@@ -340,7 +340,8 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
   const bool t128 = w.trav_threads == 128;
   const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext[t128 ? 1 : 0]),
                  g_shade = (uint32_t)num_sms * (shade4 ? 8 : 6),
-                 g_sh = (uint32_t)(num_sms * per_sm_sh[t128 ? 1 : 0]), g_wide = (uint32_t)num_sms * 16;
+                 g_sh = (uint32_t)(num_sms * per_sm_sh[t128 ? 1 : 0]), g_wide = (uint32_t)num_sms * 16,
+                 g_nee = (uint32_t)num_sms * 8;
   tm.mark(STAGE_RAYGEN, st);
   k_wf_raygen<<<g_wide, 256, 0, st>>>(w);
   for (uint32_t it = 0; it < w.iterations; ++it) {
@@ -355,6 +356,8 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
       k_wf_sort_scan<<<1, kSortBuckets, 0, st>>>(w, it);
       k_wf_sort_scatter<<<g_shade, 256, 0, st>>>(w, it);
     }
+    tm.mark(STAGE_NEE, st);
+    k_wf_nee<<<g_nee, 256, 0, st>>>(w, it);
     tm.mark(STAGE_SHADE, st);
     if (shade4)
       k_wf_shade<4><<<g_shade, 128, 0, st>>>(w, it);

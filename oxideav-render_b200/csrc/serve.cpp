@@ -160,7 +160,7 @@ struct Flight {
 struct pt_server {
   pt_context *eng = nullptr;
   uint64_t budget = 0;
-  uint32_t wave_slots = 1u << 22, max_active = 256, depth = 2;
+  uint32_t wave_slots = 1u << 22, max_active = 256, depth = 3;
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::thread worker;
@@ -477,6 +477,20 @@ void launch_next_wave(pt_server *s) {
   }
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
   std::vector<WaveSegment> segs = pack_wave(jobs, order, s->wave_slots);
+  // The priority order chose what goes into the wave; inside it, the
+  // segments are laid out scene by scene (a job has at most one segment per
+  // wave, so samples stay in order), so the wave's first rays walk one BVH
+  // at a time.
+  std::stable_sort(segs.begin(), segs.end(), [&](const WaveSegment &a, const WaveSegment &b) {
+    return jobs[a.request].scene_key < jobs[b.request].scene_key;
+  });
+  {
+    uint32_t slot = 0;
+    for (WaveSegment &sg : segs) {
+      sg.slot_begin = slot;
+      slot += sg.pixel_count * sg.spp;
+    }
+  }
   // Compact request table: only the jobs this wave carries.
   std::vector<int> remap(n, -1);
   std::vector<DevRequest> table;

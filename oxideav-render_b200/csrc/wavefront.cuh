@@ -5,6 +5,10 @@
 //   k_wf_raygen   camera rays for every slot of the wave (active queue 0);
 //   k_wf_extend   closest hit of each queued path (traversal only: small
 //                 register footprint, high occupancy);
+//   k_wf_nee      per queued vertex, the area-light sample of next-event
+//                 estimation and the emission MIS pdf (the f64
+//                 spherical-triangle and environment sampling), kept out of
+//                 the shade kernel's instruction footprint;
 //   k_wf_shade    emission, material, BSDF, NEE shadow-ray generation,
 //                 BSDF sampling, roulette; survivors are appended to the next
 //                 active queue and paths with shadow rays to the shadow queue
@@ -300,6 +304,49 @@ __global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t
   }
 }
 
+// The area-light sample and emission MIS pdf of every queued vertex that
+// hit something, in the order shade will read them (its queue). Values are
+// those shade would compute inline (the same functions on the same inputs).
+__global__ void __launch_bounds__(256) k_wf_nee(WaveBuffers w, uint32_t iter) {
+  const DevRequest *reqs = w.desc->reqs;
+  const uint32_t n = w.counters[iter * kWfCounterStride + 0];
+  const uint32_t *q = w.sort_materials ? w.q_sorted : w.q[iter & 1u];
+  const size_t cap = w.capacity;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t slot = q[i];
+    const uint32_t hg = w.hit_g[slot];
+    if (!(hg & HIT_FOUND)) continue;
+    const uint4 sd = w.seed[slot];
+    const DevRequest &rq = reqs[sd.w];
+    const DevScene &s = *rq.scene;
+    const uint32_t k = __float_as_uint(w.o[slot].w);
+    const uint32_t g = hg & HIT_G_MASK;
+    const float4 tb = w.hit_tb[slot];
+    const V3 pos = interp3(s.pos, g, tb.y, tb.z, tb.w);
+    float pl_emit = 0.0f;
+    if (k > 0) {
+      const float4 pv = w.prev[slot];
+      pl_emit = emission_light_pdf(rq, s, g, {pv.x, pv.y, pv.z}, pos);
+    }
+    AreaSample as;
+    as.go = false;
+    if (k < rq.max_bounces && area_nee(rq, s)) {
+      Sampler smp;
+      smp.pixel_seed = sd.x;
+      smp.index = sd.y;
+      smp.path_seed = sd.z;
+      float pl_u[4];
+      smp.pattern(2 + 2 * k, pl_u);
+      as = sample_area_light(rq, s, pos, pl_u);
+    }
+    if (as.go) {
+      w.nee[slot] = make_float4(as.l.x, as.l.y, as.l.z, as.pl);
+      w.nee[cap + slot] = make_float4(as.le.x, as.le.y, as.le.z, as.tmax);
+    }
+    w.nee[2 * cap + slot] = make_float4(__uint_as_float(as.skip), as.go ? 1.0f : 0.0f, pl_emit, 0.0f);
+  }
+}
+
 // kBlocks 128-thread blocks per SM. Three (168 registers) measured faster
 // than the unconstrained 234-register build despite a few spills, and than
 // four on scenes with light shading (C1); four (128 registers, more
@@ -331,7 +378,22 @@ __global__ void __launch_bounds__(128, kBlocks) k_wf_shade(WaveBuffers w, uint32
       h.front = (hg & HIT_FRONT) != 0;
     }
     DeferredSink sink{&w, slot, 0};
-    bool alive = shade(rq, ps, found, h, sink);
+    NeeInput pre;
+    if (found) {
+      const size_t cap = w.capacity;
+      const float4 n2 = w.nee[2 * cap + slot];
+      pre.area.go = n2.y != 0.0f;
+      pre.area.skip = __float_as_uint(n2.x);
+      pre.pl_emit = n2.z;
+      if (pre.area.go) {
+        const float4 n0 = w.nee[slot], n1 = w.nee[cap + slot];
+        pre.area.l = {n0.x, n0.y, n0.z};
+        pre.area.pl = n0.w;
+        pre.area.le = {n1.x, n1.y, n1.z};
+        pre.area.tmax = n1.w;
+      }
+    }
+    bool alive = shade<DeferredSink, true>(rq, ps, found, h, sink, &pre);
     wf_store_vertex(w, slot, ps);
     w.sh_n[slot] = sink.count;
     wf_append(q_next, n_next, alive, slot);

@@ -39,6 +39,7 @@ SIGNATURES = {
     "pt_last_error": (C.c_char_p, [vp]),
     "pt_scene_upload": (i32, [vp, C.POINTER(abi.pt_scene_desc), u32p]),
     "pt_scene_release": (i32, [vp, u32]),
+    "pt_scene_refit": (i32, [vp, u32, C.POINTER(abi.pt_scene_desc)]),
     "pt_scene_device_bytes": (i32, [vp, u32, u64p]),
     "pt_scene_triangle_count": (i32, [vp, u32, u64p]),
     "pt_tracer_create": (i32, [vp, C.POINTER(vp)]),

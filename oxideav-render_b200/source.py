@@ -10,11 +10,13 @@ call raises `Eof`, and the duration is one second.
 `AnimatedRenderSource` is the animation-aware variant the reference leaves
 for later (src/source.rs:12-17): frame k is the scene at time
 start + k / fps, rendered with `opts.time` set to that time; its pts is k
-in units of 1 / fps. Every frame re-prepares the scene it is given — with
-the device BVH builder that is a few milliseconds for scenes of 10^5-10^6
-triangles (upload, device mip chains, device tree) before the frame's
-refine — and the renderer keeps its device accumulator and wave buffers
-between frames.
+in units of 1 / fps. A renderer with `render_frame` (the CUDA path
+tracer) refits the resident scene's BVH when a frame keeps the previous
+frame's draw items and triangle counts (new streams and tables, the tree's
+structure kept, bounds recomputed on the device); otherwise every frame
+re-prepares the scene it is given (with the device BVH builder a few
+milliseconds for 10^5-10^6 triangles). The renderer keeps its device
+accumulator and wave buffers between frames.
 """
 from __future__ import annotations
 
@@ -122,7 +124,8 @@ class AnimatedRenderSource:
             raise Eof()
         k = self._next
         t = self.time_of(k)
-        img = self.renderer.render(self._scene_at(t), self.opts.replace(time=t))
+        render = getattr(self.renderer, "render_frame", self.renderer.render)
+        img = render(self._scene_at(t), self.opts.replace(time=t))
         self._next += 1
         return rgba_image_to_video_frame(img, k)
 

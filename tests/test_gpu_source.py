@@ -60,3 +60,58 @@ def test_animated_frames_equal_direct_renders(ctx):
     assert not np.array_equal(frames[0], frames[2])
     with pytest.raises(Eof):
         src.next_frame()
+
+
+def moving_soup(t: float, seed: int = 3) -> PreparedScene:
+    """A 20k-triangle soup whose triangles drift with time (the same draw
+    items and triangle counts in every frame): the refit case."""
+    import copy
+    s = copy.deepcopy(ts.random_soup(20000, seed=seed))
+    rng = np.random.default_rng(seed + 1)
+    for it in s.items:
+        pos = it.positions.reshape(-1, 3, 3)
+        vel = rng.normal(size=(pos.shape[0], 1, 3)).astype(np.float32) * 0.05
+        it.positions = np.ascontiguousarray((pos + vel * np.float32(t)).reshape(it.positions.shape).astype(np.float32))
+    s._bounds = None
+    return s
+
+
+@pytest.mark.parametrize("builder", ["auto", "spatial"])
+def test_refitted_frames_equal_fresh_builds(ctx, builder):
+    # render_frame refits the resident scene's tree from frame to frame; each
+    # frame must equal a fresh render (fresh upload and BVH build) of the
+    # scene at that time, bit for bit.
+    from oxideav_render_b200 import abi
+    o = ts.pt_opts(48, 4, 4, scene_camera=0, ambient=0.1)
+    ctx.set_bvh_builder(abi.PT_BVH_BUILD_HOST_SPATIAL if builder == "spatial" else abi.PT_BVH_BUILD_AUTO)
+    try:
+        r = api.PathTraceCudaRenderer(ctx)
+        for k, t in enumerate([0.0, 0.5, 1.0, 3.0]):
+            scene = moving_soup(t)
+            got = r.render_frame(scene, o.replace(time=t))
+            sid = r.tracer.scene_id
+            secs = ctx.upload_seconds(sid)
+            if k > 0:
+                # The tracer kept its scene id: the frame was a refit, not an upload.
+                assert sid == first_sid
+                assert secs["device_bvh"] >= 0.0
+            else:
+                first_sid = sid
+            want = api.PathTraceCudaRenderer(ctx).render(scene, o.replace(time=t))
+            assert np.array_equal(got, want), (builder, t)
+        r.tracer.close()
+    finally:
+        ctx.set_bvh_builder(abi.PT_BVH_BUILD_AUTO)
+
+
+def test_refit_rejects_a_different_topology(ctx):
+    o = ts.pt_opts(32, 2, 2, scene_camera=0, ambient=0.1)
+    a = ts.random_soup(5000, seed=1)
+    sid = ctx.upload(a.to_desc(o))
+    try:
+        with pytest.raises(api.RenderError):
+            ctx.refit(sid, ts.random_soup(5001, seed=1).to_desc(o))
+        # A frame of the same topology refits in place.
+        ctx.refit(sid, ts.random_soup(5000, seed=2).to_desc(o))
+    finally:
+        ctx.release(sid)

@@ -28,6 +28,7 @@ def test_autotune_records_a_class_choice_and_keeps_images(ctx):
     assert choice["node_width_extension"] in (2, 4) and choice["node_width_shadow"] in (2, 4)
     assert choice["material_sort"] in (0, 1) and choice["wave_slots"] > 0
     assert choice["shade_blocks_per_sm"] in (3, 4) and choice["wave_arenas"] in (2, 3)
+    assert choice["traversal_threads"] in (128, 256) and choice["claim_chunk"] in (1, 2, 4)
     assert choice["samples_per_s"] > 0
     assert ctx.tune_lookup(t) == choice
     # The tracer's own accumulator was not touched; tuned refines continue it.
@@ -87,3 +88,26 @@ def test_server_without_material_sort_matches(ctx):
         assert np.array_equal(srv.wait(srv.submit(k, o))[0], want)
     finally:
         srv.close()
+
+
+@pytest.mark.parametrize("threads,chunk", [(128, 1), (256, 2), (256, 4), (128, 4)])
+def test_traversal_block_size_and_claim_chunk_keep_images(ctx, threads, chunk):
+    # The traversal kernels' block size and refill chunk only change which
+    # lane traces which ray and when: accumulators and ray counts are equal.
+    cases = [(ts.random_soup(20000, seed=3), ts.pt_opts(48, 4, 6)), ts.sphere_grid_c1(48, 2)]
+    for scene, o in cases:
+        ref = api.PathTracer(ctx)
+        ref.sync(scene, o)
+        ref.refine(o.path_trace.samples_per_pixel)
+        want, rays = ref.accum(), ref.ray_counts()
+        ref.close()
+        ctx.set_traversal(threads, chunk)
+        try:
+            t = api.PathTracer(ctx)
+            t.sync(scene, o)
+            t.refine(o.path_trace.samples_per_pixel)
+            assert np.array_equal(t.accum(), want)
+            assert t.ray_counts() == rays
+            t.close()
+        finally:
+            ctx.set_traversal(256, 1)
