@@ -62,11 +62,11 @@ def test_animated_frames_equal_direct_renders(ctx):
         src.next_frame()
 
 
-def moving_soup(t: float, seed: int = 3) -> PreparedScene:
-    """A 20k-triangle soup whose triangles drift with time (the same draw
-    items and triangle counts in every frame): the refit case."""
+def moving_soup(t: float, seed: int = 3, tris: int = 20000) -> PreparedScene:
+    """A random soup whose triangles drift with time (the same draw items and
+    triangle counts in every frame): the refit case."""
     import copy
-    s = copy.deepcopy(ts.random_soup(20000, seed=seed))
+    s = copy.deepcopy(ts.random_soup(tris, seed=seed))
     rng = np.random.default_rng(seed + 1)
     for it in s.items:
         pos = it.positions.reshape(-1, 3, 3)
@@ -106,12 +106,12 @@ def test_refitted_frames_equal_fresh_builds(ctx, builder):
 
 def test_refit_rejects_a_different_topology(ctx):
     o = ts.pt_opts(32, 2, 2, scene_camera=0, ambient=0.1)
-    a = ts.random_soup(5000, seed=1)
+    a = moving_soup(0.0, seed=1, tris=5000)
     sid = ctx.upload(a.to_desc(o))
     try:
         with pytest.raises(api.RenderError):
             ctx.refit(sid, ts.random_soup(5001, seed=1).to_desc(o))
-        # A frame of the same topology refits in place.
-        ctx.refit(sid, ts.random_soup(5000, seed=2).to_desc(o))
+        # A frame of the same topology (the same soup, moved) refits in place.
+        ctx.refit(sid, moving_soup(0.7, seed=1, tris=5000).to_desc(o))
     finally:
         ctx.release(sid)
