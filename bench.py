@@ -304,10 +304,10 @@ def run_served_batch(ctx, api, torch, reqs, args, tracers):
         st = srv.stats()
     finally:
         srv.close()
-    wall = sum(r["wall_s"] for r in runs) / len(runs)
-    return {"value": total / wall, "unit": "samples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": 1000 * wall, "p50_ms": statistics.mean(r["p50_ms"] for r in runs),
-            "p99_ms": statistics.mean(r["p99_ms"] for r in runs),
+    wall = statistics.median(r["wall_s"] for r in runs)
+    return {"value": total / wall, "walls_s": [r["wall_s"] for r in runs], "wall_stat": "median", "unit": "samples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": 1000 * wall, "p50_ms": statistics.median(r["p50_ms"] for r in runs),
+            "p99_ms": statistics.median(r["p99_ms"] for r in runs),
             "call": "pt_server_submit of every request at once to a warm server (scenes resident), "
                     "pt_server_wait copies each HDR image to host memory; wall clock first submit -> last image",
             "steps": len(runs), "server_gpu_mrays_per_s": st["rays"] / (st["gpu_ms"] / 1000.0) / 1e6
@@ -515,6 +515,30 @@ def profiled_traffic(kernel: str, config: str, wave_paths: int):
             w = re.search(r"profiled_wave_paths \| (\d+)", text)
             scale = wave_paths / int(w.group(1)) if w else 1.0
             return int(int(m.group(1)) * scale)
+    return None
+
+
+def profiled_l2(kernel: str, config: str, wave_paths: int):
+    """L2 figures of `kernel` from the committed ncu summary (lines
+    `l2_bytes_per_launch | N` and `l2_pct_of_peak | X`): the L2 traffic
+    (lts__t_sectors x 32 B) per launch, scaled like the DRAM traffic, and the
+    L2 throughput as a share of its peak (the traversal kernels' tree and
+    records live in L2, so this is their nearer bound)."""
+    import glob
+    import re
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_*.md"))):
+        text = open(path).read()
+        if f"config={config}" not in text:
+            continue
+        b = re.search(r"l2_bytes_per_launch \| (\d+)", text)
+        pct = re.search(r"l2_pct_of_peak \| ([0-9.]+)", text)
+        if not b and not pct:
+            continue
+        w = re.search(r"profiled_wave_paths \| (\d+)", text)
+        scale = wave_paths / int(w.group(1)) if w else 1.0
+        return {"bytes_per_launch": int(int(b.group(1)) * scale) if b else None,
+                "pct_of_peak": float(pct.group(1)) if pct else None,
+                "source": os.path.relpath(path, ROOT)}
     return None
 
 
@@ -763,7 +787,9 @@ def stage_roofline(bc, peak, peak_kind, config_tag, wave_paths):
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": profiled_traffic(names[dom], config_tag, wave_paths), "peak_kind": peak_kind,
             "kernel": names[dom], "bytes_per_launch": stage_bytes[dom] / max(launches, 1),
-            "ms_per_launch": stage[dom] / max(launches, 1), "launches": int(launches)}
+            "ms_per_launch": stage[dom] / max(launches, 1), "launches": int(launches),
+            "l2": profiled_l2(names[dom], config_tag, wave_paths),
+            "stage_share": stage[dom] / max(sum(v for v in stage.values() if v > 0), 1e-9)}
 
 
 def run_frame(ctx, api, torch, args, ws, rank, flush):
@@ -966,7 +992,7 @@ def main():
                     help="scene of the secondary single-frame measurement")
     ap.add_argument("--no-frame", dest="frame", action="store_false", help="skip the single-frame measurement")
     ap.add_argument("--frame-steps", type=int, default=5)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed-per-rank", action="store_true")

@@ -101,6 +101,7 @@ struct Request {
   uint32_t w = 0, h = 0;
   float *hdr = nullptr;               // pinned host image, w * h * 4 floats
   size_t hdr_bytes = 0;
+  uint32_t readers = 0;               // waits copying `hdr` out (outside the lock)
   bool has_deadline = false;
   Clock::time_point deadline;
   // Cancelled (or timed out) while its last wave was on the GPU: it ends
@@ -780,6 +781,18 @@ pt_status pt_server_create(pt_context *ctx, const pt_server_config *cfg, pt_serv
       s->eng->overlap_arenas = 0;
     }
     s->autotune = c.autotune != 0;
+    {
+      // Accumulators and wave tables are stream-ordered allocations from the
+      // device's default pool: keep freed memory cached in the pool instead
+      // of returning it at every synchronisation (a request's accumulator
+      // comes and goes with every request).
+      cudaMemPool_t pool = nullptr;
+      if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+        uint64_t keep = c.hbm_budget_bytes ? c.hbm_budget_bytes : UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      cudaGetLastError();
+    }
     s->spatial_bvh = c.bvh_binned == 0;
     s->flights.resize(s->depth + 1);
     cudaError_t e = cudaSuccess;
@@ -976,7 +989,13 @@ pt_status pt_server_wait(pt_server *s, uint64_t ticket, int32_t timeout_ms, floa
   const size_t nf = (size_t)r->w * r->h * 4;
   if (hdr) {
     if (hdr_floats < nf) return sfail(PT_ERR_INVALID_ARG, "output buffer too small");
+    // The copy runs without the lock (the worker keeps launching waves);
+    // release waits for readers before the pinned buffer is recycled.
+    r->readers++;
+    lk.unlock();
     std::memcpy(hdr, r->hdr, nf * sizeof(float));
+    lk.lock();
+    if (--r->readers == 0) s->cv_done.notify_all();
   }
   if (stats) {
     stats->queue_ms = ms_between(r->t_submit, r->t_admit);
@@ -1011,12 +1030,17 @@ pt_status pt_server_debug_fail_allocations(pt_server *s, uint32_t count) {
 
 pt_status pt_server_release(pt_server *s, uint64_t ticket) {
   if (!s) return sfail(PT_ERR_INVALID_ARG, "server is NULL");
-  std::lock_guard<std::mutex> g(s->mu);
+  std::unique_lock<std::mutex> lk(s->mu);
   auto it = s->reqs.find(ticket);
   if (it == s->reqs.end()) return sfail(PT_ERR_NOT_FOUND, "ticket " + std::to_string(ticket) + " is unknown");
-  Request &r = *it->second;
+  std::shared_ptr<Request> keep = it->second;
+  Request &r = *keep;
   if (r.state != RState::Done && r.state != RState::Failed)
     return sfail(PT_ERR_INVALID_ARG, "request " + std::to_string(ticket) + " is still running");
+  // A wait of another thread may still be copying the image out.
+  s->cv_done.wait(lk, [&] { return r.readers == 0; });
+  it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return sfail(PT_ERR_NOT_FOUND, "ticket " + std::to_string(ticket) + " is unknown");
   s->pinned.put(r.hdr, r.hdr_bytes);
   r.hdr = nullptr;
   if (r.acc && --r.acc->refs == 0) s->dead_accums.push_back(r.acc);
