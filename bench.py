@@ -315,35 +315,42 @@ def run_served_batch(ctx, api, torch, reqs, args, tracers):
             "bit_identical_checked": len(identical), "bit_identical": all(identical) if identical else None}
 
 
-def run_plain_requests(ctx, api, torch, reqs, tracers):
+def run_plain_requests(ctx, api, torch, reqs, tracers, passes: int = 3):
     """The plain per-request GPU path on the same requests, one after
     another in request order: PathTraceCudaRenderer.render_hdr per request
     (PathTraceRenderer::render_hdr: the scene prepared and uploaded per call,
     refine, HDR read back), and refine + hdr on the request's tracer whose
-    scene is already uploaded. Latencies assume every request arrived at
-    once (first come, first served)."""
+    scene is already uploaded. Each request's times are the median of
+    `passes` passes (host-side preparation is sensitive to other load on the
+    host). Latencies assume every request arrived at once (first come, first
+    served)."""
     renderer = api.PathTraceCudaRenderer(ctx)
-    one, res = [], []
-    for (k, s, o, env), t in zip(reqs, tracers):
-        renderer.tracer_mut().set_environment(api.EnvironmentMap(env) if env is not None else None)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        renderer.render_hdr(s, o)
-        one.append(time.perf_counter() - t0)
-        t.reset()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        t.refine(o.path_trace.samples_per_pixel)
-        t.hdr()
-        res.append(time.perf_counter() - t0)
+    one = [[] for _ in reqs]
+    res = [[] for _ in reqs]
+    for _ in range(passes):
+        for i, ((k, s, o, env), t) in enumerate(zip(reqs, tracers)):
+            renderer.tracer_mut().set_environment(api.EnvironmentMap(env) if env is not None else None)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            renderer.render_hdr(s, o)
+            one[i].append(time.perf_counter() - t0)
+            t.reset()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            t.refine(o.path_trace.samples_per_pixel)
+            t.hdr()
+            res[i].append(time.perf_counter() - t0)
     renderer.tracer.close()
+    one = [statistics.median(x) for x in one]
+    res = [statistics.median(x) for x in res]
     total = sum(request_samples(o) for _, _, o, _ in reqs)
     return {"one_shot": {"samples_per_s": total / sum(one), "wall_s": sum(one),
                          **percentiles(1000 * np.cumsum(one)),
                          "call": "PathTraceCudaRenderer.render_hdr per request (scene prepared + uploaded per call)"},
             "resident": {"samples_per_s": total / sum(res), "wall_s": sum(res),
                          **percentiles(1000 * np.cumsum(res)),
-                         "call": "PathTracer.refine + hdr per request, its scene already on the device"}}
+                         "call": "PathTracer.refine + hdr per request, its scene already on the device"},
+            "passes": passes, "per_request_stat": "median"}
 
 
 def serving_scenes(n: int, seed: int):
