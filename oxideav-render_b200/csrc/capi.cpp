@@ -144,6 +144,7 @@ Job make_job(const pt_tracer &t, const SceneHost &sc, const EnvHost *env, uint32
   j.iterations = t.opts.path_trace.max_bounces + 1;
   j.shadow_slots = sc.light_count + 1;
   j.scene_key = t.scene_id;
+  j.area = sc.dev.em_count > 0 || env != nullptr;
   return j;
 }
 
@@ -343,9 +344,13 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
   if (overlap && (st = engine_overlap_begin(ctx)) != PT_OK) return st;
   for (size_t i = 0; i < waves.size(); ++i) {
     uint32_t iters = 1;
-    for (const WaveSegment &s : waves[i]) iters = std::max(iters, jobs[s.request].iterations);
+    bool area = false;
+    for (const WaveSegment &s : waves[i]) {
+      iters = std::max(iters, jobs[s.request].iterations);
+      area = area || jobs[s.request].area;
+    }
     st = launch_wave(ctx, ctx->d_reqs, ctx->d_segs + first_seg[i], waves[i], iters, &timer,
-                     overlap ? (int)(i % ctx->overlap_arenas) : -1);
+                     overlap ? (int)(i % ctx->overlap_arenas) : -1, area);
     if (st != PT_OK) return st;
   }
   timer.mark(STAGE_END, ctx->stream);
@@ -716,7 +721,8 @@ pt_status engine_overlap_begin(pt_context *ctx) {
 }
 
 pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
-                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena) {
+                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena,
+                      bool area) {
   uint32_t nseg = (uint32_t)segs.size(), total = 0, max_pix = 0;
   for (const WaveSegment &s : segs) {
     total += s.pixel_count * s.spp;
@@ -737,7 +743,7 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
     if (own_stream) CK(ctx, cudaStreamWaitEvent(ws, ctx->ev_accumulated[arena], 0));
     // Pageable source: the copy is staged before the call returns and lands
     // in stream order, after the previous wave has read its descriptor.
-    WaveDesc wd{d_reqs, d_segs, nseg, total, max_pix, 0};
+    WaveDesc wd{d_reqs, d_segs, nseg, total, max_pix, area ? (uint32_t)WAVE_AREA_LIGHTS : 0u};
     CK(ctx, cudaMemcpyAsync(w.desc, &wd, sizeof wd, cudaMemcpyHostToDevice, ws));
     const bool timed = timer && timer->events;
     if (ctx->use_graphs && !timed) {

@@ -134,6 +134,7 @@ struct Job {
   uint32_t iterations = 1;
   uint32_t shadow_slots = 1;
   uint32_t scene_key = 0;  // only orders the packing (locality)
+  bool area = false;       // emissive triangles or an environment: the wave runs k_wf_nee
   bool finished() const { return done >= target; }
 };
 
@@ -160,8 +161,10 @@ pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, u
 // in that arena on its own stream (after the arena's previous accumulate)
 // and accumulated on ctx->stream after the trace (engine_reserve must have
 // been asked for both arenas, and engine_overlap_begin called).
+// `area`: some job of the wave has emissive triangles or an environment.
 pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
-                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena = -1);
+                      const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena = -1,
+                      bool area = true);
 // Makes both wave streams wait for the work enqueued on ctx->stream so far
 // (request / segment uploads, counter reset) before overlapped waves.
 pt_status engine_overlap_begin(pt_context *ctx);

@@ -168,8 +168,10 @@ struct WaveBuffers {
 struct WaveDesc {
   const DevRequest *reqs;
   const WaveSegment *segs;
-  uint32_t nseg, total, max_pix, pad;
+  uint32_t nseg, total, max_pix;
+  uint32_t flags;  // WAVE_AREA_LIGHTS: some request has emissive triangles or an environment
 };
+enum WaveFlags : uint32_t { WAVE_AREA_LIGHTS = 1u };
 constexpr uint32_t kSortBuckets = 256;
 
 // Per-launch device counters (rays traced, traversal work, errors).

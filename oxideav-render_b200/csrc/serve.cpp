@@ -497,6 +497,7 @@ void launch_next_wave(pt_server *s) {
   std::vector<DevRequest> table;
   std::vector<uint32_t> carried;
   uint32_t iters = 1, shadow = 1;
+  bool area = false;
   uint64_t total = 0;
   for (WaveSegment &sg : segs) {
     if (remap[sg.request] < 0) {
@@ -505,6 +506,7 @@ void launch_next_wave(pt_server *s) {
       carried.push_back(sg.request);
       iters = std::max(iters, jobs[sg.request].iterations);
       shadow = std::max(shadow, jobs[sg.request].shadow_slots);
+      area = area || jobs[sg.request].area;
     }
     total += (uint64_t)sg.pixel_count * sg.spp;
     sg.request = (uint32_t)remap[sg.request];
@@ -539,7 +541,7 @@ void launch_next_wave(pt_server *s) {
     break_server(s, std::string("wave upload: ") + cudaGetErrorString(e));
     return;
   }
-  pst = launch_wave(s->eng, f.d_reqs, f.d_segs, segs, iters, nullptr, arena);
+  pst = launch_wave(s->eng, f.d_reqs, f.d_segs, segs, iters, nullptr, arena, area);
   if (pst != PT_OK) {
     break_server(s, "wave launch: " + s->eng->err);
     return;

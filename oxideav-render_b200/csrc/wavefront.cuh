@@ -308,6 +308,7 @@ __global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t
 // hit something, in the order shade will read them (its queue). Values are
 // those shade would compute inline (the same functions on the same inputs).
 __global__ void __launch_bounds__(256) k_wf_nee(WaveBuffers w, uint32_t iter) {
+  if (!(w.desc->flags & WAVE_AREA_LIGHTS)) return;  // nothing to sample in this wave
   const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
   const uint32_t *q = w.sort_materials ? w.q_sorted : w.q[iter & 1u];
@@ -319,6 +320,7 @@ __global__ void __launch_bounds__(256) k_wf_nee(WaveBuffers w, uint32_t iter) {
     const uint4 sd = w.seed[slot];
     const DevRequest &rq = reqs[sd.w];
     const DevScene &s = *rq.scene;
+    if (!rq.env && s.em_count == 0) continue;  // shade reads nothing for this request
     const uint32_t k = __float_as_uint(w.o[slot].w);
     const uint32_t g = hg & HIT_G_MASK;
     const float4 tb = w.hit_tb[slot];
@@ -379,7 +381,9 @@ __global__ void __launch_bounds__(128, kBlocks) k_wf_shade(WaveBuffers w, uint32
     }
     DeferredSink sink{&w, slot, 0};
     NeeInput pre;
-    if (found) {
+    pre.area.go = false;
+    pre.pl_emit = 0.0f;
+    if (found && (rq.env || rq.scene->em_count > 0)) {
       const size_t cap = w.capacity;
       const float4 n2 = w.nee[2 * cap + slot];
       pre.area.go = n2.y != 0.0f;
