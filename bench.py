@@ -781,15 +781,23 @@ def stage_roofline(bc, peak, peak_kind, config_tag, wave_paths):
     stage_bytes = {
         "extend": 48 * ext + 64 * bc["ext_nodes"] + 48 * bc["ext_tris"],
         "shadow": 48 * shadow + 64 * bc["sh_nodes"] + 48 * bc["sh_tris"],
-        "shade": ext * (16 + 128 + 32) + 32 * shadow,
+        # Per shaded vertex: hit (t, barycentrics, id: 20 B), path state read
+        # (7 x 16 B) and written back (5 x 16 B), the triangle's corner
+        # positions and normals (2 x 36 B) and material / flag word (8 B), the
+        # NEE kernel's precomputed sample (16 B read), queue traffic (3 x 4 B);
+        # per shadow ray written: origin, direction, contribution (48 B).
+        "shade": ext * (20 + 112 + 80 + 72 + 8 + 16 + 12) + 48 * shadow,
+        # Per vertex: hit and seeds read (36 B), corner positions (36 B),
+        # previous vertex (16 B), the sample written (48 B).
+        "nee": ext * (36 + 36 + 16 + 48),
         "megakernel": algorithmic_bytes(ext, shadow, bc["ext_nodes"] + bc["sh_nodes"],
                                         bc["ext_tris"] + bc["sh_tris"], 0),
         "accumulate": 32 * bc["samples"],
     }
     names = {"extend": "k_wf_extend", "shade": "k_wf_shade", "shadow": "k_wf_shadow", "megakernel": "k_megakernel",
-             "accumulate": "k_accumulate"}
+             "accumulate": "k_accumulate", "nee": "k_wf_nee"}
     dom = max((k for k in stage_bytes if stage.get(k, 0) > 0), key=lambda k: stage[k])
-    launches = bc["rounds"] if dom in ("extend", "shade", "shadow") else bc["waves"]
+    launches = bc["rounds"] if dom in ("extend", "shade", "shadow", "nee") else bc["waves"]
     achieved = stage_bytes[dom] / (stage[dom] / 1000.0) / 1e9
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": profiled_traffic(names[dom], config_tag, wave_paths), "peak_kind": peak_kind,
