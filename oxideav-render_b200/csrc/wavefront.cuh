@@ -207,8 +207,10 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_extend(WaveBuf
       ts.ext_rays++;
     }
     if (!__any_sync(0xffffffffu, has)) break;
-    // Node phase: while any lane still looks for its first leaf.
-    while (__any_sync(0xffffffffu, has && cr.core.searching())) {
+    // Node phase: until at most kNodePhaseStragglers lanes still look for
+    // their first leaf (they go on in the next round).
+    while (node_phase_goes_on(has && cr.core.searching(),
+                              has && (cr.core.leaf != kTravDone || cr.core.finished()))) {
       if (has && cr.core.can_step()) cr.node_step(*rq->scene, stk, ts.ext_nodes, ts.err);
     }
     // Leaf phase.
@@ -456,8 +458,9 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_shadow(WaveBuf
       if (has) start_ray();
     }
     if (!__any_sync(0xffffffffu, has)) break;
-    // Node phase: while any lane still looks for its first leaf.
-    while (__any_sync(0xffffffffu, has && tr.core.searching())) {
+    // Node phase: until at most kNodePhaseStragglers lanes still search.
+    while (node_phase_goes_on(has && tr.core.searching(),
+                              has && (tr.core.leaf != kTravDone || tr.core.finished()))) {
       if (has && tr.core.can_step()) tr.node_step(*rq->scene, stk, ts.sh_nodes, ts.err);
     }
     // Leaf phase.
