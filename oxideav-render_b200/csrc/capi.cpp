@@ -145,6 +145,7 @@ Job make_job(const pt_tracer &t, const SceneHost &sc, const EnvHost *env, uint32
   j.shadow_slots = sc.light_count + 1;
   j.scene_key = t.scene_id;
   j.area = sc.dev.em_count > 0 || env != nullptr;
+  j.wide = sc.dev.nodes4 ? j.req.wide_nodes & (uint32_t)(WIDE_EXTENSION | WIDE_SHADOW) : 0u;
   return j;
 }
 
@@ -343,14 +344,15 @@ pt_status run_jobs(pt_context *ctx, std::vector<pt_tracer *> &tracers, std::vect
   CK(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
   if (overlap && (st = engine_overlap_begin(ctx)) != PT_OK) return st;
   for (size_t i = 0; i < waves.size(); ++i) {
-    uint32_t iters = 1;
+    uint32_t iters = 1, wide = WIDE_EXTENSION | WIDE_SHADOW;
     bool area = false;
     for (const WaveSegment &s : waves[i]) {
       iters = std::max(iters, jobs[s.request].iterations);
       area = area || jobs[s.request].area;
+      wide &= jobs[s.request].wide;
     }
     st = launch_wave(ctx, ctx->d_reqs, ctx->d_segs + first_seg[i], waves[i], iters, &timer,
-                     overlap ? (int)(i % ctx->overlap_arenas) : -1, area);
+                     overlap ? (int)(i % ctx->overlap_arenas) : -1, area, wide);
     if (st != PT_OK) return st;
   }
   timer.mark(STAGE_END, ctx->stream);
@@ -514,6 +516,7 @@ pt_status autotune_scene(pt_context *ctx, const pt_tracer *t, SceneHost *sc, con
       std::vector<pt_tracer *> tr{&s};
       std::vector<Job> jobs{make_job(s, *sc, env, spp)};
       jobs[0].req.wide_nodes = c.wide_nodes;
+      jobs[0].wide = sc->dev.nodes4 ? c.wide_nodes : 0u;
       pt_status st = run_jobs(ctx, tr, jobs, nullptr);
       if (st != PT_OK) return st;
       if (ms < 0.0f || ctx->last_batch_ms < ms) ms = ctx->last_batch_ms;
@@ -722,7 +725,7 @@ pt_status engine_overlap_begin(pt_context *ctx) {
 
 pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
                       const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena,
-                      bool area) {
+                      bool area, uint32_t all_wide) {
   uint32_t nseg = (uint32_t)segs.size(), total = 0, max_pix = 0;
   for (const WaveSegment &s : segs) {
     total += s.pixel_count * s.spp;
@@ -737,6 +740,7 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
     w.shade_blocks = ctx->shade_blocks == 4 ? 4u : 3u;
     w.trav_threads = ctx->trav_threads == 128 ? 128u : 256u;
     w.claim_chunk = ctx->claim_chunk == 2 || ctx->claim_chunk == 4 ? ctx->claim_chunk : 1u;
+    w.all_wide = all_wide & (uint32_t)(WIDE_EXTENSION | WIDE_SHADOW);
     cudaStream_t ws = own_stream ? ctx->wave_streams[arena] : ctx->stream;
     // The arena's previous wave must be accumulated before this one
     // overwrites its descriptor, queues and per-slot radiance.
@@ -747,10 +751,10 @@ pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegme
     CK(ctx, cudaMemcpyAsync(w.desc, &wd, sizeof wd, cudaMemcpyHostToDevice, ws));
     const bool timed = timer && timer->events;
     if (ctx->use_graphs && !timed) {
-      // One captured graph per (bounce count, arena / whole wave, shade
-      // variant, material sort) replays the wave: one launch instead of ~6
-      // per bounce.
-      const uint32_t key = iters << 10 | w.claim_chunk << 7 | (w.trav_threads == 128 ? 64u : 0u) |
+      // One captured graph per (bounce count, traversal variant, arena /
+      // whole wave, shade variant, material sort) replays the wave: one
+      // launch instead of ~6 per bounce.
+      const uint32_t key = iters << 12 | w.all_wide << 10 | w.claim_chunk << 7 | (w.trav_threads == 128 ? 64u : 0u) |
                            (own_stream ? 4u * (1u + (uint32_t)arena) : 0u) | (w.shade_blocks == 4 ? 2u : 0u) |
                            w.sort_materials;
       auto it = ctx->graphs.find(key);

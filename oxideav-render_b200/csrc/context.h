@@ -135,6 +135,7 @@ struct Job {
   uint32_t shadow_slots = 1;
   uint32_t scene_key = 0;  // only orders the packing (locality)
   bool area = false;       // emissive triangles or an environment: the wave runs k_wf_nee
+  uint32_t wide = 0;       // WIDE_* bits of the request that its scene's layouts honour
   bool finished() const { return done >= target; }
 };
 
@@ -164,7 +165,7 @@ pt_status engine_reserve(pt_context *ctx, size_t slots, uint32_t shadow_slots, u
 // `area`: some job of the wave has emissive triangles or an environment.
 pt_status launch_wave(pt_context *ctx, const DevRequest *d_reqs, const WaveSegment *d_segs,
                       const std::vector<WaveSegment> &segs, uint32_t iters, StageTimer *timer, int arena = -1,
-                      bool area = true);
+                      bool area = true, uint32_t all_wide = 0);
 // Makes both wave streams wait for the work enqueued on ctx->stream so far
 // (request / segment uploads, counter reset) before overlapped waves.
 pt_status engine_overlap_begin(pt_context *ctx);

@@ -160,6 +160,7 @@ struct WaveBuffers {
   uint32_t shade_blocks;       // 3 or 4: the k_wf_shade instantiation (blocks per SM)
   uint32_t trav_threads;       // 128 or 256: block size of the traversal kernels (1,024 threads per SM)
   uint32_t claim_chunk;        // 1, 2 or 4: queue entries a traversal lane claims per refill
+  uint32_t all_wide;           // WIDE_* bits that hold for every request of the wave (host-side launch choice)
 };
 
 // What changes from one wave to the next, read by the kernels from device

@@ -467,7 +467,9 @@ struct SpatialBuilder {
     uint64_t budget;
   };
   static constexpr int kObjBins = 16, kSpatialBins = 32;
-  static constexpr uint32_t kMaxLeaf = 8;
+  // Leaves of at most four references: a warp's leaf phase waits for its
+  // largest leaf, and on the request mix 4 traced 1 % faster than 8.
+  static constexpr uint32_t kMaxLeaf = 4;
   static constexpr uint32_t kLocalThreshold = 4096;
   static constexpr uint32_t kParallelNode = 262144;  // nodes binned on three threads
   static constexpr float kAlpha = 1e-5f;

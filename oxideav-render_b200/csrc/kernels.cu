@@ -308,22 +308,45 @@ cudaError_t launch_megakernel(const DevRequest *reqs, const WaveSegment *segs, u
 // extend / shade / shadow over device-side queue counters (no host sync).
 // The traversal kernels are persistent: exactly the blocks that fit at once
 // (occupancy queried once, outside any stream capture).
-// Index 0: the 256-thread instantiations, 1: the 128-thread ones.
-void persistent_blocks(int per_sm_ext[2], int per_sm_sh[2]) {
-  static int ext[2] = {0, 0}, sh[2] = {0, 0};
-  if (ext[0] == 0) {
+// Index [t][o]: t = 0 the 256-thread instantiations, 1 the 128-thread ones;
+// o = 1 the four-child-only ones.
+void persistent_blocks(int per_sm_ext[2][2], int per_sm_sh[2][2]) {
+  static int ext[2][2] = {}, sh[2][2] = {};
+  if (ext[0][0] == 0) {
     auto q = [](int &v, const void *fn, int threads) {
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, fn, threads, 0) != cudaSuccess || v < 1) v = 1;
     };
-    q(ext[0], (const void *)k_wf_extend<256>, 256);
-    q(sh[0], (const void *)k_wf_shadow<256>, 256);
-    q(ext[1], (const void *)k_wf_extend<128>, 128);
-    q(sh[1], (const void *)k_wf_shadow<128>, 128);
+    q(ext[0][0], (const void *)k_wf_extend<256, false>, 256);
+    q(ext[0][1], (const void *)k_wf_extend<256, true>, 256);
+    q(sh[0][0], (const void *)k_wf_shadow<256, false>, 256);
+    q(sh[0][1], (const void *)k_wf_shadow<256, true>, 256);
+    q(ext[1][0], (const void *)k_wf_extend<128, false>, 128);
+    q(ext[1][1], (const void *)k_wf_extend<128, true>, 128);
+    q(sh[1][0], (const void *)k_wf_shadow<128, false>, 128);
+    q(sh[1][1], (const void *)k_wf_shadow<128, true>, 128);
   }
-  for (int k = 0; k < 2; ++k) {
-    per_sm_ext[k] = ext[k];
-    per_sm_sh[k] = sh[k];
-  }
+  for (int t = 0; t < 2; ++t)
+    for (int o = 0; o < 2; ++o) {
+      per_sm_ext[t][o] = ext[t][o];
+      per_sm_sh[t][o] = sh[t][o];
+    }
+}
+
+// The traversal launches of one bounce iteration: block size and node
+// layout choose the instantiation.
+template <int kThreads>
+void launch_extend(const WaveBuffers &w, uint32_t it, DevCounters *ctr, uint32_t grid, bool only4, cudaStream_t st) {
+  if (only4)
+    k_wf_extend<kThreads, true><<<grid, kThreads, 0, st>>>(w, it, ctr);
+  else
+    k_wf_extend<kThreads, false><<<grid, kThreads, 0, st>>>(w, it, ctr);
+}
+template <int kThreads>
+void launch_shadow(const WaveBuffers &w, uint32_t it, DevCounters *ctr, uint32_t grid, bool only4, cudaStream_t st) {
+  if (only4)
+    k_wf_shadow<kThreads, true><<<grid, kThreads, 0, st>>>(w, it, ctr);
+  else
+    k_wf_shadow<kThreads, false><<<grid, kThreads, 0, st>>>(w, it, ctr);
 }
 
 cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaStream_t st,
@@ -334,22 +357,23 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
   if (e == cudaSuccess && w.sort_materials)
     e = cudaMemsetAsync(w.sort_counts, 0, sizeof(uint32_t) * 2 * kSortBuckets * (w.iterations + 1), st);
   if (e != cudaSuccess) return e;
-  int per_sm_ext[2], per_sm_sh[2];
+  int per_sm_ext[2][2], per_sm_sh[2][2];
   persistent_blocks(per_sm_ext, per_sm_sh);
   const bool shade4 = w.shade_blocks == 4;
   const bool t128 = w.trav_threads == 128;
-  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext[t128 ? 1 : 0]),
+  const bool ext4 = (w.all_wide & WIDE_EXTENSION) != 0, sh4 = (w.all_wide & WIDE_SHADOW) != 0;
+  const uint32_t g_ext = (uint32_t)(num_sms * per_sm_ext[t128 ? 1 : 0][ext4 ? 1 : 0]),
                  g_shade = (uint32_t)num_sms * (shade4 ? 8 : 6),
-                 g_sh = (uint32_t)(num_sms * per_sm_sh[t128 ? 1 : 0]), g_wide = (uint32_t)num_sms * 16,
+                 g_sh = (uint32_t)(num_sms * per_sm_sh[t128 ? 1 : 0][sh4 ? 1 : 0]), g_wide = (uint32_t)num_sms * 16,
                  g_nee = (uint32_t)num_sms * 8;
   tm.mark(STAGE_RAYGEN, st);
   k_wf_raygen<<<g_wide, 256, 0, st>>>(w);
   for (uint32_t it = 0; it < w.iterations; ++it) {
     tm.mark(STAGE_EXTEND, st);
     if (t128)
-      k_wf_extend<128><<<g_ext, 128, 0, st>>>(w, it, ctr);
+      launch_extend<128>(w, it, ctr, g_ext, ext4, st);
     else
-      k_wf_extend<256><<<g_ext, 256, 0, st>>>(w, it, ctr);
+      launch_extend<256>(w, it, ctr, g_ext, ext4, st);
     if (w.sort_materials) {
       tm.mark(STAGE_SORT, st);
       k_wf_sort_count<<<g_shade, 256, 0, st>>>(w, it);
@@ -365,9 +389,9 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
       k_wf_shade<3><<<g_shade, 128, 0, st>>>(w, it);
     tm.mark(STAGE_SHADOW, st);
     if (t128)
-      k_wf_shadow<128><<<g_sh, 128, 0, st>>>(w, it, ctr);
+      launch_shadow<128>(w, it, ctr, g_sh, sh4, st);
     else
-      k_wf_shadow<256><<<g_sh, 256, 0, st>>>(w, it, ctr);
+      launch_shadow<256>(w, it, ctr, g_sh, sh4, st);
   }
   if (accumulate) {
     tm.mark(STAGE_ACCUMULATE, st);
@@ -384,7 +408,7 @@ cudaError_t launch_wave_accumulate(const WaveBuffers &w, int num_sms, cudaStream
 cudaError_t capture_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms, cudaGraphExec_t *out,
                               bool accumulate) {
   *out = nullptr;
-  int a[2], b[2];
+  int a[2][2], b[2][2];
   persistent_blocks(a, b);
   cudaStream_t cs = nullptr;
   cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);

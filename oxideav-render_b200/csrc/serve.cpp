@@ -496,7 +496,7 @@ void launch_next_wave(pt_server *s) {
   std::vector<int> remap(n, -1);
   std::vector<DevRequest> table;
   std::vector<uint32_t> carried;
-  uint32_t iters = 1, shadow = 1;
+  uint32_t iters = 1, shadow = 1, wide = WIDE_EXTENSION | WIDE_SHADOW;
   bool area = false;
   uint64_t total = 0;
   for (WaveSegment &sg : segs) {
@@ -507,6 +507,7 @@ void launch_next_wave(pt_server *s) {
       iters = std::max(iters, jobs[sg.request].iterations);
       shadow = std::max(shadow, jobs[sg.request].shadow_slots);
       area = area || jobs[sg.request].area;
+      wide &= jobs[sg.request].wide;
     }
     total += (uint64_t)sg.pixel_count * sg.spp;
     sg.request = (uint32_t)remap[sg.request];
@@ -541,7 +542,7 @@ void launch_next_wave(pt_server *s) {
     break_server(s, std::string("wave upload: ") + cudaGetErrorString(e));
     return;
   }
-  pst = launch_wave(s->eng, f.d_reqs, f.d_segs, segs, iters, nullptr, arena, area);
+  pst = launch_wave(s->eng, f.d_reqs, f.d_segs, segs, iters, nullptr, arena, area, wide);
   if (pst != PT_OK) {
     break_server(s, "wave launch: " + s->eng->err);
     return;

@@ -172,7 +172,9 @@ PT_DEV uint32_t sort_key(const DevScene *s, bool found, uint32_t g) {
 // Closest hit of every queued path: persistent lanes, one ray each, refilled
 // from the queue as rays finish (dev_traverse.cuh), in runs of
 // w.claim_chunk entries. kThreads per block, 1,024 threads per SM.
-template <int kThreads>
+// kOnly4: every request of the wave walks the four-child layout for
+// extension rays (WaveBuffers::all_wide).
+template <int kThreads, bool kOnly4>
 __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_extend(WaveBuffers w, uint32_t iter,
                                                                        DevCounters *ctr) {
   const DevRequest *reqs = w.desc->reqs;
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_extend(WaveBuf
     // their first leaf (they go on in the next round).
     while (node_phase_goes_on(has && cr.core.searching(),
                               has && (cr.core.leaf != kTravDone || cr.core.finished()))) {
-      if (has && cr.core.can_step()) cr.node_step(*rq->scene, stk, ts.ext_nodes, ts.err);
+      if (has && cr.core.can_step()) cr.template node_step<kOnly4>(*rq->scene, stk, ts.ext_nodes, ts.err);
     }
     // Leaf phase.
     if (has) {
@@ -412,7 +414,9 @@ __global__ void __launch_bounds__(128, kBlocks) k_wf_shade(WaveBuffers w, uint32
 // sum rounds as in the megakernel). Persistent lanes own one path at a time
 // and are refilled from the queue when its last ray finishes (runs of
 // w.claim_chunk entries). kThreads per block, 1,024 threads per SM.
-template <int kThreads>
+// kOnly4: every request of the wave walks the four-child layout for shadow
+// rays.
+template <int kThreads, bool kOnly4>
 __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_shadow(WaveBuffers w, uint32_t iter,
                                                                        DevCounters *ctr) {
   const DevRequest *reqs = w.desc->reqs;
@@ -461,7 +465,7 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_shadow(WaveBuf
     // Node phase: until at most kNodePhaseStragglers lanes still search.
     while (node_phase_goes_on(has && tr.core.searching(),
                               has && (tr.core.leaf != kTravDone || tr.core.finished()))) {
-      if (has && tr.core.can_step()) tr.node_step(*rq->scene, stk, ts.sh_nodes, ts.err);
+      if (has && tr.core.can_step()) tr.template node_step<kOnly4>(*rq->scene, stk, ts.sh_nodes, ts.err);
     }
     // Leaf phase.
     if (has) {
