@@ -298,7 +298,9 @@ struct ShadowTrav {
 // meanwhile. Measured on the request mix: closest-hit traversal 701 -> 652
 // ms and shadow rays 519 -> 493 ms per step with 4 (2: 677 / 498, 8: 648 /
 // 487, 12: 672 / 496); on the sphere grid frame 36.6 -> 35.6 ms extend.
-constexpr int kNodePhaseStragglers = 4;
+// With the four-child-only kernels, 6 traced the mix 1 % faster than 4 and
+// the sphere grid frame within 0.2 %.
+constexpr int kNodePhaseStragglers = 6;
 
 // Warp-collective: whether the node phase goes on, given this lane's
 // `searching` (it has a ray and no parked leaf yet) and `ready` (it has a
