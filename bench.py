@@ -861,15 +861,22 @@ def run_frame(ctx, api, torch, args, ws, rank, flush):
     renderer = api.PathTraceCudaRenderer(ctx)
     if env is not None:
         renderer.tracer_mut().set_environment(api.EnvironmentMap(env))
-    e2e_s = []
-    for i in range(3):
+    # One untimed call, then the median of five: a call's host-side
+    # preparation varies from call to call (allocation, page faults), and the
+    # upload's own split is recorded per call.
+    e2e_s, uploads = [], []
+    for i in range(6):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         img = renderer.render(scene, opts)
         if i > 0:
             e2e_s.append(time.perf_counter() - t0)
-    e2e_t = max_over_ranks(sum(e2e_s) / len(e2e_s), ws)
+            uploads.append(ctx.upload_seconds(renderer.tracer.scene_id))
+    e2e_t = max_over_ranks(statistics.median(e2e_s), ws)
+    up = {k: round(1000 * statistics.median(u[k] for u in uploads), 2) for k in uploads[0]}
     out["e2e"] = {"value": samples_per_step * ws / e2e_t, "unit": "samples/s", "ms_per_step": 1000 * e2e_t,
+                  "walls_ms": [round(1000 * t, 1) for t in e2e_s], "wall_stat": "median",
+                  "upload_ms_median": up,
                   "h2d_bytes_per_step": int(ctx.scene_bytes(renderer.tracer.scene_id)),
                   "d2h_bytes_per_step": int(img.nbytes),
                   "call": "PathTraceCudaRenderer.render (scene preparation and upload incl. the BVH build, "
