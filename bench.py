@@ -932,7 +932,7 @@ def run_b200(args):
     peak, peak_kind = load_peaks()
     bc = b["counters"]
     roofline = stage_roofline(bc, peak, peak_kind, "mixed", min(args.wave_slots or (1 << 23), b["total"]))
-    launches = args.steps * (2 * bc["waves"] + 6 * bc["rounds"])
+    launches = args.steps * (2 * bc["waves"] + 8 * bc["rounds"])
 
     # End to end on the same requests through the serving C ABI (host I/O).
     e2e = run_served_batch(ctx, api, torch, reqs, args, tracers)

@@ -237,7 +237,8 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
                     4 * (size_t)kWfCounterStride * (iterations + 1),
                     4 * P, 4 * 2 * (size_t)kSortBuckets * (iterations + 1),   // q_sorted sort_counts
                     sizeof(WaveDesc), 4 * P,                                   // desc sort_keys
-                    3 * 16 * P};                                               // nee
+                    3 * 16 * P,                                                // nee
+                    P * S};                                                    // sh_vis
   size_t off[sizeof(sizes) / sizeof(sizes[0])], total = 0;
   for (size_t i = 0; i < sizeof(sizes) / sizeof(sizes[0]); ++i) {
     total = (total + 255) & ~(size_t)255;
@@ -270,6 +271,7 @@ pt_status ensure_wavefront(pt_context *ctx, uint32_t capacity, uint32_t shadow_s
   w.desc = (WaveDesc *)(b + off[k++]);
   w.sort_keys = (uint32_t *)(b + off[k++]);
   w.nee = (float4 *)(b + off[k++]);
+  w.sh_vis = (uint8_t *)(b + off[k++]);
   w.capacity = capacity;
   w.shadow_slots = shadow_slots;
   w.iterations = iterations;

@@ -139,7 +139,10 @@ struct WaveSegment {
 // Structure-of-arrays path state of one wave of the wavefront schedule
 // (wavefront.cuh), `capacity` slots, `shadow_slots` queued shadow rays per
 // slot.
-constexpr uint32_t kWfCounterStride = 4;  // per iteration: active count, shadow count, spare, spare
+// Per iteration: [0] active count, [1] shadow-queue count, [2] extend claim
+// cursor, [3] shadow claim cursor, [4] most shadow rays of a queued path,
+// [5..7] spare.
+constexpr uint32_t kWfCounterStride = 8;
 
 struct WaveBuffers {
   float4 *o, *d, *beta, *rad, *prev, *sigma;
@@ -148,6 +151,7 @@ struct WaveBuffers {
   uint32_t *hit_g;             // global id | front << 31 | found << 30
   float4 *sh_o, *sh_d, *sh_c;  // [shadow_slots][capacity]: (o, tmax), (d, ray id), (contrib, skip)
   uint32_t *sh_n;              // shadow rays queued per slot
+  uint8_t *sh_vis;             // [shadow_slots][capacity]: 1 where the shadow ray reached its light
   uint32_t *q[2];              // active queues (ping-pong by iteration)
   uint32_t *q_shadow;
   uint32_t *counters;          // [iterations][kWfCounterStride]

@@ -409,6 +409,7 @@ cudaError_t launch_wavefront(const WaveBuffers &w, DevCounters *ctr, int num_sms
       launch_shadow<128>(w, it, ctr, g_sh, sh4, st);
     else
       launch_shadow<256>(w, it, ctr, g_sh, sh4, st);
+    k_wf_shadow_add<<<g_wide, 256, 0, st>>>(w, it);
   }
   if (accumulate) {
     tm.mark(STAGE_ACCUMULATE, st);

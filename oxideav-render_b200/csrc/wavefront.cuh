@@ -13,8 +13,10 @@
 //                 BSDF sampling, roulette; survivors are appended to the next
 //                 active queue and paths with shadow rays to the shadow queue
 //                 (warp-aggregated atomics);
-//   k_wf_shadow   each queued path's shadow rays, in generation order; a
-//                 visible ray adds its contribution to the path radiance.
+//   k_wf_shadow   one lane per queued shadow ray (ray k of every path
+//                 before ray k + 1): whether it reaches its light;
+//   k_wf_shadow_add  each path's visible contributions, added to its
+//                 radiance in generation order.
 // The contributions of a vertex therefore reach the radiance sum in the
 // reference's order (emission, punctual lights, area sample, next vertex):
 // the per-sample radiance is bit-identical to the megakernel's.
@@ -90,6 +92,13 @@ PT_DEV void wf_append(uint32_t *queue, uint32_t *count, bool pred, uint32_t valu
   if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(mask));
   base = __shfl_sync(active, base, leader);
   if (pred) queue[base + __popc(mask & ((1u << lane) - 1u))] = value;
+}
+
+// Warp-aggregated maximum: one atomic per warp.
+PT_DEV void wf_max(uint32_t *dst, uint32_t v) {
+  const uint32_t active = __activemask();
+  const uint32_t m = __reduce_max_sync(active, v);
+  if ((threadIdx.x & 31u) == (uint32_t)(__ffs(active) - 1) && m) atomicMax(dst, m);
 }
 
 struct DeferredSink {
@@ -406,14 +415,18 @@ __global__ void __launch_bounds__(128, kBlocks) k_wf_shade(WaveBuffers w, uint32
     w.sh_n[slot] = sink.count;
     wf_append(q_next, n_next, alive, slot);
     wf_append(w.q_shadow, n_shadow, sink.count > 0, slot);
+    wf_max(n_shadow + 3, sink.count);
   }
 }
 
-// Shadow rays of every queued path, each path's rays in generation order
-// (a visible ray adds its contribution to the path radiance, so the float
-// sum rounds as in the megakernel). Persistent lanes own one path at a time
-// and are refilled from the queue when its last ray finishes (runs of
-// w.claim_chunk entries). kThreads per block, 1,024 threads per SM.
+// Shadow rays of the queued paths, one lane per ray: entry i of the
+// flattened queue is ray k = i / n of queued path i % n (n paths, k below
+// the wave's largest per-path count), so neighbouring lanes trace the same
+// light's rays from neighbouring queue positions. A lane records whether
+// its ray reached the light (sh_vis); k_wf_shadow_add then adds each path's
+// visible contributions in generation order. Entries past a path's own
+// count carry no ray. n times the largest count fits 32 bits: the arena
+// holds 48 bytes per (ray, slot).
 // kOnly4: every request of the wave walks the four-child layout for shadow
 // rays.
 template <int kThreads, bool kOnly4>
@@ -422,46 +435,46 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_shadow(WaveBuf
   const DevRequest *reqs = w.desc->reqs;
   __shared__ int s_stack[kShortStack * kThreads];
   const uint32_t n = w.counters[iter * kWfCounterStride + 1];
+  const uint32_t kmax = min(w.counters[iter * kWfCounterStride + 4], w.shadow_slots);
+  const uint32_t total = n * kmax;
   uint32_t *claim = w.counters + iter * kWfCounterStride + 3;
   TravStack stk;
   stk.sm = s_stack + threadIdx.x;
   stk.stride = blockDim.x;
   ThreadStats ts{0, 0, 0, 0, 0, 0, 0};
   bool has = false, exhausted = false;
-  uint32_t slot = 0, j = 0, cnt = 0, ray_id = 0, skip = 0;
+  size_t e = 0;
+  uint32_t ray_id = 0, skip = 0;
   const DevRequest *rq = nullptr;
   Sampler smp;
-  V3 rad = vzero(), contrib = vzero();
-  float covered = 0.0f;
   ShadowTrav tr;
-  auto start_ray = [&]() {
-    size_t e = (size_t)j * w.capacity + slot;
-    float4 so = w.sh_o[e], sdd = w.sh_d[e], sc = w.sh_c[e];
-    tr.init(*rq->scene, {so.x, so.y, so.z}, {sdd.x, sdd.y, sdd.z}, so.w, (rq->wide_nodes & WIDE_SHADOW) != 0);
-    ray_id = __float_as_uint(sdd.w);
-    contrib = {sc.x, sc.y, sc.z};
-    skip = __float_as_uint(sc.w);
-    ts.shadow_rays++;
-  };
   ClaimedRun run;
   for (;;) {
     uint32_t idx = 0;
-    if (run.take(claim, has, n, exhausted, w.claim_chunk, idx)) {
-      slot = w.q_shadow[idx];
-      uint4 sd = w.seed[slot];
-      rq = reqs + sd.w;
-      smp.pixel_seed = sd.x;
-      smp.index = sd.y;
-      smp.path_seed = sd.z;
-      float4 r = w.rad[slot];
-      rad = {r.x, r.y, r.z};
-      covered = r.w;
-      cnt = w.sh_n[slot];
-      j = 0;
-      has = cnt > 0;
-      if (has) start_ray();
+    if (run.take(claim, has, total, exhausted, w.claim_chunk, idx)) {
+      const uint32_t k = idx / n, q = idx - k * n;
+      const uint32_t slot = w.q_shadow[q];
+      if (k < w.sh_n[slot]) {
+        const uint4 sd = w.seed[slot];
+        rq = reqs + sd.w;
+        smp.pixel_seed = sd.x;
+        smp.index = sd.y;
+        smp.path_seed = sd.z;
+        e = (size_t)k * w.capacity + slot;
+        const float4 so = w.sh_o[e], sdd = w.sh_d[e];
+        tr.init(*rq->scene, {so.x, so.y, so.z}, {sdd.x, sdd.y, sdd.z}, so.w, (rq->wide_nodes & WIDE_SHADOW) != 0);
+        ray_id = __float_as_uint(sdd.w);
+        skip = __float_as_uint(w.sh_c[e].w);
+        ts.shadow_rays++;
+        has = true;
+      }
     }
-    if (!__any_sync(0xffffffffu, has)) break;
+    if (!__any_sync(0xffffffffu, has)) {
+      // Lanes that drew entries without a ray draw again; the warp ends
+      // once the queue is exhausted and no lane holds unstarted entries.
+      if (exhausted && !__any_sync(0xffffffffu, run.left > 0)) break;
+      continue;
+    }
     // Node phase: until at most kNodePhaseStragglers lanes still search.
     while (node_phase_goes_on(has && tr.core.searching(),
                               has && (tr.core.leaf != kTravDone || tr.core.finished()))) {
@@ -473,17 +486,32 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads) k_wf_shadow(WaveBuf
       AcceptFilter acc{&s, &smp, ray_id, false, skip};
       tr.leaf_step(s, acc, ts.sh_tris);
       if (tr.done()) {
-        if (!tr.occluded) rad = vadd(rad, contrib);
-        if (++j < cnt) {
-          start_ray();
-        } else {
-          w.rad[slot] = make_float4(rad.x, rad.y, rad.z, covered);
-          has = false;
-        }
+        w.sh_vis[e] = tr.occluded ? 0 : 1;
+        has = false;
       }
     }
   }
   flush_stats(ctr, ts);
+}
+
+// Each queued path's visible shadow-ray contributions, added to its
+// radiance in generation order (the order the reference adds them).
+__global__ void __launch_bounds__(256) k_wf_shadow_add(WaveBuffers w, uint32_t iter) {
+  const uint32_t n = w.counters[iter * kWfCounterStride + 1];
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const uint32_t slot = w.q_shadow[q];
+    const uint32_t cnt = w.sh_n[slot];
+    const float4 r = w.rad[slot];
+    V3 rad = {r.x, r.y, r.z};
+    for (uint32_t k = 0; k < cnt; ++k) {
+      const size_t e = (size_t)k * w.capacity + slot;
+      if (w.sh_vis[e]) {
+        const float4 c = w.sh_c[e];
+        rad = vadd(rad, {c.x, c.y, c.z});
+      }
+    }
+    w.rad[slot] = make_float4(rad.x, rad.y, rad.z, r.w);
+  }
 }
 
 }  // namespace ptd
