@@ -104,10 +104,30 @@ def _accum_with(ctx, schedule, scene, opts, env=None):
         ctx.set_schedule(abi.PT_SCHEDULE_WAVEFRONT)
 
 
-@pytest.mark.parametrize("case", ["cornell", "spheres", "materials", "env", "alpha", "dispersion"])
+def _many_lights_scene() -> PreparedScene:
+    """An emissive quad over a floor with a blocker, lit besides by a
+    directional light, two range-limited point lights and two narrow spot
+    lights: paths queue from zero to six shadow rays each (a light outside
+    its range or cone adds none), so the shadow queue's rays per path vary
+    from path to path."""
+    from oxideav_render_b200.scene import directional_light, point_light, spot_light
+    s = ts.area_light_scene(0.4, 0.3)
+    grey = s.add_material(ts.diffuse_material((0.6, 0.6, 0.6), 0.8))
+    s.add_primitive(ts.with_material(ts.cuboid([-0.3, 0.0, -0.3], [0.3, 0.5, 0.3]), grey))
+    s.add_light(directional_light((1.0, 0.9, 0.8), 2.0), [0.0, 0.0, 0.0], [0.3, -1.0, 0.2])
+    s.add_light(point_light((1.0, 0.2, 0.2), 6.0, range=1.5), [1.2, 0.8, 0.5], [0.0, -1.0, 0.0])
+    s.add_light(point_light((0.2, 1.0, 0.2), 6.0, range=1.0), [-1.0, 0.6, -0.8], [0.0, -1.0, 0.0])
+    s.add_light(spot_light((0.2, 0.2, 1.0), 9.0, inner=0.1, outer=0.3), [0.0, 1.8, 1.2], [0.0, -1.0, -0.5])
+    s.add_light(spot_light((1.0, 1.0, 0.2), 9.0, range=3.0, inner=0.0, outer=0.2), [-1.5, 1.5, 0.0], [1.0, -1.0, 0.0])
+    return s
+
+
+@pytest.mark.parametrize("case", ["cornell", "spheres", "materials", "env", "alpha", "dispersion", "lights"])
 def test_wavefront_schedule_is_bit_identical_to_megakernel(ctx, case):
     env = None
-    if case == "cornell":
+    if case == "lights":
+        scene, opts = _many_lights_scene(), ts.pt_opts(64, 8, 5)
+    elif case == "cornell":
         scene, opts = ts.cornell_c0()
         opts = opts.replace(width=96, height=80, path_trace=PathTraceOptions(samples_per_pixel=8, max_bounces=8))
     elif case == "spheres":
