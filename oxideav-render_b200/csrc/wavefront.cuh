@@ -320,7 +320,10 @@ __global__ void __launch_bounds__(256) k_wf_sort_scatter(WaveBuffers w, uint32_t
 // The area-light sample and emission MIS pdf of every queued vertex that
 // hit something, in the order shade will read them (its queue). Values are
 // those shade would compute inline (the same functions on the same inputs).
-__global__ void __launch_bounds__(256) k_wf_nee(WaveBuffers w, uint32_t iter) {
+// Four blocks of 256 per SM (64 registers, a few spills): the sampling is
+// latency bound (CDF searches, dependent f64 steps), so occupancy beats the
+// spill-free 106-register form (NEE stage 128 -> 120 ms per mix step).
+__global__ void __launch_bounds__(256, 4) k_wf_nee(WaveBuffers w, uint32_t iter) {
   if (!(w.desc->flags & WAVE_AREA_LIGHTS)) return;  // nothing to sample in this wave
   const DevRequest *reqs = w.desc->reqs;
   const uint32_t n = w.counters[iter * kWfCounterStride + 0];
